@@ -1,0 +1,123 @@
+"""Generates the committed golden fixtures under tests/golden/ (run here, where the reference is mounted;
+the fixtures travel, the reference does not):
+
+  w512_pgmjax.npz   the reference's pGM-JAX FP64 goldens of 512 pGM3P-25 waters
+                    (tests/data/ref_w512_{q,qp,qi,qpi}_novdw.npz of larryhuang98/pGM-MD: positions, box,
+                    energies, forces, induced dipoles at tol 1e-10, no predictor, no peek) together with the
+                    pGM parameters read from tests/data/water512/pgm3p25_512.prmtop (POL_GAUSS_* sections,
+                    converted to nm as openmm/python/pgm_prmtop.py:96-116 does).
+  ref_<name>.npz    outputs of the reference pgm_core itself (core/pgm_core.cpp, built from its sources
+                    into oracle/_ref by oracle/Makefile) on the seeded synthetic systems: energy terms,
+                    forces, strain derivative, induced and permanent dipoles, iterations, tol 1e-10,
+                    predictor none, peek 0.
+
+    make -C oracle && python tests/golden/make_golden.py
+"""
+
+from __future__ import annotations
+
+import importlib.util
+import re
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+REF = Path("/root/reference")
+OUT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+
+def load_systems():
+    spec = importlib.util.spec_from_file_location("pgm_md_b200_systems", ROOT / "pgm-md_b200" / "systems.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def read_prmtop_sections(path, wanted):
+    """Reads the named %FLAG sections of an Amber prmtop (fixed-width fields given by %FORMAT)."""
+    out, name, fmt, lines = {}, None, None, []
+
+    def flush():
+        if name in wanted:
+            m = re.match(r"\((\d+)([aAiIeEfF])(\d+)", fmt)
+            width = int(m.group(3))
+            kind = m.group(2).lower()
+            toks = [ln[k:k + width].strip() for ln in lines for k in range(0, len(ln), width)]
+            toks = [t for t in toks if t]
+            out[name] = np.array([int(t) for t in toks]) if kind == "i" else np.array([float(t) for t in toks])
+
+    for raw in open(path):
+        line = raw.rstrip("\n")
+        if line.startswith("%FLAG"):
+            if name is not None:
+                flush()
+            name, fmt, lines = line.split()[1], None, []
+        elif line.startswith("%FORMAT"):
+            fmt = line[line.index("("):]
+        elif line.startswith("%"):
+            continue
+        elif name is not None:
+            lines.append(line)
+    if name is not None:
+        flush()
+    return out
+
+
+def w512():
+    sec = read_prmtop_sections(REF / "tests/data/water512/pgm3p25_512.prmtop",
+                               {"POL_GAUSS_MONOPOLES_LIST", "POL_GAUSS_RADII_LIST", "POL_GAUSS_POLARIZABILITY_LIST",
+                                "POL_GAUSS_COVALENT_POINTERS_LIST", "POL_GAUSS_COVALENT_ATOMS_LIST",
+                                "POL_GAUSS_COVALENT_DIPOLES_LIST"})
+    nptr = sec["POL_GAUSS_COVALENT_POINTERS_LIST"].astype(np.int64)
+    out = dict(q=sec["POL_GAUSS_MONOPOLES_LIST"], radius=sec["POL_GAUSS_RADII_LIST"] * 0.1,
+               alpha=sec["POL_GAUSS_POLARIZABILITY_LIST"] * 1e-3,
+               cov_atom=np.repeat(np.arange(len(nptr)), nptr).astype(np.int32),
+               cov_partner=(sec["POL_GAUSS_COVALENT_ATOMS_LIST"] - 1).astype(np.int32),
+               cov_strength=sec["POL_GAUSS_COVALENT_DIPOLES_LIST"] * 0.1)
+    for lvl in ("q", "qp", "qi", "qpi"):
+        d = np.load(REF / f"tests/data/ref_w512_{lvl}_novdw.npz")
+        if lvl == "q":
+            out["pos"] = d["pos"]
+            out["H"] = d["H"]
+        else:
+            assert np.array_equal(out["pos"], d["pos"]) and np.array_equal(out["H"], d["H"])
+        out[f"{lvl}_energy"] = d["term_elec"]
+        out[f"{lvl}_forces"] = d["forces"]
+        out[f"{lvl}_mu"] = d["mu"]
+        out[f"{lvl}_iterations"] = d["iterations"]
+    # settings of the goldens: tests/openmm_tests.sh:18-21, tests/ref_pgmjax.py:22-40
+    out.update(ke=138.935458, beta=3.5, cutoff=0.9, grid=np.array([36, 36, 36]), order=6, tol=1e-10)
+    np.savez_compressed(OUT / "w512_pgmjax.npz", **out)
+    print("w512_pgmjax.npz", {k: np.shape(v) for k, v in out.items()})
+
+
+def ref_outputs():
+    from oracle import pgm_oracle as O
+    from oracle import ref as R
+    systems = load_systems()
+    cases = {"tiny_triclinic": systems.tiny_triclinic(), "water216": systems.water216()}
+    for name, S in cases.items():
+        top = O.Topology(S.q, S.radius, S.alpha, S.cov_atom, S.cov_partner, S.cov_strength)
+        st = O.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=1e-10, max_iter=500, peek=0.0,
+                        predictor=0, ke=systems.KE_DEFAULT)
+        eng = R.RefEngine(top, st)
+        e = eng.compute(S.pos, S.box)
+        t = eng.terms()
+        i, j, _ = O.pair_set(S.pos, S.box, S.cutoff)
+        np.savez_compressed(
+            OUT / f"ref_{name}.npz", pos=S.pos, box=S.box, q=S.q, radius=S.radius, alpha=S.alpha,
+            cov_atom=S.cov_atom, cov_partner=S.cov_partner, cov_strength=S.cov_strength, cutoff=S.cutoff,
+            beta=S.beta, grid=np.array(S.grid), order=S.order, ke=systems.KE_DEFAULT, tol=1e-10, energy=e,
+            terms=np.array([t[k] for k in ("direct", "reciprocal", "self", "background", "polarization")]),
+            forces=eng.forces, strain=eng.strain(), mu=eng.induced(), perm=eng.permanent(),
+            iterations=eng.iterations(), npairs=len(i))
+        print(f"ref_{name}.npz", S.n, "atoms", e, eng.iterations(), "iterations", len(i), "pairs")
+
+
+if __name__ == "__main__":
+    w512()
+    ref_outputs()
