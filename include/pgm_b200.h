@@ -1,0 +1,158 @@
+/*
+ * pgm_b200: periodic pGM electrostatics (Gaussian charges, covalent permanent dipoles, Gaussian induced
+ * dipoles, smooth PME) on one NVIDIA B200, as a C ABI.
+ *
+ * The entry points replace the reference's GPU engine interface pgmcuda::Engine
+ * (core/cuda/pgm_cuda.h:47-127 of larryhuang98/pGM-MD) one to one, and add batched multi-system
+ * evaluation and parameter gradients.  Every call returns PGM_OK (0) or a negative status; the message of
+ * the last failure on the calling thread is pgm_last_error().  No call aborts or traps.
+ *
+ * Units: nm, e, e nm, nm^3; energies kJ/mol, forces kJ/mol/nm, strain derivative kJ/mol (the Coulomb
+ * constant is a setting).  Boxes are three rows a, b, c in the reduced triclinic form
+ * a = (ax, 0, 0), b = (bx, by, 0), c = (cx, cy, cz), row-major double[9].
+ * Threading: one thread at a time per engine (any thread), like the reference engine.
+ */
+#ifndef PGM_B200_H_
+#define PGM_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PGM_OK 0
+#define PGM_ERR_ARGUMENT (-1)   /* invalid argument (the reference throws std::invalid_argument) */
+#define PGM_ERR_CUDA (-2)       /* CUDA / cuFFT failure (the reference throws std::runtime_error) */
+#define PGM_ERR_STATE (-3)      /* call out of order (e.g. compute before set_atoms) */
+#define PGM_ERR_CAPACITY (-4)   /* an input beyond a stated maximum */
+
+#define PGM_PRECISION_FP64 0    /* every kernel in double precision */
+#define PGM_PRECISION_MIXED 1   /* FP32 pair/PME/matvec arithmetic, FP64 accumulation, CG vectors and scalars */
+
+typedef struct pgm_engine pgm_engine;
+
+/* pgmcuda::Settings (core/cuda/pgm_cuda.h:25-39) plus the precision and the initial guess. */
+typedef struct pgm_settings {
+    double cutoff;       /* direct-space cutoff [nm] */
+    double beta;         /* Ewald coefficient [1/nm] */
+    int grid[3];         /* PME grid */
+    int order;           /* B-spline order, 3..12 */
+    double tol;          /* max|alpha r| / mean|alpha E_perm| */
+    int max_iter;
+    double peek;         /* final mu += peek alpha r */
+    int predictor;       /* 0 none (guess alpha E_perm), 1 mu3, 2 mu4 (history in the global order) */
+    double ke;           /* Coulomb constant [kJ mol^-1 nm e^-2] */
+    int device;          /* CUDA device; < 0: the device current on the calling thread */
+    double skin;         /* accepted for interface parity; the pair list is rebuilt at every evaluation */
+    int precision;       /* PGM_PRECISION_FP64 or PGM_PRECISION_MIXED */
+    int zero_guess;      /* 1: initial guess mu = 0 when the predictor has no history (instead of alpha E_perm) */
+    int polarizable;     /* 0: no induced dipoles (pgmcore::Settings::polarizable) */
+} pgm_settings;
+
+/* pgmcuda::Terms (core/cuda/pgm_cuda.h:41-45). gvdw is always 0 (combination-rule GVDW is not part of this
+ * engine). */
+typedef struct pgm_terms {
+    double direct, reciprocal, self, background, polarization, gvdw;
+} pgm_terms;
+
+/* Fills *s with the reference defaults of pgmcuda::Settings (core/cuda/pgm_cuda.h:25-39). */
+void pgm_settings_default(pgm_settings* s);
+
+const char* pgm_last_error(void);
+const char* pgm_version(void);
+
+/* pgmcuda::Engine::Engine(const Settings&) (core/cuda/pgm_cuda.h:49). */
+int pgm_engine_create(const pgm_settings* s, pgm_engine** out);
+/* pgmcuda::Engine::~Engine (core/cuda/pgm_cuda.h:50). */
+void pgm_engine_destroy(pgm_engine* e);
+
+/* pgmcuda::Engine::setAtoms (core/cuda/pgm_cuda.h:55-56): atoms in the caller's order; global_index (NULL:
+ * identity) keys the predictor history; alpha <= 1e-9 nm^3 is not polarizable (core/pgm_constants.h:9). */
+int pgm_engine_set_atoms(pgm_engine* e, int n, const double* q, const double* radius, const double* alpha,
+                         const int* global_index, int num_global);
+/* pgmcuda::Engine::setCovalent (core/cuda/pgm_cuda.h:67): p_atom += strength unit(r_partner - r_atom). */
+int pgm_engine_set_covalent(pgm_engine* e, int ncov, const int* atom, const int* partner, const double* strength);
+
+/* pgmcuda::Engine::compute (core/cuda/pgm_cuda.h:79): positions pos (n*3, host), box (9); forces ADDED to
+ * f (n*3, may be NULL), strain derivative ADDED to strain (9, may be NULL); terms (may be NULL).
+ * new_step: this evaluation starts a new MD step (its solution enters the predictor history). */
+int pgm_engine_compute(pgm_engine* e, const double* pos, const double* box, int new_step, double* f,
+                       double* strain, pgm_terms* terms);
+/* pgmcuda::Engine::computeF (core/cuda/pgm_cuda.h:82): float positions; the forces stay in the engine
+ * (pgm_engine_forces). */
+int pgm_engine_compute_f(pgm_engine* e, const float* pos, const double* box, int new_step, double* strain,
+                         pgm_terms* terms);
+/* pgmcuda::Engine::forces (core/cuda/pgm_cuda.h:86): forces of the last compute_f (n*3, valid until the next
+ * call). */
+const double* pgm_engine_forces(pgm_engine* e);
+/* pgmcuda::Engine::releasePositions (core/cuda/pgm_cuda.h:85): no registered memory is kept; accepted. */
+int pgm_engine_release_positions(pgm_engine* e);
+
+/* pgmcuda::Engine::launchDevice / finishDevice / waitDevice / computeDevice (core/cuda/pgm_cuda.h:93-111):
+ * positions from the device array posq4 (float4, w ignored, caller order); forces added atomically to the
+ * device 64-bit fixed-point buffer force_fixed (x of atom i at i, y at i + stride, z at i + 2 stride,
+ * scale fixed_scale); stream: the caller's cudaStream_t (its work so far comes first).  finish_device sets
+ * *valid = 1 (the list is rebuilt every evaluation, so an evaluation is never stale). */
+int pgm_engine_launch_device(pgm_engine* e, const void* posq4, const double* box, int new_step,
+                             long long* force_fixed, int stride, double fixed_scale, void* stream);
+int pgm_engine_finish_device(pgm_engine* e, pgm_terms* terms, int* valid);
+int pgm_engine_wait_device(pgm_engine* e, void* stream);
+int pgm_engine_compute_device(pgm_engine* e, const void* posq4, const double* box, int new_step,
+                              long long* force_fixed, int stride, double fixed_scale, void* stream, pgm_terms* terms);
+/* Device-resident evaluation for benchmarks and device callers: positions pos_dev (device double n*3),
+ * forces written (not added) to forces_dev (device double n*3, may be NULL), no host synchronisation;
+ * pgm_engine_finish_device returns its terms.  No counterpart in the reference. */
+int pgm_engine_launch_resident(pgm_engine* e, const double* pos_dev, const double* box, int new_step,
+                               double* forces_dev, void* stream);
+
+/* Getters of pgmcuda::Engine (core/cuda/pgm_cuda.h:112-122). */
+int pgm_engine_iterations(pgm_engine* e);
+double pgm_engine_residual(pgm_engine* e);
+int pgm_engine_induced_dipoles(pgm_engine* e, double* mu);
+int pgm_engine_permanent_dipoles(pgm_engine* e, double* p);
+int pgm_engine_reset_history(pgm_engine* e);
+long pgm_engine_list_builds(pgm_engine* e);
+long pgm_engine_late_list_checks(pgm_engine* e);
+int pgm_engine_num_candidates(pgm_engine* e);
+
+/* pgmcore::Engine::strainDerivative (core/pgm_core.h:67-73) of the last evaluation (9, row-major). */
+int pgm_engine_strain(pgm_engine* e, double* strain);
+/* pgmcore::Engine::field (core/pgm_core.h:76-77): field [e/nm^2] of charges q (n) and dipoles d (n*3) at
+ * the atoms (direct + reciprocal + self) for positions pos and box; E (n*3). */
+int pgm_engine_field(pgm_engine* e, const double* pos, const double* box, const double* q, const double* d,
+                     double* E);
+/* The directed pair list of the last evaluation (both directions, r < cutoff by the reference's minimum
+ * image, core/pgm_core.cpp:64-87): pairs i < j written to pi, pj (capacity cap); *npairs = count.  No
+ * counterpart in the reference (its list is internal). */
+int pgm_engine_pairs(pgm_engine* e, int* pi, int* pj, long long cap, long long* npairs);
+
+/* Predictor history as a blob (checkpoint/resume): size in bytes, get, set.  No counterpart in the
+ * reference. */
+long long pgm_engine_history_size(pgm_engine* e);
+int pgm_engine_get_history(pgm_engine* e, void* blob);
+int pgm_engine_set_history(pgm_engine* e, const void* blob);
+
+/* Parameter gradients of the total energy at the solved dipoles of the last evaluation (E is stationary in
+ * the induced dipoles; run with peek = 0): dE/dq, dE/dradius, dE/dalpha per atom (n each), dE/dstrength per
+ * covalent dipole (ncov).  Any output may be NULL.  No counterpart in the reference. */
+int pgm_engine_param_grad(pgm_engine* e, double* dq, double* dradius, double* dalpha, double* dstrength);
+
+/* Batched evaluation: nsys independent systems of uneven sizes in one launch.  Atom arrays are the systems'
+ * arrays concatenated; atom_count[s] atoms per system; per-system cutoff, beta and grid (3 ints); covalent
+ * indices are local to their system.  The shared settings (order, tol, max_iter, peek, ke, precision) come
+ * from the engine's settings.  No counterpart in the reference. */
+int pgm_engine_set_systems(pgm_engine* e, int nsys, const int* atom_count, const double* cutoff, const double* beta,
+                           const int* grid, const double* q, const double* radius, const double* alpha,
+                           const int* cov_count, const int* cov_atom, const int* cov_partner, const double* strength);
+/* Positions (concatenated, n_total*3), boxes (nsys*9); energies per system (nsys*6 terms in pgm_terms order,
+ * may be NULL), forces (n_total*3, written, may be NULL), strain (nsys*9, written, may be NULL), iterations
+ * per system (nsys, may be NULL). */
+int pgm_engine_compute_batch(pgm_engine* e, const double* pos, const double* boxes, double* energies, double* forces,
+                             double* strain, int* iterations);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

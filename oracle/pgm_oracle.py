@@ -414,7 +414,7 @@ class Engine:
             for a in range(3):
                 for b in range(3):
                     strain[3 * a + b] += float(np.sum(ew * ((-1.0 if a == b else 0.0) + c2 * ms[a] * ms[b])))
-        phi = np.fft.irfftn(F * g, s=(K1, K2, K3)) * (K1 * K2 * K3)
+        phi = np.fft.irfftn(F * g, s=(K1, K2, K3), axes=(0, 1, 2)) * (K1 * K2 * K3)
         return energy, phi.reshape(-1)
 
     def _interp(self, phi, want_second=False, want_pot=False):

@@ -1,0 +1,334 @@
+// C ABI of the pgm_b200 engine (include/pgm_b200.h): exceptions become status codes and a per-thread message.
+#include "../../include/pgm_b200.h"
+#include "pgm_engine.h"
+
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+
+struct pgm_engine {
+    pgmb200::Engine* e;
+};
+
+namespace {
+thread_local std::string g_lastError;
+
+template <class F> int guarded(F&& f) {
+    try {
+        f();
+        return PGM_OK;
+    } catch (const std::invalid_argument& ex) {
+        g_lastError = ex.what();
+        return PGM_ERR_ARGUMENT;
+    } catch (const std::logic_error& ex) {
+        g_lastError = ex.what();
+        return PGM_ERR_STATE;
+    } catch (const std::bad_alloc&) {
+        g_lastError = "pgm_b200: host allocation failed";
+        return PGM_ERR_CAPACITY;
+    } catch (const std::exception& ex) {
+        g_lastError = ex.what();
+        return PGM_ERR_CUDA;
+    } catch (...) {
+        g_lastError = "pgm_b200: unknown error";
+        return PGM_ERR_CUDA;
+    }
+}
+
+pgmb200::Settings toSettings(const pgm_settings* s) {
+    pgmb200::Settings o;
+    o.cutoff = s->cutoff;
+    o.beta = s->beta;
+    for (int a = 0; a < 3; a++)
+        o.grid[a] = s->grid[a];
+    o.order = s->order;
+    o.tol = s->tol;
+    o.maxIter = s->max_iter;
+    o.peek = s->peek;
+    o.predictor = s->predictor;
+    o.ke = s->ke;
+    o.device = s->device;
+    o.skin = s->skin;
+    o.precision = s->precision;
+    o.zeroGuess = s->zero_guess;
+    o.polarizable = s->polarizable;
+    return o;
+}
+
+void toBox(const double* b, double (&box)[3][3]) {
+    for (int a = 0; a < 3; a++)
+        for (int c = 0; c < 3; c++)
+            box[a][c] = b[3 * a + c];
+}
+
+void fill(pgm_terms* t, const pgmb200::Terms& x) {
+    if (!t)
+        return;
+    t->direct = x.direct;
+    t->reciprocal = x.reciprocal;
+    t->self = x.self;
+    t->background = x.background;
+    t->polarization = x.polarization;
+    t->gvdw = x.gvdw;
+}
+
+#define NEED(e)                                                              \
+    if (!(e) || !(e)->e) {                                                   \
+        g_lastError = "pgm_b200: null engine";                               \
+        return PGM_ERR_ARGUMENT;                                             \
+    }
+}  // namespace
+
+extern "C" {
+
+void pgm_settings_default(pgm_settings* s) {
+    if (!s)
+        return;
+    const pgmb200::Settings d;
+    s->cutoff = d.cutoff;
+    s->beta = d.beta;
+    for (int a = 0; a < 3; a++)
+        s->grid[a] = d.grid[a];
+    s->order = d.order;
+    s->tol = d.tol;
+    s->max_iter = d.maxIter;
+    s->peek = d.peek;
+    s->predictor = d.predictor;
+    s->ke = d.ke;
+    s->device = d.device;
+    s->skin = d.skin;
+    s->precision = d.precision;
+    s->zero_guess = d.zeroGuess;
+    s->polarizable = d.polarizable;
+}
+
+const char* pgm_last_error(void) { return g_lastError.c_str(); }
+const char* pgm_version(void) { return "pgm_b200 1.0 (sm_100a)"; }
+
+int pgm_engine_create(const pgm_settings* s, pgm_engine** out) {
+    if (!s || !out) {
+        g_lastError = "pgm_b200: null argument";
+        return PGM_ERR_ARGUMENT;
+    }
+    *out = nullptr;
+    return guarded([&] {
+        if (s->order < 3 || s->order > 12)
+            throw std::invalid_argument("pgm_b200: PME order must be 3..12");
+        if (s->precision != PGM_PRECISION_FP64 && s->precision != PGM_PRECISION_MIXED)
+            throw std::invalid_argument("pgm_b200: unknown precision");
+        if (!(s->tol >= 0) || s->max_iter < 0)
+            throw std::invalid_argument("pgm_b200: tolerance and max_iter must be non-negative");
+        pgm_engine* h = new pgm_engine{new pgmb200::Engine(toSettings(s))};
+        *out = h;
+    });
+}
+
+void pgm_engine_destroy(pgm_engine* e) {
+    if (!e)
+        return;
+    try {
+        delete e->e;
+    } catch (...) {
+    }
+    delete e;
+}
+
+int pgm_engine_set_atoms(pgm_engine* e, int n, const double* q, const double* radius, const double* alpha,
+                         const int* global_index, int num_global) {
+    NEED(e);
+    return guarded([&] {
+        if (n <= 0 || !q || !radius || !alpha)
+            throw std::invalid_argument("pgm_b200: set_atoms needs n > 0 and q, radius, alpha");
+        e->e->setAtoms(n, q, radius, alpha, global_index, num_global);
+    });
+}
+
+int pgm_engine_set_covalent(pgm_engine* e, int ncov, const int* atom, const int* partner, const double* strength) {
+    NEED(e);
+    return guarded([&] {
+        if (ncov < 0 || (ncov > 0 && (!atom || !partner || !strength)))
+            throw std::invalid_argument("pgm_b200: set_covalent arguments");
+        e->e->setCovalent(ncov, atom, partner, strength);
+    });
+}
+
+int pgm_engine_compute(pgm_engine* e, const double* pos, const double* box, int new_step, double* f, double* strain,
+                       pgm_terms* terms) {
+    NEED(e);
+    return guarded([&] {
+        if (!pos || !box)
+            throw std::invalid_argument("pgm_b200: compute needs positions and box");
+        double b[3][3];
+        toBox(box, b);
+        fill(terms, e->e->compute(pos, b, new_step != 0, f, strain));
+    });
+}
+
+int pgm_engine_compute_f(pgm_engine* e, const float* pos, const double* box, int new_step, double* strain,
+                         pgm_terms* terms) {
+    NEED(e);
+    return guarded([&] {
+        if (!pos || !box)
+            throw std::invalid_argument("pgm_b200: compute_f needs positions and box");
+        double b[3][3];
+        toBox(box, b);
+        fill(terms, e->e->computeF(pos, b, new_step != 0, strain));
+    });
+}
+
+const double* pgm_engine_forces(pgm_engine* e) { return (e && e->e) ? e->e->forces() : nullptr; }
+
+int pgm_engine_release_positions(pgm_engine* e) {
+    NEED(e);
+    return guarded([&] { e->e->releasePositions(); });
+}
+
+int pgm_engine_launch_device(pgm_engine* e, const void* posq4, const double* box, int new_step, long long* force_fixed,
+                             int stride, double fixed_scale, void* stream) {
+    NEED(e);
+    return guarded([&] {
+        if (!posq4 || !box)
+            throw std::invalid_argument("pgm_b200: launch_device needs positions and box");
+        double b[3][3];
+        toBox(box, b);
+        e->e->launchDevice(posq4, b, new_step != 0, force_fixed, stride, fixed_scale, stream);
+    });
+}
+
+int pgm_engine_finish_device(pgm_engine* e, pgm_terms* terms, int* valid) {
+    NEED(e);
+    return guarded([&] {
+        pgmb200::Terms t;
+        const bool ok = e->e->finishDevice(t);
+        fill(terms, t);
+        if (valid)
+            *valid = ok ? 1 : 0;
+    });
+}
+
+int pgm_engine_wait_device(pgm_engine* e, void* stream) {
+    NEED(e);
+    return guarded([&] { e->e->waitDevice(stream); });
+}
+
+int pgm_engine_compute_device(pgm_engine* e, const void* posq4, const double* box, int new_step,
+                              long long* force_fixed, int stride, double fixed_scale, void* stream, pgm_terms* terms) {
+    NEED(e);
+    return guarded([&] {
+        double b[3][3];
+        toBox(box, b);
+        fill(terms, e->e->computeDevice(posq4, b, new_step != 0, force_fixed, stride, fixed_scale, stream));
+    });
+}
+
+int pgm_engine_launch_resident(pgm_engine* e, const double* pos_dev, const double* box, int new_step,
+                               double* forces_dev, void* stream) {
+    NEED(e);
+    return guarded([&] {
+        if (!pos_dev || !box)
+            throw std::invalid_argument("pgm_b200: launch_resident needs positions and box");
+        double b[3][3];
+        toBox(box, b);
+        e->e->launchResident(pos_dev, b, new_step != 0, forces_dev, stream);
+    });
+}
+
+int pgm_engine_iterations(pgm_engine* e) { return (e && e->e) ? e->e->iterations() : -1; }
+double pgm_engine_residual(pgm_engine* e) { return (e && e->e) ? e->e->residual() : -1.0; }
+
+int pgm_engine_induced_dipoles(pgm_engine* e, double* mu) {
+    NEED(e);
+    return guarded([&] { e->e->inducedDipoles(mu); });
+}
+
+int pgm_engine_permanent_dipoles(pgm_engine* e, double* p) {
+    NEED(e);
+    return guarded([&] { e->e->permanentDipoles(p); });
+}
+
+int pgm_engine_reset_history(pgm_engine* e) {
+    NEED(e);
+    return guarded([&] { e->e->resetHistory(); });
+}
+
+long pgm_engine_list_builds(pgm_engine* e) { return (e && e->e) ? e->e->listBuilds() : -1; }
+long pgm_engine_late_list_checks(pgm_engine* e) { return (e && e->e) ? e->e->lateListChecks() : -1; }
+int pgm_engine_num_candidates(pgm_engine* e) {
+    if (!e || !e->e)
+        return -1;
+    int v = -1;
+    guarded([&] { v = e->e->numCandidates(); });
+    return v;
+}
+
+int pgm_engine_strain(pgm_engine* e, double* strain) {
+    NEED(e);
+    return guarded([&] {
+        const auto s = e->e->strainDerivative();
+        for (int k = 0; k < 9; k++)
+            strain[k] = s[k];
+    });
+}
+
+int pgm_engine_field(pgm_engine* e, const double* pos, const double* box, const double* q, const double* d,
+                     double* E) {
+    NEED(e);
+    return guarded([&] {
+        if (!pos || !box || !q || !d || !E)
+            throw std::invalid_argument("pgm_b200: field arguments");
+        double b[3][3];
+        toBox(box, b);
+        e->e->field(pos, b, q, d, E);
+    });
+}
+
+int pgm_engine_pairs(pgm_engine* e, int* pi, int* pj, long long cap, long long* npairs) {
+    NEED(e);
+    return guarded([&] {
+        const long long m = e->e->pairs(pi, pj, cap);
+        if (npairs)
+            *npairs = m;
+    });
+}
+
+long long pgm_engine_history_size(pgm_engine* e) { return (e && e->e) ? e->e->historySize() : -1; }
+
+int pgm_engine_get_history(pgm_engine* e, void* blob) {
+    NEED(e);
+    return guarded([&] { e->e->getHistory(blob); });
+}
+
+int pgm_engine_set_history(pgm_engine* e, const void* blob) {
+    NEED(e);
+    return guarded([&] { e->e->setHistory(blob); });
+}
+
+int pgm_engine_param_grad(pgm_engine* e, double* dq, double* dradius, double* dalpha, double* dstrength) {
+    NEED(e);
+    return guarded([&] { e->e->paramGrad(dq, dradius, dalpha, dstrength); });
+}
+
+int pgm_engine_set_systems(pgm_engine* e, int nsys, const int* atom_count, const double* cutoff, const double* beta,
+                           const int* grid, const double* q, const double* radius, const double* alpha,
+                           const int* cov_count, const int* cov_atom, const int* cov_partner, const double* strength) {
+    NEED(e);
+    return guarded([&] {
+        if (nsys <= 0 || !atom_count || !cutoff || !beta || !grid || !q || !radius || !alpha || !cov_count)
+            throw std::invalid_argument("pgm_b200: set_systems arguments");
+        e->e->setSystems(nsys, atom_count, cutoff, beta, grid, q, radius, alpha, cov_count, cov_atom, cov_partner,
+                         strength);
+    });
+}
+
+int pgm_engine_compute_batch(pgm_engine* e, const double* pos, const double* boxes, double* energies, double* forces,
+                             double* strain, int* iterations) {
+    NEED(e);
+    return guarded([&] {
+        if (!pos || !boxes)
+            throw std::invalid_argument("pgm_b200: compute_batch needs positions and boxes");
+        e->e->computeBatch(pos, boxes, energies, forces, strain, iterations);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,1343 @@
+// pgm_b200 engine: host orchestration of one or many periodic pGM systems on one B200.
+//
+// One evaluation is one CUDA graph: preparation and the cell list, the pair list, the permanent field, the
+// initial guess, the CG loop as a conditional while node (its body: spread || pair pass, FFT chain, gather,
+// two CG kernels), and the final pass.  Kernels are in kernels.cuh; the C ABI is in capi.cu.
+#include "kernels.cuh"
+#include "pgm_engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+namespace pgmb200 {
+
+#define CU(call)                                                                                             \
+    do {                                                                                                     \
+        cudaError_t e_ = (call);                                                                             \
+        if (e_ != cudaSuccess)                                                                               \
+            throw std::runtime_error(std::string("pgm_b200: ") + #call + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+#define CUFFT(call)                                                                                          \
+    do {                                                                                                     \
+        cufftResult r_ = (call);                                                                             \
+        if (r_ != CUFFT_SUCCESS)                                                                             \
+            throw std::runtime_error(std::string("pgm_b200: ") + #call + " failed with cufftResult " +        \
+                                     std::to_string((int) r_));                                              \
+    } while (0)
+
+namespace {
+
+// Device allocation owned by the engine.
+struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void ensure(size_t b) {
+        if (b <= bytes && p)
+            return;
+        release();
+        if (b == 0)
+            b = 16;
+        CU(cudaMalloc(&p, b));
+        bytes = b;
+    }
+    void release() {
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T> T* as() const { return (T*) p; }
+};
+
+// |sum_k M_p(k+1) exp(2 pi i m k/K)|^2 with zeros replaced by the mean of their neighbours: the B-spline
+// moduli of the smooth-PME influence function (the formula of core/pgm_math.h:98-126).
+std::vector<double> bsplineModuli(int K, int p) {
+    std::vector<double> M(p + 1, 0.0), tmp(p + 1, 0.0);
+    M[0] = 1.0;
+    for (int k = 2; k <= p; k++) {
+        for (int j = 0; j < k; j++) {
+            const double cur = (j < k - 1 ? M[j] : 0.0), prev = (j > 0 ? M[j - 1] : 0.0);
+            tmp[j] = (j * cur + (k - j) * prev) / (k - 1);
+        }
+        for (int j = 0; j < k; j++)
+            M[j] = tmp[j];
+    }
+    std::vector<double> data(K, 0.0), mod(K), out(K);
+    for (int k = 0; k < p - 1 && k < K; k++)
+        data[k] = M[k + 1];
+    for (int m = 0; m < K; m++) {
+        double sc = 0, ss = 0;
+        for (int k = 0; k < K; k++) {
+            const double arg = 2 * PI_D * m * k / K;
+            sc += data[k] * std::cos(arg);
+            ss += data[k] * std::sin(arg);
+        }
+        mod[m] = sc * sc + ss * ss;
+    }
+    for (int m = 0; m < K; m++)
+        out[m] = mod[m] < 1e-7 ? 0.5 * (mod[(m - 1 + K) % K] + mod[(m + 1) % K]) : mod[m];
+    return out;
+}
+
+// H^-1 by cofactors and |det H| (core/pgm_core.cpp:94-111).
+void boxInverse(const double* H, double* inv, double& volume) {
+    const double det = H[0] * (H[4] * H[8] - H[5] * H[7]) - H[1] * (H[3] * H[8] - H[5] * H[6]) +
+                       H[2] * (H[3] * H[7] - H[4] * H[6]);
+    volume = std::fabs(det);
+    inv[0] = (H[4] * H[8] - H[5] * H[7]) / det;
+    inv[1] = (H[2] * H[7] - H[1] * H[8]) / det;
+    inv[2] = (H[1] * H[5] - H[2] * H[4]) / det;
+    inv[3] = (H[5] * H[6] - H[3] * H[8]) / det;
+    inv[4] = (H[0] * H[8] - H[2] * H[6]) / det;
+    inv[5] = (H[2] * H[3] - H[0] * H[5]) / det;
+    inv[6] = (H[3] * H[7] - H[4] * H[6]) / det;
+    inv[7] = (H[1] * H[6] - H[0] * H[7]) / det;
+    inv[8] = (H[0] * H[4] - H[1] * H[3]) / det;
+}
+
+template <class T> void upload(Buf& b, const std::vector<T>& v, cudaStream_t st) {
+    b.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
+    if (!v.empty())
+        CU(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+int envInt(const char* name, int def) {
+    const char* v = std::getenv(name);
+    return v ? std::atoi(v) : def;
+}
+
+}  // namespace
+
+struct Engine::Impl {
+    Settings s;
+    cudaStream_t st = nullptr, side = nullptr;
+    cudaStream_t callerStream = nullptr;
+    cudaEvent_t evFork = nullptr, evJoin = nullptr, evCaller = nullptr, evDone = nullptr;
+    int devId = 0;
+
+    // systems and atoms (host)
+    int n = 0, nsys = 0, numGlobal = 0;
+    std::vector<int> atomBegin;                 // nsys + 1
+    std::vector<double> sysCutoff, sysBeta;
+    std::vector<std::array<int, 3>> sysK;
+    std::vector<double> q, radius, alpha;
+    std::vector<int> atomSys, globalIdx;
+    std::vector<int> covAtom, covPartner;       // global atom indices
+    std::vector<double> covStrength;
+    std::vector<SysDev> sysHost;
+    std::vector<int> chunkSys, chunkBegin, chunkEnd;
+    std::vector<double> moduliHost;
+    std::map<int, int> moduliOff;
+    struct FftGroup {
+        int K[3];
+        int first, count;   // systems (contiguous in grid storage)
+        long long gridOff, specOff;
+        cufftHandle r2c = 0, c2r = 0;
+    };
+    std::vector<FftGroup> groups;
+    std::vector<int> sysOrder;   // unused (systems stored in caller order within their group)
+    long long gridTotal = 0, specTotal = 0;
+    int totalCells = 0, cellCapacity = 0;
+    int cap = 0;
+    int convBlocks = 1;
+    bool configured = false, atomsSet = false;
+
+    // device
+    Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
+        dSlotAtom, dPosS, dRadS, dList, dListCount, dG12, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
+        dScal, dPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
+        dConvPartial, dConvOff, dGrid, dSpec, dInfl, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
+        dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
+        dGradQ, dGradR;
+    // pinned host staging
+    double* hPos = nullptr;
+    float* hPosF = nullptr;
+    double* hForces = nullptr;
+    double* hResults = nullptr;
+    int* hFlags = nullptr;
+    Ctl* hCtl = nullptr;
+    SysDev* hSys = nullptr;
+    size_t hPosCap = 0, hSysCap = 0, hResCap = 0;
+
+    // graph
+    cudaGraphExec_t exec = nullptr;
+    bool useGraph = true;
+    int pairGS = 8;
+
+    // predictor history: NHIST slots, newest at head
+    static constexpr int NHIST = 5;
+    int histHead = 0, histCount = 0;
+    int pendingSlot = -1;
+
+    // last evaluation
+    std::vector<double> lastResults;   // nsys * NRES
+    bool haveResult = false;
+    long builds = 0;
+    std::vector<double> forcesHostCache;
+    bool launched = false;
+    int launchedMode = 0;
+
+    Impl() {}
+    ~Impl() { teardown(); }
+
+    void teardown() {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        for (auto& g : groups) {
+            if (g.r2c)
+                cufftDestroy(g.r2c);
+            if (g.c2r)
+                cufftDestroy(g.c2r);
+        }
+        groups.clear();
+        Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
+                      &dCellCount, &dCellStart, &dSlotAtom, &dPosS, &dRadS, &dList, &dListCount, &dG12, &dFlags, &dDS,
+                      &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dSysCounter, &dEpair,
+                      &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
+                      &dConvOff, &dGrid, &dSpec, &dInfl, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
+                      &dCovByAtomOff, &dCovByAtom, &dCovByPartnerOff, &dCovByPartner, &dChunkSys, &dChunkBegin,
+                      &dChunkEnd, &dHist, &dGlobal, &dCtl, &dGradQ, &dGradR};
+        for (Buf* b : all)
+            b->release();
+        if (hPos) cudaFreeHost(hPos);
+        if (hPosF) cudaFreeHost(hPosF);
+        if (hForces) cudaFreeHost(hForces);
+        if (hResults) cudaFreeHost(hResults);
+        if (hFlags) cudaFreeHost(hFlags);
+        if (hCtl) cudaFreeHost(hCtl);
+        if (hSys) cudaFreeHost(hSys);
+        hPos = nullptr;
+        hPosF = nullptr;
+        hForces = nullptr;
+        hResults = nullptr;
+        hFlags = nullptr;
+        hCtl = nullptr;
+        hSys = nullptr;
+        hPosCap = hSysCap = hResCap = 0;
+        if (st) cudaStreamDestroy(st);
+        if (side) cudaStreamDestroy(side);
+        if (evFork) cudaEventDestroy(evFork);
+        if (evJoin) cudaEventDestroy(evJoin);
+        if (evCaller) cudaEventDestroy(evCaller);
+        if (evDone) cudaEventDestroy(evDone);
+        st = side = nullptr;
+        evFork = evJoin = evCaller = evDone = nullptr;
+    }
+
+    bool mixed() const { return s.precision != 0; }
+    size_t realSize() const { return mixed() ? sizeof(float) : sizeof(double); }
+
+    void init(const Settings& settings) {
+        s = settings;
+        if (s.order < 3 || s.order > MAXP)
+            throw std::invalid_argument("pgm_b200: PME order must be 3..12");
+        if (s.device >= 0)
+            CU(cudaSetDevice(s.device));
+        CU(cudaGetDevice(&devId));
+        CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CU(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        CU(cudaEventCreateWithFlags(&evFork, cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&evCaller, cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&evDone, cudaEventDisableTiming));
+        CU(cudaMallocHost((void**) &hFlags, 16 * sizeof(int)));
+        CU(cudaMallocHost((void**) &hCtl, sizeof(Ctl)));
+        useGraph = envInt("PGM_B200_NO_GRAPH", 0) == 0;
+        pairGS = envInt("PGM_B200_PAIR_LANES", 8);
+        if (pairGS != 4 && pairGS != 8 && pairGS != 16 && pairGS != 32)
+            pairGS = 8;
+    }
+
+    void selectDevice() {
+        if (s.device >= 0)
+            CU(cudaSetDevice(devId));
+    }
+
+    // ------------------------------------------------------------------------------------------ topology
+    void setAtomsSingle(int nAt, const double* qq, const double* rr, const double* aa, const int* gidx, int nGlobal) {
+        if (nAt <= 0)
+            throw std::invalid_argument("pgm_b200: setAtoms needs at least one atom");
+        const bool sameCount = atomsSet && nsys == 1 && n == nAt;
+        n = nAt;
+        nsys = 1;
+        atomBegin = {0, n};
+        sysCutoff = {s.cutoff};
+        sysBeta = {s.beta};
+        sysK = {{s.grid[0], s.grid[1], s.grid[2]}};
+        q.assign(qq, qq + n);
+        radius.assign(rr, rr + n);
+        alpha.assign(aa, aa + n);
+        for (double& a : alpha)
+            if (a <= 1e-9)
+                a = 0.0;   // not polarizable (core/pgm_constants.h:9)
+        atomSys.assign(n, 0);
+        numGlobal = gidx ? nGlobal : n;
+        globalIdx.clear();
+        if (gidx) {
+            globalIdx.assign(gidx, gidx + n);
+            for (int g : globalIdx)
+                if (g < 0 || g >= numGlobal)
+                    throw std::invalid_argument("pgm_b200: global index out of range");
+        }
+        covAtom.clear();
+        covPartner.clear();
+        covStrength.clear();
+        if (!sameCount)
+            resetHistoryState();
+        atomsSet = true;
+        configure();
+    }
+
+    void setSystemsBatch(int ns, const int* count, const double* cut, const double* bet, const int* grd,
+                         const double* qq, const double* rr, const double* aa, const int* covCount, const int* ca,
+                         const int* cp, const double* cs) {
+        if (ns <= 0)
+            throw std::invalid_argument("pgm_b200: setSystems needs at least one system");
+        nsys = ns;
+        atomBegin.assign(ns + 1, 0);
+        for (int k = 0; k < ns; k++) {
+            if (count[k] <= 0)
+                throw std::invalid_argument("pgm_b200: every system needs at least one atom");
+            atomBegin[k + 1] = atomBegin[k] + count[k];
+        }
+        n = atomBegin[ns];
+        sysCutoff.assign(cut, cut + ns);
+        sysBeta.assign(bet, bet + ns);
+        sysK.resize(ns);
+        for (int k = 0; k < ns; k++)
+            for (int a = 0; a < 3; a++) {
+                sysK[k][a] = grd[3 * k + a];
+                if (sysK[k][a] < s.order - 1 || sysK[k][a] <= 0)
+                    throw std::invalid_argument("pgm_b200: PME grid smaller than the spline order");
+            }
+        q.assign(qq, qq + n);
+        radius.assign(rr, rr + n);
+        alpha.assign(aa, aa + n);
+        for (double& a : alpha)
+            if (a <= 1e-9)
+                a = 0.0;
+        atomSys.resize(n);
+        for (int k = 0; k < ns; k++)
+            for (int i = atomBegin[k]; i < atomBegin[k + 1]; i++)
+                atomSys[i] = k;
+        numGlobal = n;
+        globalIdx.clear();
+        covAtom.clear();
+        covPartner.clear();
+        covStrength.clear();
+        int m = 0;
+        for (int k = 0; k < ns; k++)
+            for (int c = 0; c < covCount[k]; c++, m++) {
+                const int nk = atomBegin[k + 1] - atomBegin[k];
+                if (ca[m] < 0 || ca[m] >= nk || cp[m] < 0 || cp[m] >= nk || ca[m] == cp[m])
+                    throw std::invalid_argument("pgm_b200: covalent dipole indices out of range");
+                covAtom.push_back(atomBegin[k] + ca[m]);
+                covPartner.push_back(atomBegin[k] + cp[m]);
+                covStrength.push_back(cs[m]);
+            }
+        resetHistoryState();
+        atomsSet = true;
+        configure();
+        uploadCovalent();
+    }
+
+    void setCovalentSingle(int ncov, const int* a, const int* p, const double* c) {
+        if (!atomsSet)
+            throw std::logic_error("pgm_b200: setCovalent before setAtoms");
+        covAtom.clear();
+        covPartner.clear();
+        covStrength.clear();
+        for (int m = 0; m < ncov; m++) {
+            if (a[m] < 0 || a[m] >= n || p[m] < 0 || p[m] >= n || a[m] == p[m])
+                throw std::invalid_argument("pgm_b200: covalent dipole indices out of range");
+            covAtom.push_back(a[m]);
+            covPartner.push_back(p[m]);
+            covStrength.push_back(c[m]);
+        }
+        uploadCovalent();
+    }
+
+    void uploadCovalent() {
+        const int ncov = (int) covAtom.size();
+        std::vector<int> byAtomOff(n + 1, 0), byPartnerOff(n + 1, 0), byAtom(ncov), byPartner(ncov);
+        for (int m = 0; m < ncov; m++) {
+            byAtomOff[covAtom[m] + 1]++;
+            byPartnerOff[covPartner[m] + 1]++;
+        }
+        for (int i = 0; i < n; i++) {
+            byAtomOff[i + 1] += byAtomOff[i];
+            byPartnerOff[i + 1] += byPartnerOff[i];
+        }
+        std::vector<int> fa(byAtomOff.begin(), byAtomOff.end() - 1), fp(byPartnerOff.begin(), byPartnerOff.end() - 1);
+        for (int m = 0; m < ncov; m++) {
+            byAtom[fa[covAtom[m]]++] = m;
+            byPartner[fp[covPartner[m]]++] = m;
+        }
+        upload(dCovAtom, covAtom, st);
+        upload(dCovPartner, covPartner, st);
+        upload(dCovStrength, covStrength, st);
+        upload(dCovByAtomOff, byAtomOff, st);
+        upload(dCovByAtom, byAtom, st);
+        upload(dCovByPartnerOff, byPartnerOff, st);
+        upload(dCovByPartner, byPartner, st);
+        CU(cudaStreamSynchronize(st));
+    }
+
+    void resetHistoryState() {
+        histHead = 0;
+        histCount = 0;
+    }
+
+    // Allocations, tables and FFT plans for the current atoms/systems.
+    void configure() {
+        if (exec) {
+            cudaGraphExecDestroy(exec);
+            exec = nullptr;
+        }
+        for (auto& g : groups) {
+            if (g.r2c) cufftDestroy(g.r2c);
+            if (g.c2r) cufftDestroy(g.c2r);
+        }
+        groups.clear();
+        // systems grouped by grid shape; grid storage group after group
+        std::map<std::array<int, 3>, std::vector<int>> byShape;
+        for (int k = 0; k < nsys; k++)
+            byShape[sysK[k]].push_back(k);
+        sysHost.assign(nsys, SysDev());
+        gridTotal = specTotal = 0;
+        moduliHost.clear();
+        moduliOff.clear();
+        int maxSpec = 0;
+        for (auto& kv : byShape) {
+            FftGroup g;
+            for (int a = 0; a < 3; a++)
+                g.K[a] = kv.first[a];
+            g.gridOff = gridTotal;
+            g.specOff = specTotal;
+            g.count = (int) kv.second.size();
+            g.first = kv.second[0];
+            const int gn = g.K[0] * g.K[1] * g.K[2], sn = g.K[0] * g.K[1] * (g.K[2] / 2 + 1);
+            for (int k : kv.second) {
+                SysDev& S = sysHost[k];
+                for (int a = 0; a < 3; a++)
+                    S.K[a] = g.K[a];
+                S.gridOff = gridTotal;
+                S.specOff = specTotal;
+                S.gridN = gn;
+                S.specN = sn;
+                gridTotal += gn;
+                specTotal += sn;
+            }
+            maxSpec = std::max(maxSpec, sn);
+            for (int a = 0; a < 3; a++)
+                if (!moduliOff.count(g.K[a])) {
+                    moduliOff[g.K[a]] = (int) moduliHost.size();
+                    std::vector<double> m = bsplineModuli(g.K[a], s.order);
+                    moduliHost.insert(moduliHost.end(), m.begin(), m.end());
+                }
+            groups.push_back(g);
+        }
+        // the FFT groups need their systems contiguous in storage: systems of one shape are stored in index
+        // order, so a group is contiguous; the plan batch covers gridOff..gridOff + count * gn
+        for (auto& g : groups) {
+            int dims[3] = {g.K[0], g.K[1], g.K[2]};
+            const int gn = g.K[0] * g.K[1] * g.K[2], sn = g.K[0] * g.K[1] * (g.K[2] / 2 + 1);
+            CUFFT(cufftPlanMany(&g.r2c, 3, dims, nullptr, 1, gn, nullptr, 1, sn, mixed() ? CUFFT_R2C : CUFFT_D2Z,
+                                g.count));
+            CUFFT(cufftPlanMany(&g.c2r, 3, dims, nullptr, 1, sn, nullptr, 1, gn, mixed() ? CUFFT_C2R : CUFFT_Z2D,
+                                g.count));
+        }
+        convBlocks = std::max(1, std::min(512, (maxSpec + 255) / 256));
+        // chunks
+        chunkSys.clear();
+        chunkBegin.clear();
+        chunkEnd.clear();
+        for (int k = 0; k < nsys; k++) {
+            SysDev& S = sysHost[k];
+            S.atomBegin = atomBegin[k];
+            S.atomEnd = atomBegin[k + 1];
+            S.chunkFirst = (int) chunkSys.size();
+            for (int b = atomBegin[k]; b < atomBegin[k + 1]; b += CHUNK) {
+                chunkSys.push_back(k);
+                chunkBegin.push_back(b);
+                chunkEnd.push_back(std::min(b + CHUNK, atomBegin[k + 1]));
+            }
+            S.chunkCount = (int) chunkSys.size() - S.chunkFirst;
+            S.convBlocks = convBlocks;
+            for (int a = 0; a < 3; a++)
+                S.modOff[a] = moduliOff[S.K[a]];
+        }
+        // capacity of the pair list: density estimate at the first evaluation (grown on overflow)
+        cap = 0;
+        // device buffers sized by n
+        const size_t R = realSize();
+        dAtomSys.ensure(n * sizeof(int));
+        dQ.ensure(n * 8);
+        dR.ensure(n * 8);
+        dAlpha.ensure(n * 8);
+        dPosIn.ensure(3 * n * 8);
+        dWrap.ensure(3 * n * sizeof(int));
+        dCellOf.ensure(n * sizeof(int));
+        dCellRank.ensure(n * sizeof(int));
+        dBase.ensure(3 * n * sizeof(int));
+        dFr.ensure(3 * n * 8);
+        dSlotAtom.ensure(n * sizeof(int));
+        dPosS.ensure(n * sizeof(double4));
+        dRadS.ensure(n * 8);
+        dListCount.ensure(n * sizeof(int));
+        dFlags.ensure(16 * sizeof(int));
+        dDS.ensure(n * 4 * R);
+        for (Buf* b : {&dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dEpair, &dErec, &dFpair, &dFrec, &dEtot,
+                       &dForces})
+            b->ensure(3 * n * 8);
+        dSpair.ensure(9 * (size_t) n * 8);
+        dFin.ensure((size_t) n * NFIN * 8);
+        dPot.ensure(n * 8);
+        dGradQ.ensure(n * 8);
+        dGradR.ensure(n * 8);
+        dScal.ensure(nsys * NSCAL * 8);
+        dPartial.ensure(chunkSys.size() * 16 * 8);
+        dSysCounter.ensure(nsys * sizeof(int));
+        CU(cudaMemset(dSysCounter.p, 0, nsys * sizeof(int)));
+        dResults.ensure(nsys * NRES * 8);
+        dConvPartial.ensure((size_t) nsys * convBlocks * NCONV * 8);
+        std::vector<int> convOff(nsys);
+        for (int k = 0; k < nsys; k++)
+            convOff[k] = k * convBlocks;
+        upload(dConvOff, convOff, st);
+        dGrid.ensure(gridTotal * R);
+        dSpec.ensure(specTotal * 2 * R);
+        dInfl.ensure(specTotal * R);
+        upload(dModuli, moduliHost, st);
+        upload(dChunkSys, chunkSys, st);
+        upload(dChunkBegin, chunkBegin, st);
+        upload(dChunkEnd, chunkEnd, st);
+        upload(dAtomSys, atomSys, st);
+        upload(dQ, q, st);
+        upload(dR, radius, st);
+        upload(dAlpha, alpha, st);
+        if (!globalIdx.empty())
+            upload(dGlobal, globalIdx, st);
+        dHist.ensure((size_t) NHIST * 3 * numGlobal * 8);
+        dCtl.ensure(sizeof(Ctl));
+        dSys.ensure(nsys * sizeof(SysDev));
+        // pinned staging
+        if (hPosCap < (size_t) 3 * n) {
+            if (hPos) cudaFreeHost(hPos);
+            if (hPosF) cudaFreeHost(hPosF);
+            if (hForces) cudaFreeHost(hForces);
+            CU(cudaMallocHost((void**) &hPos, 3 * (size_t) n * 8));
+            CU(cudaMallocHost((void**) &hPosF, 3 * (size_t) n * 4));
+            CU(cudaMallocHost((void**) &hForces, 3 * (size_t) n * 8));
+            hPosCap = 3 * (size_t) n;
+        }
+        if (hSysCap < (size_t) nsys) {
+            if (hSys) cudaFreeHost(hSys);
+            if (hResults) cudaFreeHost(hResults);
+            CU(cudaMallocHost((void**) &hSys, nsys * sizeof(SysDev)));
+            CU(cudaMallocHost((void**) &hResults, nsys * NRES * 8));
+            hSysCap = nsys;
+        }
+        totalCells = 0;
+        cellCapacity = 0;
+        // no covalent dipoles until setCovalent
+        uploadCovalent();
+        haveResult = false;
+        configured = true;
+    }
+
+    // Box-dependent per-system constants; cell grids sized so that cells are at least rc/2 wide in every
+    // fractional direction (offsets -2..2 cover the cutoff sphere).  Returns true if the cell storage grew.
+    bool setBoxes(const double* boxes) {
+        int cells = 0;
+        double maxDensity = 0.0;
+        for (int k = 0; k < nsys; k++) {
+            SysDev& S = sysHost[k];
+            const double* H = boxes + 9 * k;
+            for (int a = 0; a < 9; a++)
+                S.H[a] = H[a];
+            if (H[1] != 0 || H[2] != 0 || H[5] != 0)
+                throw std::invalid_argument("pgm_b200: box not in the reduced triclinic form (a = (ax,0,0), b = (bx,by,0))");
+            if (!(H[0] > 0 && H[4] > 0 && H[8] > 0))
+                throw std::invalid_argument("pgm_b200: box diagonal must be positive");
+            boxInverse(H, S.recip, S.volume);
+            S.cutoff = sysCutoff[k];
+            S.rc2 = sysCutoff[k] * sysCutoff[k];
+            S.beta = sysBeta[k];
+            if (!(S.cutoff > 0) || !(S.beta > 0))
+                throw std::invalid_argument("pgm_b200: cutoff and Ewald coefficient must be positive");
+            S.cellOff = cells;
+            for (int a = 0; a < 3; a++) {
+                const double col = std::sqrt(S.recip[a] * S.recip[a] + S.recip[3 + a] * S.recip[3 + a] +
+                                             S.recip[6 + a] * S.recip[6 + a]);
+                const double rho = S.cutoff * col;   // fractional extent of the cutoff along a
+                int nc = (int) std::floor(2.0 / rho);
+                nc = std::max(1, std::min(nc, 1024));
+                S.cellN[a] = nc;
+                S.cellM[a] = std::max(1, (int) std::ceil(rho * nc * (1.0 + 1e-12)));
+            }
+            S.cellCount = S.cellN[0] * S.cellN[1] * S.cellN[2];
+            cells += S.cellCount;
+            const int na = atomBegin[k + 1] - atomBegin[k];
+            maxDensity = std::max(maxDensity, na / S.volume);
+        }
+        totalCells = cells;
+        bool grew = false;
+        if (cells + 1 > cellCapacity) {
+            cellCapacity = std::max(cells + 1, (int) (cellCapacity * 1.25));
+            dCellCount.ensure(cellCapacity * sizeof(int));
+            dCellStart.ensure((cellCapacity + 1) * sizeof(int));
+            grew = true;
+        }
+        if (cap == 0) {
+            // neighbours within rc at the highest density, +50 % for fluctuations
+            double maxNb = 0;
+            for (int k = 0; k < nsys; k++) {
+                const int na = atomBegin[k + 1] - atomBegin[k];
+                const double nb = 4.0 / 3.0 * PI_D * std::pow(sysCutoff[k], 3) * (na / sysHost[k].volume);
+                maxNb = std::max(maxNb, std::min(nb * 1.5 + 64.0, (double) na * 27));
+            }
+            cap = ((int) maxNb + 31) / 32 * 32;
+            allocList();
+            grew = true;
+        }
+        return grew;
+    }
+
+    void allocList() {
+        dList.ensure((size_t) n * cap * sizeof(uint32_t));
+        dG12.ensure((size_t) n * cap * 2 * realSize());
+    }
+
+    Dev makeDev(bool forGraph, cudaGraphConditionalHandle h) {
+        Dev d;
+        std::memset(&d, 0, sizeof(d));
+        d.nAtoms = n;
+        d.nSys = nsys;
+        d.nChunks = (int) chunkSys.size();
+        d.cap = cap;
+        d.order = s.order;
+        d.totalCells = totalCells;
+        d.gridTotal = gridTotal;
+        d.gridWords = gridTotal * (long long) (realSize() / 4);
+        d.ctl = dCtl.as<Ctl>();
+        d.ke = s.ke;
+        d.tol = s.tol;
+        d.peek = s.peek;
+        d.maxIter = s.maxIter;
+        d.sys = dSys.as<SysDev>();
+        d.atomSys = dAtomSys.as<int>();
+        d.q = dQ.as<double>();
+        d.radius = dR.as<double>();
+        d.alpha = dAlpha.as<double>();
+        d.posIn = dPosIn.as<double>();
+        d.wrapN = dWrap.as<int>();
+        d.cellOf = dCellOf.as<int>();
+        d.cellRank = dCellRank.as<int>();
+        d.pmeBase = dBase.as<int>();
+        d.pmeFr = dFr.as<double>();
+        d.cellCount = dCellCount.as<int>();
+        d.cellStart = dCellStart.as<int>();
+        d.slotAtom = dSlotAtom.as<int>();
+        d.posS = dPosS.as<double4>();
+        d.radS = dRadS.as<double>();
+        d.list = dList.as<uint32_t>();
+        d.listCount = dListCount.as<int>();
+        d.G12 = dG12.p;
+        d.flags = dFlags.as<int>();
+        d.dS = dDS.p;
+        d.perm = dPerm.as<double>();
+        d.mu = dMu.as<double>();
+        d.dtot = dDtot.as<double>();
+        d.b = dB.as<double>();
+        d.x = dX.as<double>();
+        d.r = dRv.as<double>();
+        d.z = dZ.as<double>();
+        d.p = dP.as<double>();
+        d.Ap = dAp.as<double>();
+        d.scal = dScal.as<double>();
+        d.partial = dPartial.as<double>();
+        d.sysCounter = dSysCounter.as<int>();
+        d.Epair = dEpair.as<double>();
+        d.Erec = dErec.as<double>();
+        d.Fpair = dFpair.as<double>();
+        d.spair = dSpair.as<double>();
+        d.Frec = dFrec.as<double>();
+        d.Etot = dEtot.as<double>();
+        d.fin = dFin.as<double>();
+        d.potRec = dPot.as<double>();
+        d.forces = dForces.as<double>();
+        d.results = dResults.as<double>();
+        d.convPartial = dConvPartial.as<double>();
+        d.convPartialOff = dConvOff.as<int>();
+        d.grid = dGrid.p;
+        d.spec = dSpec.p;
+        d.infl = dInfl.p;
+        d.moduli = dModuli.as<double>();
+        d.ncov = (int) covAtom.size();
+        d.covAtom = dCovAtom.as<int>();
+        d.covPartner = dCovPartner.as<int>();
+        d.covStrength = dCovStrength.as<double>();
+        d.covByAtomOff = dCovByAtomOff.as<int>();
+        d.covByAtom = dCovByAtom.as<int>();
+        d.covByPartnerOff = dCovByPartnerOff.as<int>();
+        d.covByPartner = dCovByPartner.as<int>();
+        d.chunkSys = dChunkSys.as<int>();
+        d.chunkBegin = dChunkBegin.as<int>();
+        d.chunkEnd = dChunkEnd.as<int>();
+        d.hist = dHist.as<double>();
+        d.globalIndex = globalIdx.empty() ? nullptr : dGlobal.as<int>();
+        d.numGlobal = numGlobal;
+        d.cond = h;
+        d.useCond = forGraph ? 1 : 0;
+        return d;
+    }
+
+    // ------------------------------------------------------------------------------------------ launches
+    template <typename R> void fftChain(cudaStream_t sm, const Dev& d, bool energy, bool gate) {
+        typedef typename CplxT<R>::T C;
+        for (auto& g : groups) {
+            CUFFT(cufftSetStream(g.r2c, sm));
+            R* gp = (R*) d.grid + g.gridOff;
+            C* sp = (C*) d.spec + g.specOff;
+            if (mixed())
+                CUFFT(cufftExecR2C(g.r2c, (cufftReal*) gp, (cufftComplex*) sp));
+            else
+                CUFFT(cufftExecD2Z(g.r2c, (cufftDoubleReal*) gp, (cufftDoubleComplex*) sp));
+        }
+        dim3 cg(convBlocks, nsys);
+        if (energy)
+            k_conv<R, true><<<cg, 256, 0, sm>>>(d, 0);
+        else
+            k_conv<R, false><<<cg, 256, 0, sm>>>(d, gate ? 1 : 0);
+        CU(cudaGetLastError());
+        for (auto& g : groups) {
+            CUFFT(cufftSetStream(g.c2r, sm));
+            R* gp = (R*) d.grid + g.gridOff;
+            C* sp = (C*) d.spec + g.specOff;
+            if (mixed())
+                CUFFT(cufftExecC2R(g.c2r, (cufftComplex*) sp, (cufftReal*) gp));
+            else
+                CUFFT(cufftExecZ2D(g.c2r, (cufftDoubleComplex*) sp, (cufftDoubleReal*) gp));
+        }
+    }
+
+    template <typename R, bool WITHQ> void pairField(cudaStream_t sm, const Dev& d, int gate) {
+        const long long threads = (long long) n * pairGS;
+        const int blocks = (int) ((threads + 255) / 256);
+        switch (pairGS) {
+        case 4: k_pair_field<R, WITHQ, 4><<<blocks, 256, 0, sm>>>(d, gate); break;
+        case 16: k_pair_field<R, WITHQ, 16><<<blocks, 256, 0, sm>>>(d, gate); break;
+        case 32: k_pair_field<R, WITHQ, 32><<<blocks, 256, 0, sm>>>(d, gate); break;
+        default: k_pair_field<R, WITHQ, 8><<<blocks, 256, 0, sm>>>(d, gate);
+        }
+        CU(cudaGetLastError());
+    }
+
+    // field of (q?, vec) at every atom into Epair / Erec: spread on sm, then the pair pass on sm beside the
+    // FFT chain on the side stream; joined on sm.
+    template <typename R, bool WITHQ>
+    void fieldPass(cudaStream_t sm, cudaStream_t sd, const Dev& d, int spreadMode, double* vec, bool gate) {
+        const int wblocks = (n + 7) / 8;
+        k_spread<R><<<wblocks, 256, 0, sm>>>(d, spreadMode, vec);
+        CU(cudaGetLastError());
+        CU(cudaEventRecord(evFork, sm));
+        CU(cudaStreamWaitEvent(sd, evFork, 0));
+        fftChain<R>(sd, d, false, gate);
+        pairField<R, WITHQ>(sm, d, gate ? 1 : 0);
+        CU(cudaEventRecord(evJoin, sd));
+        CU(cudaStreamWaitEvent(sm, evJoin, 0));
+        k_gather<R, false><<<wblocks, 256, 0, sm>>>(d, gate ? 1 : 0);
+        CU(cudaGetLastError());
+    }
+
+    template <typename R> void enqueuePre(cudaStream_t sm, cudaStream_t sd, const Dev& d) {
+        const int tb = (n + 255) / 256;
+        CU(cudaMemsetAsync(d.cellCount, 0, (size_t) totalCells * sizeof(int), sm));
+        CU(cudaMemsetAsync(d.flags, 0, 16 * sizeof(int), sm));
+        k_prep<<<tb, 256, 0, sm>>>(d, dPosIn.as<double>());
+        k_cell_scan<<<1, 1024, 0, sm>>>(d);
+        k_cell_scatter<<<tb, 256, 0, sm>>>(d);
+        k_cell_sort<<<(totalCells + 127) / 128, 128, 0, sm>>>(d);
+        k_build_list<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
+        k_perm<<<tb, 256, 0, sm>>>(d);
+        k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
+        CU(cudaGetLastError());
+        if (s.polarizable) {
+            CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
+            fieldPass<R, true>(sm, sd, d, 0, d.perm, false);
+            k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+            CU(cudaGetLastError());
+            CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
+            fieldPass<R, false>(sm, sd, d, 1, d.x, false);
+            k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+            CU(cudaGetLastError());
+        }
+    }
+
+    template <typename R> void enqueueIteration(cudaStream_t sm, cudaStream_t sd, const Dev& d) {
+        fieldPass<R, false>(sm, sd, d, 2, d.p, true);
+        k_cg_a<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+        k_cg_upd<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+        CU(cudaGetLastError());
+    }
+
+    template <typename R> void enqueuePost(cudaStream_t sm, cudaStream_t sd, const Dev& d) {
+        const int tb = (n + 255) / 256, wblocks = (n + 7) / 8;
+        CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
+        k_final_prep<<<tb, 256, 0, sm>>>(d, s.polarizable ? 1 : 0);
+        k_spread<R><<<wblocks, 256, 0, sm>>>(d, 0, d.dtot);
+        CU(cudaEventRecord(evFork, sm));
+        CU(cudaStreamWaitEvent(sd, evFork, 0));
+        fftChain<R>(sd, d, true, false);
+        {
+            const long long threads = (long long) n * pairGS;
+            const int blocks = (int) ((threads + 255) / 256);
+            switch (pairGS) {
+            case 4: k_pair_final<R, 4><<<blocks, 256, 0, sm>>>(d); break;
+            case 16: k_pair_final<R, 16><<<blocks, 256, 0, sm>>>(d); break;
+            case 32: k_pair_final<R, 32><<<blocks, 256, 0, sm>>>(d); break;
+            default: k_pair_final<R, 8><<<blocks, 256, 0, sm>>>(d);
+            }
+        }
+        CU(cudaEventRecord(evJoin, sd));
+        CU(cudaStreamWaitEvent(sm, evJoin, 0));
+        k_gather<R, true><<<wblocks, 256, 0, sm>>>(d, 0);
+        k_final_field<<<tb, 256, 0, sm>>>(d);
+        k_final_forces<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d, s.polarizable ? 1 : 0);
+        CU(cudaGetLastError());
+    }
+
+    template <typename R> void captureGraph() {
+        if (exec) {
+            cudaGraphExecDestroy(exec);
+            exec = nullptr;
+        }
+        cudaGraph_t graph;
+        CU(cudaGraphCreate(&graph, 0));
+        cudaGraphConditionalHandle handle = 0;
+        if (s.polarizable)
+            CU(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
+        const Dev d = makeDev(true, handle);
+        CU(cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t body = nullptr;
+        try {
+            enqueuePre<R>(st, side, d);
+            if (s.polarizable) {
+                cudaStreamCaptureStatus status;
+                const cudaGraphNode_t* deps = nullptr;
+                size_t numDeps = 0;
+                cudaGraph_t capturing;
+                CU(cudaStreamGetCaptureInfo(st, &status, nullptr, &capturing, &deps, &numDeps));
+                cudaGraphNodeParams cp = {};
+                cp.type = cudaGraphNodeTypeConditional;
+                cp.conditional.handle = handle;
+                cp.conditional.type = cudaGraphCondTypeWhile;
+                cp.conditional.size = 1;
+                cudaGraphNode_t node;
+                CU(cudaGraphAddNode(&node, capturing, deps, numDeps, &cp));
+                body = cp.conditional.phGraph_out[0];
+                CU(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+            }
+            enqueuePost<R>(st, side, d);
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(st, &g);
+            if (g)
+                cudaGraphDestroy(g);
+            cudaGraphDestroy(graph);
+            throw;
+        }
+        CU(cudaStreamEndCapture(st, &graph));
+        if (body) {
+            CU(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueueIteration<R>(st, side, d);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(st, &g);
+                cudaGraphDestroy(graph);
+                throw;
+            }
+            CU(cudaStreamEndCapture(st, &body));
+        }
+        CU(cudaGraphInstantiate(&exec, graph, 0));
+        CU(cudaGraphDestroy(graph));
+    }
+
+    template <typename R> void runDirect() {
+        const Dev d = makeDev(false, 0);
+        enqueuePre<R>(st, side, d);
+        if (s.polarizable) {
+            for (int it = 0; it <= s.maxIter + 1; it++) {
+                CU(cudaMemcpyAsync(hFlags, d.flags, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));
+                CU(cudaStreamSynchronize(st));
+                if (hFlags[2] >= nsys)
+                    break;
+                enqueueIteration<R>(st, side, d);
+            }
+        }
+        enqueuePost<R>(st, side, d);
+    }
+
+    // ------------------------------------------------------------------------------------------ evaluation
+    void prepareControl(bool newStep, int posMode, const void* posDevice, long long* forceFixed, int stride,
+                        double fixedScale, double* forcesOut) {
+        Ctl& c = *hCtl;
+        std::memset(&c, 0, sizeof(c));
+        const int h = histCount;
+        auto slot = [&](int back) { return (histHead + back) % NHIST; };
+        if (!s.polarizable)
+            c.guess = 0;
+        else if (!newStep && h > 0)
+            c.guess = 2;
+        else if (s.predictor == 2 && h >= 4)
+            c.guess = 4;
+        else if (s.predictor >= 1 && h >= 3)
+            c.guess = 3;
+        else if (s.predictor >= 1 && h >= 1)
+            c.guess = 2;
+        else
+            c.guess = s.zeroGuess ? 1 : 0;
+        for (int k = 0; k < 4; k++)
+            c.h[k] = slot(k);
+        const bool push = s.polarizable && (newStep || h == 0) && nsys == 1;
+        pendingSlot = push ? (histHead + NHIST - 1) % NHIST : -1;
+        c.histSlot = pendingSlot;
+        c.posMode = posMode;
+        c.posDevice = posDevice;
+        c.forceFixed = forceFixed;
+        c.fixedStride = stride;
+        c.fixedScale = fixedScale;
+        c.forcesOut = forcesOut;
+    }
+
+    // Enqueues one evaluation on st (inputs already staged); host waits only in finish().
+    void launch(const double* boxes) {
+        if (!configured || !atomsSet)
+            throw std::logic_error("pgm_b200: compute before setAtoms");
+        const bool grew = setBoxes(boxes);
+        if (grew && exec) {
+            cudaGraphExecDestroy(exec);
+            exec = nullptr;
+        }
+        std::memcpy(hSys, sysHost.data(), nsys * sizeof(SysDev));
+        CU(cudaMemcpyAsync(dSys.p, hSys, nsys * sizeof(SysDev), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(dCtl.p, hCtl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+        if (useGraph) {
+            if (!exec) {
+                try {
+                    if (mixed())
+                        captureGraph<float>();
+                    else
+                        captureGraph<double>();
+                } catch (const std::exception& e) {
+                    fprintf(stderr, "pgm_b200: graph capture failed (%s), running without graphs\n", e.what());
+                    cudaGetLastError();
+                    useGraph = false;
+                }
+            }
+        }
+        if (useGraph)
+            CU(cudaGraphLaunch(exec, st));
+        else if (mixed())
+            runDirect<float>();
+        else
+            runDirect<double>();
+        CU(cudaMemcpyAsync(hResults, dResults.p, nsys * NRES * 8, cudaMemcpyDeviceToHost, st));
+        CU(cudaMemcpyAsync(hFlags, dFlags.p, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CU(cudaEventRecord(evDone, st));
+        builds++;
+        launched = true;
+    }
+
+    // Waits for the launched evaluation; false if it must be repeated (pair-list capacity grown).
+    bool finish() {
+        CU(cudaEventSynchronize(evDone));
+        launched = false;
+        if (hFlags[1])
+            throw std::runtime_error("pgm_b200: pair image shift beyond 3 boxes (positions far outside the box?)");
+        if (hFlags[0] > cap) {
+            cap = (hFlags[0] + hFlags[0] / 4 + 31) / 32 * 32;
+            allocList();
+            if (exec) {
+                cudaGraphExecDestroy(exec);
+                exec = nullptr;
+            }
+            return false;
+        }
+        lastResults.assign(hResults, hResults + nsys * NRES);
+        haveResult = true;
+        if (pendingSlot >= 0) {
+            histHead = pendingSlot;
+            histCount = std::min(histCount + 1, 4);
+            pendingSlot = -1;
+        }
+        return true;
+    }
+
+    Terms termsOf(int k) const {
+        Terms t;
+        const double* r = lastResults.data() + (size_t) k * NRES;
+        t.direct = r[0];
+        t.reciprocal = r[1];
+        t.self = r[2];
+        t.background = r[3];
+        t.polarization = r[4];
+        return t;
+    }
+
+    void checkPositions(const double* pos, size_t m) {
+        for (size_t k = 0; k < m; k++)
+            if (!std::isfinite(pos[k]))
+                throw std::invalid_argument("pgm_b200: non-finite position");
+    }
+
+    // Host double positions, full evaluation, forces to the pinned buffer.
+    Terms evalHost(const double* pos, const double* boxes, bool newStep, bool wantForces) {
+        checkPositions(pos, 3 * (size_t) n);
+        selectDevice();
+        std::memcpy(hPos, pos, 3 * (size_t) n * 8);
+        for (int attempt = 0; attempt < 4; attempt++) {
+            prepareControl(newStep, 0, nullptr, nullptr, 0, 0.0, nullptr);
+            CU(cudaMemcpyAsync(dPosIn.p, hPos, 3 * (size_t) n * 8, cudaMemcpyHostToDevice, st));
+            launch(boxes);
+            if (wantForces) {
+                CU(cudaMemcpyAsync(hForces, dForces.p, 3 * (size_t) n * 8, cudaMemcpyDeviceToHost, st));
+                CU(cudaEventRecord(evDone, st));
+            }
+            if (finish())
+                return termsOf(0);
+        }
+        throw std::runtime_error("pgm_b200: pair list did not fit after growing it");
+    }
+};
+
+// ---------------------------------------------------------------------------------------------- Engine
+
+Engine::Engine(const Settings& settings) : impl(new Impl) {
+    try {
+        impl->init(settings);
+    } catch (...) {
+        delete impl;
+        throw;
+    }
+}
+
+Engine::~Engine() { delete impl; }
+
+void Engine::setAtoms(int n, const double* q, const double* radius, const double* alpha, const int* globalIndex,
+                      int numGlobal) {
+    impl->selectDevice();
+    impl->setAtomsSingle(n, q, radius, alpha, globalIndex, numGlobal);
+}
+
+void Engine::setCovalent(int ncov, const int* atom, const int* partner, const double* strength) {
+    impl->selectDevice();
+    impl->setCovalentSingle(ncov, atom, partner, strength);
+}
+
+Terms Engine::compute(const double* pos, const double box[3][3], bool newStep, double* f, double* strain) {
+    Impl& I = *impl;
+    if (I.nsys != 1)
+        throw std::logic_error("pgm_b200: compute on a batched engine (use computeBatch)");
+    const Terms t = I.evalHost(pos, &box[0][0], newStep, f != nullptr);
+    if (f)
+        for (int k = 0; k < 3 * I.n; k++)
+            f[k] += I.hForces[k];
+    if (strain)
+        for (int k = 0; k < 9; k++)
+            strain[k] += I.lastResults[5 + k];
+    return t;
+}
+
+Terms Engine::computeF(const float* pos, const double box[3][3], bool newStep, double* strain) {
+    Impl& I = *impl;
+    if (!I.atomsSet)
+        throw std::logic_error("pgm_b200: compute before setAtoms");
+    std::vector<double> pd(pos, pos + 3 * (size_t) I.n);
+    const Terms t = I.evalHost(pd.data(), &box[0][0], newStep, true);
+    I.forcesHostCache.assign(I.hForces, I.hForces + 3 * (size_t) I.n);
+    if (strain)
+        for (int k = 0; k < 9; k++)
+            strain[k] += I.lastResults[5 + k];
+    return t;
+}
+
+const double* Engine::forces() const { return impl->forcesHostCache.data(); }
+
+void Engine::launchDevice(const void* posq4, const double box[3][3], bool newStep, long long* forceFixed, int stride,
+                          double fixedScale, void* stream) {
+    Impl& I = *impl;
+    I.selectDevice();
+    I.callerStream = (cudaStream_t) stream;
+    // the caller's work so far comes first
+    CU(cudaEventRecord(I.evCaller, I.callerStream));
+    CU(cudaStreamWaitEvent(I.st, I.evCaller, 0));
+    I.prepareControl(newStep, 1, posq4, forceFixed, stride, fixedScale, nullptr);
+    I.launch(&box[0][0]);
+}
+
+bool Engine::finishDevice(Terms& terms) {
+    Impl& I = *impl;
+    if (!I.launched)
+        throw std::logic_error("pgm_b200: finishDevice without launchDevice");
+    if (!I.finish())
+        throw std::runtime_error("pgm_b200: pair list overflow on a device evaluation; capacity grown, repeat the call");
+    terms = I.termsOf(0);
+    return true;
+}
+
+void Engine::waitDevice(void* stream) {
+    Impl& I = *impl;
+    CU(cudaStreamWaitEvent((cudaStream_t) stream, I.evDone, 0));
+}
+
+Terms Engine::computeDevice(const void* posq4, const double box[3][3], bool newStep, long long* forceFixed, int stride,
+                            double fixedScale, void* stream) {
+    launchDevice(posq4, box, newStep, forceFixed, stride, fixedScale, stream);
+    Terms t;
+    finishDevice(t);
+    return t;
+}
+
+void Engine::launchResident(const double* posDev, const double box[3][3], bool newStep, double* forcesDev,
+                            void* stream) {
+    Impl& I = *impl;
+    I.selectDevice();
+    if (stream) {
+        CU(cudaEventRecord(I.evCaller, (cudaStream_t) stream));
+        CU(cudaStreamWaitEvent(I.st, I.evCaller, 0));
+    }
+    I.prepareControl(newStep, 2, posDev, nullptr, 0, 0.0, forcesDev);
+    I.launch(&box[0][0]);
+}
+
+int Engine::iterations() const { return impl->haveResult ? (int) impl->lastResults[14] : 0; }
+double Engine::residual() const { return impl->haveResult ? impl->lastResults[15] : 0.0; }
+
+void Engine::inducedDipoles(double* mu) const {
+    CU(cudaMemcpy(mu, impl->dMu.p, 3 * (size_t) impl->n * 8, cudaMemcpyDeviceToHost));
+}
+
+void Engine::permanentDipoles(double* p) const {
+    CU(cudaMemcpy(p, impl->dPerm.p, 3 * (size_t) impl->n * 8, cudaMemcpyDeviceToHost));
+}
+
+void Engine::resetHistory() { impl->resetHistoryState(); }
+long Engine::listBuilds() const { return impl->builds; }
+
+int Engine::numCandidates() const {
+    std::vector<int> c(impl->n);
+    CU(cudaMemcpy(c.data(), impl->dListCount.p, impl->n * sizeof(int), cudaMemcpyDeviceToHost));
+    long long s = 0;
+    for (int v : c)
+        s += v;
+    return (int) s;
+}
+
+std::array<double, 9> Engine::strainDerivative() const {
+    std::array<double, 9> a{};
+    if (impl->haveResult)
+        for (int k = 0; k < 9; k++)
+            a[k] = impl->lastResults[5 + k];
+    return a;
+}
+
+long long Engine::pairs(int* pi, int* pj, long long cap) {
+    Impl& I = *impl;
+    std::vector<int> cnt(I.n), slotAtom(I.n);
+    std::vector<uint32_t> list((size_t) I.n * I.cap);
+    CU(cudaMemcpy(cnt.data(), I.dListCount.p, I.n * sizeof(int), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(slotAtom.data(), I.dSlotAtom.p, I.n * sizeof(int), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(list.data(), I.dList.p, list.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    long long m = 0;
+    for (int sl = 0; sl < I.n; sl++) {
+        const int i = slotAtom[sl];
+        for (int t = 0; t < cnt[sl]; t++) {
+            const int j = slotAtom[list[(size_t) sl * I.cap + t] & 0x7FFFFFu];
+            if (i < j) {
+                if (m < cap) {
+                    pi[m] = i;
+                    pj[m] = j;
+                }
+                m++;
+            }
+        }
+    }
+    return m;
+}
+
+long long Engine::historySize() const {
+    return (long long) (Impl::NHIST * 3 * (size_t) impl->numGlobal * 8 + 2 * sizeof(int));
+}
+
+void Engine::getHistory(void* blob) const {
+    Impl& I = *impl;
+    int* hdr = (int*) blob;
+    hdr[0] = I.histHead;
+    hdr[1] = I.histCount;
+    CU(cudaMemcpy((char*) blob + 2 * sizeof(int), I.dHist.p, Impl::NHIST * 3 * (size_t) I.numGlobal * 8,
+                  cudaMemcpyDeviceToHost));
+}
+
+void Engine::setHistory(const void* blob) {
+    Impl& I = *impl;
+    const int* hdr = (const int*) blob;
+    if (hdr[0] < 0 || hdr[0] >= Impl::NHIST || hdr[1] < 0 || hdr[1] > 4)
+        throw std::invalid_argument("pgm_b200: history blob header out of range");
+    I.histHead = hdr[0];
+    I.histCount = hdr[1];
+    CU(cudaMemcpy(I.dHist.p, (const char*) blob + 2 * sizeof(int), Impl::NHIST * 3 * (size_t) I.numGlobal * 8,
+                  cudaMemcpyHostToDevice));
+}
+
+void Engine::field(const double* pos, const double box[3][3], const double* qf, const double* d, double* E) {
+    Impl& I = *impl;
+    if (!I.atomsSet || I.nsys != 1)
+        throw std::logic_error("pgm_b200: field needs a single-system engine with atoms set");
+    I.checkPositions(pos, 3 * (size_t) I.n);
+    I.selectDevice();
+    for (int attempt = 0; attempt < 4; attempt++) {
+        I.setBoxes(&box[0][0]);
+        I.prepareControl(true, 0, nullptr, nullptr, 0, 0.0, nullptr);
+        std::memcpy(I.hSys, I.sysHost.data(), I.nsys * sizeof(SysDev));
+        CU(cudaMemcpyAsync(I.dSys.p, I.hSys, I.nsys * sizeof(SysDev), cudaMemcpyHostToDevice, I.st));
+        CU(cudaMemcpyAsync(I.dCtl.p, I.hCtl, sizeof(Ctl), cudaMemcpyHostToDevice, I.st));
+        CU(cudaMemcpyAsync(I.dPosIn.p, pos, 3 * (size_t) I.n * 8, cudaMemcpyHostToDevice, I.st));
+        CU(cudaMemcpyAsync(I.dQ.p, qf, (size_t) I.n * 8, cudaMemcpyHostToDevice, I.st));
+        CU(cudaMemcpyAsync(I.dDtot.p, d, 3 * (size_t) I.n * 8, cudaMemcpyHostToDevice, I.st));
+        const Dev dv = I.makeDev(false, 0);
+        const int tb = (I.n + 255) / 256;
+        CU(cudaMemsetAsync(dv.cellCount, 0, (size_t) I.totalCells * sizeof(int), I.st));
+        CU(cudaMemsetAsync(dv.flags, 0, 16 * sizeof(int), I.st));
+        k_prep<<<tb, 256, 0, I.st>>>(dv, I.dPosIn.as<double>());
+        k_cell_scan<<<1, 1024, 0, I.st>>>(dv);
+        k_cell_scatter<<<tb, 256, 0, I.st>>>(dv);
+        k_cell_sort<<<(I.totalCells + 127) / 128, 128, 0, I.st>>>(dv);
+        if (I.mixed()) {
+            k_build_list<float><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
+            k_influence<float><<<dim3(I.convBlocks, I.nsys), 256, 0, I.st>>>(dv);
+            CU(cudaMemsetAsync(dv.grid, 0, I.gridTotal * I.realSize(), I.st));
+            I.fieldPass<float, true>(I.st, I.side, dv, 0, dv.dtot, false);
+        } else {
+            k_build_list<double><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
+            k_influence<double><<<dim3(I.convBlocks, I.nsys), 256, 0, I.st>>>(dv);
+            CU(cudaMemsetAsync(dv.grid, 0, I.gridTotal * I.realSize(), I.st));
+            I.fieldPass<double, true>(I.st, I.side, dv, 0, dv.dtot, false);
+        }
+        CU(cudaGetLastError());
+        std::vector<double> ep(3 * (size_t) I.n), er(3 * (size_t) I.n);
+        CU(cudaMemcpyAsync(ep.data(), I.dEpair.p, ep.size() * 8, cudaMemcpyDeviceToHost, I.st));
+        CU(cudaMemcpyAsync(er.data(), I.dErec.p, er.size() * 8, cudaMemcpyDeviceToHost, I.st));
+        CU(cudaMemcpyAsync(I.hFlags, I.dFlags.p, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
+        CU(cudaMemcpyAsync(I.dQ.p, I.q.data(), (size_t) I.n * 8, cudaMemcpyHostToDevice, I.st));
+        CU(cudaStreamSynchronize(I.st));
+        if (I.hFlags[0] > I.cap) {
+            I.cap = (I.hFlags[0] + I.hFlags[0] / 4 + 31) / 32 * 32;
+            I.allocList();
+            if (I.exec) {
+                cudaGraphExecDestroy(I.exec);
+                I.exec = nullptr;
+            }
+            continue;
+        }
+        const double beta = I.sysBeta[0];
+        const double cs = 4.0 * beta * beta * beta / (3.0 * SQRT_PI);
+        for (size_t k = 0; k < 3 * (size_t) I.n; k++)
+            E[k] = ep[k] + er[k] + cs * d[k];
+        I.haveResult = false;
+        return;
+    }
+    throw std::runtime_error("pgm_b200: pair list did not fit after growing it");
+}
+
+void Engine::paramGrad(double* dq, double* dradius, double* dalpha, double* dstrength) {
+    Impl& I = *impl;
+    if (!I.haveResult)
+        throw std::logic_error("pgm_b200: paramGrad needs a completed evaluation");
+    I.selectDevice();
+    const Dev dv = I.makeDev(false, 0);
+    const int blocks = (int) (((long long) I.n * 8 + 255) / 256);
+    k_pair_grad<8><<<blocks, 256, 0, I.st>>>(dv, I.dGradQ.as<double>(), I.dGradR.as<double>());
+    CU(cudaGetLastError());
+    const size_t n = I.n;
+    std::vector<double> gq(n), gR(n), pot(n), mu(3 * n), Et(3 * n), pos(3 * n);
+    CU(cudaMemcpyAsync(gq.data(), I.dGradQ.p, n * 8, cudaMemcpyDeviceToHost, I.st));
+    CU(cudaMemcpyAsync(gR.data(), I.dGradR.p, n * 8, cudaMemcpyDeviceToHost, I.st));
+    CU(cudaMemcpyAsync(pot.data(), I.dPot.p, n * 8, cudaMemcpyDeviceToHost, I.st));
+    CU(cudaMemcpyAsync(mu.data(), I.dMu.p, 3 * n * 8, cudaMemcpyDeviceToHost, I.st));
+    CU(cudaMemcpyAsync(Et.data(), I.dEtot.p, 3 * n * 8, cudaMemcpyDeviceToHost, I.st));
+    CU(cudaMemcpyAsync(pos.data(), I.dPosIn.p, 3 * n * 8, cudaMemcpyDeviceToHost, I.st));
+    CU(cudaStreamSynchronize(I.st));
+    const double ke = I.s.ke;
+    std::vector<double> Qs(I.nsys, 0.0);
+    for (size_t i = 0; i < n; i++)
+        Qs[I.atomSys[i]] += I.q[i];
+    for (size_t i = 0; i < n; i++) {
+        const SysDev& S = I.sysHost[I.atomSys[i]];
+        if (dq)
+            dq[i] = ke * (gq[i] + pot[i] - 2.0 * S.beta / SQRT_PI * I.q[i] -
+                          PI_D * Qs[I.atomSys[i]] / (S.volume * S.beta * S.beta));
+        if (dradius)
+            dradius[i] = ke * gR[i];
+        if (dalpha) {
+            const double a = I.alpha[i];
+            const double m2 = mu[3 * i] * mu[3 * i] + mu[3 * i + 1] * mu[3 * i + 1] + mu[3 * i + 2] * mu[3 * i + 2];
+            dalpha[i] = a > 0 ? -ke * m2 / (2.0 * a * a) : 0.0;
+        }
+    }
+    if (dstrength)
+        for (size_t m = 0; m < I.covAtom.size(); m++) {
+            const int i = I.covAtom[m], j = I.covPartner[m];
+            const SysDev& S = I.sysHost[I.atomSys[i]];
+            double v[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1], pos[3 * j + 2] - pos[3 * i + 2]};
+            for (int c = 2; c >= 0; c--) {
+                const double k = std::round(v[c] / S.H[4 * c]);
+                for (int a = 0; a < 3; a++)
+                    v[a] -= k * S.H[3 * c + a];
+            }
+            const double L = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            dstrength[m] = -ke * (Et[3 * i] * v[0] + Et[3 * i + 1] * v[1] + Et[3 * i + 2] * v[2]) / L;
+        }
+}
+
+void Engine::setSystems(int nsys, const int* atomCount, const double* cutoff, const double* beta, const int* grid,
+                        const double* q, const double* radius, const double* alpha, const int* covCount,
+                        const int* covAtom, const int* covPartner, const double* strength) {
+    impl->selectDevice();
+    impl->setSystemsBatch(nsys, atomCount, cutoff, beta, grid, q, radius, alpha, covCount, covAtom, covPartner,
+                          strength);
+}
+
+void Engine::computeBatch(const double* pos, const double* boxes, double* energies, double* forces, double* strain,
+                          int* iterations) {
+    Impl& I = *impl;
+    I.evalHost(pos, boxes, true, forces != nullptr);
+    for (int k = 0; k < I.nsys; k++) {
+        const double* r = I.lastResults.data() + (size_t) k * NRES;
+        if (energies)
+            for (int c = 0; c < 5; c++)
+                energies[6 * k + c] = r[c];
+        if (energies)
+            energies[6 * k + 5] = 0.0;
+        if (strain)
+            for (int c = 0; c < 9; c++)
+                strain[9 * k + c] = r[5 + c];
+        if (iterations)
+            iterations[k] = (int) r[14];
+    }
+    if (forces)
+        std::memcpy(forces, I.hForces, 3 * (size_t) I.n * 8);
+}
+
+}  // namespace pgmb200

@@ -1,0 +1,1001 @@
+// Kernels of the pgm_b200 engine.  One evaluation:
+//   prep -> cell scan -> cell scatter -> cell sort -> pair list (+ G1, G2) -> permanent dipoles
+//   -> E_perm = field(q, p) [spread || pair pass, FFT, convolution, gather]
+//   -> initial guess, A x0 -> CG loop (graph while node) -> final pass (energies, forces, field, strain)
+// Every per-atom array is in the caller's atom order; the hot loops run over "slots" (atoms sorted by cell).
+#pragma once
+
+#include "common.cuh"
+
+namespace pgmb200 {
+
+__device__ __forceinline__ int wrapIndex(int g, int K) {
+    g += (g < 0) ? K : 0;
+    g -= (g >= K) ? K : 0;
+    return g;
+}
+
+// ------------------------------------------------------------------------------------------------ prep
+
+// Per atom: fractional coordinates, wrap into the primary cell, cell index (with a within-cell rank from an
+// atomic counter, made deterministic by k_cell_sort), PME base index and fraction
+// (core/pgm_core.cpp:134-152: t = s - floor(s), w = K t, base = floor(w), fr = w - base).
+// posMode 0: dv.posIn (double 3n); 1: device float4 posq4 (dv.posDevice); 2: device double 3n (dv.posDevice).
+__global__ void k_prep(Dev dv, double* posCopy) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= dv.nAtoms)
+        return;
+    const SysDev& S = dv.sys[dv.atomSys[i]];
+    const int posMode = dv.ctl->posMode;
+    double r[3];
+    if (posMode == 1) {
+        const float4 v = ((const float4*) dv.ctl->posDevice)[i];
+        r[0] = v.x;
+        r[1] = v.y;
+        r[2] = v.z;
+    } else if (posMode == 2) {
+        const double* pd = (const double*) dv.ctl->posDevice;
+        r[0] = pd[3 * i];
+        r[1] = pd[3 * i + 1];
+        r[2] = pd[3 * i + 2];
+    } else {
+        r[0] = dv.posIn[3 * i];
+        r[1] = dv.posIn[3 * i + 1];
+        r[2] = dv.posIn[3 * i + 2];
+    }
+    if (posMode != 0) {
+        posCopy[3 * i] = r[0];
+        posCopy[3 * i + 1] = r[1];
+        posCopy[3 * i + 2] = r[2];
+    }
+    int cell[3];
+    double pw[3] = {r[0], r[1], r[2]};
+    for (int a = 0; a < 3; a++) {
+        const double s = __dadd_rn(__dadd_rn(__dmul_rn(r[0], S.recip[a]), __dmul_rn(r[1], S.recip[3 + a])),
+                                   __dmul_rn(r[2], S.recip[6 + a]));
+        const double fl = floor(s);
+        const double t = s - fl;
+        const double w = (double) S.K[a] * t;
+        const double base = floor(w);
+        dv.pmeBase[3 * i + a] = (int) base;
+        dv.pmeFr[3 * i + a] = w - base;
+        dv.wrapN[3 * i + a] = (int) fl;
+        int c = (int) floor(t * S.cellN[a]);
+        cell[a] = min(max(c, 0), S.cellN[a] - 1);
+        for (int k = 0; k < 3; k++)
+            pw[k] -= fl * S.H[3 * a + k];
+    }
+    const int lin = S.cellOff + (cell[0] * S.cellN[1] + cell[1]) * S.cellN[2] + cell[2];
+    dv.cellOf[i] = lin;
+    dv.cellRank[i] = atomicAdd(&dv.cellCount[lin], 1);
+    // wrapped position kept per atom until the slot copy
+    dv.Etot[3 * i] = pw[0];
+    dv.Etot[3 * i + 1] = pw[1];
+    dv.Etot[3 * i + 2] = pw[2];
+}
+
+// Exclusive scan of the cell counts (one block; totalCells + 1 entries written).
+__global__ void k_cell_scan(Dev dv) {
+    __shared__ int warpSums[32];
+    const int nT = blockDim.x, t = threadIdx.x;
+    const int n = dv.totalCells;
+    const int per = (n + nT - 1) / nT;
+    const int b = t * per, e = min(n, b + per);
+    int sum = 0;
+    for (int k = b; k < e; k++)
+        sum += dv.cellCount[k];
+    // inclusive warp scan
+    int v = sum;
+    const int lane = t & 31, w = t >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o)
+            v += y;
+    }
+    if (lane == 31)
+        warpSums[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        int ws = (lane < (nT >> 5)) ? warpSums[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, ws, o);
+            if (lane >= o)
+                ws += y;
+        }
+        warpSums[lane] = ws;
+    }
+    __syncthreads();
+    int run = v - sum + (w > 0 ? warpSums[w - 1] : 0);
+    for (int k = b; k < e; k++) {
+        dv.cellStart[k] = run;
+        run += dv.cellCount[k];
+    }
+    if (t == nT - 1)
+        dv.cellStart[n] = run;
+}
+
+__global__ void k_cell_scatter(Dev dv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= dv.nAtoms)
+        return;
+    dv.slotAtom[dv.cellStart[dv.cellOf[i]] + dv.cellRank[i]] = i;
+}
+
+// Sorts each cell's atoms by atom index (deterministic slot order), then fills the slot-order copies.
+__global__ void k_cell_sort(Dev dv) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= dv.totalCells)
+        return;
+    const int b = dv.cellStart[c], e = dv.cellStart[c + 1];
+    for (int k = b + 1; k < e; k++) {
+        const int v = dv.slotAtom[k];
+        int m = k - 1;
+        while (m >= b && dv.slotAtom[m] > v) {
+            dv.slotAtom[m + 1] = dv.slotAtom[m];
+            m--;
+        }
+        dv.slotAtom[m + 1] = v;
+    }
+    for (int k = b; k < e; k++) {
+        const int i = dv.slotAtom[k];
+        dv.posS[k] = make_double4(dv.Etot[3 * i], dv.Etot[3 * i + 1], dv.Etot[3 * i + 2], dv.q[i]);
+        dv.radS[k] = dv.radius[i];
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ pair list
+
+// One warp per slot: scans the neighbour cells (offsets -m..m per dimension, runs along the last dimension
+// merged into contiguous slot ranges), prefilters on the wrapped positions, then applies the reference's
+// exact test (minimum image of the original positions, r^2 < rc^2, core/pgm_core.cpp:64-87) and keeps a
+// candidate only at the image that test chose, so every pair enters once.  Accepted pairs are compacted with
+// a ballot (deterministic order) and get G1, G2 in precision R.
+template <typename R>
+__global__ void __launch_bounds__(256) k_build_list(Dev dv) {
+    typedef typename V2T<R>::T R2;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= dv.nAtoms)
+        return;
+    const int slot = warp;
+    const int i = dv.slotAtom[slot];
+    const int s = dv.atomSys[i];
+    const SysDev& S = dv.sys[s];
+    const double4 pwi = dv.posS[slot];
+    const double pi0 = dv.posIn[3 * i], pi1 = dv.posIn[3 * i + 1], pi2 = dv.posIn[3 * i + 2];
+    const int Ni0 = dv.wrapN[3 * i], Ni1 = dv.wrapN[3 * i + 1], Ni2 = dv.wrapN[3 * i + 2];
+    const double Ri = dv.radius[i];
+    const int lc = dv.cellOf[i] - S.cellOff;
+    const int n0 = S.cellN[0], n1 = S.cellN[1], n2 = S.cellN[2];
+    const int c2 = lc % n2, c1 = (lc / n2) % n1, c0 = lc / (n2 * n1);
+    const double pre = S.rc2 * (1.0 + 1e-10) + 1e-300;
+    uint32_t* row = dv.list + (size_t) slot * dv.cap;
+    R2* grow = (R2*) dv.G12 + (size_t) slot * dv.cap;
+    int count = 0;
+    bool badShift = false;
+    for (int d0 = -S.cellM[0]; d0 <= S.cellM[0]; d0++) {
+        const int u0 = c0 + d0;
+        const int w0 = (int) floor((double) u0 / n0), v0 = u0 - w0 * n0;
+        for (int d1 = -S.cellM[1]; d1 <= S.cellM[1]; d1++) {
+            const int u1 = c1 + d1;
+            const int w1 = (int) floor((double) u1 / n1), v1 = u1 - w1 * n1;
+            int d2 = -S.cellM[2];
+            while (d2 <= S.cellM[2]) {
+                // a run of consecutive cells with the same image shift along the last dimension
+                const int u2 = c2 + d2;
+                const int w2 = (int) floor((double) u2 / n2), v2 = u2 - w2 * n2;
+                int len = 1;
+                while (d2 + len <= S.cellM[2] && v2 + len < n2)
+                    len++;
+                const int cb = S.cellOff + (v0 * n1 + v1) * n2 + v2;
+                const int sb = dv.cellStart[cb], se = dv.cellStart[cb + len];
+                d2 += len;
+                const double sh0 = w0 * S.H[0] + w1 * S.H[3] + w2 * S.H[6];
+                const double sh1 = w1 * S.H[4] + w2 * S.H[7];
+                const double sh2 = w2 * S.H[8];
+                for (int base = sb; base < se; base += 32) {
+                    const int js = base + lane;
+                    bool acc = false;
+                    double x[3];
+                    int j = -1;
+                    if (js < se) {
+                        const double4 pwj = dv.posS[js];
+                        const double y0 = pwi.x - pwj.x - sh0, y1 = pwi.y - pwj.y - sh1, y2 = pwi.z - pwj.z - sh2;
+                        j = dv.slotAtom[js];
+                        if (j != i && y0 * y0 + y1 * y1 + y2 * y2 < pre) {
+                            x[0] = __dsub_rn(pi0, dv.posIn[3 * j]);
+                            x[1] = __dsub_rn(pi1, dv.posIn[3 * j + 1]);
+                            x[2] = __dsub_rn(pi2, dv.posIn[3 * j + 2]);
+                            int k[3];
+                            minImageExact(x, S.H, k);
+                            if (dot3exact(x) < S.rc2) {
+                                // image of the exact test relative to the wrapped positions
+                                const int k0 = k[0] - (Ni0 - dv.wrapN[3 * j]);
+                                const int k1 = k[1] - (Ni1 - dv.wrapN[3 * j + 1]);
+                                const int k2 = k[2] - (Ni2 - dv.wrapN[3 * j + 2]);
+                                acc = (k0 == w0 && k1 == w1 && k2 == w2);
+                            }
+                        }
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, acc);
+                    if (acc) {
+                        const int pos = count + __popc(m & ((1u << lane) - 1u));
+                        if (w0 < -4 || w0 > 3 || w1 < -4 || w1 > 3 || w2 < -4 || w2 > 3)
+                            badShift = true;
+                        if (pos < dv.cap) {
+                            row[pos] = packEntry(js, w0, w1, w2);
+                            const R rr = fsqrt((R) (x[0] * x[0] + x[1] * x[1] + x[2] * x[2]));
+                            const double Rj = dv.radius[j];
+                            const R a = (R) (1.0 / sqrt(2.0 * (Ri * Ri + Rj * Rj)));
+                            R G[3];
+                            pairKernels<R, 3>(a, (R) S.beta, rr, G);
+                            R2 g;
+                            g.x = G[1];
+                            g.y = G[2];
+                            grow[pos] = g;
+                        }
+                    }
+                    count += __popc(m);
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        dv.listCount[slot] = min(count, dv.cap);
+        if (count > dv.cap)
+            atomicMax(&dv.flags[0], count);
+    }
+    if (badShift)
+        atomicExch(&dv.flags[1], 1);
+}
+
+// ------------------------------------------------------------------------------------------------ dipoles
+
+// Permanent dipoles p_i = sum_m c_m unit(minimage(r_partner - r_atom)) over the dipoles of atom i
+// (core/pgm_core.cpp:51-62).
+__global__ void k_perm(Dev dv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= dv.nAtoms)
+        return;
+    const SysDev& S = dv.sys[dv.atomSys[i]];
+    double p[3] = {0, 0, 0};
+    for (int k = dv.covByAtomOff[i]; k < dv.covByAtomOff[i + 1]; k++) {
+        const int m = dv.covByAtom[k];
+        const int j = dv.covPartner[m];
+        double v[3] = {dv.posIn[3 * j] - dv.posIn[3 * i], dv.posIn[3 * j + 1] - dv.posIn[3 * i + 1],
+                       dv.posIn[3 * j + 2] - dv.posIn[3 * i + 2]};
+        int kk[3];
+        minImageExact(v, S.H, kk);
+        const double L = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        for (int a = 0; a < 3; a++)
+            p[a] += dv.covStrength[m] * v[a] / L;
+    }
+    for (int a = 0; a < 3; a++)
+        dv.perm[3 * i + a] = p[a];
+}
+
+// ------------------------------------------------------------------------------------------------ PME
+
+// Influence function G(m) = exp(-pi^2 m^2/beta^2)/(pi V m^2)/(b1 b2 b3), G(0) = 0 (core/pgm_core.cpp:155-177),
+// one value per half-spectrum element, stored in precision R.
+template <typename R>
+__global__ void k_influence(Dev dv) {
+    const int s = blockIdx.y;
+    const SysDev& S = dv.sys[s];
+    const int K0 = S.K[0], K1 = S.K[1], K2h = S.K[2] / 2 + 1;
+    R* infl = (R*) dv.infl + S.specOff;
+    const double fac = PI_D * PI_D / (S.beta * S.beta);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < S.specN; e += gridDim.x * blockDim.x) {
+        const int m3 = e % K2h, m2 = (e / K2h) % K1, m1 = e / (K2h * K1);
+        const double mm1 = (m1 <= K0 / 2) ? m1 : m1 - K0, mm2 = (m2 <= K1 / 2) ? m2 : m2 - K1, mm3 = m3;
+        double g = 0.0;
+        if (e != 0) {
+            double ms[3];
+            for (int k = 0; k < 3; k++)
+                ms[k] = mm1 * S.recip[3 * k] + mm2 * S.recip[3 * k + 1] + mm3 * S.recip[3 * k + 2];
+            const double m2s = ms[0] * ms[0] + ms[1] * ms[1] + ms[2] * ms[2];
+            g = exp(-fac * m2s) / (PI_D * S.volume * m2s) /
+                (dv.moduli[S.modOff[0] + m1] * dv.moduli[S.modOff[1] + m2] * dv.moduli[S.modOff[2] + m3]);
+        }
+        infl[e] = (R) g;
+    }
+}
+
+// Spread of charges and dipoles onto the grid: Q[g] += q t1 t2 t3 + e1 u1 t2 t3 + e2 t1 u2 t3 + e3 t1 t2 u3,
+// e_a = K_a d . recip[:, a] (core/pgm_core.cpp:187-207).  One warp per slot, p^3 points over the lanes.
+// mode 0: q and vec; 1: vec only; 2: CG direction update p = z + beta p first (vec = p), no charges.
+// Also writes the slot-order copy dS = (d, q) in precision R for the pair passes.
+template <typename R>
+__global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
+    typedef typename V4T<R>::T R4;
+    __shared__ R sth[8][3][MAXP], sdth[8][3][MAXP];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = blockIdx.x * 8 + wib;
+    if (slot >= dv.nAtoms)
+        return;
+    const int i = dv.slotAtom[slot];
+    const int s = dv.atomSys[i];
+    if (mode == 2 && dv.scal[s * NSCAL + SC_DONE] != 0.0)
+        return;
+    const SysDev& S = dv.sys[s];
+    const int p = dv.order;
+    double dl = 0.0;
+    if (lane < 3) {
+        if (mode == 2) {
+            dl = dv.z[3 * i + lane] + dv.scal[s * NSCAL + SC_BETA] * vec[3 * i + lane];
+            vec[3 * i + lane] = dl;
+        } else {
+            dl = vec[3 * i + lane];
+        }
+    }
+    const double d0 = __shfl_sync(0xffffffffu, dl, 0), d1 = __shfl_sync(0xffffffffu, dl, 1),
+                 d2 = __shfl_sync(0xffffffffu, dl, 2);
+    const double qv = (mode == 0) ? dv.q[i] : 0.0;
+    if (lane == 0) {
+        R4 o;
+        o.x = (R) d0;
+        o.y = (R) d1;
+        o.z = (R) d2;
+        o.w = (R) qv;
+        ((R4*) dv.dS)[slot] = o;
+    }
+    int bl = 0;
+    if (lane < 3) {
+        R t[MAXP], u[MAXP], v[MAXP];
+        bspline<R>((R) dv.pmeFr[3 * i + lane], p, t, u, v);
+#pragma unroll
+        for (int j = 0; j < MAXP; j++)
+            if (j < p) {
+                sth[wib][lane][j] = t[j];
+                sdth[wib][lane][j] = u[j];
+            }
+        bl = dv.pmeBase[3 * i + lane];
+    }
+    const int b0 = __shfl_sync(0xffffffffu, bl, 0), b1 = __shfl_sync(0xffffffffu, bl, 1),
+              b2 = __shfl_sync(0xffffffffu, bl, 2);
+    __syncwarp();
+    const R e0 = (R) (S.K[0] * (d0 * S.recip[0] + d1 * S.recip[3] + d2 * S.recip[6]));
+    const R e1 = (R) (S.K[1] * (d0 * S.recip[1] + d1 * S.recip[4] + d2 * S.recip[7]));
+    const R e2 = (R) (S.K[2] * (d0 * S.recip[2] + d1 * S.recip[5] + d2 * S.recip[8]));
+    const R qr = (R) qv;
+    R* grid = (R*) dv.grid + S.gridOff;
+    const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
+    const int pp = p * p, p3 = pp * p;
+    for (int t = lane; t < p3; t += 32) {
+        const int j1 = t / pp, j2 = (t / p) % p, j3 = t % p;
+        const R t1 = sth[wib][0][j1], u1 = sdth[wib][0][j1];
+        const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
+        const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+        const R w = qr * t1 * t2 * t3 + e0 * u1 * t2 * t3 + e1 * t1 * u2 * t3 + e2 * t1 * t2 * u3;
+        const int g1 = wrapIndex(b0 - j1, K0), g2 = wrapIndex(b1 - j2, K1), g3 = wrapIndex(b2 - j3, K2);
+        atomicAdd(&grid[((size_t) g1 * K1 + g2) * K2 + g3], w);
+    }
+}
+
+// Multiplies the spectrum by the influence function.  ENERGY: also the reciprocal energy
+// (1/2) sum w G |F|^2 (w = 1 on the m3 = 0 and Nyquist planes, else 2) and its strain derivative
+// e (-delta + 2 (pi^2/beta^2 + 1/m^2) m m) per block (core/pgm_core.cpp:214-235).  gateDone: skip systems whose
+// CG has converged.
+template <typename R, bool ENERGY>
+__global__ void __launch_bounds__(256) k_conv(Dev dv, int gateDone) {
+    typedef typename CplxT<R>::T C;
+    const int s = blockIdx.y;
+    if (gateDone && dv.scal[s * NSCAL + SC_DONE] != 0.0)
+        return;
+    const SysDev& S = dv.sys[s];
+    C* spec = (C*) dv.spec + S.specOff;
+    const R* infl = (const R*) dv.infl + S.specOff;
+    double acc[NCONV];
+#pragma unroll
+    for (int k = 0; k < NCONV; k++)
+        acc[k] = 0.0;
+    const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2], K2h = K2 / 2 + 1;
+    const double fac = PI_D * PI_D / (S.beta * S.beta);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < S.specN; e += gridDim.x * blockDim.x) {
+        C F = spec[e];
+        const R g = infl[e];
+        if (ENERGY && e != 0) {
+            const int m3 = e % K2h, m2 = (e / K2h) % K1, m1 = e / (K2h * K1);
+            const double w = (m3 == 0 || ((K2 & 1) == 0 && m3 == K2 / 2)) ? 1.0 : 2.0;
+            const double nrm = (double) F.x * F.x + (double) F.y * F.y;
+            const double en = 0.5 * w * (double) g * nrm;
+            acc[0] += en;
+            const double mm1 = (m1 <= K0 / 2) ? m1 : m1 - K0, mm2 = (m2 <= K1 / 2) ? m2 : m2 - K1, mm3 = m3;
+            double ms[3];
+            for (int k = 0; k < 3; k++)
+                ms[k] = mm1 * S.recip[3 * k] + mm2 * S.recip[3 * k + 1] + mm3 * S.recip[3 * k + 2];
+            const double m2s = ms[0] * ms[0] + ms[1] * ms[1] + ms[2] * ms[2];
+            const double c2 = 2.0 * (fac + 1.0 / m2s);
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int b = 0; b < 3; b++)
+                    acc[1 + 3 * a + b] += en * ((a == b ? -1.0 : 0.0) + c2 * ms[a] * ms[b]);
+        }
+        F.x *= g;
+        F.y *= g;
+        spec[e] = F;
+    }
+    if (ENERGY) {
+        blockReduce<NCONV>(acc, 0u);
+        if (threadIdx.x == 0)
+            for (int k = 0; k < NCONV; k++)
+                dv.convPartial[(size_t) (dv.convPartialOff[s] + blockIdx.x) * NCONV + k] = acc[k];
+    }
+}
+
+// Interpolation from the potential grid: f_a = sum (d theta_a) theta theta phi (the field, E_rec = -sum_a K_a
+// recip[:, a] f_a, core/pgm_core.cpp:241-264); FINAL also the second derivatives, the potential and the
+// reciprocal forces -K_a recip[k][a] (q f1_a + sum_b e_b f2_ab) (core/pgm_core.cpp:452-487) and E_rec (x) d.
+template <typename R, bool FINAL>
+__global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
+    __shared__ R sth[8][3][MAXP], sdth[8][3][MAXP], sd2[8][3][MAXP];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = blockIdx.x * 8 + wib;
+    if (slot >= dv.nAtoms)
+        return;
+    const int i = dv.slotAtom[slot];
+    const int s = dv.atomSys[i];
+    if (gateDone && dv.scal[s * NSCAL + SC_DONE] != 0.0)
+        return;
+    const SysDev& S = dv.sys[s];
+    const int p = dv.order;
+    int bl = 0;
+    if (lane < 3) {
+        R t[MAXP], u[MAXP], v[MAXP];
+        bspline<R>((R) dv.pmeFr[3 * i + lane], p, t, u, v);
+#pragma unroll
+        for (int j = 0; j < MAXP; j++)
+            if (j < p) {
+                sth[wib][lane][j] = t[j];
+                sdth[wib][lane][j] = u[j];
+                if (FINAL)
+                    sd2[wib][lane][j] = v[j];
+            }
+        bl = dv.pmeBase[3 * i + lane];
+    }
+    const int b0 = __shfl_sync(0xffffffffu, bl, 0), b1 = __shfl_sync(0xffffffffu, bl, 1),
+              b2 = __shfl_sync(0xffffffffu, bl, 2);
+    __syncwarp();
+    const R* grid = (const R*) dv.grid + S.gridOff;
+    const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
+    const int pp = p * p, p3 = pp * p;
+    R f[3] = {0, 0, 0}, f2[6] = {0, 0, 0, 0, 0, 0}, pot = 0;
+    for (int t = lane; t < p3; t += 32) {
+        const int j1 = t / pp, j2 = (t / p) % p, j3 = t % p;
+        const R t1 = sth[wib][0][j1], u1 = sdth[wib][0][j1];
+        const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
+        const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+        const int g1 = wrapIndex(b0 - j1, K0), g2 = wrapIndex(b1 - j2, K1), g3 = wrapIndex(b2 - j3, K2);
+        const R ph = grid[((size_t) g1 * K1 + g2) * K2 + g3];
+        f[0] += u1 * t2 * t3 * ph;
+        f[1] += t1 * u2 * t3 * ph;
+        f[2] += t1 * t2 * u3 * ph;
+        if (FINAL) {
+            const R v1 = sd2[wib][0][j1], v2 = sd2[wib][1][j2], v3 = sd2[wib][2][j3];
+            f2[0] += v1 * t2 * t3 * ph;
+            f2[1] += t1 * v2 * t3 * ph;
+            f2[2] += t1 * t2 * v3 * ph;
+            f2[3] += u1 * u2 * t3 * ph;
+            f2[4] += u1 * t2 * u3 * ph;
+            f2[5] += t1 * u2 * u3 * ph;
+            pot += t1 * t2 * t3 * ph;
+        }
+    }
+    double F[3] = {(double) f[0], (double) f[1], (double) f[2]};
+    double F2[7] = {(double) f2[0], (double) f2[1], (double) f2[2], (double) f2[3], (double) f2[4], (double) f2[5],
+                    (double) pot};
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            F[k] += __shfl_xor_sync(0xffffffffu, F[k], o);
+        if (FINAL)
+#pragma unroll
+            for (int k = 0; k < 7; k++)
+                F2[k] += __shfl_xor_sync(0xffffffffu, F2[k], o);
+    }
+    if (lane < 3) {
+        const int k = lane;
+        const double E = -(S.K[0] * S.recip[3 * k] * F[0] + S.K[1] * S.recip[3 * k + 1] * F[1] +
+                           S.K[2] * S.recip[3 * k + 2] * F[2]);
+        dv.Erec[3 * i + k] = E;
+        if (FINAL) {
+            const double* d = dv.dtot + 3 * i;
+            double e[3];
+            for (int a = 0; a < 3; a++)
+                e[a] = S.K[a] * (d[0] * S.recip[a] + d[1] * S.recip[3 + a] + d[2] * S.recip[6 + a]);
+            const double f2m[3][3] = {{F2[0], F2[3], F2[4]}, {F2[3], F2[1], F2[5]}, {F2[4], F2[5], F2[2]}};
+            const double qi = dv.q[i];
+            double Fk = 0.0;
+            for (int a = 0; a < 3; a++) {
+                const double c = qi * F[a] + e[0] * f2m[a][0] + e[1] * f2m[a][1] + e[2] * f2m[a][2];
+                Fk -= S.K[a] * S.recip[3 * k + a] * c;
+            }
+            dv.Frec[3 * i + k] = Fk;
+            // E_rec (x) d: fractional dipoles change with the box (core/pgm_core.cpp:446-451)
+            for (int b = 0; b < 3; b++)
+                dv.fin[(size_t) i * NFIN + 3 + 3 * k + b] = E * d[b];
+        }
+    }
+    if (FINAL && lane == 0)
+        dv.potRec[i] = F2[6];
+}
+
+// ------------------------------------------------------------------------------------------------ pair passes
+
+// Direct field at slot's atom of the dipoles (and with WITHQ the charges) of its list: E_i += q_j x G1 - d_j G1
+// + (d_j . x) x G2 (core/pgm_core.cpp:274-284), products in precision R, sums in double.  GS lanes per atom.
+template <typename R, bool WITHQ, int GS>
+__global__ void __launch_bounds__(256) k_pair_field(Dev dv, int gateDone) {
+    typedef typename V4T<R>::T R4;
+    typedef typename V2T<R>::T R2;
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / GS, lane = threadIdx.x % GS;
+    if (g >= dv.nAtoms)
+        return;
+    const int slot = g;
+    const int i = dv.slotAtom[slot];
+    const int s = dv.atomSys[i];
+    if (gateDone && dv.scal[s * NSCAL + SC_DONE] != 0.0)
+        return;
+    const SysDev& S = dv.sys[s];
+    const double4 pwi = dv.posS[slot];
+    const uint32_t* row = dv.list + (size_t) slot * dv.cap;
+    const R2* grow = (const R2*) dv.G12 + (size_t) slot * dv.cap;
+    const R4* dS = (const R4*) dv.dS;
+    const int cnt = dv.listCount[slot];
+    double E0 = 0, E1 = 0, E2 = 0;
+    for (int t = lane; t < cnt; t += GS) {
+        const uint32_t e = row[t];
+        const R2 G = grow[t];
+        const int js = entrySlot(e);
+        double sh[3];
+        entryShift(e, S.H, sh);
+        const double4 pwj = dv.posS[js];
+        const R x0 = (R) (pwi.x - pwj.x - sh[0]), x1 = (R) (pwi.y - pwj.y - sh[1]), x2 = (R) (pwi.z - pwj.z - sh[2]);
+        const R4 dj = dS[js];
+        const R djx = dj.x * x0 + dj.y * x1 + dj.z * x2;
+        R c = djx * G.y;
+        if (WITHQ)
+            c += dj.w * G.x;
+        E0 += (double) (c * x0 - dj.x * G.x);
+        E1 += (double) (c * x1 - dj.y * G.x);
+        E2 += (double) (c * x2 - dj.z * G.x);
+    }
+#pragma unroll
+    for (int o = GS / 2; o > 0; o >>= 1) {
+        E0 += __shfl_xor_sync(0xffffffffu, E0, o, GS);
+        E1 += __shfl_xor_sync(0xffffffffu, E1, o, GS);
+        E2 += __shfl_xor_sync(0xffffffffu, E2, o, GS);
+    }
+    if (lane == 0) {
+        dv.Epair[3 * i] = E0;
+        dv.Epair[3 * i + 1] = E1;
+        dv.Epair[3 * i + 2] = E2;
+    }
+}
+
+// Final pair pass at fixed d (core/pgm_core.cpp:422-440), per directed pair from i's side: half the pair
+// energy, the force on i (-dE/dx), the field at i and half the strain dE/dx (x) x.  G_0..G_3 recomputed in
+// precision R.
+template <typename R, int GS>
+__global__ void __launch_bounds__(256) k_pair_final(Dev dv) {
+    typedef typename V4T<R>::T R4;
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / GS, lane = threadIdx.x % GS;
+    if (g >= dv.nAtoms)
+        return;
+    const int slot = g;
+    const int i = dv.slotAtom[slot];
+    const SysDev& S = dv.sys[dv.atomSys[i]];
+    const double4 pwi = dv.posS[slot];
+    const R Ri = (R) dv.radS[slot];
+    const uint32_t* row = dv.list + (size_t) slot * dv.cap;
+    const R4* dS = (const R4*) dv.dS;
+    const R4 di = dS[slot];
+    const R beta = (R) S.beta;
+    const int cnt = dv.listCount[slot];
+    double acc[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+        acc[k] = 0.0;   // 0 energy, 1-3 force, 4-6 field, 7-15 strain
+    for (int t = lane; t < cnt; t += GS) {
+        const uint32_t e = row[t];
+        const int js = entrySlot(e);
+        double sh[3];
+        entryShift(e, S.H, sh);
+        const double4 pwj = dv.posS[js];
+        const R x[3] = {(R) (pwi.x - pwj.x - sh[0]), (R) (pwi.y - pwj.y - sh[1]), (R) (pwi.z - pwj.z - sh[2])};
+        const R4 dj = dS[js];
+        const R Rj = (R) dv.radS[js];
+        const R r = fsqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+        const R a = R(1) / fsqrt(R(2) * (Ri * Ri + Rj * Rj));
+        R G[4];
+        pairKernels<R, 4>(a, beta, r, G);
+        const R qi = di.w, qj = dj.w;
+        const R dix = di.x * x[0] + di.y * x[1] + di.z * x[2];
+        const R djx = dj.x * x[0] + dj.y * x[1] + dj.z * x[2];
+        const R didj = di.x * dj.x + di.y * dj.y + di.z * dj.z;
+        const R U = qi * qj * G[0] + (qi * djx - qj * dix) * G[1] + didj * G[1] - dix * djx * G[2];
+        const R sc = -qi * qj * G[1] - (qi * djx - qj * dix) * G[2] - didj * G[2] + dix * djx * G[3];
+        const R dcomp[3] = {dj.x, dj.y, dj.z}, icomp[3] = {di.x, di.y, di.z};
+        acc[0] += 0.5 * (double) U;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const R dedx = sc * x[k] + (qi * dcomp[k] - qj * icomp[k]) * G[1] - (djx * icomp[k] + dix * dcomp[k]) * G[2];
+            acc[1 + k] -= (double) dedx;
+            acc[4 + k] += (double) (qj * x[k] * G[1] - dcomp[k] * G[1] + djx * x[k] * G[2]);
+#pragma unroll
+            for (int b = 0; b < 3; b++)
+                acc[7 + 3 * k + b] += 0.5 * (double) (dedx * x[b]);
+        }
+    }
+#pragma unroll
+    for (int o = GS / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < 16; k++)
+            acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o, GS);
+    if (lane == 0) {
+        dv.fin[(size_t) i * NFIN + 0] = acc[0];
+        for (int k = 0; k < 3; k++) {
+            dv.Fpair[3 * i + k] = acc[1 + k];
+            dv.Epair[3 * i + k] = acc[4 + k];
+        }
+        for (int k = 0; k < 9; k++)
+            dv.spair[(size_t) i * 9 + k] = acc[7 + k];
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ CG
+
+// b = E_perm (pair + reciprocal + self), norm = mean|alpha b| per system, initial guess x0
+// (guess 0: alpha b; 1: zero; 2: history slot; 3: mu3 from history; 4: mu4 from history)
+// (core/pgm_core.cpp:297-329).
+__global__ void __launch_bounds__(CHUNK) k_cg_b(Dev dv) {
+    const int chunk = blockIdx.x;
+    const int s = dv.chunkSys[chunk];
+    const SysDev& S = dv.sys[s];
+    const int i = dv.chunkBegin[chunk] + threadIdx.x;
+    double v[1] = {0.0};
+    if (i < dv.chunkEnd[chunk]) {
+        const double cs = 4.0 * S.beta * S.beta * S.beta / (3.0 * SQRT_PI);
+        const double al = dv.alpha[i];
+        const int gi = dv.globalIndex ? dv.globalIndex[i] : i;
+        const size_t hs = (size_t) 3 * dv.numGlobal;
+        const int guess = dv.ctl->guess, h0 = dv.ctl->h[0], h1 = dv.ctl->h[1], h2 = dv.ctl->h[2], h3 = dv.ctl->h[3];
+        for (int k = 0; k < 3; k++) {
+            const double bk = dv.Epair[3 * i + k] + dv.Erec[3 * i + k] + cs * dv.perm[3 * i + k];
+            dv.b[3 * i + k] = bk;
+            v[0] += fabs(al * bk);
+            double x0;
+            const size_t g = (size_t) 3 * gi + k;
+            switch (guess) {
+            case 0: x0 = al * bk; break;
+            case 1: x0 = 0.0; break;
+            case 2: x0 = dv.hist[h0 * hs + g]; break;
+            case 3: x0 = 3 * dv.hist[h0 * hs + g] - 3 * dv.hist[h1 * hs + g] + dv.hist[h2 * hs + g]; break;
+            default:
+                x0 = 4 * dv.hist[h0 * hs + g] - 6 * dv.hist[h1 * hs + g] + 4 * dv.hist[h2 * hs + g] - dv.hist[h3 * hs + g];
+            }
+            dv.x[3 * i + k] = (guess >= 2 && !(al > 0)) ? 0.0 : x0;
+        }
+    }
+    double tot[1];
+    if (chunkFinish<1>(dv, chunk, s, v, 0u, tot) && threadIdx.x == 0)
+        dv.scal[s * NSCAL + SC_NORM] = tot[0] / (3.0 * (S.atomEnd - S.atomBegin)) + 1e-300;
+}
+
+// r = b - A x0 (rows of polarizable atoms), z = alpha r, direction p = 0 (so the first direction is z),
+// rz, err (core/pgm_core.cpp:351-361).  A v = v/alpha - T v, T v = pair + reciprocal + self field of v.
+__global__ void __launch_bounds__(CHUNK) k_cg_init(Dev dv) {
+    const int chunk = blockIdx.x;
+    const int s = dv.chunkSys[chunk];
+    const SysDev& S = dv.sys[s];
+    const int i = dv.chunkBegin[chunk] + threadIdx.x;
+    double v[2] = {0.0, 0.0};
+    if (i < dv.chunkEnd[chunk]) {
+        const double cs = 4.0 * S.beta * S.beta * S.beta / (3.0 * SQRT_PI);
+        const double al = dv.alpha[i];
+        for (int k = 0; k < 3; k++) {
+            const double xk = dv.x[3 * i + k];
+            const double Tx = dv.Epair[3 * i + k] + dv.Erec[3 * i + k] + cs * xk;
+            const double rk = (al > 0) ? dv.b[3 * i + k] - (xk / al - Tx) : 0.0;
+            const double zk = al * rk;
+            dv.r[3 * i + k] = rk;
+            dv.z[3 * i + k] = zk;
+            dv.p[3 * i + k] = 0.0;
+            v[0] += rk * zk;
+            v[1] = fmax(v[1], fabs(zk));
+        }
+    }
+    double tot[2];
+    if (chunkFinish<2>(dv, chunk, s, v, 2u, tot) && threadIdx.x == 0) {
+        double* sc = dv.scal + s * NSCAL;
+        sc[SC_RZ] = tot[0];
+        sc[SC_ERR] = tot[1] / sc[SC_NORM];
+        sc[SC_BETA] = 0.0;
+        sc[SC_IT] = 0.0;
+        const bool more = sc[SC_ERR] > dv.tol && 0 < dv.maxIter;
+        sc[SC_DONE] = more ? 0.0 : 1.0;
+        if (!more)
+            atomicAdd(&dv.flags[2], 1);
+        __threadfence();
+        if (atomicAdd(&dv.flags[3], 1) == dv.nSys - 1) {
+            // the last system to finish its initialisation decides whether the loop runs at all
+            const int ndone = atomicAdd(&dv.flags[2], 0);
+            dv.flags[5] = dv.nSys - ndone;
+            dv.flags[4] = 0;
+            dv.flags[3] = 0;
+            if (dv.useCond)
+                cudaGraphSetConditional(dv.cond, (ndone < dv.nSys) ? 1u : 0u);
+        }
+    }
+}
+
+// Ap = p/alpha - T p and p.Ap, then alph = rz / p.Ap per system (core/pgm_core.cpp:363-364).
+__global__ void __launch_bounds__(CHUNK) k_cg_a(Dev dv) {
+    const int chunk = blockIdx.x;
+    const int s = dv.chunkSys[chunk];
+    double* sc = dv.scal + s * NSCAL;
+    if (sc[SC_DONE] != 0.0)
+        return;
+    const SysDev& S = dv.sys[s];
+    const int i = dv.chunkBegin[chunk] + threadIdx.x;
+    double v[1] = {0.0};
+    if (i < dv.chunkEnd[chunk]) {
+        const double cs = 4.0 * S.beta * S.beta * S.beta / (3.0 * SQRT_PI);
+        const double al = dv.alpha[i];
+        for (int k = 0; k < 3; k++) {
+            const double pk = dv.p[3 * i + k];
+            const double Tp = dv.Epair[3 * i + k] + dv.Erec[3 * i + k] + cs * pk;
+            const double apk = (al > 0) ? pk / al - Tp : 0.0;
+            dv.Ap[3 * i + k] = apk;
+            v[0] += pk * apk;
+        }
+    }
+    double tot[1];
+    if (chunkFinish<1>(dv, chunk, s, v, 0u, tot) && threadIdx.x == 0)
+        sc[SC_ALPH] = sc[SC_RZ] / fmax(tot[0], 1e-300);
+}
+
+// x += alph p, r' = r - alph Ap, z' = alpha r', beta = z'.(r' - r)/rz, rz = r'.z', err = max|alpha r'|/norm,
+// convergence (core/pgm_core.cpp:362-385).  Also clears the PME grid for the next spread.
+__global__ void __launch_bounds__(CHUNK) k_cg_upd(Dev dv) {
+    // grid clearing for the next spread, every block (all systems), in 32-bit words
+    {
+        const size_t nth = (size_t) gridDim.x * blockDim.x;
+        for (size_t k = (size_t) blockIdx.x * blockDim.x + threadIdx.x; k < (size_t) dv.gridWords; k += nth)
+            ((uint32_t*) dv.grid)[k] = 0u;
+    }
+    const int chunk = blockIdx.x;
+    const int s = dv.chunkSys[chunk];
+    double* sc = dv.scal + s * NSCAL;
+    if (sc[SC_DONE] != 0.0)
+        return;
+    const int i = dv.chunkBegin[chunk] + threadIdx.x;
+    double v[3] = {0.0, 0.0, 0.0};
+    if (i < dv.chunkEnd[chunk]) {
+        const double al = dv.alpha[i], alph = sc[SC_ALPH];
+        for (int k = 0; k < 3; k++) {
+            const double pk = dv.p[3 * i + k];
+            dv.x[3 * i + k] += alph * pk;
+            const double rold = dv.r[3 * i + k];
+            const double rn = rold - alph * dv.Ap[3 * i + k];
+            const double zn = al * rn;
+            dv.r[3 * i + k] = rn;
+            dv.z[3 * i + k] = zn;
+            v[0] += zn * (rn - rold);
+            v[1] += rn * zn;
+            v[2] = fmax(v[2], fabs(zn));
+        }
+    }
+    double tot[3];
+    if (chunkFinish<3>(dv, chunk, s, v, 4u, tot) && threadIdx.x == 0) {
+        sc[SC_BETA] = tot[0] / fmax(sc[SC_RZ], 1e-300);
+        sc[SC_RZ] = tot[1];
+        sc[SC_ERR] = tot[2] / sc[SC_NORM];
+        sc[SC_IT] += 1.0;
+        const bool more = sc[SC_ERR] > dv.tol && sc[SC_IT] < dv.maxIter;
+        if (!more) {
+            sc[SC_DONE] = 1.0;
+            atomicAdd(&dv.flags[2], 1);
+        }
+        __threadfence();
+        // the last active system of this iteration to finish decides whether the loop goes on
+        const int active = atomicAdd(&dv.flags[4], 1) + 1;
+        if (active == dv.flags[5]) {
+            const int ndone = atomicAdd(&dv.flags[2], 0);
+            dv.flags[5] = dv.nSys - ndone;   // systems active in the next iteration
+            dv.flags[4] = 0;
+            if (dv.useCond)
+                cudaGraphSetConditional(dv.cond, (ndone < dv.nSys) ? 1u : 0u);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ final
+
+// mu = x + peek alpha r (core/pgm_core.cpp:386-389), d = p + mu, self and polarization energies per atom,
+// history push of mu (global order).
+__global__ void k_final_prep(Dev dv, int solved) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= dv.nAtoms)
+        return;
+    const int histSlot = dv.ctl->histSlot;
+    const SysDev& S = dv.sys[dv.atomSys[i]];
+    const double al = dv.alpha[i];
+    double m2 = 0.0, d2 = 0.0;
+    const int gi = dv.globalIndex ? dv.globalIndex[i] : i;
+    for (int k = 0; k < 3; k++) {
+        const double m = solved ? dv.x[3 * i + k] + dv.peek * al * dv.r[3 * i + k] : 0.0;
+        dv.mu[3 * i + k] = m;
+        const double d = dv.perm[3 * i + k] + m;
+        dv.dtot[3 * i + k] = d;
+        m2 += m * m;
+        d2 += d * d;
+        if (histSlot >= 0)
+            dv.hist[(size_t) histSlot * 3 * dv.numGlobal + 3 * gi + k] = m;
+    }
+    const double cs = 4.0 * S.beta * S.beta * S.beta / (3.0 * SQRT_PI);
+    const double qi = dv.q[i];
+    dv.fin[(size_t) i * NFIN + 1] = -(S.beta / SQRT_PI) * qi * qi - 0.5 * cs * d2;
+    dv.fin[(size_t) i * NFIN + 2] = (al > 0) ? m2 / (2.0 * al) : 0.0;
+}
+
+// Total field E = E_pair + E_rec + cs d (core/pgm_core.cpp:437-438, 445-448, 494-495).
+__global__ void k_final_field(Dev dv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= dv.nAtoms)
+        return;
+    const SysDev& S = dv.sys[dv.atomSys[i]];
+    const double cs = 4.0 * S.beta * S.beta * S.beta / (3.0 * SQRT_PI);
+    for (int k = 0; k < 3; k++)
+        dv.Etot[3 * i + k] = dv.Epair[3 * i + k] + dv.Erec[3 * i + k] + cs * dv.dtot[3 * i + k];
+}
+
+__device__ __forceinline__ void covalentTerm(const Dev& dv, const SysDev& S, int m, double* t, double* v) {
+    const int i = dv.covAtom[m], j = dv.covPartner[m];
+    v[0] = dv.posIn[3 * j] - dv.posIn[3 * i];
+    v[1] = dv.posIn[3 * j + 1] - dv.posIn[3 * i + 1];
+    v[2] = dv.posIn[3 * j + 2] - dv.posIn[3 * i + 2];
+    int kk[3];
+    minImageExact(v, S.H, kk);
+    const double L = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const double u[3] = {v[0] / L, v[1] / L, v[2] / L};
+    const double g[3] = {-dv.Etot[3 * i], -dv.Etot[3 * i + 1], -dv.Etot[3 * i + 2]};
+    const double gu = g[0] * u[0] + g[1] * u[1] + g[2] * u[2];
+    for (int k = 0; k < 3; k++)
+        t[k] = dv.covStrength[m] * (g[k] - gu * u[k]) / L;
+}
+
+// Forces F = ke (pair + reciprocal + covalent chain rule, core/pgm_core.cpp:511-535), written to the
+// outputs; per-system sums of the energies and the strain derivative, finished by the last chunk of each
+// system together with the reciprocal energy and strain of the convolution blocks.
+__global__ void __launch_bounds__(CHUNK) k_final_forces(Dev dv, int iterationsSolved) {
+    const int chunk = blockIdx.x;
+    const int s = dv.chunkSys[chunk];
+    const SysDev& S = dv.sys[s];
+    const int i = dv.chunkBegin[chunk] + threadIdx.x;
+    double v[14];
+#pragma unroll
+    for (int k = 0; k < 14; k++)
+        v[k] = 0.0;
+    if (i < dv.chunkEnd[chunk]) {
+        double F[3];
+        for (int k = 0; k < 3; k++)
+            F[k] = dv.Fpair[3 * i + k] + dv.Frec[3 * i + k];
+        double Sv[9];
+        for (int k = 0; k < 9; k++)
+            Sv[k] = dv.spair[(size_t) i * 9 + k] + dv.fin[(size_t) i * NFIN + 3 + k];
+        for (int c = dv.covByAtomOff[i]; c < dv.covByAtomOff[i + 1]; c++) {
+            double t[3], vv[3];
+            covalentTerm(dv, S, dv.covByAtom[c], t, vv);
+            for (int k = 0; k < 3; k++) {
+                F[k] += t[k];
+                for (int b = 0; b < 3; b++)
+                    Sv[3 * k + b] += t[k] * vv[b];
+            }
+        }
+        for (int c = dv.covByPartnerOff[i]; c < dv.covByPartnerOff[i + 1]; c++) {
+            double t[3], vv[3];
+            covalentTerm(dv, S, dv.covByPartner[c], t, vv);
+            for (int k = 0; k < 3; k++)
+                F[k] -= t[k];
+        }
+        for (int k = 0; k < 3; k++)
+            F[k] *= dv.ke;
+        for (int k = 0; k < 3; k++)
+            dv.forces[3 * i + k] = F[k];
+        const Ctl& io = *dv.ctl;
+        if (io.forcesOut)
+            for (int k = 0; k < 3; k++)
+                io.forcesOut[3 * i + k] = F[k];
+        if (io.forceFixed)
+            for (int k = 0; k < 3; k++)
+                atomicAdd((unsigned long long*) &io.forceFixed[i + k * io.fixedStride],
+                          (unsigned long long) llrint(F[k] * io.fixedScale));
+        v[0] = dv.fin[(size_t) i * NFIN + 0];
+        v[1] = dv.fin[(size_t) i * NFIN + 1];
+        v[2] = dv.fin[(size_t) i * NFIN + 2];
+        for (int k = 0; k < 9; k++)
+            v[3 + k] = Sv[k];
+        v[12] = dv.q[i];
+    }
+    double tot[14];
+    if (chunkFinish<14>(dv, chunk, s, v, 0u, tot) && threadIdx.x == 0) {
+        double conv[NCONV];
+        for (int k = 0; k < NCONV; k++)
+            conv[k] = 0.0;
+        for (int bk = 0; bk < S.convBlocks; bk++)
+            for (int k = 0; k < NCONV; k++)
+                conv[k] += dv.convPartial[(size_t) (dv.convPartialOff[s] + bk) * NCONV + k];
+        const double Q = tot[12];
+        const double bg = -PI_D * Q * Q / (2.0 * S.volume * S.beta * S.beta);
+        double* res = dv.results + (size_t) s * NRES;
+        res[0] = dv.ke * tot[0];
+        res[1] = dv.ke * conv[0];
+        res[2] = dv.ke * tot[1];
+        res[3] = dv.ke * bg;
+        res[4] = dv.ke * tot[2];
+        for (int k = 0; k < 9; k++) {
+            double sk = tot[3 + k] + conv[1 + k];
+            if (k % 4 == 0)
+                sk -= bg;
+            res[5 + k] = dv.ke * sk;
+        }
+        res[14] = iterationsSolved ? dv.scal[s * NSCAL + SC_IT] : 0.0;
+        res[15] = iterationsSolved ? dv.scal[s * NSCAL + SC_ERR] : 0.0;
+    }
+}
+
+// Pair parts of the parameter gradients at the final dipoles: dE/dq_i = sum_j q_j G0 + d_j.x G1 (x = r_i - r_j)
+// and dE/dR_i = sum_j U(dG/da) da/dR_i with dG_n/da = (2/sqrt(pi)) (2a^2)^n exp(-a^2 r^2), da/dR_i = -2 R_i a^3.
+// Double precision.  GS lanes per atom; writes gq[i], gR[i] (before the factor ke).
+template <int GS>
+__global__ void __launch_bounds__(256) k_pair_grad(Dev dv, double* gq, double* gR) {
+    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / GS, lane = threadIdx.x % GS;
+    if (g >= dv.nAtoms)
+        return;
+    const int slot = g;
+    const int i = dv.slotAtom[slot];
+    const SysDev& S = dv.sys[dv.atomSys[i]];
+    const double4 pwi = dv.posS[slot];
+    const double Ri = dv.radS[slot];
+    const uint32_t* row = dv.list + (size_t) slot * dv.cap;
+    const int cnt = dv.listCount[slot];
+    const double qi = dv.q[i];
+    const double di[3] = {dv.dtot[3 * i], dv.dtot[3 * i + 1], dv.dtot[3 * i + 2]};
+    double aq = 0.0, aR = 0.0;
+    for (int t = lane; t < cnt; t += GS) {
+        const uint32_t e = row[t];
+        const int js = entrySlot(e);
+        const int j = dv.slotAtom[js];
+        double sh[3];
+        entryShift(e, S.H, sh);
+        const double4 pwj = dv.posS[js];
+        const double x[3] = {pwi.x - pwj.x - sh[0], pwi.y - pwj.y - sh[1], pwi.z - pwj.z - sh[2]};
+        const double Rj = dv.radS[js];
+        const double r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+        const double a = 1.0 / sqrt(2.0 * (Ri * Ri + Rj * Rj));
+        double G[3];
+        pairKernels<double, 3>(a, S.beta, r, G);
+        const double qj = pwj.w;
+        const double dj[3] = {dv.dtot[3 * j], dv.dtot[3 * j + 1], dv.dtot[3 * j + 2]};
+        const double dix = di[0] * x[0] + di[1] * x[1] + di[2] * x[2];
+        const double djx = dj[0] * x[0] + dj[1] * x[1] + dj[2] * x[2];
+        const double didj = di[0] * dj[0] + di[1] * dj[1] + di[2] * dj[2];
+        aq += qj * G[0] + djx * G[1];
+        const double H0 = (2.0 / SQRT_PI) * exp(-(a * r) * (a * r)), H1 = H0 * 2.0 * a * a, H2 = H1 * 2.0 * a * a;
+        const double U = qi * qj * H0 + (qi * djx - qj * dix) * H1 + didj * H1 - dix * djx * H2;
+        aR += U * (-2.0 * Ri * a * a * a);
+    }
+#pragma unroll
+    for (int o = GS / 2; o > 0; o >>= 1) {
+        aq += __shfl_xor_sync(0xffffffffu, aq, o, GS);
+        aR += __shfl_xor_sync(0xffffffffu, aR, o, GS);
+    }
+    if (lane == 0) {
+        gq[i] = aq;
+        gR[i] = aR;
+    }
+}
+
+}  // namespace pgmb200

@@ -1,0 +1,87 @@
+// pgm_b200 C++ surface: the same methods as the reference GPU engine pgmcuda::Engine
+// (core/cuda/pgm_cuda.h:47-127 of larryhuang98/pGM-MD) plus batched systems and parameter gradients.
+// The C ABI (include/pgm_b200.h) wraps this class.
+#pragma once
+
+#include <array>
+#include <string>
+#include <vector>
+
+namespace pgmb200 {
+
+// pgmcuda::Settings (core/cuda/pgm_cuda.h:25-39) + precision / initial guess / polarizable.
+struct Settings {
+    double cutoff = 0.9;
+    double beta = 3.5;
+    int grid[3] = {36, 36, 36};
+    int order = 6;
+    double tol = 1e-5;
+    int maxIter = 100;
+    double peek = 0.65;
+    int predictor = 2;
+    double ke = 138.935458;
+    int device = 0;
+    double skin = 0.15;
+    int precision = 1;    // 0 FP64, 1 mixed
+    int zeroGuess = 0;
+    int polarizable = 1;
+};
+
+// pgmcuda::Terms (core/cuda/pgm_cuda.h:41-45).
+struct Terms {
+    double direct = 0, reciprocal = 0, self = 0, background = 0, polarization = 0, gvdw = 0;
+    double total() const { return direct + reciprocal + self + background + polarization + gvdw; }
+};
+
+class Engine {
+public:
+    explicit Engine(const Settings& settings);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    void setAtoms(int n, const double* q, const double* radius, const double* alpha, const int* globalIndex,
+                  int numGlobal);
+    void setCovalent(int ncov, const int* atom, const int* partner, const double* strength);
+    Terms compute(const double* pos, const double box[3][3], bool newStep, double* f, double* strain);
+    Terms computeF(const float* pos, const double box[3][3], bool newStep, double* strain);
+    void releasePositions() {}
+    const double* forces() const;
+    Terms computeDevice(const void* posq4, const double box[3][3], bool newStep, long long* forceFixed, int stride,
+                        double fixedScale, void* stream);
+    void launchDevice(const void* posq4, const double box[3][3], bool newStep, long long* forceFixed, int stride,
+                      double fixedScale, void* stream);
+    bool finishDevice(Terms& terms);
+    void waitDevice(void* stream);
+    void launchResident(const double* posDev, const double box[3][3], bool newStep, double* forcesDev, void* stream);
+    long lateListChecks() const { return 0; }
+
+    int iterations() const;
+    double residual() const;
+    void inducedDipoles(double* mu) const;
+    void permanentDipoles(double* p) const;
+    void resetHistory();
+    long listBuilds() const;
+    int numCandidates() const;
+    std::array<double, 9> strainDerivative() const;
+    void field(const double* pos, const double box[3][3], const double* q, const double* d, double* E);
+    long long pairs(int* pi, int* pj, long long cap);
+    long long historySize() const;
+    void getHistory(void* blob) const;
+    void setHistory(const void* blob);
+    void paramGrad(double* dq, double* dradius, double* dalpha, double* dstrength);
+
+    // batched systems
+    void setSystems(int nsys, const int* atomCount, const double* cutoff, const double* beta, const int* grid,
+                    const double* q, const double* radius, const double* alpha, const int* covCount,
+                    const int* covAtom, const int* covPartner, const double* strength);
+    void computeBatch(const double* pos, const double* boxes, double* energies, double* forces, double* strain,
+                      int* iterations);
+
+    struct Impl;
+
+private:
+    Impl* impl;
+};
+
+}  // namespace pgmb200

@@ -1,0 +1,199 @@
+"""CUDA engine against the FP64 oracle, through the C ABI, on cuda:0.
+
+Tolerances (stated per test): the FP64 path within 1e-7 relative in every energy term and 1e-6 relative
+RMS in forces (the reference's bar for pgm_core parity); the mixed path within 1e-5 relative RMS in forces
+against the FP64 oracle at tol 1e-10, the pair set bit-exact in both.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, PKG, load_golden_system, oracle_settings, oracle_topology
+from oracle import pgm_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TERMS = ("direct", "reciprocal", "self", "background", "polarization")
+
+
+def make_engine(S, precision, tol=1e-10, predictor=0, peek=0.0, ke=None, **kw):
+    eng = PKG.Engine(PKG.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=tol, max_iter=1000,
+                                  peek=peek, predictor=predictor, ke=PKG.systems.KE_DEFAULT if ke is None else ke,
+                                  precision=precision, **kw))
+    eng.set_system(S)
+    return eng
+
+
+def rel_rms(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("name", ["tiny_triclinic", "water216"])
+def test_fp64_matches_reference_outputs(name):
+    S, d = load_golden_system(name)
+    eng = make_engine(S, PKG.FP64)
+    r = eng.compute(S.pos, S.box)
+    t = r.terms.as_dict()
+    for k, nm in enumerate(TERMS):
+        assert abs(t[nm] - d["terms"][k]) <= 1e-7 * max(abs(d["terms"][k]), 1e-3), nm
+    assert abs(r.energy - float(d["energy"])) <= 1e-9 * abs(float(d["energy"]))
+    assert rel_rms(r.forces, d["forces"]) <= 1e-6
+    assert np.abs(r.strain - d["strain"]).max() <= 1e-6 * np.abs(d["strain"]).max()
+    assert np.abs(eng.induced_dipoles() - d["mu"]).max() <= 1e-6 * np.abs(d["mu"]).max()
+    assert np.abs(eng.permanent_dipoles() - d["perm"]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("name", ["tiny_triclinic", "water216"])
+def test_mixed_matches_reference_outputs(name):
+    S, d = load_golden_system(name)
+    eng = make_engine(S, PKG.MIXED)
+    r = eng.compute(S.pos, S.box)
+    assert abs(r.energy - float(d["energy"])) <= 1e-6 * abs(float(d["energy"]))
+    assert rel_rms(r.forces, d["forces"]) <= 1e-5
+    assert np.abs(r.strain - d["strain"]).max() <= 1e-5 * np.abs(d["strain"]).max()
+
+
+@pytest.mark.parametrize("name", ["tiny_triclinic", "water216"])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_pair_set_bit_exact(name, precision):
+    S, _ = load_golden_system(name)
+    eng = make_engine(S, precision)
+    eng.compute(S.pos, S.box)
+    gi, gj = eng.pairs()
+    oi, oj, _ = O.pair_set(S.pos, S.box, S.cutoff)
+    assert np.array_equal(gi, oi) and np.array_equal(gj, oj)
+    assert eng.num_candidates() == 2 * len(oi)
+
+
+def test_pair_set_knife_edge_and_far_images():
+    """Pairs at r == rc exactly are out, one ulp inside in; positions many boxes away from the primary cell
+    and a triclinic box give the reference's minimum image."""
+    rng = np.random.default_rng(1)
+    S = PKG.systems.tiny_triclinic(nmol=10, seed=4)
+    rc = S.cutoff
+    pos = S.pos.copy()
+    pos[1] = pos[0] + np.array([rc, 0.0, 0.0])
+    pos[2] = pos[0] + np.array([0.0, np.nextafter(rc, 0), 0.0])
+    pos[5:] += np.round(rng.uniform(-3, 3, (len(pos) - 5, 1))) * S.box[2]   # far images along c
+    for prec in (0, 1):
+        eng = make_engine(S, prec)
+        eng.compute(pos, S.box)
+        gi, gj = eng.pairs()
+        oi, oj, _ = O.pair_set(pos, S.box, rc)
+        assert np.array_equal(gi, oi) and np.array_equal(gj, oj)
+
+
+@pytest.mark.parametrize("level", ["q", "qp", "qi", "qpi"])
+def test_fp64_matches_pgmjax_goldens(level):
+    g = np.load(GOLDEN / "w512_pgmjax.npz")
+    cs = g["cov_strength"] if "p" in level else 0 * g["cov_strength"]
+    eng = PKG.Engine(PKG.Settings(cutoff=float(g["cutoff"]), beta=float(g["beta"]), grid=tuple(g["grid"]),
+                                  order=int(g["order"]), tol=float(g["tol"]), max_iter=1000, peek=0.0, predictor=0,
+                                  ke=float(g["ke"]), precision=PKG.FP64, polarizable="i" in level))
+    eng.set_atoms(g["q"], g["radius"], g["alpha"])
+    eng.set_covalent(g["cov_atom"], g["cov_partner"], cs)
+    r = eng.compute(g["pos"], g["H"])
+    e = float(g[f"{level}_energy"])
+    assert abs(r.energy - e) <= 1e-7 * abs(e)
+    assert rel_rms(r.forces, g[f"{level}_forces"]) <= 1e-6
+    if "i" in level:
+        assert np.abs(eng.induced_dipoles() - g[f"{level}_mu"]).max() <= 1e-6 * np.abs(g[f"{level}_mu"]).max()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_field_matches_oracle(precision):
+    S = PKG.systems.tiny_triclinic(nmol=20, seed=9)
+    rng = np.random.default_rng(2)
+    q = rng.normal(0, 0.5, S.n)
+    d = rng.normal(0, 0.01, (S.n, 3))
+    eng = make_engine(S, precision)
+    E = eng.field(S.pos, S.box, q, d)
+    ora = O.Engine(oracle_topology(S), oracle_settings(S))
+    ora.set_geometry(S.pos, S.box)
+    Eo = ora.field(q, d)
+    assert rel_rms(E, Eo) <= (1e-12 if precision == 0 else 2e-6)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_predictor_history_over_steps(precision):
+    """mu4 predictor over moved steps (the reference harness core/cuda/tests/test_cuda.cpp:300-341): energies
+    track the oracle at tol 1e-10 within 1e-6 relative; a repeated evaluation (new_step False) reuses the guess."""
+    S = PKG.systems.tiny_triclinic(nmol=20, seed=13)
+    eng = make_engine(S, precision, predictor=2)
+    rng = np.random.default_rng(11)
+    pos = S.pos.copy()
+    its = []
+    for step in range(6):
+        pos = pos + rng.uniform(-0.002, 0.002, pos.shape)
+        r = eng.compute(pos, S.box, new_step=True)
+        ora = O.Engine(oracle_topology(S), oracle_settings(S))
+        e = ora.compute(pos, S.box)
+        assert abs(r.energy - e) <= 1e-6 * abs(e)
+        its.append(r.iterations)
+    assert its[-1] < its[0]   # the extrapolation saves iterations
+    again = eng.compute(pos, S.box, new_step=False)
+    assert again.iterations <= 1
+    blob = eng.get_history()
+    eng.reset_history()
+    eng.set_history(blob)
+    assert eng.compute(pos, S.box, new_step=False).iterations <= 1
+
+
+def test_compute_f_and_device_paths():
+    """computeF (float positions) and launchDevice into a 64-bit fixed-point force buffer (OpenMM's layout,
+    x at i, y at i + stride, z at i + 2 stride, scale 2^32) give the forces of compute()."""
+    import torch
+    S = PKG.systems.tiny_triclinic(nmol=20, seed=17)
+    pf = S.pos.astype(np.float32)
+    eng = make_engine(S, PKG.MIXED)
+    r = eng.compute(pf.astype(np.float64), S.box)
+    rf = eng.compute_f(pf, S.box)
+    assert abs(rf.energy - r.energy) <= 1e-9 * abs(r.energy)
+    assert rel_rms(rf.forces, r.forces) <= 1e-9
+    dev = torch.device("cuda:0")
+    posq = torch.zeros((S.n, 4), dtype=torch.float32, device=dev)
+    posq[:, :3] = torch.from_numpy(pf).to(dev)
+    stride = ((S.n + 31) // 32) * 32
+    fixed = torch.zeros(3 * stride, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    eng.launch_device(posq.data_ptr(), S.box, True, fixed.data_ptr(), stride, 2.0 ** 32, stream.cuda_stream)
+    valid, t = eng.finish_device()
+    assert valid
+    torch.cuda.synchronize()
+    f = fixed.cpu().numpy().astype(np.float64) / 2.0 ** 32
+    F = np.stack([f[:S.n], f[stride:stride + S.n], f[2 * stride:2 * stride + S.n]], axis=1)
+    assert abs(t.total() - r.energy) <= 1e-9 * abs(r.energy)
+    assert rel_rms(F, r.forces) <= 1e-7
+    # device-resident double path
+    pd = torch.from_numpy(pf.astype(np.float64)).to(dev).contiguous()
+    fo = torch.zeros((S.n, 3), dtype=torch.float64, device=dev)
+    eng.launch_resident(pd.data_ptr(), S.box, True, fo.data_ptr(), stream.cuda_stream)
+    valid, t2 = eng.finish_device()
+    torch.cuda.synchronize()
+    assert abs(t2.total() - r.energy) <= 1e-9 * abs(r.energy)
+    assert rel_rms(fo.cpu().numpy(), r.forces) <= 1e-9
+
+
+def test_repeatable_bits():
+    """The same evaluation twice gives the same bits (deterministic reductions, fixed list order)."""
+    S = PKG.systems.water216()
+    eng = make_engine(S, PKG.FP64)
+    a = eng.compute(S.pos, S.box)
+    b = eng.compute(S.pos, S.box)
+    assert a.energy == b.energy
+    assert np.array_equal(a.forces, b.forces) or rel_rms(a.forces, b.forces) < 1e-14
+
+
+def test_errors_are_status_codes():
+    S = PKG.systems.tiny_triclinic(nmol=4, seed=1)
+    eng = make_engine(S, PKG.FP64)
+    bad = S.pos.copy()
+    bad[0, 0] = np.nan
+    with pytest.raises(PKG.PgmArgumentError, match="non-finite"):
+        eng.compute(bad, S.box)
+    with pytest.raises(PKG.PgmArgumentError, match="reduced"):
+        eng.compute(S.pos, np.array([[2.0, 0.1, 0], [0, 2, 0], [0, 0, 2]]))
+    with pytest.raises(PKG.PgmArgumentError):
+        eng.set_covalent([0], [0], [0.1])
+    r = eng.compute(S.pos, S.box)   # still usable
+    assert np.isfinite(r.energy)
