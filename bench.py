@@ -1,0 +1,423 @@
+#!/usr/bin/env python
+"""Benchmark: pGM energy + force + virial evaluations per second of the 8550-atom periodic liquid
+(450 rigid C8H10O molecules, 44.5 A box, beta 0.35/A, cutoff 9 A, 48^3 grid, order 6, tol 1e-5) on one
+B200, mixed precision, beside this engine's FP64 path on the same input.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pgm_b200|reference]
+
+A step is one full evaluation (cell and pair list, permanent field, CG induced-dipole solve from the
+alpha E_perm guess, final energies, forces and strain derivative).  N > 1 runs N independent replicas, one
+process per GPU (the single-system evaluation does not shard; weak scaling).  Inputs are resident in HBM
+for ``value``; ``e2e`` goes through the C ABI's host call with host positions and host forces.  L2 is
+flushed (a 256 MiB write) before every timed step.  ``--impl reference`` times the reference's own FP64
+CPU engine (core/pgm_core.cpp built from its sources into oracle/_ref) on every host core.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "pGM E+F evals/s, 8550-atom PME, mixed vs FP64 GPU at force relRMS≤1e-5"
+WORKLOAD = "dimethylphenol8550"
+TOL = 1e-5
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="pgm_b200", choices=["pgm_b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--ref-steps-cap", type=int, default=0, help="reference arm: cap on timed steps (0: --steps)")
+    return ap.parse_args()
+
+
+def system():
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    return pkg, pkg.systems.dimethylphenol8550(tol=TOL)
+
+
+def config(S, extra=None):
+    c = {"workload": WORKLOAD, "atoms": S.n, "molecules": 450, "box_nm": float(S.box[0, 0]), "cutoff_nm": S.cutoff,
+         "beta_per_nm": S.beta, "grid": list(S.grid), "order": S.order, "tol": TOL, "predictor": "none",
+         "peek": 0.65, "l2": "flushed (256 MiB write) before every timed step"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_of(kernel):
+    """DRAM bytes per launch of a kernel from the committed ncu summary (profiles/traffic.json), or None."""
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        v = d.get(WORKLOAD, {}).get(kernel)
+        return v
+    return None
+
+
+def algorithmic_bytes(kernel, S, precision, it):
+    """Algorithmic bytes per launch of the main kernels (the units and per-unit bytes are the ones DESIGN.md
+    states): s = real size, g = grid real size, P = directed pairs, p = order."""
+    s = 4 if precision else 8
+    n, p = S.n, S.order
+    P = S.meta.get("pairs", 0)
+    K1, K2, K3 = S.grid
+    G = K1 * K2 * K3
+    Gc = K1 * K2 * (K3 // 2 + 1)
+    if kernel == "spread":           # q, d, base, fraction in; p^3 grid updates
+        return n * (7 * s + p ** 3 * s)
+    if kernel == "gather":           # splines in, p^3 grid reads, 3 field values out
+        return n * (7 * s + 3 * 8 + p ** 3 * s)
+    if kernel == "pair_field":       # per directed pair: 4 B entry + 2 s (G1, G2); per atom: position, dipole, field
+        return P * (4 + 2 * s) + n * (32 + 4 * s + 24)
+    if kernel == "fft_chain":        # r2c + convolution (read F, G, write F) + c2r
+        return 2 * (G * s + Gc * 2 * s) + Gc * (2 * s + s + 2 * s)
+    if kernel == "pair_list":        # candidates' positions, list entries + G1, G2 written
+        return n * 32 * 125 // 4 + P * (4 + 2 * s)
+    if kernel == "pair_final":
+        return P * 4 + n * (32 + 4 * s + 8 * 16)
+    if kernel == "cg_update":
+        return n * 3 * 8 * 6
+    return None
+
+
+def launches_per_eval(kernel, it):
+    return {"pair_list": 1, "pair_field": it + 2, "spread": it + 3, "gather": it + 3, "pair_final": 1,
+            "fft_chain": it + 3, "cg_update": it}.get(kernel, 1)
+
+
+def reference_arm(args):
+    """The reference's own CPU implementation (pgm_core, FP64) on all host cores: one process per core, each
+    step one evaluation per process."""
+    import multiprocessing as mp
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import ref as R
+    pkg, S = system()
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpgmcore_ref.so not built "
+                          "(make -C oracle where the reference sources are present)"}))
+        return 0
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    ctx = mp.get_context("spawn")
+    steps = args.steps if not args.ref_steps_cap else min(args.steps, args.ref_steps_cap)
+    with ctx.Pool(cores, initializer=_ref_worker_init) as pool:
+        pool.map(_ref_worker_eval, range(cores))          # untimed: every worker builds its engine
+        for _ in range(args.warmup):
+            pool.map(_ref_worker_eval, range(cores))
+        times = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            pool.map(_ref_worker_eval, range(cores))
+            times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = cores * steps / total
+    line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+            "config": config(S, {"implementation": "reference pgm_core (core/pgm_core.cpp) FP64, one process per core",
+                                 "step": f"{cores} evaluations in parallel, one per process"}),
+            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "reference",
+                             "sample": f"{steps} steps x {cores} full evaluations of {WORKLOAD}"},
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+_REF = {}
+
+
+def _ref_worker_init():
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, str(ROOT))
+    from oracle import pgm_oracle as O
+    from oracle import ref as R
+    pkg, S = system()
+    top = O.Topology(S.q, S.radius, S.alpha, S.cov_atom, S.cov_partner, S.cov_strength)
+    st = O.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=TOL, max_iter=500, peek=0.65,
+                    predictor=0, ke=pkg.systems.KE_DEFAULT)
+    _REF["eng"] = R.RefEngine(top, st)
+    _REF["S"] = S
+
+
+def _ref_worker_eval(_):
+    from oracle import ref as R
+    e = _REF["eng"]
+    S = _REF["S"]
+    R.lib().ref_reset_history(e.h)   # an independent evaluation (no reuse of the previous solution)
+    return e.compute(S.pos, S.box)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device(f"cuda:{local}"))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    pkg, S = system()
+
+    def make(precision):
+        eng = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=TOL,
+                                      max_iter=200, peek=0.65, predictor=0, ke=pkg.systems.KE_DEFAULT,
+                                      precision=precision, device=local))
+        eng.set_system(S)
+        return eng
+
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    pos_d = torch.from_numpy(S.pos).to(dev).contiguous()
+    f_d = torch.zeros((S.n, 3), dtype=torch.float64, device=dev)
+
+    def timed_resident(eng, steps, warmup, sampler=None):
+        for _ in range(warmup):
+            eng.launch_resident(pos_d.data_ptr(), S.box, True, f_d.data_ptr(), stream.cuda_stream)
+            eng.wait_device(stream.cuda_stream)
+            eng.finish_device()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        its = []
+        ctx = sampler if sampler is not None else _Null()
+        with ctx:
+            for k in range(steps):
+                flush.zero_()
+                evs[k][0].record(stream)
+                eng.launch_resident(pos_d.data_ptr(), S.box, True, f_d.data_ptr(), stream.cuda_stream)
+                eng.wait_device(stream.cuda_stream)
+                evs[k][1].record(stream)
+                eng.finish_device()
+                its.append(eng.iterations())
+            torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        return ms, its
+
+    # mixed: autotune, time
+    mixed = make(pkg.MIXED)
+    r0 = mixed.compute(S.pos, S.box)
+    lanes = mixed.autotune(S.pos, S.box)
+    S.meta["pairs"] = mixed.num_candidates()
+    sampler = ClockSampler(local)
+    ms_mixed, its_mixed = timed_resident(mixed, args.steps, max(args.warmup, 3), sampler)
+    clocks = sampler.summary()
+    t = torch.tensor([ms_mixed], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_mixed = float(t.item())
+    value = world * args.steps / (ms_mixed / 1e3)
+    # FP64 path on the same input (the metric's denominator)
+    fp64 = make(pkg.FP64)
+    fp64.compute(S.pos, S.box)
+    fp64.set_pair_lanes(lanes)
+    fsteps = max(3, min(args.steps, 20))
+    ms_fp64, its_fp64 = timed_resident(fp64, fsteps, 3)
+    t = torch.tensor([ms_fp64], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    fp64_value = world * fsteps / (float(t.item()) / 1e3)
+    # end to end through the C ABI host call (host positions in, host forces out)
+    for _ in range(2):
+        mixed.compute(S.pos, S.box)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    e2e_steps = args.steps
+    for _ in range(e2e_steps):
+        res = mixed.compute(S.pos, S.box)
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps / float(t.item())
+    # roofline of the dominant kernel (relaunched alone, CUDA events on the engine's stream)
+    mixed.compute(S.pos, S.box)
+    it = mixed.iterations()
+    kt = mixed.kernel_times(reps=20)
+    share = {k: v * launches_per_eval(k, it) for k, v in kt.items()}
+    dom = max(share, key=share.get)
+    alg = algorithmic_bytes(dom, S, 1, it)
+    peak, peak_kind = peaks()
+    achieved = alg / (kt[dom] * 1e-3) / 1e9 if alg else None
+    roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
+            "traffic": traffic_of(dom), "bytes_per_launch": alg, "ms_per_launch": kt[dom],
+            "kernel_ms": kt, "kernel_share_of_eval": {k: v / sum(share.values()) for k, v in share.items()}}
+    line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+            "config": config(S, {"parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                                 "pair_lanes": lanes, "cg_iterations": int(np.median(its_mixed))}),
+            "fp64": {"value": fp64_value, "unit": "evals/s", "steps": fsteps,
+                     "cg_iterations": int(np.median(its_fp64))},
+            "mixed_over_fp64": value / fp64_value,
+            "ns_per_day_2fs": value / world * 86400 * 2e-6,
+            "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": S.n * 3 * 8,
+                    "d2h_bytes_per_step": S.n * 3 * 8 + 16 * 8},
+            "gpu_launches": mixed.kernel_launches() * args.steps,
+            "roofline": roof, "clocks": clocks}
+    if rank == 0 and not args.no_accuracy:
+        line["accuracy"] = accuracy(pkg, S, mixed, fp64)
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(pkg, S)
+    mixed.close()
+    fp64.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def _oracle_reference(pkg, S, tol):
+    from oracle import pgm_oracle as O
+    from oracle import ref as R
+    top = O.Topology(S.q, S.radius, S.alpha, S.cov_atom, S.cov_partner, S.cov_strength)
+    st = O.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=tol, max_iter=1000, peek=0.0,
+                    predictor=0, ke=pkg.systems.KE_DEFAULT)
+    if R.available():
+        e = R.RefEngine(top, st)
+        E = e.compute(S.pos, S.box)
+        return E, e.forces, "reference pgm_core (oracle/_ref), tol 1e-10"
+    e = O.Engine(top, st)
+    E = e.compute(S.pos, S.box)
+    return E, e.forces, "numpy oracle, tol 1e-10"
+
+
+def accuracy(pkg, S, mixed, fp64):
+    """Errors of both GPU paths (at the benchmark tolerance) against the FP64 oracle at tol 1e-10."""
+    E0, F0, kind = _oracle_reference(pkg, S, 1e-10)
+    out = {"oracle": kind}
+    for name, eng in (("mixed", mixed), ("fp64", fp64)):
+        r = eng.compute(S.pos, S.box)
+        out[name] = {"force_rel_rms": float(np.linalg.norm(r.forces - F0) / np.linalg.norm(F0)),
+                     "energy_rel": float(abs(r.energy - E0) / abs(E0)), "iterations": r.iterations}
+    return out
+
+
+def cpu_baseline(pkg, S):
+    """The reference pgm_core on one host core: two full evaluations of the same workload."""
+    from oracle import pgm_oracle as O
+    from oracle import ref as R
+    if not R.available():
+        return None
+    top = O.Topology(S.q, S.radius, S.alpha, S.cov_atom, S.cov_partner, S.cov_strength)
+    st = O.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=TOL, max_iter=500, peek=0.65,
+                    predictor=0, ke=pkg.systems.KE_DEFAULT)
+    e = R.RefEngine(top, st)
+    e.compute(S.pos, S.box)
+    n = 2
+    t0 = time.perf_counter()
+    for _ in range(n):
+        R.lib().ref_reset_history(e.h)
+        e.compute(S.pos, S.box)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "evals/s", "cores": 1, "kind": "reference",
+            "sample": f"{n} full evaluations of {WORKLOAD} (pgm_core, single-threaded)"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -138,6 +138,16 @@ int pgm_engine_set_history(pgm_engine* e, const void* blob);
  * covalent dipole (ncov).  Any output may be NULL.  No counterpart in the reference. */
 int pgm_engine_param_grad(pgm_engine* e, double* dq, double* dradius, double* dalpha, double* dstrength);
 
+/* Measurement (no counterpart in the reference): the number of this library's kernels the last evaluation
+ * ran (cuFFT transforms not counted); average device durations [ms] over reps launches of the main kernels
+ * relaunched alone on the engine's stream after an evaluation: ms[0] pair list build, [1] pair field pass,
+ * [2] PME spread, [3] PME gather, [4] final pair pass, [5] FFT chain (r2c, convolution, c2r), [6] CG kernel.
+ * pair lanes: lanes per atom of the pair passes (4, 8, 16 or 32; the autotuner's knob). */
+int pgm_engine_kernel_launches(pgm_engine* e);
+int pgm_engine_kernel_times(pgm_engine* e, int reps, double* ms);
+int pgm_engine_set_pair_lanes(pgm_engine* e, int lanes);
+int pgm_engine_pair_lanes(pgm_engine* e);
+
 /* Batched evaluation: nsys independent systems of uneven sizes in one launch.  Atom arrays are the systems'
  * arrays concatenated; atom_count[s] atoms per system; per-system cutoff, beta and grid (3 ints); covalent
  * indices are local to their system.  The shared settings (order, tol, max_iter, peek, ke, precision) come

@@ -63,6 +63,10 @@ SIGNATURES = {
     "pgm_engine_get_history": (c_int, [c_void_p, c_void_p]),
     "pgm_engine_set_history": (c_int, [c_void_p, c_void_p]),
     "pgm_engine_param_grad": (c_int, [c_void_p, P_D, P_D, P_D, P_D]),
+    "pgm_engine_kernel_launches": (c_int, [c_void_p]),
+    "pgm_engine_kernel_times": (c_int, [c_void_p, c_int, P_D]),
+    "pgm_engine_set_pair_lanes": (c_int, [c_void_p, c_int]),
+    "pgm_engine_pair_lanes": (c_int, [c_void_p]),
     "pgm_engine_set_systems": (c_int, [c_void_p, c_int, P_I, P_D, P_D, P_I, P_D, P_D, P_D, P_I, P_I, P_I, P_D]),
     "pgm_engine_compute_batch": (c_int, [c_void_p, P_D, P_D, P_D, P_D, P_D, P_I]),
 }

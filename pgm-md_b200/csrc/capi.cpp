@@ -309,6 +309,24 @@ int pgm_engine_param_grad(pgm_engine* e, double* dq, double* dradius, double* da
     return guarded([&] { e->e->paramGrad(dq, dradius, dalpha, dstrength); });
 }
 
+int pgm_engine_kernel_launches(pgm_engine* e) { return (e && e->e) ? e->e->kernelLaunches() : -1; }
+
+int pgm_engine_kernel_times(pgm_engine* e, int reps, double* ms) {
+    NEED(e);
+    return guarded([&] {
+        if (reps <= 0 || !ms)
+            throw std::invalid_argument("pgm_b200: kernel_times arguments");
+        e->e->kernelTimes(reps, ms);
+    });
+}
+
+int pgm_engine_set_pair_lanes(pgm_engine* e, int lanes) {
+    NEED(e);
+    return guarded([&] { e->e->setPairLanes(lanes); });
+}
+
+int pgm_engine_pair_lanes(pgm_engine* e) { return (e && e->e) ? e->e->pairLanes() : -1; }
+
 int pgm_engine_set_systems(pgm_engine* e, int nsys, const int* atom_count, const double* cutoff, const double* beta,
                            const int* grid, const double* q, const double* radius, const double* alpha,
                            const int* cov_count, const int* cov_atom, const int* cov_partner, const double* strength) {

@@ -165,14 +165,14 @@ __device__ __forceinline__ void erfKernels(R a, R r, R* B) {
         t[0] = R(1);
 #pragma unroll
         for (int m = 1; m < 15; m++)
-            t[m] = t[m - 1] * (-s) / R(m);
+            t[m] = t[m - 1] * (-s) * R(1.0 / m);
         R pw = R(1);
 #pragma unroll
         for (int k = 0; k < NMAX; k++) {
             R sum = R(0);
 #pragma unroll
             for (int m = 14; m >= 0; m--)
-                sum += t[m] / R(2 * m + 2 * k + 1);
+                sum += t[m] * R(1.0 / (2 * m + 2 * k + 1));
             B[k] = c0 * pw * sum;
             pw *= a2;
         }
@@ -291,6 +291,11 @@ __device__ __forceinline__ void entryShift(uint32_t e, const double* H, double* 
     sh[0] = w0 * H[0] + w1 * H[3] + w2 * H[6];
     sh[1] = w1 * H[4] + w2 * H[7];
     sh[2] = w2 * H[8];
+}
+
+// Shuffle mask of the GS-lane group holding this thread (GS a power of two <= 32).
+template <int GS> __device__ __forceinline__ unsigned groupMask() {
+    return GS == 32 ? 0xffffffffu : (((1u << GS) - 1u) << ((threadIdx.x & 31) & ~(GS - 1)));
 }
 
 // Deterministic block reduction of NV doubles (sum, or max where the bit of maxMask is set); valid in

@@ -279,6 +279,9 @@ struct Engine::Impl {
         for (double& a : alpha)
             if (a <= 1e-9)
                 a = 0.0;   // not polarizable (core/pgm_constants.h:9)
+        for (int a = 0; a < 3; a++)
+            if (s.grid[a] < s.order)
+                throw std::invalid_argument("pgm_b200: PME grid smaller than the spline order");
         atomSys.assign(n, 0);
         numGlobal = gidx ? nGlobal : n;
         globalIdx.clear();
@@ -316,7 +319,7 @@ struct Engine::Impl {
         for (int k = 0; k < ns; k++)
             for (int a = 0; a < 3; a++) {
                 sysK[k][a] = grd[3 * k + a];
-                if (sysK[k][a] < s.order - 1 || sysK[k][a] <= 0)
+                if (sysK[k][a] < s.order)
                     throw std::invalid_argument("pgm_b200: PME grid smaller than the spline order");
             }
         q.assign(qq, qq + n);
@@ -585,6 +588,20 @@ struct Engine::Impl {
                 S.cellN[a] = nc;
                 S.cellM[a] = std::max(1, (int) std::ceil(rho * nc * (1.0 + 1e-12)));
             }
+            // at most ~8 cells per atom (very short cutoffs): widen the cells, offsets shrink accordingly
+            const int na0 = atomBegin[k + 1] - atomBegin[k];
+            while ((long long) S.cellN[0] * S.cellN[1] * S.cellN[2] > 8LL * na0 + 64) {
+                int a = 0;
+                for (int b = 1; b < 3; b++)
+                    if (S.cellN[b] > S.cellN[a])
+                        a = b;
+                S.cellN[a] = std::max(1, S.cellN[a] / 2);
+            }
+            for (int a = 0; a < 3; a++) {
+                const double col = std::sqrt(S.recip[a] * S.recip[a] + S.recip[3 + a] * S.recip[3 + a] +
+                                             S.recip[6 + a] * S.recip[6 + a]);
+                S.cellM[a] = std::max(1, (int) std::ceil(S.cutoff * col * S.cellN[a] * (1.0 + 1e-12)));
+            }
             S.cellCount = S.cellN[0] * S.cellN[1] * S.cellN[2];
             cells += S.cellCount;
             const int na = atomBegin[k + 1] - atomBegin[k];
@@ -781,6 +798,8 @@ struct Engine::Impl {
             fieldPass<R, false>(sm, sd, d, 1, d.x, false);
             k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
             CU(cudaGetLastError());
+            // the loop's first spread needs a clear grid (each iteration clears it for the next one)
+            CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
         }
     }
 
@@ -878,9 +897,17 @@ struct Engine::Impl {
         const Dev d = makeDev(false, 0);
         enqueuePre<R>(st, side, d);
         if (s.polarizable) {
+            static const bool trace = std::getenv("PGM_B200_TRACE") != nullptr;
             for (int it = 0; it <= s.maxIter + 1; it++) {
                 CU(cudaMemcpyAsync(hFlags, d.flags, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));
                 CU(cudaStreamSynchronize(st));
+                if (trace) {
+                    double sc[NSCAL];
+                    CU(cudaMemcpy(sc, d.scal, sizeof(sc), cudaMemcpyDeviceToHost));
+                    fprintf(stderr, "pgm_b200 trace: it %d done %d/%d system 0: norm %.6e rz %.6e alph %.6e beta %.6e "
+                            "err %.6e\n", it, hFlags[2], nsys, sc[SC_NORM], sc[SC_RZ], sc[SC_ALPH], sc[SC_BETA],
+                            sc[SC_ERR]);
+                }
                 if (hFlags[2] >= nsys)
                     break;
                 enqueueIteration<R>(st, side, d);
@@ -1092,7 +1119,7 @@ bool Engine::finishDevice(Terms& terms) {
     if (!I.launched)
         throw std::logic_error("pgm_b200: finishDevice without launchDevice");
     if (!I.finish())
-        throw std::runtime_error("pgm_b200: pair list overflow on a device evaluation; capacity grown, repeat the call");
+        return false;   // the pair list outgrew its capacity: grown now; the caller repeats the evaluation
     terms = I.termsOf(0);
     return true;
 }
@@ -1310,6 +1337,79 @@ void Engine::paramGrad(double* dq, double* dradius, double* dalpha, double* dstr
             dstrength[m] = -ke * (Et[3 * i] * v[0] + Et[3 * i + 1] * v[1] + Et[3 * i + 2] * v[2]) / L;
         }
 }
+
+int Engine::kernelLaunches() const {
+    const Impl& I = *impl;
+    if (!I.haveResult)
+        return 0;
+    // own kernels per evaluation: preparation 8, the two field passes before the loop 3 + 1 + 3 + 1,
+    // 4 per CG iteration, final 7 (the cuFFT transforms are not counted)
+    int it = 0;
+    for (int k = 0; k < I.nsys; k++)
+        it = std::max(it, (int) I.lastResults[(size_t) k * NRES + 14]);
+    return 8 + (I.s.polarizable ? 8 + 4 * it : 0) + 7;
+}
+
+void Engine::kernelTimes(int reps, double* ms) {
+    Impl& I = *impl;
+    if (!I.haveResult)
+        throw std::logic_error("pgm_b200: kernelTimes needs a completed evaluation");
+    I.selectDevice();
+    const Dev d = I.makeDev(false, 0);
+    cudaEvent_t a, b;
+    CU(cudaEventCreate(&a));
+    CU(cudaEventCreate(&b));
+    const int wb = (I.n + 7) / 8;
+    auto timeIt = [&](auto&& fn) {
+        fn();
+        CU(cudaEventRecord(a, I.st));
+        for (int r = 0; r < reps; r++)
+            fn();
+        CU(cudaEventRecord(b, I.st));
+        CU(cudaEventSynchronize(b));
+        float t = 0;
+        CU(cudaEventElapsedTime(&t, a, b));
+        return (double) t / reps;
+    };
+    auto run = [&](auto tag) {
+        typedef decltype(tag) R;
+        ms[0] = timeIt([&] { k_build_list<R><<<(I.n + 7) / 8, 256, 0, I.st>>>(d); });
+        ms[1] = timeIt([&] { I.pairField<R, false>(I.st, d, 0); });
+        ms[2] = timeIt([&] { k_spread<R><<<wb, 256, 0, I.st>>>(d, 1, d.x); });
+        ms[3] = timeIt([&] { k_gather<R, false><<<wb, 256, 0, I.st>>>(d, 0); });
+        ms[4] = timeIt([&] {
+            const int blocks = (int) (((long long) I.n * I.pairGS + 255) / 256);
+            switch (I.pairGS) {
+            case 4: k_pair_final<R, 4><<<blocks, 256, 0, I.st>>>(d); break;
+            case 16: k_pair_final<R, 16><<<blocks, 256, 0, I.st>>>(d); break;
+            case 32: k_pair_final<R, 32><<<blocks, 256, 0, I.st>>>(d); break;
+            default: k_pair_final<R, 8><<<blocks, 256, 0, I.st>>>(d);
+            }
+        });
+        ms[5] = timeIt([&] { I.fftChain<R>(I.st, d, false, false); });
+        ms[6] = timeIt([&] { k_cg_a<<<(int) I.chunkSys.size(), CHUNK, 0, I.st>>>(d); });
+    };
+    if (I.mixed())
+        run(float());
+    else
+        run(double());
+    CU(cudaGetLastError());
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    I.haveResult = true;
+}
+
+void Engine::setPairLanes(int lanes) {
+    if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+        throw std::invalid_argument("pgm_b200: pair lanes must be 4, 8, 16 or 32");
+    if (lanes != impl->pairGS && impl->exec) {
+        cudaGraphExecDestroy(impl->exec);
+        impl->exec = nullptr;
+    }
+    impl->pairGS = lanes;
+}
+
+int Engine::pairLanes() const { return impl->pairGS; }
 
 void Engine::setSystems(int nsys, const int* atomCount, const double* cutoff, const double* beta, const int* grid,
                         const double* q, const double* radius, const double* alpha, const int* covCount,

@@ -561,11 +561,12 @@ __global__ void __launch_bounds__(256) k_pair_field(Dev dv, int gateDone) {
         E1 += (double) (c * x1 - dj.y * G.x);
         E2 += (double) (c * x2 - dj.z * G.x);
     }
+    const unsigned gm = groupMask<GS>();
 #pragma unroll
     for (int o = GS / 2; o > 0; o >>= 1) {
-        E0 += __shfl_xor_sync(0xffffffffu, E0, o, GS);
-        E1 += __shfl_xor_sync(0xffffffffu, E1, o, GS);
-        E2 += __shfl_xor_sync(0xffffffffu, E2, o, GS);
+        E0 += __shfl_xor_sync(gm, E0, o, GS);
+        E1 += __shfl_xor_sync(gm, E1, o, GS);
+        E2 += __shfl_xor_sync(gm, E2, o, GS);
     }
     if (lane == 0) {
         dv.Epair[3 * i] = E0;
@@ -628,11 +629,12 @@ __global__ void __launch_bounds__(256) k_pair_final(Dev dv) {
                 acc[7 + 3 * k + b] += 0.5 * (double) (dedx * x[b]);
         }
     }
+    const unsigned gm = groupMask<GS>();
 #pragma unroll
     for (int o = GS / 2; o > 0; o >>= 1)
 #pragma unroll
         for (int k = 0; k < 16; k++)
-            acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o, GS);
+            acc[k] += __shfl_xor_sync(gm, acc[k], o, GS);
     if (lane == 0) {
         dv.fin[(size_t) i * NFIN + 0] = acc[0];
         for (int k = 0; k < 3; k++) {
@@ -799,9 +801,11 @@ __global__ void __launch_bounds__(CHUNK) k_cg_upd(Dev dv) {
             atomicAdd(&dv.flags[2], 1);
         }
         __threadfence();
-        // the last active system of this iteration to finish decides whether the loop goes on
+        // the last active system of this iteration to finish decides whether the loop goes on (the count of
+        // active systems is read before this system's arrival, so before the last arrival resets it)
+        const int expected = atomicAdd(&dv.flags[5], 0);
         const int active = atomicAdd(&dv.flags[4], 1) + 1;
-        if (active == dv.flags[5]) {
+        if (active == expected) {
             const int ndone = atomicAdd(&dv.flags[2], 0);
             dv.flags[5] = dv.nSys - ndone;   // systems active in the next iteration
             dv.flags[4] = 0;
@@ -987,10 +991,11 @@ __global__ void __launch_bounds__(256) k_pair_grad(Dev dv, double* gq, double* g
         const double U = qi * qj * H0 + (qi * djx - qj * dix) * H1 + didj * H1 - dix * djx * H2;
         aR += U * (-2.0 * Ri * a * a * a);
     }
+    const unsigned gm = groupMask<GS>();
 #pragma unroll
     for (int o = GS / 2; o > 0; o >>= 1) {
-        aq += __shfl_xor_sync(0xffffffffu, aq, o, GS);
-        aR += __shfl_xor_sync(0xffffffffu, aR, o, GS);
+        aq += __shfl_xor_sync(gm, aq, o, GS);
+        aR += __shfl_xor_sync(gm, aR, o, GS);
     }
     if (lane == 0) {
         gq[i] = aq;

@@ -71,6 +71,13 @@ public:
     void setHistory(const void* blob);
     void paramGrad(double* dq, double* dradius, double* dalpha, double* dstrength);
 
+    // measurement: own kernels per evaluation; average durations [ms] of the main kernels relaunched
+    // alone (0 pair list, 1 pair field pass, 2 spread, 3 gather, 4 final pair pass, 5 FFT chain, 6 CG update)
+    int kernelLaunches() const;
+    void kernelTimes(int reps, double* ms);
+    void setPairLanes(int lanes);
+    int pairLanes() const;
+
     // batched systems
     void setSystems(int nsys, const int* atomCount, const double* cutoff, const double* beta, const int* grid,
                     const double* q, const double* radius, const double* alpha, const int* covCount,

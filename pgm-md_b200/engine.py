@@ -278,6 +278,37 @@ class Engine:
         _check(self._L.pgm_engine_param_grad(self._h, _d(dq), _d(dR), _d(da), _d(dc)))
         return dict(q=dq, radius=dR, alpha=da, cov_strength=dc[: self.ncov])
 
+    def kernel_launches(self):
+        return int(self._L.pgm_engine_kernel_launches(self._h))
+
+    KERNELS = ("pair_list", "pair_field", "spread", "gather", "pair_final", "fft_chain", "cg_update")
+
+    def kernel_times(self, reps=20):
+        """Average device durations [ms] of the main kernels relaunched alone (CUDA events on the engine's
+        stream) after an evaluation."""
+        ms = np.zeros(7)
+        _check(self._L.pgm_engine_kernel_times(self._h, int(reps), _d(ms)))
+        return dict(zip(self.KERNELS, ms.tolist()))
+
+    def set_pair_lanes(self, lanes):
+        _check(self._L.pgm_engine_set_pair_lanes(self._h, int(lanes)))
+
+    def pair_lanes(self):
+        return int(self._L.pgm_engine_pair_lanes(self._h))
+
+    def autotune(self, pos, box, reps=10, candidates=(4, 8, 16, 32)):
+        """Picks the lanes per atom of the pair passes by timing each candidate on this system."""
+        best, best_t = None, None
+        for lanes in candidates:
+            self.set_pair_lanes(lanes)
+            self.compute(pos, box, new_step=False)
+            kt = self.kernel_times(reps)
+            t = kt["pair_field"] + kt["pair_final"] / max(1, self.iterations() + 2)
+            if best_t is None or t < best_t:
+                best, best_t = lanes, t
+        self.set_pair_lanes(best)
+        return best
+
     # ---------------------------------------------------------------- batched
     def set_systems(self, systems):
         """Many independent systems (``systems.System`` list) evaluated together by compute_batch."""
