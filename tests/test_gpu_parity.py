@@ -131,12 +131,15 @@ def test_predictor_history_over_steps(precision):
         assert abs(r.energy - e) <= 1e-6 * abs(e)
         its.append(r.iterations)
     assert its[-1] < its[0]   # the extrapolation saves iterations
+    # a repeated evaluation of the same step starts from that step's solution (FP64: already converged; the
+    # mixed path's FP32 matvec cannot hold a residual of 1e-10, so it only starts far ahead)
+    limit = 1 if precision == 0 else its[0] // 2
     again = eng.compute(pos, S.box, new_step=False)
-    assert again.iterations <= 1
+    assert again.iterations <= limit
     blob = eng.get_history()
     eng.reset_history()
     eng.set_history(blob)
-    assert eng.compute(pos, S.box, new_step=False).iterations <= 1
+    assert eng.compute(pos, S.box, new_step=False).iterations <= limit
 
 
 def test_compute_f_and_device_paths():
