@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--ref-steps-cap", type=int, default=0, help="reference arm: cap on timed steps (0: --steps)")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run for ncu: only warmup + steps evaluations of one precision, no other legs")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="with --profile")
     return ap.parse_args()
 
 
@@ -255,6 +258,19 @@ def main():
         return eng
 
     stream = torch.cuda.current_stream(dev)
+    if args.profile:
+        eng = make(pkg.MIXED if args.precision == "mixed" else pkg.FP64)
+        pos_p = torch.from_numpy(S.pos).to(dev).contiguous()
+        f_p = torch.zeros((S.n, 3), dtype=torch.float64, device=dev)
+        for _ in range(args.warmup + args.steps):
+            eng.launch_resident(pos_p.data_ptr(), S.box, True, f_p.data_ptr(), stream.cuda_stream)
+            eng.wait_device(stream.cuda_stream)
+            eng.finish_device()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.precision, "evaluations": args.warmup + args.steps,
+                          "iterations": eng.iterations(), "launches_per_eval": eng.kernel_launches()}))
+        eng.close()
+        return 0
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     pos_d = torch.from_numpy(S.pos).to(dev).contiguous()
     f_d = torch.zeros((S.n, 3), dtype=torch.float64, device=dev)
