@@ -73,7 +73,10 @@ struct Dev {
     int* cellStart;           // totalCells + 1
     // slot order (cell-sorted)
     int* slotAtom;
+    int* slotTmp;             // cell-scatter order before the per-cell sort
     double4* posS;            // wrapped position + q
+    double4* origS;           // original position + radius
+    int4* wrapS;              // wraps N
     double* radS;
     // pair list
     uint32_t* list;           // [slot][cap]
@@ -331,10 +334,12 @@ __device__ __forceinline__ void blockReduce(double* v, unsigned maxMask) {
 }
 
 // Writes this chunk's reduced values and returns true in the last chunk of its system to finish (all
-// threads), with the system's totals (chunks summed in chunk order) in tot.
+// threads), with the system's totals (chunks summed in chunk order, one value per thread) in tot for every
+// thread of that block.
 template <int NV>
 __device__ __forceinline__ bool chunkFinish(const Dev& dv, int chunk, int s, double* v, unsigned maxMask, double* tot) {
     __shared__ int isLast;
+    __shared__ double stot[NV];
     blockReduce<NV>(v, maxMask);
     if (threadIdx.x == 0) {
 #pragma unroll
@@ -348,19 +353,23 @@ __device__ __forceinline__ bool chunkFinish(const Dev& dv, int chunk, int s, dou
     if (!isLast)
         return false;
     __threadfence();
-    if (threadIdx.x == 0) {
-        const SysDev& S = dv.sys[s];
-        for (int k = 0; k < NV; k++) {
-            double acc = ((maxMask >> k) & 1u) ? 0.0 : 0.0;
-            for (int c = 0; c < S.chunkCount; c++) {
-                const double val = __ldcg(&dv.partial[(size_t) (S.chunkFirst + c) * 16 + k]);
-                acc = ((maxMask >> k) & 1u) ? fmax(acc, val) : acc + val;
-            }
-            tot[k] = acc;
+    const SysDev& S = dv.sys[s];
+    if (threadIdx.x < NV) {
+        const int k = threadIdx.x;
+        const bool isMax = (maxMask >> k) & 1u;
+        double acc = 0.0;
+        for (int c = 0; c < S.chunkCount; c++) {
+            const double val = __ldcg(&dv.partial[(size_t) (S.chunkFirst + c) * 16 + k]);
+            acc = isMax ? fmax(acc, val) : acc + val;
         }
-        dv.sysCounter[s] = 0;
+        stot[k] = acc;
     }
     __syncthreads();
+    if (threadIdx.x == 0)
+        dv.sysCounter[s] = 0;
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+        tot[k] = stot[k];
     return true;
 }
 

@@ -152,7 +152,7 @@ struct Engine::Impl {
 
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
-        dSlotAtom, dPosS, dRadS, dList, dListCount, dG12, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
+        dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dRadS, dList, dListCount, dG12, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
         dScal, dPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
@@ -200,7 +200,7 @@ struct Engine::Impl {
         }
         groups.clear();
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
-                      &dCellCount, &dCellStart, &dSlotAtom, &dPosS, &dRadS, &dList, &dListCount, &dG12, &dFlags, &dDS,
+                      &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dRadS, &dList, &dListCount, &dG12, &dFlags, &dDS,
                       &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
@@ -264,8 +264,8 @@ struct Engine::Impl {
 
     // ------------------------------------------------------------------------------------------ topology
     void setAtomsSingle(int nAt, const double* qq, const double* rr, const double* aa, const int* gidx, int nGlobal) {
-        if (nAt <= 0)
-            throw std::invalid_argument("pgm_b200: setAtoms needs at least one atom");
+        if (nAt <= 0 || nAt >= (1 << 23))
+            throw std::invalid_argument("pgm_b200: setAtoms needs 1 .. 8388607 atoms");
         const bool sameCount = atomsSet && nsys == 1 && n == nAt;
         n = nAt;
         nsys = 1;
@@ -313,6 +313,8 @@ struct Engine::Impl {
             atomBegin[k + 1] = atomBegin[k] + count[k];
         }
         n = atomBegin[ns];
+        if (n >= (1 << 23))
+            throw std::invalid_argument("pgm_b200: at most 8388607 atoms in all systems together");
         sysCutoff.assign(cut, cut + ns);
         sysBeta.assign(bet, bet + ns);
         sysK.resize(ns);
@@ -494,7 +496,10 @@ struct Engine::Impl {
         dBase.ensure(3 * n * sizeof(int));
         dFr.ensure(3 * n * 8);
         dSlotAtom.ensure(n * sizeof(int));
+        dSlotTmp.ensure(n * sizeof(int));
         dPosS.ensure(n * sizeof(double4));
+        dOrigS.ensure(n * sizeof(double4));
+        dWrapS.ensure(n * sizeof(int4));
         dRadS.ensure(n * 8);
         dListCount.ensure(n * sizeof(int));
         dFlags.ensure(16 * sizeof(int));
@@ -583,6 +588,8 @@ struct Engine::Impl {
                 const double col = std::sqrt(S.recip[a] * S.recip[a] + S.recip[3 + a] * S.recip[3 + a] +
                                              S.recip[6 + a] * S.recip[6 + a]);
                 const double rho = S.cutoff * col;   // fractional extent of the cutoff along a
+                if (rho > 0.5 * (1.0 + 1e-12))
+                    throw std::invalid_argument("pgm_b200: cut-off beyond half the box");
                 int nc = (int) std::floor(2.0 / rho);
                 nc = std::max(1, std::min(nc, 1024));
                 S.cellN[a] = nc;
@@ -665,7 +672,10 @@ struct Engine::Impl {
         d.cellCount = dCellCount.as<int>();
         d.cellStart = dCellStart.as<int>();
         d.slotAtom = dSlotAtom.as<int>();
+        d.slotTmp = dSlotTmp.as<int>();
         d.posS = dPosS.as<double4>();
+        d.origS = dOrigS.as<double4>();
+        d.wrapS = dWrapS.as<int4>();
         d.radS = dRadS.as<double>();
         d.list = dList.as<uint32_t>();
         d.listCount = dListCount.as<int>();
@@ -748,6 +758,30 @@ struct Engine::Impl {
         }
     }
 
+    template <typename R> void launchSpread(cudaStream_t sm, const Dev& d, int mode, double* vec) {
+        const int wb = (n + 7) / 8;
+        switch (s.order) {
+        case 4: k_spread<R, 4><<<wb, 256, 0, sm>>>(d, mode, vec); break;
+        case 5: k_spread<R, 5><<<wb, 256, 0, sm>>>(d, mode, vec); break;
+        case 6: k_spread<R, 6><<<wb, 256, 0, sm>>>(d, mode, vec); break;
+        case 8: k_spread<R, 8><<<wb, 256, 0, sm>>>(d, mode, vec); break;
+        default: k_spread<R, 0><<<wb, 256, 0, sm>>>(d, mode, vec);
+        }
+        CU(cudaGetLastError());
+    }
+
+    template <typename R, bool FINAL> void launchGather(cudaStream_t sm, const Dev& d, int gate) {
+        const int wb = (n + 7) / 8;
+        switch (s.order) {
+        case 4: k_gather<R, FINAL, 4><<<wb, 256, 0, sm>>>(d, gate); break;
+        case 5: k_gather<R, FINAL, 5><<<wb, 256, 0, sm>>>(d, gate); break;
+        case 6: k_gather<R, FINAL, 6><<<wb, 256, 0, sm>>>(d, gate); break;
+        case 8: k_gather<R, FINAL, 8><<<wb, 256, 0, sm>>>(d, gate); break;
+        default: k_gather<R, FINAL, 0><<<wb, 256, 0, sm>>>(d, gate);
+        }
+        CU(cudaGetLastError());
+    }
+
     template <typename R, bool WITHQ> void pairField(cudaStream_t sm, const Dev& d, int gate) {
         const long long threads = (long long) n * pairGS;
         const int blocks = (int) ((threads + 255) / 256);
@@ -764,17 +798,14 @@ struct Engine::Impl {
     // FFT chain on the side stream; joined on sm.
     template <typename R, bool WITHQ>
     void fieldPass(cudaStream_t sm, cudaStream_t sd, const Dev& d, int spreadMode, double* vec, bool gate) {
-        const int wblocks = (n + 7) / 8;
-        k_spread<R><<<wblocks, 256, 0, sm>>>(d, spreadMode, vec);
-        CU(cudaGetLastError());
+        launchSpread<R>(sm, d, spreadMode, vec);
         CU(cudaEventRecord(evFork, sm));
         CU(cudaStreamWaitEvent(sd, evFork, 0));
         fftChain<R>(sd, d, false, gate);
         pairField<R, WITHQ>(sm, d, gate ? 1 : 0);
         CU(cudaEventRecord(evJoin, sd));
         CU(cudaStreamWaitEvent(sm, evJoin, 0));
-        k_gather<R, false><<<wblocks, 256, 0, sm>>>(d, gate ? 1 : 0);
-        CU(cudaGetLastError());
+        launchGather<R, false>(sm, d, gate ? 1 : 0);
     }
 
     template <typename R> void enqueuePre(cudaStream_t sm, cudaStream_t sd, const Dev& d) {
@@ -784,8 +815,9 @@ struct Engine::Impl {
         k_prep<<<tb, 256, 0, sm>>>(d, dPosIn.as<double>());
         k_cell_scan<<<1, 1024, 0, sm>>>(d);
         k_cell_scatter<<<tb, 256, 0, sm>>>(d);
-        k_cell_sort<<<(totalCells + 127) / 128, 128, 0, sm>>>(d);
-        k_build_list<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
+        k_cell_sort<<<(totalCells + 7) / 8, 256, 0, sm>>>(d);
+        k_build_list<<<totalCells, LIST_THREADS, 0, sm>>>(d);
+        k_pair_kernels<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
         k_perm<<<tb, 256, 0, sm>>>(d);
         k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
         CU(cudaGetLastError());
@@ -814,7 +846,7 @@ struct Engine::Impl {
         const int tb = (n + 255) / 256, wblocks = (n + 7) / 8;
         CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
         k_final_prep<<<tb, 256, 0, sm>>>(d, s.polarizable ? 1 : 0);
-        k_spread<R><<<wblocks, 256, 0, sm>>>(d, 0, d.dtot);
+        launchSpread<R>(sm, d, 0, d.dtot);
         CU(cudaEventRecord(evFork, sm));
         CU(cudaStreamWaitEvent(sd, evFork, 0));
         fftChain<R>(sd, d, true, false);
@@ -830,7 +862,7 @@ struct Engine::Impl {
         }
         CU(cudaEventRecord(evJoin, sd));
         CU(cudaStreamWaitEvent(sm, evJoin, 0));
-        k_gather<R, true><<<wblocks, 256, 0, sm>>>(d, 0);
+        launchGather<R, true>(sm, d, 0);
         k_final_field<<<tb, 256, 0, sm>>>(d);
         k_final_forces<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d, s.polarizable ? 1 : 0);
         CU(cudaGetLastError());
@@ -1250,14 +1282,16 @@ void Engine::field(const double* pos, const double box[3][3], const double* qf, 
         k_prep<<<tb, 256, 0, I.st>>>(dv, I.dPosIn.as<double>());
         k_cell_scan<<<1, 1024, 0, I.st>>>(dv);
         k_cell_scatter<<<tb, 256, 0, I.st>>>(dv);
-        k_cell_sort<<<(I.totalCells + 127) / 128, 128, 0, I.st>>>(dv);
+        k_cell_sort<<<(I.totalCells + 7) / 8, 256, 0, I.st>>>(dv);
         if (I.mixed()) {
-            k_build_list<float><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
+            k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(dv);
+            k_pair_kernels<float><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
             k_influence<float><<<dim3(I.convBlocks, I.nsys), 256, 0, I.st>>>(dv);
             CU(cudaMemsetAsync(dv.grid, 0, I.gridTotal * I.realSize(), I.st));
             I.fieldPass<float, true>(I.st, I.side, dv, 0, dv.dtot, false);
         } else {
-            k_build_list<double><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
+            k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(dv);
+            k_pair_kernels<double><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
             k_influence<double><<<dim3(I.convBlocks, I.nsys), 256, 0, I.st>>>(dv);
             CU(cudaMemsetAsync(dv.grid, 0, I.gridTotal * I.realSize(), I.st));
             I.fieldPass<double, true>(I.st, I.side, dv, 0, dv.dtot, false);
@@ -1342,12 +1376,12 @@ int Engine::kernelLaunches() const {
     const Impl& I = *impl;
     if (!I.haveResult)
         return 0;
-    // own kernels per evaluation: preparation 8, the two field passes before the loop 3 + 1 + 3 + 1,
+    // own kernels per evaluation: preparation 9, the two field passes before the loop 3 + 1 + 3 + 1,
     // 4 per CG iteration, final 7 (the cuFFT transforms are not counted)
     int it = 0;
     for (int k = 0; k < I.nsys; k++)
         it = std::max(it, (int) I.lastResults[(size_t) k * NRES + 14]);
-    return 8 + (I.s.polarizable ? 8 + 4 * it : 0) + 7;
+    return 9 + (I.s.polarizable ? 8 + 4 * it : 0) + 7;
 }
 
 void Engine::kernelTimes(int reps, double* ms) {
@@ -1373,10 +1407,13 @@ void Engine::kernelTimes(int reps, double* ms) {
     };
     auto run = [&](auto tag) {
         typedef decltype(tag) R;
-        ms[0] = timeIt([&] { k_build_list<R><<<(I.n + 7) / 8, 256, 0, I.st>>>(d); });
+        ms[0] = timeIt([&] {
+            k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(d);
+            k_pair_kernels<R><<<(I.n + 7) / 8, 256, 0, I.st>>>(d);
+        });
         ms[1] = timeIt([&] { I.pairField<R, false>(I.st, d, 0); });
-        ms[2] = timeIt([&] { k_spread<R><<<wb, 256, 0, I.st>>>(d, 1, d.x); });
-        ms[3] = timeIt([&] { k_gather<R, false><<<wb, 256, 0, I.st>>>(d, 0); });
+        ms[2] = timeIt([&] { I.launchSpread<R>(I.st, d, 1, d.x); });
+        ms[3] = timeIt([&] { I.launchGather<R, false>(I.st, d, 0); });
         ms[4] = timeIt([&] {
             const int blocks = (int) (((long long) I.n * I.pairGS + 255) / 256);
             switch (I.pairGS) {

@@ -118,134 +118,254 @@ __global__ void k_cell_scatter(Dev dv) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= dv.nAtoms)
         return;
-    dv.slotAtom[dv.cellStart[dv.cellOf[i]] + dv.cellRank[i]] = i;
+    dv.slotTmp[dv.cellStart[dv.cellOf[i]] + dv.cellRank[i]] = i;
 }
 
-// Sorts each cell's atoms by atom index (deterministic slot order), then fills the slot-order copies.
+// One warp per cell: each atom's place is its rank by atom index among the cell's atoms (deterministic slot
+// order whatever order the atomics gave); fills the slot-order copies.
 __global__ void k_cell_sort(Dev dv) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (c >= dv.totalCells)
         return;
-    const int b = dv.cellStart[c], e = dv.cellStart[c + 1];
-    for (int k = b + 1; k < e; k++) {
-        const int v = dv.slotAtom[k];
-        int m = k - 1;
-        while (m >= b && dv.slotAtom[m] > v) {
-            dv.slotAtom[m + 1] = dv.slotAtom[m];
-            m--;
+    const int b = dv.cellStart[c], e = dv.cellStart[c + 1], m = e - b;
+    for (int base = 0; base < m; base += 32) {
+        const int k = base + lane;
+        if (k < m) {
+            const int v = dv.slotTmp[b + k];
+            int rank = 0;
+            for (int o = 0; o < m; o++)
+                rank += dv.slotTmp[b + o] < v;
+            const int sl = b + rank;
+            dv.slotAtom[sl] = v;
+            dv.posS[sl] = make_double4(dv.Etot[3 * v], dv.Etot[3 * v + 1], dv.Etot[3 * v + 2], dv.q[v]);
+            dv.origS[sl] = make_double4(dv.posIn[3 * v], dv.posIn[3 * v + 1], dv.posIn[3 * v + 2], dv.radius[v]);
+            dv.wrapS[sl] = make_int4(dv.wrapN[3 * v], dv.wrapN[3 * v + 1], dv.wrapN[3 * v + 2], 0);
+            dv.radS[sl] = dv.radius[v];
         }
-        dv.slotAtom[m + 1] = v;
-    }
-    for (int k = b; k < e; k++) {
-        const int i = dv.slotAtom[k];
-        dv.posS[k] = make_double4(dv.Etot[3 * i], dv.Etot[3 * i + 1], dv.Etot[3 * i + 2], dv.q[i]);
-        dv.radS[k] = dv.radius[i];
     }
 }
 
 // ------------------------------------------------------------------------------------------------ pair list
 
-// One warp per slot: scans the neighbour cells (offsets -m..m per dimension, runs along the last dimension
-// merged into contiguous slot ranges), prefilters on the wrapped positions, then applies the reference's
-// exact test (minimum image of the original positions, r^2 < rc^2, core/pgm_core.cpp:64-87) and keeps a
-// candidate only at the image that test chose, so every pair enters once.  Accepted pairs are compacted with
-// a ballot (deterministic order) and get G1, G2 in precision R.
-template <typename R>
-__global__ void __launch_bounds__(256) k_build_list(Dev dv) {
-    typedef typename V2T<R>::T R2;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= dv.nAtoms)
+// Minimum image of v as minImageExact, with the divisions replaced by products with the inverse box diagonal
+// unless the quotient lies within 1e-9 of a half-integer (then the exact division decides): the same image
+// counts, hence the same vector, bit for bit.
+__device__ __forceinline__ void minImageFast(double* v, const double* H, const double* invDiag, int* k) {
+#pragma unroll
+    for (int c = 2; c >= 0; c--) {
+        const double qd = v[c] * invDiag[c];
+        const double fr = fabs(qd - trunc(qd));
+        const double kk = (fabs(fr - 0.5) < 1e-9) ? round(__ddiv_rn(v[c], H[4 * c])) : round(qd);
+        k[c] = (int) kk;
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            v[j] = __dsub_rn(v[j], __dmul_rn(kk, H[3 * c + j]));
+    }
+}
+
+constexpr int LIST_THREADS = 256;
+constexpr int LIST_CHUNK = 512;   // candidates staged in shared memory at a time
+constexpr int MAX_RUNS = 343;     // (2m+1)^3 with m <= 3
+
+// System of a global cell index (binary search over the systems' first cells).
+__device__ __forceinline__ int systemOfCell(const Dev& dv, int c) {
+    int lo = 0, hi = dv.nSys - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (dv.sys[mid].cellOff <= c)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// One block per cell.  The neighbour cells (offsets -m..m per dimension) become at most (2m+1)^3 runs of
+// consecutive slots with one image shift each (cells along the last dimension merged); their atoms are
+// staged through shared memory in chunks (wrapped position, original position and radius, wraps) and every
+// warp tests them against the cell's atoms it owns: a prefilter on the wrapped positions, then the
+// reference's exact test (minimum image of the original positions, r^2 < rc^2, core/pgm_core.cpp:64-87),
+// keeping a candidate only at the image that test chose, so every pair enters once.  Accepted pairs are
+// appended in candidate order (deterministic); k_pair_kernels then gives them G1, G2.
+__global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
+    __shared__ int runSlot[MAX_RUNS], runOff[MAX_RUNS + 1], runShift[MAX_RUNS];
+    __shared__ double4 cPos[LIST_CHUNK], cOrig[LIST_CHUNK];
+    __shared__ int4 cWrap[LIST_CHUNK];
+    const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    constexpr int NW = LIST_THREADS / 32;
+    if (c >= dv.totalCells)
         return;
-    const int slot = warp;
-    const int i = dv.slotAtom[slot];
-    const int s = dv.atomSys[i];
+    const int cb = dv.cellStart[c], ce = dv.cellStart[c + 1];
+    if (cb == ce)
+        return;
+    const int s = systemOfCell(dv, c);
     const SysDev& S = dv.sys[s];
-    const double4 pwi = dv.posS[slot];
-    const double pi0 = dv.posIn[3 * i], pi1 = dv.posIn[3 * i + 1], pi2 = dv.posIn[3 * i + 2];
-    const int Ni0 = dv.wrapN[3 * i], Ni1 = dv.wrapN[3 * i + 1], Ni2 = dv.wrapN[3 * i + 2];
-    const double Ri = dv.radius[i];
-    const int lc = dv.cellOf[i] - S.cellOff;
+    const int lc = c - S.cellOff;
     const int n0 = S.cellN[0], n1 = S.cellN[1], n2 = S.cellN[2];
     const int c2 = lc % n2, c1 = (lc / n2) % n1, c0 = lc / (n2 * n1);
-    const double pre = S.rc2 * (1.0 + 1e-10) + 1e-300;
-    uint32_t* row = dv.list + (size_t) slot * dv.cap;
-    R2* grow = (R2*) dv.G12 + (size_t) slot * dv.cap;
-    int count = 0;
-    bool badShift = false;
-    for (int d0 = -S.cellM[0]; d0 <= S.cellM[0]; d0++) {
-        const int u0 = c0 + d0;
+    const int m0 = S.cellM[0], m1 = S.cellM[1], m2 = S.cellM[2];
+    const int rows = (2 * m0 + 1) * (2 * m1 + 1), per = 2 * m2 + 1;
+    for (int row = tid; row < rows; row += LIST_THREADS) {
+        const int d0 = row / (2 * m1 + 1) - m0, d1 = row % (2 * m1 + 1) - m1;
+        const int u0 = c0 + d0, u1 = c1 + d1;
         const int w0 = (int) floor((double) u0 / n0), v0 = u0 - w0 * n0;
-        for (int d1 = -S.cellM[1]; d1 <= S.cellM[1]; d1++) {
-            const int u1 = c1 + d1;
-            const int w1 = (int) floor((double) u1 / n1), v1 = u1 - w1 * n1;
-            int d2 = -S.cellM[2];
-            while (d2 <= S.cellM[2]) {
-                // a run of consecutive cells with the same image shift along the last dimension
-                const int u2 = c2 + d2;
-                const int w2 = (int) floor((double) u2 / n2), v2 = u2 - w2 * n2;
-                int len = 1;
-                while (d2 + len <= S.cellM[2] && v2 + len < n2)
-                    len++;
-                const int cb = S.cellOff + (v0 * n1 + v1) * n2 + v2;
-                const int sb = dv.cellStart[cb], se = dv.cellStart[cb + len];
-                d2 += len;
-                const double sh0 = w0 * S.H[0] + w1 * S.H[3] + w2 * S.H[6];
-                const double sh1 = w1 * S.H[4] + w2 * S.H[7];
-                const double sh2 = w2 * S.H[8];
-                for (int base = sb; base < se; base += 32) {
-                    const int js = base + lane;
-                    bool acc = false;
-                    double x[3];
-                    int j = -1;
-                    if (js < se) {
-                        const double4 pwj = dv.posS[js];
-                        const double y0 = pwi.x - pwj.x - sh0, y1 = pwi.y - pwj.y - sh1, y2 = pwi.z - pwj.z - sh2;
-                        j = dv.slotAtom[js];
-                        if (j != i && y0 * y0 + y1 * y1 + y2 * y2 < pre) {
-                            x[0] = __dsub_rn(pi0, dv.posIn[3 * j]);
-                            x[1] = __dsub_rn(pi1, dv.posIn[3 * j + 1]);
-                            x[2] = __dsub_rn(pi2, dv.posIn[3 * j + 2]);
-                            int k[3];
-                            minImageExact(x, S.H, k);
-                            if (dot3exact(x) < S.rc2) {
-                                // image of the exact test relative to the wrapped positions
-                                const int k0 = k[0] - (Ni0 - dv.wrapN[3 * j]);
-                                const int k1 = k[1] - (Ni1 - dv.wrapN[3 * j + 1]);
-                                const int k2 = k[2] - (Ni2 - dv.wrapN[3 * j + 2]);
-                                acc = (k0 == w0 && k1 == w1 && k2 == w2);
-                            }
-                        }
-                    }
-                    const unsigned m = __ballot_sync(0xffffffffu, acc);
-                    if (acc) {
-                        const int pos = count + __popc(m & ((1u << lane) - 1u));
-                        if (w0 < -4 || w0 > 3 || w1 < -4 || w1 > 3 || w2 < -4 || w2 > 3)
-                            badShift = true;
-                        if (pos < dv.cap) {
-                            row[pos] = packEntry(js, w0, w1, w2);
-                            const R rr = fsqrt((R) (x[0] * x[0] + x[1] * x[1] + x[2] * x[2]));
-                            const double Rj = dv.radius[j];
-                            const R a = (R) (1.0 / sqrt(2.0 * (Ri * Ri + Rj * Rj)));
-                            R G[3];
-                            pairKernels<R, 3>(a, (R) S.beta, rr, G);
-                            R2 g;
-                            g.x = G[1];
-                            g.y = G[2];
-                            grow[pos] = g;
-                        }
-                    }
-                    count += __popc(m);
-                }
-            }
+        const int w1 = (int) floor((double) u1 / n1), v1 = u1 - w1 * n1;
+        int r = 0, d2 = -m2;
+        while (d2 <= m2) {
+            const int u2 = c2 + d2;
+            const int w2 = (int) floor((double) u2 / n2), v2 = u2 - w2 * n2;
+            int len = 1;
+            while (d2 + len <= m2 && v2 + len < n2)
+                len++;
+            const int cc = S.cellOff + (v0 * n1 + v1) * n2 + v2;
+            runSlot[row * per + r] = dv.cellStart[cc];
+            runOff[row * per + r] = dv.cellStart[cc + len] - dv.cellStart[cc];   // length, scanned below
+            runShift[row * per + r] = (w0 + 4) | ((w1 + 4) << 3) | ((w2 + 4) << 6);
+            r++;
+            d2 += len;
+        }
+        for (; r < per; r++) {
+            runSlot[row * per + r] = 0;
+            runOff[row * per + r] = 0;
+            runShift[row * per + r] = 4 | (4 << 3) | (4 << 6);
         }
     }
-    if (lane == 0) {
-        dv.listCount[slot] = min(count, dv.cap);
-        if (count > dv.cap)
-            atomicMax(&dv.flags[0], count);
+    const int nr = rows * per;
+    __syncthreads();
+    if (wid == 0) {   // exclusive scan of the run lengths
+        int carry = 0;
+        for (int base = 0; base < nr; base += 32) {
+            const int k = base + lane;
+            const int len = (k < nr) ? runOff[k] : 0;
+            int v = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o)
+                    v += y;
+            }
+            if (k < nr)
+                runOff[k] = carry + v - len;
+            carry += __shfl_sync(0xffffffffu, v, 31);
+        }
+        if (lane == 0)
+            runOff[nr] = carry;
     }
-    if (badShift)
-        atomicExch(&dv.flags[1], 1);
+    for (int ii = cb + tid; ii < ce; ii += LIST_THREADS)
+        dv.listCount[ii] = 0;
+    __syncthreads();
+    const int total = runOff[nr];
+    const double pre = S.rc2 * (1.0 + 1e-10) + 1e-300;
+    const double invDiag[3] = {1.0 / S.H[0], 1.0 / S.H[4], 1.0 / S.H[8]};
+    for (int base = 0; base < total; base += LIST_CHUNK) {
+        const int nc = min(LIST_CHUNK, total - base);
+        for (int t = tid; t < nc; t += LIST_THREADS) {
+            const int k = base + t;
+            int lo = 0, hi = nr - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (runOff[mid] <= k)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            const int js = runSlot[lo] + (k - runOff[lo]);
+            cPos[t] = dv.posS[js];
+            cOrig[t] = dv.origS[js];
+            const int4 w = dv.wrapS[js];
+            cWrap[t] = make_int4(w.x, w.y, w.z, js | (runShift[lo] << 23));
+        }
+        __syncthreads();
+        for (int ii = cb + wid; ii < ce; ii += NW) {
+            const double4 pwi = dv.posS[ii];
+            const double4 oi = dv.origS[ii];
+            const int4 wi = dv.wrapS[ii];
+            uint32_t* row = dv.list + (size_t) ii * dv.cap;
+            int count = dv.listCount[ii];
+            for (int t0 = 0; t0 < nc; t0 += 32) {
+                const int t = t0 + lane;
+                bool acc = false;
+                double x[3];
+                uint32_t entry = 0;
+                if (t < nc) {
+                    const int4 cw = cWrap[t];
+                    entry = (uint32_t) cw.w;
+                    const int js = (int) (entry & 0x7FFFFFu);
+                    const int w0 = (int) ((entry >> 23) & 7u) - 4, w1 = (int) ((entry >> 26) & 7u) - 4,
+                              w2 = (int) ((entry >> 29) & 7u) - 4;
+                    const double sh0 = w0 * S.H[0] + w1 * S.H[3] + w2 * S.H[6];
+                    const double sh1 = w1 * S.H[4] + w2 * S.H[7];
+                    const double sh2 = w2 * S.H[8];
+                    const double4 pwj = cPos[t];
+                    const double y0 = pwi.x - pwj.x - sh0, y1 = pwi.y - pwj.y - sh1, y2 = pwi.z - pwj.z - sh2;
+                    if (js != ii && y0 * y0 + y1 * y1 + y2 * y2 < pre) {
+                        const double4 oj = cOrig[t];
+                        x[0] = __dsub_rn(oi.x, oj.x);
+                        x[1] = __dsub_rn(oi.y, oj.y);
+                        x[2] = __dsub_rn(oi.z, oj.z);
+                        int kk[3];
+                        minImageFast(x, S.H, invDiag, kk);
+                        if (dot3exact(x) < S.rc2) {
+                            // image of the exact test relative to the wrapped positions
+                            acc = (kk[0] - (wi.x - cw.x) == w0 && kk[1] - (wi.y - cw.y) == w1 &&
+                                   kk[2] - (wi.z - cw.z) == w2);
+                        }
+                    }
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, acc);
+                if (acc) {
+                    const int pos = count + __popc(m & ((1u << lane) - 1u));
+                    if (pos < dv.cap)
+                        row[pos] = entry;
+                }
+                count += __popc(m);
+            }
+            if (lane == 0)
+                dv.listCount[ii] = count;
+        }
+        __syncthreads();
+    }
+    for (int ii = cb + tid; ii < ce; ii += LIST_THREADS) {
+        const int cnt = dv.listCount[ii];
+        if (cnt > dv.cap) {
+            atomicMax(&dv.flags[0], cnt);
+            dv.listCount[ii] = dv.cap;
+        }
+    }
+}
+
+// G1, G2 of every listed pair in precision R (core/pgm_math.h:77-93 via pairKernels), one warp per slot, the
+// pairs of its row over the lanes: separate from the list build so that every lane of a warp evaluates one.
+template <typename R>
+__global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
+    typedef typename V2T<R>::T R2;
+    const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (slot >= dv.nAtoms)
+        return;
+    const SysDev& S = dv.sys[dv.atomSys[dv.slotAtom[slot]]];
+    const double4 pwi = dv.posS[slot];
+    const double Ri = dv.radS[slot];
+    const uint32_t* row = dv.list + (size_t) slot * dv.cap;
+    R2* grow = (R2*) dv.G12 + (size_t) slot * dv.cap;
+    const int cnt = dv.listCount[slot];
+    const R beta = (R) S.beta;
+    for (int t = lane; t < cnt; t += 32) {
+        const uint32_t e = row[t];
+        const int js = entrySlot(e);
+        double sh[3];
+        entryShift(e, S.H, sh);
+        const double4 pwj = dv.posS[js];
+        const double x0 = pwi.x - pwj.x - sh[0], x1 = pwi.y - pwj.y - sh[1], x2 = pwi.z - pwj.z - sh[2];
+        const double Rj = dv.radS[js];
+        const R r = (R) sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+        const R a = (R) (1.0 / sqrt(2.0 * (Ri * Ri + Rj * Rj)));
+        R G[3];
+        pairKernels<R, 3>(a, beta, r, G);
+        R2 g;
+        g.x = G[1];
+        g.y = G[2];
+        grow[t] = g;
+    }
 }
 
 // ------------------------------------------------------------------------------------------------ dipoles
@@ -302,12 +422,14 @@ __global__ void k_influence(Dev dv) {
 
 // Spread of charges and dipoles onto the grid: Q[g] += q t1 t2 t3 + e1 u1 t2 t3 + e2 t1 u2 t3 + e3 t1 t2 u3,
 // e_a = K_a d . recip[:, a] (core/pgm_core.cpp:187-207).  One warp per slot, p^3 points over the lanes.
+// P: the spline order as a compile-time constant (0: the runtime order).
 // mode 0: q and vec; 1: vec only; 2: CG direction update p = z + beta p first (vec = p), no charges.
 // Also writes the slot-order copy dS = (d, q) in precision R for the pair passes.
-template <typename R>
+template <typename R, int P>
 __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
     typedef typename V4T<R>::T R4;
-    __shared__ R sth[8][3][MAXP], sdth[8][3][MAXP];
+    constexpr int PM = P > 0 ? P : MAXP;
+    __shared__ R sth[8][3][PM], sdth[8][3][PM];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int slot = blockIdx.x * 8 + wib;
     if (slot >= dv.nAtoms)
@@ -317,8 +439,9 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
     if (mode == 2 && dv.scal[s * NSCAL + SC_DONE] != 0.0)
         return;
     const SysDev& S = dv.sys[s];
-    const int p = dv.order;
+    const int p = P > 0 ? P : dv.order;
     double dl = 0.0;
+    int bl = 0;
     if (lane < 3) {
         if (mode == 2) {
             dl = dv.z[3 * i + lane] + dv.scal[s * NSCAL + SC_BETA] * vec[3 * i + lane];
@@ -326,9 +449,20 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
         } else {
             dl = vec[3 * i + lane];
         }
+        R t[MAXP], u[MAXP], v[MAXP];
+        bspline<R>((R) dv.pmeFr[3 * i + lane], p, t, u, v);
+#pragma unroll
+        for (int j = 0; j < PM; j++)
+            if (j < p) {
+                sth[wib][lane][j] = t[j];
+                sdth[wib][lane][j] = u[j];
+            }
+        bl = dv.pmeBase[3 * i + lane];
     }
     const double d0 = __shfl_sync(0xffffffffu, dl, 0), d1 = __shfl_sync(0xffffffffu, dl, 1),
                  d2 = __shfl_sync(0xffffffffu, dl, 2);
+    const int b0 = __shfl_sync(0xffffffffu, bl, 0), b1 = __shfl_sync(0xffffffffu, bl, 1),
+              b2 = __shfl_sync(0xffffffffu, bl, 2);
     const double qv = (mode == 0) ? dv.q[i] : 0.0;
     if (lane == 0) {
         R4 o;
@@ -338,20 +472,6 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
         o.w = (R) qv;
         ((R4*) dv.dS)[slot] = o;
     }
-    int bl = 0;
-    if (lane < 3) {
-        R t[MAXP], u[MAXP], v[MAXP];
-        bspline<R>((R) dv.pmeFr[3 * i + lane], p, t, u, v);
-#pragma unroll
-        for (int j = 0; j < MAXP; j++)
-            if (j < p) {
-                sth[wib][lane][j] = t[j];
-                sdth[wib][lane][j] = u[j];
-            }
-        bl = dv.pmeBase[3 * i + lane];
-    }
-    const int b0 = __shfl_sync(0xffffffffu, bl, 0), b1 = __shfl_sync(0xffffffffu, bl, 1),
-              b2 = __shfl_sync(0xffffffffu, bl, 2);
     __syncwarp();
     const R e0 = (R) (S.K[0] * (d0 * S.recip[0] + d1 * S.recip[3] + d2 * S.recip[6]));
     const R e1 = (R) (S.K[1] * (d0 * S.recip[1] + d1 * S.recip[4] + d2 * S.recip[7]));
@@ -360,14 +480,18 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
     R* grid = (R*) dv.grid + S.gridOff;
     const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
     const int pp = p * p, p3 = pp * p;
-    for (int t = lane; t < p3; t += 32) {
-        const int j1 = t / pp, j2 = (t / p) % p, j3 = t % p;
-        const R t1 = sth[wib][0][j1], u1 = sdth[wib][0][j1];
-        const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
-        const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
-        const R w = qr * t1 * t2 * t3 + e0 * u1 * t2 * t3 + e1 * t1 * u2 * t3 + e2 * t1 * t2 * u3;
-        const int g1 = wrapIndex(b0 - j1, K0), g2 = wrapIndex(b1 - j2, K1), g3 = wrapIndex(b2 - j3, K2);
-        atomicAdd(&grid[((size_t) g1 * K1 + g2) * K2 + g3], w);
+    constexpr int NIT = P > 0 ? (P * P * P + 31) / 32 : 1;
+#pragma unroll
+    for (int it = 0; it < NIT; it++) {
+        for (int t = lane + 32 * it; t < p3; t += (P > 0 ? p3 : 32)) {
+            const int j1 = t / pp, j2 = (t / p) % p, j3 = t % p;
+            const R t1 = sth[wib][0][j1], u1 = sdth[wib][0][j1];
+            const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
+            const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+            const R w = t3 * (t2 * (qr * t1 + e0 * u1) + e1 * t1 * u2) + e2 * t1 * t2 * u3;
+            const int g1 = wrapIndex(b0 - j1, K0), g2 = wrapIndex(b1 - j2, K1), g3 = wrapIndex(b2 - j3, K2);
+            atomicAdd(&grid[((size_t) g1 * K1 + g2) * K2 + g3], w);
+        }
     }
 }
 
@@ -426,9 +550,10 @@ __global__ void __launch_bounds__(256) k_conv(Dev dv, int gateDone) {
 // Interpolation from the potential grid: f_a = sum (d theta_a) theta theta phi (the field, E_rec = -sum_a K_a
 // recip[:, a] f_a, core/pgm_core.cpp:241-264); FINAL also the second derivatives, the potential and the
 // reciprocal forces -K_a recip[k][a] (q f1_a + sum_b e_b f2_ab) (core/pgm_core.cpp:452-487) and E_rec (x) d.
-template <typename R, bool FINAL>
+template <typename R, bool FINAL, int P>
 __global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
-    __shared__ R sth[8][3][MAXP], sdth[8][3][MAXP], sd2[8][3][MAXP];
+    constexpr int PM = P > 0 ? P : MAXP;
+    __shared__ R sth[8][3][PM], sdth[8][3][PM], sd2[8][3][FINAL ? PM : 1];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int slot = blockIdx.x * 8 + wib;
     if (slot >= dv.nAtoms)
@@ -438,18 +563,18 @@ __global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
     if (gateDone && dv.scal[s * NSCAL + SC_DONE] != 0.0)
         return;
     const SysDev& S = dv.sys[s];
-    const int p = dv.order;
+    const int p = P > 0 ? P : dv.order;
     int bl = 0;
     if (lane < 3) {
         R t[MAXP], u[MAXP], v[MAXP];
         bspline<R>((R) dv.pmeFr[3 * i + lane], p, t, u, v);
 #pragma unroll
-        for (int j = 0; j < MAXP; j++)
+        for (int j = 0; j < PM; j++)
             if (j < p) {
                 sth[wib][lane][j] = t[j];
                 sdth[wib][lane][j] = u[j];
                 if (FINAL)
-                    sd2[wib][lane][j] = v[j];
+                    sd2[wib][lane][FINAL ? j : 0] = v[j];
             }
         bl = dv.pmeBase[3 * i + lane];
     }
@@ -460,7 +585,10 @@ __global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
     const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
     const int pp = p * p, p3 = pp * p;
     R f[3] = {0, 0, 0}, f2[6] = {0, 0, 0, 0, 0, 0}, pot = 0;
-    for (int t = lane; t < p3; t += 32) {
+    constexpr int NIT = P > 0 ? (P * P * P + 31) / 32 : 1;
+#pragma unroll
+    for (int it = 0; it < NIT; it++)
+    for (int t = lane + 32 * it; t < p3; t += (P > 0 ? p3 : 32)) {
         const int j1 = t / pp, j2 = (t / p) % p, j3 = t % p;
         const R t1 = sth[wib][0][j1], u1 = sdth[wib][0][j1];
         const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
@@ -471,7 +599,7 @@ __global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
         f[1] += t1 * u2 * t3 * ph;
         f[2] += t1 * t2 * u3 * ph;
         if (FINAL) {
-            const R v1 = sd2[wib][0][j1], v2 = sd2[wib][1][j2], v3 = sd2[wib][2][j3];
+            const R v1 = sd2[wib][0][FINAL ? j1 : 0], v2 = sd2[wib][1][FINAL ? j2 : 0], v3 = sd2[wib][2][FINAL ? j3 : 0];
             f2[0] += v1 * t2 * t3 * ph;
             f2[1] += t1 * v2 * t3 * ph;
             f2[2] += t1 * t2 * v3 * ph;
@@ -924,13 +1052,18 @@ __global__ void __launch_bounds__(CHUNK) k_final_forces(Dev dv, int iterationsSo
         v[12] = dv.q[i];
     }
     double tot[14];
-    if (chunkFinish<14>(dv, chunk, s, v, 0u, tot) && threadIdx.x == 0) {
-        double conv[NCONV];
-        for (int k = 0; k < NCONV; k++)
-            conv[k] = 0.0;
+    __shared__ double sconv[NCONV];
+    if (!chunkFinish<14>(dv, chunk, s, v, 0u, tot))
+        return;
+    if (threadIdx.x < NCONV) {
+        double acc = 0.0;
         for (int bk = 0; bk < S.convBlocks; bk++)
-            for (int k = 0; k < NCONV; k++)
-                conv[k] += dv.convPartial[(size_t) (dv.convPartialOff[s] + bk) * NCONV + k];
+            acc += __ldcg(&dv.convPartial[(size_t) (dv.convPartialOff[s] + bk) * NCONV + threadIdx.x]);
+        sconv[threadIdx.x] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double* conv = sconv;
         const double Q = tot[12];
         const double bg = -PI_D * Q * Q / (2.0 * S.volume * S.beta * S.beta);
         double* res = dv.results + (size_t) s * NRES;
