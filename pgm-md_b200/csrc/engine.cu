@@ -426,6 +426,9 @@ struct Engine::Impl {
             FftGroup g;
             for (int a = 0; a < 3; a++)
                 g.K[a] = kv.first[a];
+            // every group's grid and spectrum start 256-byte aligned (cuFFT's vector loads need aligned bases)
+            gridTotal = (gridTotal + 63) / 64 * 64;
+            specTotal = (specTotal + 31) / 32 * 32;
             g.gridOff = gridTotal;
             g.specOff = specTotal;
             g.count = (int) kv.second.size();
@@ -461,6 +464,10 @@ struct Engine::Impl {
             CUFFT(cufftPlanMany(&g.c2r, 3, dims, nullptr, 1, sn, nullptr, 1, gn, mixed() ? CUFFT_C2R : CUFFT_Z2D,
                                 g.count));
         }
+        if (std::getenv("PGM_B200_TRACE"))
+            for (auto& g : groups)
+                fprintf(stderr, "pgm_b200 trace: FFT group %dx%dx%d, %d systems from %d, grid offset %lld, spectrum "
+                        "offset %lld\n", g.K[0], g.K[1], g.K[2], g.count, g.first, g.gridOff, g.specOff);
         convBlocks = std::max(1, std::min(512, (maxSpec + 255) / 256));
         // chunks
         chunkSys.clear();

@@ -1,0 +1,61 @@
+"""Parameter gradients (the engine's adjoint of the stationary energy) against the FP64 oracle's analytic
+gradient and central finite differences of the oracle energy (h = 1e-5 relative), per atom and per type
+through the torch.autograd.Function.  Tolerance: 1e-5 relative (FP64 engine 1e-7 against the analytic
+oracle gradient)."""
+
+import numpy as np
+import pytest
+
+from conftest import PKG, oracle_settings, oracle_topology
+from oracle import pgm_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def engine_for(S, precision, tol=1e-12):
+    eng = PKG.Engine(PKG.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=tol, max_iter=1000,
+                                  peek=0.0, predictor=0, ke=PKG.systems.KE_DEFAULT, precision=precision))
+    eng.set_system(S)
+    return eng
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_param_grad_matches_oracle(precision):
+    S = PKG.systems.tiny_triclinic(nmol=16, seed=23)
+    eng = engine_for(S, precision)
+    eng.compute(S.pos, S.box)
+    g = eng.param_grad()
+    ora = O.Engine(oracle_topology(S), oracle_settings(S, tol=1e-12))
+    ora.compute(S.pos, S.box)
+    go = ora.param_gradients()
+    tol = 1e-7 if precision == 0 else 1e-5
+    for k in ("q", "radius", "alpha", "cov_strength"):
+        err = np.linalg.norm(g[k] - go[k]) / np.linalg.norm(go[k])
+        assert err <= tol, (k, err)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_autograd_per_type_vs_finite_differences(precision):
+    import torch
+    grad_mod = __import__("pgm_md_b200.autograd", fromlist=["autograd"])
+    S = PKG.systems.waters(27, 9.6, seed=4, grid=(12, 12, 12), cutoff=4.7, tol=1e-12, lattice=3)
+    eng = engine_for(S, precision)
+    params = grad_mod.type_parameters(S)
+    E = grad_mod.energy(eng, S, *params)
+    E.backward()
+    names = ("q", "cov_strength", "alpha", "radius")
+    s = oracle_settings(S, tol=1e-12)
+    for name, p in zip(names, params):
+        for t in range(len(p)):
+            fd = []
+            for sgn in (1, -1):
+                T = oracle_topology(S)
+                vals = getattr(T, name).copy()
+                idx = (S.cov_types if name == "cov_strength" else S.types) == t
+                h = 1e-5 * abs(float(p[t]))
+                vals[idx] += sgn * h
+                setattr(T, name, vals)
+                fd.append(O.Engine(T, s).compute(S.pos, S.box, want_forces=False))
+            d = (fd[0] - fd[1]) / (2 * h)
+            got = float(p.grad[t])
+            assert abs(got - d) <= 1e-5 * max(abs(d), 1e-2), (name, t, got, d)
