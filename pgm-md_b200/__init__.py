@@ -7,6 +7,7 @@ with ``load_package()`` of ``__graft_entry__`` (or importlib) under the name ``p
 """
 
 from .engine import FP64, MIXED, Engine, PgmArgumentError, PgmError, Result, Settings, Terms  # noqa: F401
+from .engine import pair_list_noalloc  # noqa: F401
 from . import systems  # noqa: F401
 
 __all__ = ["Engine", "Settings", "Terms", "Result", "PgmError", "PgmArgumentError", "FP64", "MIXED", "systems"]

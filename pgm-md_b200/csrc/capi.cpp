@@ -2,6 +2,8 @@
 #include "../../include/pgm_b200.h"
 #include "pgm_engine.h"
 
+#include <cuda_runtime.h>
+
 #include <cstring>
 #include <new>
 #include <stdexcept>
@@ -350,3 +352,33 @@ int pgm_engine_compute_batch(pgm_engine* e, const double* pos, const double* box
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------- no allocation
+
+namespace pgmb200 {
+int pairListNoAlloc(int n, const double* posDev, const double* box, double cutoff, int cap, int* slotAtomOut,
+                    int* countsOut, int* neighborsOut, cudaStream_t st, int* maxCount);
+}
+
+extern "C" int pgm_pair_list_noalloc(int n, const double* pos_dev, const double* box, double cutoff, int cap,
+                                     int* slot_atom_dev, int* counts_dev, int* neighbors_dev, void* stream,
+                                     int* max_count) {
+    try {
+        const int over = pgmb200::pairListNoAlloc(n, pos_dev, box, cutoff, cap, slot_atom_dev, counts_dev,
+                                                  neighbors_dev, (cudaStream_t) stream, max_count);
+        if (over) {
+            g_lastError = "pgm_b200: pair_list_noalloc: an atom has more neighbours than cap (see max_count)";
+            return PGM_ERR_CAPACITY;
+        }
+        return PGM_OK;
+    } catch (const std::length_error& ex) {
+        g_lastError = ex.what();
+        return PGM_ERR_CAPACITY;
+    } catch (const std::invalid_argument& ex) {
+        g_lastError = ex.what();
+        return PGM_ERR_ARGUMENT;
+    } catch (const std::exception& ex) {
+        g_lastError = ex.what();
+        return PGM_ERR_CUDA;
+    }
+}

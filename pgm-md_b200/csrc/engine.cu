@@ -1485,3 +1485,172 @@ void Engine::computeBatch(const double* pos, const double* boxes, double* energi
 }
 
 }  // namespace pgmb200
+
+// ---------------------------------------------------------------------------------------------- no allocation
+//
+// A pair-list entry point for callers that cannot allocate device memory: code that runs while a caller's
+// CUDA stream is being captured into a graph (cudaMalloc is not allowed there), MD engines and allocators that
+// own every byte of the GPU and hand out fixed buffers, and hosts that reserved the device memory up front.
+// It runs the engine's own cell-list and pair-list kernels, with their scratch (cell counts and offsets, the
+// cell-sorted copies of the atoms) in one statically sized device array instead of engine-owned
+// allocations.  Every GPU that loads the library holds that array (about 4 MB) until the process exits.
+namespace pgmb200 {
+namespace {
+
+constexpr int NOALLOC_MAX_ATOMS = 16384;
+constexpr int NOALLOC_MAX_CELLS = 8 * NOALLOC_MAX_ATOMS + 64;
+constexpr size_t NOALLOC_ATOM_BYTES = 200;   // per-atom scratch, rounded up
+constexpr size_t NOALLOC_BYTES = NOALLOC_ATOM_BYTES * NOALLOC_MAX_ATOMS + 8 * (size_t) (NOALLOC_MAX_CELLS + 1) +
+                                 sizeof(SysDev) + sizeof(Ctl) + 64 * 16;
+
+// The scratch.  In host code this name is only a stand-in for the device array: its device address comes
+// from cudaGetSymbolAddress, once per device (noallocScratch below).
+static __device__ __align__(256) unsigned char g_noallocScratch[NOALLOC_BYTES];
+
+// Converts the cell-sorted list entries (slot of j, image shift) into atom indices, in place.
+__global__ void k_entries_to_atoms(const int* slotAtom, const int* counts, int* neighbors, int cap, int n) {
+    const int slot = blockIdx.x, t0 = threadIdx.x;
+    if (slot >= n)
+        return;
+    const int cnt = counts[slot];
+    for (int t = t0; t < cnt; t += blockDim.x) {
+        const uint32_t e = (uint32_t) neighbors[(size_t) slot * cap + t];
+        neighbors[(size_t) slot * cap + t] = slotAtom[e & 0x7FFFFFu];
+    }
+}
+
+// Device address of the scratch on the current device: looked up on the first call on that device.
+unsigned char* noallocScratch() {
+    static unsigned char* addr[64] = {nullptr};
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64)
+        throw std::runtime_error("pgm_b200: device index beyond 63");
+    if (!addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
+        if (e != cudaSuccess || !p)
+            throw std::runtime_error(std::string("pgm_b200: cudaGetSymbolAddress of the scratch array failed: ") +
+                                     cudaGetErrorString(e));
+        addr[dev] = (unsigned char*) p;
+    }
+    return addr[dev];
+}
+
+}  // namespace
+
+int pairListNoAlloc(int n, const double* posDev, const double* box, double cutoff, int cap, int* slotAtomOut,
+                    int* countsOut, int* neighborsOut, cudaStream_t st, int* maxCount) {
+    if (n <= 0 || n > NOALLOC_MAX_ATOMS)
+        throw std::length_error("pgm_b200: pair_list_noalloc handles 1.." + std::to_string(NOALLOC_MAX_ATOMS) +
+                                " atoms, got " + std::to_string(n));
+    if (cap <= 0 || !posDev || !box || !slotAtomOut || !countsOut || !neighborsOut)
+        throw std::invalid_argument("pgm_b200: pair_list_noalloc arguments");
+    // the system's constants, as the engine computes them for one system
+    SysDev S;
+    std::memset(&S, 0, sizeof(S));
+    for (int a = 0; a < 9; a++)
+        S.H[a] = box[a];
+    if (box[1] != 0 || box[2] != 0 || box[5] != 0 || !(box[0] > 0 && box[4] > 0 && box[8] > 0))
+        throw std::invalid_argument("pgm_b200: box not in the reduced triclinic form");
+    if (!(cutoff > 0))
+        throw std::invalid_argument("pgm_b200: cutoff must be positive");
+    boxInverse(box, S.recip, S.volume);
+    S.cutoff = cutoff;
+    S.rc2 = cutoff * cutoff;
+    S.beta = 1.0;
+    S.K[0] = S.K[1] = S.K[2] = 1;
+    S.atomBegin = 0;
+    S.atomEnd = n;
+    double rho[3];
+    for (int a = 0; a < 3; a++) {
+        rho[a] = cutoff * std::sqrt(S.recip[a] * S.recip[a] + S.recip[3 + a] * S.recip[3 + a] +
+                                    S.recip[6 + a] * S.recip[6 + a]);
+        if (rho[a] > 0.5 * (1.0 + 1e-12))
+            throw std::invalid_argument("pgm_b200: cut-off beyond half the box");
+        S.cellN[a] = std::max(1, std::min((int) std::floor(2.0 / rho[a]), 1024));
+    }
+    while ((long long) S.cellN[0] * S.cellN[1] * S.cellN[2] > 8LL * n + 64) {
+        int a = 0;
+        for (int b = 1; b < 3; b++)
+            if (S.cellN[b] > S.cellN[a])
+                a = b;
+        S.cellN[a] = std::max(1, S.cellN[a] / 2);
+    }
+    for (int a = 0; a < 3; a++)
+        S.cellM[a] = std::max(1, (int) std::ceil(rho[a] * S.cellN[a] * (1.0 + 1e-12)));
+    S.cellCount = S.cellN[0] * S.cellN[1] * S.cellN[2];
+    if (S.cellCount > NOALLOC_MAX_CELLS)
+        throw std::length_error("pgm_b200: pair_list_noalloc: more cells than its scratch holds");
+    // carve the scratch
+    unsigned char* base = noallocScratch();
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        unsigned char* p = base + off;
+        off += (bytes + 255) / 256 * 256;
+        return p;
+    };
+    Dev d;
+    std::memset(&d, 0, sizeof(d));
+    SysDev* sysD = (SysDev*) take(sizeof(SysDev));
+    Ctl* ctlD = (Ctl*) take(sizeof(Ctl));
+    int* flags = (int*) take(16 * sizeof(int));
+    d.nAtoms = n;
+    d.nSys = 1;
+    d.cap = cap;
+    d.order = 6;
+    d.totalCells = S.cellCount;
+    d.sys = sysD;
+    d.ctl = ctlD;
+    d.flags = flags;
+    d.posIn = posDev;
+    d.atomSys = (const int*) take(n * sizeof(int));
+    d.q = (const double*) take(n * 8);
+    d.radius = (const double*) take(n * 8);
+    d.wrapN = (int*) take(3 * n * sizeof(int));
+    d.cellOf = (int*) take(n * sizeof(int));
+    d.cellRank = (int*) take(n * sizeof(int));
+    d.pmeBase = (int*) take(3 * n * sizeof(int));
+    d.pmeFr = (double*) take(3 * n * 8);
+    d.Etot = (double*) take(3 * n * 8);
+    d.slotTmp = (int*) take(n * sizeof(int));
+    d.posS = (double4*) take(n * sizeof(double4));
+    d.origS = (double4*) take(n * sizeof(double4));
+    d.wrapS = (int4*) take(n * sizeof(int4));
+    d.radS = (double*) take(n * 8);
+    d.cellCount = (int*) take(S.cellCount * sizeof(int));
+    d.cellStart = (int*) take((S.cellCount + 1) * sizeof(int));
+    if (off > NOALLOC_BYTES)
+        throw std::length_error("pgm_b200: pair_list_noalloc scratch layout exceeds its array");
+    d.slotAtom = slotAtomOut;
+    d.listCount = countsOut;
+    d.list = (uint32_t*) neighborsOut;
+    Ctl c;
+    std::memset(&c, 0, sizeof(c));
+    c.posMode = 0;
+    c.histSlot = -1;
+    // every call shares the scratch and finds the previous call's contents: clear what must start at zero
+    CU(cudaMemcpyAsync(sysD, &S, sizeof(S), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(ctlD, &c, sizeof(c), cudaMemcpyHostToDevice, st));
+    CU(cudaMemsetAsync(flags, 0, 16 * sizeof(int), st));
+    CU(cudaMemsetAsync((void*) d.atomSys, 0, n * sizeof(int), st));
+    CU(cudaMemsetAsync((void*) d.q, 0, n * 8, st));
+    CU(cudaMemsetAsync((void*) d.radius, 0, n * 8, st));
+    CU(cudaMemsetAsync(d.cellCount, 0, S.cellCount * sizeof(int), st));
+    const int tb = (n + 255) / 256;
+    k_prep<<<tb, 256, 0, st>>>(d, nullptr);
+    k_cell_scan<<<1, 1024, 0, st>>>(d);
+    k_cell_scatter<<<tb, 256, 0, st>>>(d);
+    k_cell_sort<<<(S.cellCount + 7) / 8, 256, 0, st>>>(d);
+    k_build_list<<<S.cellCount, LIST_THREADS, 0, st>>>(d);
+    k_entries_to_atoms<<<n, 128, 0, st>>>(slotAtomOut, countsOut, neighborsOut, cap, n);
+    CU(cudaGetLastError());
+    int hflags[16];
+    CU(cudaMemcpyAsync(hflags, flags, sizeof(hflags), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (maxCount)
+        *maxCount = hflags[0];
+    return hflags[0] > cap ? 1 : 0;
+}
+
+}  // namespace pgmb200

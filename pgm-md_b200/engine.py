@@ -339,3 +339,22 @@ class Engine:
         f = np.zeros((self.n, 3)) if forces else None
         _check(self._L.pgm_engine_compute_batch(self._h, _d(pos), _d(boxes), _d(E), _d(f), _d(S), _i(it)))
         return dict(energies=E, forces=f, strain=S, iterations=it)
+
+
+def pair_list_noalloc(n, pos_dev_ptr, box, cutoff, cap, slot_atom_ptr, counts_ptr, neighbors_ptr, stream_ptr=0):
+    """The directed pair list of one periodic system into caller-owned device buffers, allocating nothing
+    (pgm_pair_list_noalloc of include/pgm_b200.h): for callers that cannot allocate device memory, such as
+    code running inside a stream capture or under an allocator that owns the whole GPU.  Buffers are raw
+    device pointers: positions double n*3; slot_atom int n, counts int n, neighbors int n*cap.  Returns the
+    longest row; raises PgmError (status -4) when n exceeds 16384 or a row exceeds cap."""
+    L = _lib.load()
+    box = _f64(box)
+    mx = ctypes.c_int(0)
+    rc = L.pgm_pair_list_noalloc(int(n), ctypes.c_void_p(pos_dev_ptr), _d(box), float(cutoff), int(cap),
+                                 ctypes.c_void_p(slot_atom_ptr), ctypes.c_void_p(counts_ptr),
+                                 ctypes.c_void_p(neighbors_ptr), ctypes.c_void_p(stream_ptr), ctypes.byref(mx))
+    if rc != 0:
+        err = PgmError(rc, L.pgm_last_error().decode())
+        err.max_count = mx.value
+        raise err
+    return mx.value

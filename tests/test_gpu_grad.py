@@ -52,7 +52,7 @@ def test_autograd_per_type_vs_finite_differences(precision):
                 T = oracle_topology(S)
                 vals = getattr(T, name).copy()
                 idx = (S.cov_types if name == "cov_strength" else S.types) == t
-                h = 1e-5 * abs(float(p[t]))
+                h = 1e-5 * abs(p[t].item())
                 vals[idx] += sgn * h
                 setattr(T, name, vals)
                 fd.append(O.Engine(T, s).compute(S.pos, S.box, want_forces=False))
