@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run for ncu: only warmup + steps evaluations of one precision, no other legs")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="with --profile")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched 1024-system leg")
+    ap.add_argument("--no-large", action="store_true", help="skip the 98304-atom leg")
     return ap.parse_args()
 
 
@@ -368,16 +370,105 @@ def main():
             "roofline": roof, "clocks": clocks}
     if rank == 0 and not args.no_accuracy:
         line["accuracy"] = accuracy(pkg, S, mixed, fp64)
-    if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(pkg, S)
     mixed.close()
     fp64.close()
+    if not args.no_large:
+        line["water98304"] = large_leg(pkg, local, world, dist if world > 1 else None)
+    if not args.no_batch:
+        line["water_batch1024"] = batch_leg(pkg, local, rank, world, dist if world > 1 else None)
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(pkg, S)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
     return 0
+
+
+def _timed(fn, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        fn()
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) / steps
+
+
+def large_leg(pkg, local, world, dist):
+    """32768 waters (98304 atoms), 99.4 A box, 104^3 grid, order 6, mixed precision, tol 1e-4 and 1e-5: evals/s
+    and ns/day at 2 fs (host call, positions and forces through host memory); replicas on N > 1."""
+    import torch
+    out = {"workload": "water98304", "atoms": 98304, "grid": [104, 104, 104]}
+    S = pkg.systems.water98304()
+    for tol in (1e-4, 1e-5):
+        eng = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=6, tol=tol, max_iter=200,
+                                      peek=0.65, predictor=0, ke=pkg.systems.KE_DEFAULT, precision=pkg.MIXED,
+                                      device=local))
+        eng.set_system(S)
+        res = {}
+        dt = _timed(lambda: res.__setitem__("r", eng.compute(S.pos, S.box)), 5, 2)
+        t = torch.tensor([dt], dtype=torch.float64, device=f"cuda:{local}")
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        v = world / float(t.item())
+        out[f"tol{tol:g}"] = {"evals_per_s": v, "ms_per_eval": 1e3 * float(t.item()),
+                              "ns_per_day_2fs": v / world * 86400 * 2e-6, "cg_iterations": res["r"].iterations}
+        if tol == 1e-5:
+            kt = eng.kernel_times(reps=5)
+            out["kernel_ms"] = kt
+        eng.close()
+    return out
+
+
+def batch_leg(pkg, local, rank, world, dist):
+    """1024 independent water boxes of 8..512 molecules (0.0334 / A^3, ~1 A grids, cutoff min(9 A, L/2),
+    tol 1e-5, mixed) in one launch per rank (systems partitioned by atom count across ranks), against the same
+    systems evaluated one after the other by single-system engines (a sample of 64, on rank 0)."""
+    import torch
+    import pgm_md_b200.shard as sh
+    systems = pkg.systems.water_batch(nsys=1024, seed=1024, tol=1e-5)
+    parts = sh.partition([s.n for s in systems], world)
+    mine = [systems[k] for k in parts[rank]]
+    eng = pkg.Engine(pkg.Settings(cutoff=0.9, beta=3.5, grid=(24, 24, 24), order=6, tol=1e-5, max_iter=200,
+                                  peek=0.65, predictor=0, ke=pkg.systems.KE_DEFAULT, precision=pkg.MIXED,
+                                  device=local))
+    eng.set_systems(mine)
+    pos = np.concatenate([s.pos for s in mine])
+    boxes = np.stack([s.box for s in mine])
+    res = {}
+    dt = _timed(lambda: res.__setitem__("r", eng.compute_batch(pos, boxes)), 5, 2)
+    t = torch.tensor([dt], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dt = float(t.item())
+    energies = sh.gather_energies(parts[rank], res["r"]["energies"], len(systems))
+    out = {"workload": "water_batch1024", "systems": len(systems), "atoms": int(sum(s.n for s in systems)),
+           "systems_per_s": len(systems) / dt, "ms_per_batch": 1e3 * dt,
+           "max_cg_iterations": int(res["r"]["iterations"].max()), "partition": "atom-balanced, one launch per rank",
+           "energies_finite": bool(np.isfinite(energies).all())}
+    eng.close()
+    if rank == 0:
+        sample = systems[:: len(systems) // 64][:64]
+        engines = []
+        for S in sample:
+            e = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=6, tol=1e-5, max_iter=200,
+                                        peek=0.65, predictor=0, ke=pkg.systems.KE_DEFAULT, precision=pkg.MIXED,
+                                        device=local))
+            e.set_system(S)
+            e.compute(S.pos, S.box)
+            engines.append((e, S))
+        ts = _timed(lambda: [e.compute(S.pos, S.box) for e, S in engines], 2, 1)
+        per = ts / len(engines)
+        out["sequential_systems_per_s"] = 1.0 / per
+        out["sequential_sample"] = f"{len(engines)} systems, one engine each, evaluated one after the other"
+        out["batched_over_sequential"] = out["systems_per_s"] / world / out["sequential_systems_per_s"]
+        for e, _ in engines:
+            e.close()
+    return out
 
 
 class _Null:
