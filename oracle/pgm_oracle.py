@@ -234,6 +234,56 @@ def pair_set(pos, box, cutoff, chunk=2048):
     return np.concatenate(I), np.concatenate(J), np.concatenate(X)
 
 
+def pair_set_cells(pos, box, cutoff):
+    """The set of pair_set (core/pgm_core.cpp:64-87, the same exact test on every candidate) for large systems:
+    candidates come from a grid of cells at least rc wide in every fractional direction (27 neighbour cells), so
+    only nearby pairs are tested.  Needs at least 3 cells per dimension.  Returns (i, j) sorted, i < j."""
+    pos = np.asarray(pos, np.float64)
+    box = np.asarray(box, np.float64)
+    recip, _ = box_inverse(box)
+    n = len(pos)
+    rc2 = cutoff * cutoff
+    frac = pos @ recip
+    frac -= np.floor(frac)
+    nc = []
+    for a in range(3):
+        rho = cutoff * np.linalg.norm(recip[:, a])
+        nc.append(int(np.floor(1.0 / rho)))
+    if min(nc) < 3:
+        raise ValueError("pair_set_cells needs at least 3 cells per dimension")
+    cidx = np.minimum((frac * nc).astype(np.int64), np.array(nc) - 1)
+    lin = (cidx[:, 0] * nc[1] + cidx[:, 1]) * nc[2] + cidx[:, 2]
+    order = np.argsort(lin, kind="stable")
+    starts = np.searchsorted(lin[order], np.arange(nc[0] * nc[1] * nc[2] + 1))
+    I, J = [], []
+    for c0 in range(nc[0]):
+        for c1 in range(nc[1]):
+            for c2 in range(nc[2]):
+                ca = (c0 * nc[1] + c1) * nc[2] + c2
+                A = order[starts[ca]:starts[ca + 1]]
+                if len(A) == 0:
+                    continue
+                nb = set()
+                for d0 in (-1, 0, 1):
+                    for d1 in (-1, 0, 1):
+                        for d2 in (-1, 0, 1):
+                            nb.add((((c0 + d0) % nc[0]) * nc[1] + (c1 + d1) % nc[1]) * nc[2] + (c2 + d2) % nc[2])
+                B = np.concatenate([order[starts[cb]:starts[cb + 1]] for cb in sorted(nb)])
+                ii = np.repeat(A, len(B))
+                jj = np.tile(B, len(A))
+                keep = ii < jj
+                ii, jj = ii[keep], jj[keep]
+                x = min_image(pos[ii] - pos[jj], box)
+                r2 = x[:, 0] * x[:, 0] + x[:, 1] * x[:, 1] + x[:, 2] * x[:, 2]
+                sel = r2 < rc2
+                I.append(ii[sel])
+                J.append(jj[sel])
+    I = np.concatenate(I)
+    J = np.concatenate(J)
+    o = np.lexsort((J, I))
+    return I[o], J[o]
+
+
 # ----------------------------------------------------------------------------------------- engine
 
 class Engine:

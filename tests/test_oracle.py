@@ -138,3 +138,10 @@ def test_oracle_matches_reference_live():
         assert abs(e1 - e2) <= 1e-11 * abs(e1)
         assert np.linalg.norm(ref.forces - ora.forces) <= 1e-10 * np.linalg.norm(ref.forces)
         assert ref.iterations() == ora.iterations
+
+
+def test_pair_set_cells_equals_all_pairs():
+    S = PKG.systems.water216()
+    i, j, _ = O.pair_set(S.pos, S.box, 0.6)
+    ci, cj = O.pair_set_cells(S.pos, S.box, 0.6)
+    assert np.array_equal(i, ci) and np.array_equal(j, cj)
