@@ -29,12 +29,13 @@ def test_large_pair_set_bit_exact(big):
     gi, gj = e.pairs()
     oi, oj = O.pair_set_cells(big.pos, big.box, big.cutoff)
     assert np.array_equal(gi, oi) and np.array_equal(gj, oj)
-    # rigid translation: same pair set, same direct energy (minimum image), reciprocal within PME aliasing
+    # rigid translation: the same pair set; energies change only through PME's grid aliasing (which moves the
+    # induced dipoles slightly, and with them the direct term)
     shift = np.array([0.1234, 0.4567, 0.7891])
     r2 = e.compute(big.pos + shift, big.box)
     ti, tj = e.pairs()
     assert np.array_equal(ti, gi) and np.array_equal(tj, gj)
-    assert abs(r2.terms.direct - r.terms.direct) <= 1e-9 * abs(r.terms.direct)
+    assert abs(r2.terms.direct - r.terms.direct) <= 1e-7 * abs(r.terms.direct)
     assert abs(r2.energy - r.energy) <= 1e-6 * abs(r.energy)
 
 
