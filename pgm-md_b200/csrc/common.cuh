@@ -68,6 +68,8 @@ struct Dev {
     int* cellRank;
     int* pmeBase;             // 3n
     double* pmeFr;            // 3n
+    void* spl;                // slot order: 9 * MAXP spline coefficients (R) per atom
+    int4* baseS;              // slot order: base grid indices
     // cells
     int* cellCount;
     int* cellStart;           // totalCells + 1

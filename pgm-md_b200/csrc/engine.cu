@@ -152,7 +152,7 @@ struct Engine::Impl {
 
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
-        dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dRadS, dList, dListCount, dG12, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
+        dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dG12, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
         dScal, dPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
@@ -200,7 +200,7 @@ struct Engine::Impl {
         }
         groups.clear();
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
-                      &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dRadS, &dList, &dListCount, &dG12, &dFlags, &dDS,
+                      &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dG12, &dFlags, &dDS,
                       &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
@@ -506,6 +506,8 @@ struct Engine::Impl {
         dSlotTmp.ensure(n * sizeof(int));
         dPosS.ensure(n * sizeof(double4));
         dOrigS.ensure(n * sizeof(double4));
+        dSpl.ensure((size_t) n * 9 * MAXP * R);
+        dBaseS.ensure(n * sizeof(int4));
         dWrapS.ensure(n * sizeof(int4));
         dRadS.ensure(n * 8);
         dListCount.ensure(n * sizeof(int));
@@ -682,6 +684,8 @@ struct Engine::Impl {
         d.slotTmp = dSlotTmp.as<int>();
         d.posS = dPosS.as<double4>();
         d.origS = dOrigS.as<double4>();
+        d.spl = dSpl.p;
+        d.baseS = dBaseS.as<int4>();
         d.wrapS = dWrapS.as<int4>();
         d.radS = dRadS.as<double>();
         d.list = dList.as<uint32_t>();
@@ -825,6 +829,7 @@ struct Engine::Impl {
         k_cell_sort<<<(totalCells + 7) / 8, 256, 0, sm>>>(d);
         k_build_list<<<totalCells, LIST_THREADS, 0, sm>>>(d);
         k_pair_kernels<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
+        k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
         k_perm<<<tb, 256, 0, sm>>>(d);
         k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
         CU(cudaGetLastError());
@@ -1293,12 +1298,14 @@ void Engine::field(const double* pos, const double box[3][3], const double* qf, 
         if (I.mixed()) {
             k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(dv);
             k_pair_kernels<float><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
+            k_splines<float><<<(3 * I.n + 255) / 256, 256, 0, I.st>>>(dv);
             k_influence<float><<<dim3(I.convBlocks, I.nsys), 256, 0, I.st>>>(dv);
             CU(cudaMemsetAsync(dv.grid, 0, I.gridTotal * I.realSize(), I.st));
             I.fieldPass<float, true>(I.st, I.side, dv, 0, dv.dtot, false);
         } else {
             k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(dv);
             k_pair_kernels<double><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
+            k_splines<double><<<(3 * I.n + 255) / 256, 256, 0, I.st>>>(dv);
             k_influence<double><<<dim3(I.convBlocks, I.nsys), 256, 0, I.st>>>(dv);
             CU(cudaMemsetAsync(dv.grid, 0, I.gridTotal * I.realSize(), I.st));
             I.fieldPass<double, true>(I.st, I.side, dv, 0, dv.dtot, false);
@@ -1383,12 +1390,12 @@ int Engine::kernelLaunches() const {
     const Impl& I = *impl;
     if (!I.haveResult)
         return 0;
-    // own kernels per evaluation: preparation 9, the two field passes before the loop 3 + 1 + 3 + 1,
+    // own kernels per evaluation: preparation 10, the two field passes before the loop 3 + 1 + 3 + 1,
     // 4 per CG iteration, final 7 (the cuFFT transforms are not counted)
     int it = 0;
     for (int k = 0; k < I.nsys; k++)
         it = std::max(it, (int) I.lastResults[(size_t) k * NRES + 14]);
-    return 9 + (I.s.polarizable ? 8 + 4 * it : 0) + 7;
+    return 10 + (I.s.polarizable ? 8 + 4 * it : 0) + 7;
 }
 
 void Engine::kernelTimes(int reps, double* ms) {

@@ -191,6 +191,7 @@ __global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
     __shared__ int runSlot[MAX_RUNS], runOff[MAX_RUNS + 1], runShift[MAX_RUNS];
     __shared__ double4 cPos[LIST_CHUNK], cOrig[LIST_CHUNK];
     __shared__ int4 cWrap[LIST_CHUNK];
+    __shared__ int wq[LIST_THREADS / 32][64];
     const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     constexpr int NW = LIST_THREADS / 32;
     if (c >= dv.totalCells)
@@ -255,7 +256,9 @@ __global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
         dv.listCount[ii] = 0;
     __syncthreads();
     const int total = runOff[nr];
-    const double pre = S.rc2 * (1.0 + 1e-10) + 1e-300;
+    const double pre = S.rc2 * (1.0 + 1e-10) + 1e-300, preLo = S.rc2 * (1.0 - 1e-10);
+    const double half0 = 0.5 * S.H[0] * (1.0 - 1e-10), half1 = 0.5 * S.H[4] * (1.0 - 1e-10),
+                 half2 = 0.5 * S.H[8] * (1.0 - 1e-10);
     const double invDiag[3] = {1.0 / S.H[0], 1.0 / S.H[4], 1.0 / S.H[8]};
     for (int base = 0; base < total; base += LIST_CHUNK) {
         const int nc = min(LIST_CHUNK, total - base);
@@ -270,10 +273,15 @@ __global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
                     hi = mid - 1;
             }
             const int js = runSlot[lo] + (k - runOff[lo]);
-            cPos[t] = dv.posS[js];
+            const int code = runShift[lo];
+            const int w0 = (code & 7) - 4, w1 = ((code >> 3) & 7) - 4, w2 = ((code >> 6) & 7) - 4;
+            // the candidate's image: wrapped position + w.H, staged once for all atoms of the cell
+            const double4 pw = dv.posS[js];
+            cPos[t] = make_double4(pw.x + (w0 * S.H[0] + w1 * S.H[3] + w2 * S.H[6]), pw.y + (w1 * S.H[4] + w2 * S.H[7]),
+                                   pw.z + w2 * S.H[8], 0.0);
             cOrig[t] = dv.origS[js];
             const int4 w = dv.wrapS[js];
-            cWrap[t] = make_int4(w.x, w.y, w.z, js | (runShift[lo] << 23));
+            cWrap[t] = make_int4(w.x, w.y, w.z, js | (code << 23));
         }
         __syncthreads();
         for (int ii = cb + wid; ii < ce; ii += NW) {
@@ -282,43 +290,67 @@ __global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
             const int4 wi = dv.wrapS[ii];
             uint32_t* row = dv.list + (size_t) ii * dv.cap;
             int count = dv.listCount[ii];
+            int qn = 0;   // prefilter survivors queued (candidate order) for the exact test
             for (int t0 = 0; t0 < nc; t0 += 32) {
                 const int t = t0 + lane;
-                bool acc = false;
-                double x[3];
-                uint32_t entry = 0;
+                bool pass = false;
+                int qv = t;
                 if (t < nc) {
-                    const int4 cw = cWrap[t];
-                    entry = (uint32_t) cw.w;
-                    const int js = (int) (entry & 0x7FFFFFu);
-                    const int w0 = (int) ((entry >> 23) & 7u) - 4, w1 = (int) ((entry >> 26) & 7u) - 4,
-                              w2 = (int) ((entry >> 29) & 7u) - 4;
-                    const double sh0 = w0 * S.H[0] + w1 * S.H[3] + w2 * S.H[6];
-                    const double sh1 = w1 * S.H[4] + w2 * S.H[7];
-                    const double sh2 = w2 * S.H[8];
-                    const double4 pwj = cPos[t];
-                    const double y0 = pwi.x - pwj.x - sh0, y1 = pwi.y - pwj.y - sh1, y2 = pwi.z - pwj.z - sh2;
-                    if (js != ii && y0 * y0 + y1 * y1 + y2 * y2 < pre) {
-                        const double4 oj = cOrig[t];
-                        x[0] = __dsub_rn(oi.x, oj.x);
-                        x[1] = __dsub_rn(oi.y, oj.y);
-                        x[2] = __dsub_rn(oi.z, oj.z);
+                    const double4 pj = cPos[t];
+                    const double y0 = pwi.x - pj.x, y1 = pwi.y - pj.y, y2 = pwi.z - pj.z;
+                    const double r2 = y0 * y0 + y1 * y1 + y2 * y2;
+                    pass = ((cWrap[t].w & 0x7FFFFF) != ii) && (r2 < pre);
+                    // clearly inside the cutoff with every component of the cell image inside half a box edge:
+                    // the reference's rounding then picks this very image and the same side of the cutoff,
+                    // so the exact test can be skipped
+                    if (pass && r2 < preLo && fabs(y0) < half0 && fabs(y1) < half1 && fabs(y2) < half2)
+                        qv = t | (1 << 30);
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, pass);
+                if (pass)
+                    wq[wid][qn + __popc(m & ((1u << lane) - 1u))] = qv;
+                qn += __popc(m);
+                __syncwarp();
+                const bool last = (t0 + 32 >= nc);
+                while (qn >= 32 || (last && qn > 0)) {
+                    const int nb = min(qn, 32);
+                    bool acc = false;
+                    uint32_t entry = 0;
+                    if (lane < nb && (wq[wid][lane] & (1 << 30))) {
+                        entry = (uint32_t) cWrap[wq[wid][lane] & 0xFFFF].w;
+                        acc = true;
+                    } else if (lane < nb) {
+                        const int tq = wq[wid][lane];
+                        const int4 cw = cWrap[tq];
+                        entry = (uint32_t) cw.w;
+                        const int w0 = (int) ((entry >> 23) & 7u) - 4, w1 = (int) ((entry >> 26) & 7u) - 4,
+                                  w2 = (int) ((entry >> 29) & 7u) - 4;
+                        const double4 oj = cOrig[tq];
+                        double x[3] = {__dsub_rn(oi.x, oj.x), __dsub_rn(oi.y, oj.y), __dsub_rn(oi.z, oj.z)};
                         int kk[3];
                         minImageFast(x, S.H, invDiag, kk);
-                        if (dot3exact(x) < S.rc2) {
-                            // image of the exact test relative to the wrapped positions
+                        if (dot3exact(x) < S.rc2)   // image of the exact test relative to the wrapped positions
                             acc = (kk[0] - (wi.x - cw.x) == w0 && kk[1] - (wi.y - cw.y) == w1 &&
                                    kk[2] - (wi.z - cw.z) == w2);
-                        }
                     }
+                    const unsigned ma = __ballot_sync(0xffffffffu, acc);
+                    if (acc) {
+                        const int pos = count + __popc(ma & ((1u << lane) - 1u));
+                        if (pos < dv.cap)
+                            row[pos] = entry;
+                    }
+                    count += __popc(ma);
+                    // move the queue's remainder to its front
+                    const int rest = qn - nb;
+                    int moved = 0;
+                    if (lane < rest)
+                        moved = wq[wid][nb + lane];
+                    __syncwarp();
+                    if (lane < rest)
+                        wq[wid][lane] = moved;
+                    __syncwarp();
+                    qn = rest;
                 }
-                const unsigned m = __ballot_sync(0xffffffffu, acc);
-                if (acc) {
-                    const int pos = count + __popc(m & ((1u << lane) - 1u));
-                    if (pos < dv.cap)
-                        row[pos] = entry;
-                }
-                count += __popc(m);
             }
             if (lane == 0)
                 dv.listCount[ii] = count;
@@ -356,9 +388,10 @@ __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
         entryShift(e, S.H, sh);
         const double4 pwj = dv.posS[js];
         const double x0 = pwi.x - pwj.x - sh[0], x1 = pwi.y - pwj.y - sh[1], x2 = pwi.z - pwj.z - sh[2];
-        const double Rj = dv.radS[js];
-        const R r = (R) sqrt(x0 * x0 + x1 * x1 + x2 * x2);
-        const R a = (R) (1.0 / sqrt(2.0 * (Ri * Ri + Rj * Rj)));
+        const R Rj = (R) dv.radS[js], Rr = (R) Ri;
+        const R xr0 = (R) x0, xr1 = (R) x1, xr2 = (R) x2;
+        const R r = fsqrt(xr0 * xr0 + xr1 * xr1 + xr2 * xr2);
+        const R a = R(1) / fsqrt(R(2) * (Rr * Rr + Rj * Rj));
         R G[3];
         pairKernels<R, 3>(a, beta, r, G);
         R2 g;
@@ -420,6 +453,29 @@ __global__ void k_influence(Dev dv) {
     }
 }
 
+// B-spline coefficients of every atom, once per evaluation (positions are fixed during it): slot-ordered
+// spl[(slot * 9 + kind * 3 + dim) * MAXP + j], kind 0 theta, 1 dtheta, 2 d2theta (core/pgm_core.cpp:131-150),
+// and the base grid index per dimension.  One thread per (slot, dimension).
+template <typename R>
+__global__ void k_splines(Dev dv) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * dv.nAtoms)
+        return;
+    const int slot = t / 3, dim = t % 3;
+    const int i = dv.slotAtom[slot];
+    R th[MAXP], dth[MAXP], d2[MAXP];
+    bspline<R>((R) dv.pmeFr[3 * i + dim], dv.order, th, dth, d2);
+    R* out = (R*) dv.spl + (size_t) slot * 9 * MAXP;
+#pragma unroll
+    for (int j = 0; j < MAXP; j++)
+        if (j < dv.order) {
+            out[(0 * 3 + dim) * MAXP + j] = th[j];
+            out[(1 * 3 + dim) * MAXP + j] = dth[j];
+            out[(2 * 3 + dim) * MAXP + j] = d2[j];
+        }
+    ((int*) dv.baseS)[4 * slot + dim] = dv.pmeBase[3 * i + dim];
+}
+
 // Spread of charges and dipoles onto the grid: Q[g] += q t1 t2 t3 + e1 u1 t2 t3 + e2 t1 u2 t3 + e3 t1 t2 u3,
 // e_a = K_a d . recip[:, a] (core/pgm_core.cpp:187-207).  One warp per slot, p^3 points over the lanes.
 // P: the spline order as a compile-time constant (0: the runtime order).
@@ -449,15 +505,28 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
         } else {
             dl = vec[3 * i + lane];
         }
-        R t[MAXP], u[MAXP], v[MAXP];
-        bspline<R>((R) dv.pmeFr[3 * i + lane], p, t, u, v);
+        if (P == 0) {
+            R t[MAXP], u[MAXP], v[MAXP];
+            bspline<R>((R) dv.pmeFr[3 * i + lane], p, t, u, v);
 #pragma unroll
-        for (int j = 0; j < PM; j++)
-            if (j < p) {
-                sth[wib][lane][j] = t[j];
-                sdth[wib][lane][j] = u[j];
-            }
+            for (int j = 0; j < PM; j++)
+                if (j < p) {
+                    sth[wib][lane][j] = t[j];
+                    sdth[wib][lane][j] = u[j];
+                }
+        }
         bl = dv.pmeBase[3 * i + lane];
+    }
+    if (P > 0) {   // the evaluation's precomputed coefficients (k_splines)
+        const R* sp = (const R*) dv.spl + (size_t) slot * 9 * MAXP;
+        for (int k = lane; k < 6 * PM; k += 32) {
+            const int kind = k / (3 * PM), dim = (k / PM) % 3, j = k % PM;
+            const R v = sp[(kind * 3 + dim) * MAXP + j];
+            if (kind == 0)
+                sth[wib][dim][j] = v;
+            else
+                sdth[wib][dim][j] = v;
+        }
     }
     const double d0 = __shfl_sync(0xffffffffu, dl, 0), d1 = __shfl_sync(0xffffffffu, dl, 1),
                  d2 = __shfl_sync(0xffffffffu, dl, 2);
@@ -479,11 +548,30 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
     const R qr = (R) qv;
     R* grid = (R*) dv.grid + S.gridOff;
     const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
-    const int pp = p * p, p3 = pp * p;
-    constexpr int NIT = P > 0 ? (P * P * P + 31) / 32 : 1;
+    if (P > 0) {
+        // lane -> (j2, j3), loop over j1: consecutive lanes hit consecutive grid points of one row, and
+        // w = t1 (q t2 t3 + e1 u2 t3 + e2 t2 u3) + u1 (e0 t2 t3) costs two products per point
+        constexpr int NPAIR = P * P, ROUNDS = (P * P + 31) / 32;
+        const size_t plane = (size_t) K1 * K2;
 #pragma unroll
-    for (int it = 0; it < NIT; it++) {
-        for (int t = lane + 32 * it; t < p3; t += (P > 0 ? p3 : 32)) {
+        for (int rd = 0; rd < ROUNDS; rd++) {
+            const int pr = lane + 32 * rd;
+            if (pr < NPAIR) {
+                const int j2 = pr / (P > 0 ? P : 1), j3 = pr % (P > 0 ? P : 1);
+                const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
+                const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+                const R c23 = t2 * t3;
+                const R a = qr * c23 + e1 * u2 * t3 + e2 * t2 * u3;
+                const R b = e0 * c23;
+                R* col = grid + (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2);
+#pragma unroll
+                for (int j1 = 0; j1 < PM; j1++)
+                    atomicAdd(col + (size_t) wrapIndex(b0 - j1, K0) * plane, a * sth[wib][0][j1] + b * sdth[wib][0][j1]);
+            }
+        }
+    } else {
+        const int pp = p * p, p3 = pp * p;
+        for (int t = lane; t < p3; t += 32) {
             const int j1 = t / pp, j2 = (t / p) % p, j3 = t % p;
             const R t1 = sth[wib][0][j1], u1 = sdth[wib][0][j1];
             const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
@@ -566,47 +654,99 @@ __global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
     const int p = P > 0 ? P : dv.order;
     int bl = 0;
     if (lane < 3) {
-        R t[MAXP], u[MAXP], v[MAXP];
-        bspline<R>((R) dv.pmeFr[3 * i + lane], p, t, u, v);
+        if (P == 0) {
+            R t[MAXP], u[MAXP], v[MAXP];
+            bspline<R>((R) dv.pmeFr[3 * i + lane], p, t, u, v);
 #pragma unroll
-        for (int j = 0; j < PM; j++)
-            if (j < p) {
-                sth[wib][lane][j] = t[j];
-                sdth[wib][lane][j] = u[j];
-                if (FINAL)
-                    sd2[wib][lane][FINAL ? j : 0] = v[j];
-            }
+            for (int j = 0; j < PM; j++)
+                if (j < p) {
+                    sth[wib][lane][j] = t[j];
+                    sdth[wib][lane][j] = u[j];
+                    if (FINAL)
+                        sd2[wib][lane][FINAL ? j : 0] = v[j];
+                }
+        }
         bl = dv.pmeBase[3 * i + lane];
+    }
+    if (P > 0) {   // the evaluation's precomputed coefficients (k_splines)
+        const R* sp = (const R*) dv.spl + (size_t) slot * 9 * MAXP;
+        constexpr int KINDS = FINAL ? 3 : 2;
+        for (int k = lane; k < KINDS * 3 * PM; k += 32) {
+            const int kind = k / (3 * PM), dim = (k / PM) % 3, j = k % PM;
+            const R v = sp[(kind * 3 + dim) * MAXP + j];
+            if (kind == 0)
+                sth[wib][dim][j] = v;
+            else if (kind == 1)
+                sdth[wib][dim][j] = v;
+            else
+                sd2[wib][dim][FINAL ? j : 0] = v;
+        }
     }
     const int b0 = __shfl_sync(0xffffffffu, bl, 0), b1 = __shfl_sync(0xffffffffu, bl, 1),
               b2 = __shfl_sync(0xffffffffu, bl, 2);
     __syncwarp();
     const R* grid = (const R*) dv.grid + S.gridOff;
     const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
-    const int pp = p * p, p3 = pp * p;
     R f[3] = {0, 0, 0}, f2[6] = {0, 0, 0, 0, 0, 0}, pot = 0;
-    constexpr int NIT = P > 0 ? (P * P * P + 31) / 32 : 1;
+    if (P > 0) {
+        // lane -> (j2, j3), loop over j1: sums S_t = sum t1 phi, S_u = sum u1 phi (S_v = sum v1 phi), then the
+        // products with the lane's t2, t3, u2, u3 (v2, v3)
+        constexpr int NPAIR = P * P, ROUNDS = (P * P + 31) / 32;
+        const size_t plane = (size_t) K1 * K2;
 #pragma unroll
-    for (int it = 0; it < NIT; it++)
-    for (int t = lane + 32 * it; t < p3; t += (P > 0 ? p3 : 32)) {
-        const int j1 = t / pp, j2 = (t / p) % p, j3 = t % p;
-        const R t1 = sth[wib][0][j1], u1 = sdth[wib][0][j1];
-        const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
-        const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
-        const int g1 = wrapIndex(b0 - j1, K0), g2 = wrapIndex(b1 - j2, K1), g3 = wrapIndex(b2 - j3, K2);
-        const R ph = grid[((size_t) g1 * K1 + g2) * K2 + g3];
-        f[0] += u1 * t2 * t3 * ph;
-        f[1] += t1 * u2 * t3 * ph;
-        f[2] += t1 * t2 * u3 * ph;
-        if (FINAL) {
-            const R v1 = sd2[wib][0][FINAL ? j1 : 0], v2 = sd2[wib][1][FINAL ? j2 : 0], v3 = sd2[wib][2][FINAL ? j3 : 0];
-            f2[0] += v1 * t2 * t3 * ph;
-            f2[1] += t1 * v2 * t3 * ph;
-            f2[2] += t1 * t2 * v3 * ph;
-            f2[3] += u1 * u2 * t3 * ph;
-            f2[4] += u1 * t2 * u3 * ph;
-            f2[5] += t1 * u2 * u3 * ph;
-            pot += t1 * t2 * t3 * ph;
+        for (int rd = 0; rd < ROUNDS; rd++) {
+            const int pr = lane + 32 * rd;
+            if (pr < NPAIR) {
+                const int j2 = pr / (P > 0 ? P : 1), j3 = pr % (P > 0 ? P : 1);
+                const R* col = grid + (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2);
+                R St = 0, Su = 0, Sv = 0;
+#pragma unroll
+                for (int j1 = 0; j1 < PM; j1++) {
+                    const R ph = col[(size_t) wrapIndex(b0 - j1, K0) * plane];
+                    St += sth[wib][0][j1] * ph;
+                    Su += sdth[wib][0][j1] * ph;
+                    if (FINAL)
+                        Sv += sd2[wib][0][FINAL ? j1 : 0] * ph;
+                }
+                const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
+                const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+                f[0] += Su * t2 * t3;
+                f[1] += St * u2 * t3;
+                f[2] += St * t2 * u3;
+                if (FINAL) {
+                    const R v2 = sd2[wib][1][FINAL ? j2 : 0], v3 = sd2[wib][2][FINAL ? j3 : 0];
+                    f2[0] += Sv * t2 * t3;
+                    f2[1] += St * v2 * t3;
+                    f2[2] += St * t2 * v3;
+                    f2[3] += Su * u2 * t3;
+                    f2[4] += Su * t2 * u3;
+                    f2[5] += St * u2 * u3;
+                    pot += St * t2 * t3;
+                }
+            }
+        }
+    } else {
+        const int pp = p * p, p3 = pp * p;
+        for (int t = lane; t < p3; t += 32) {
+            const int j1 = t / pp, j2 = (t / p) % p, j3 = t % p;
+            const R t1 = sth[wib][0][j1], u1 = sdth[wib][0][j1];
+            const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
+            const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+            const int g1 = wrapIndex(b0 - j1, K0), g2 = wrapIndex(b1 - j2, K1), g3 = wrapIndex(b2 - j3, K2);
+            const R ph = grid[((size_t) g1 * K1 + g2) * K2 + g3];
+            f[0] += u1 * t2 * t3 * ph;
+            f[1] += t1 * u2 * t3 * ph;
+            f[2] += t1 * t2 * u3 * ph;
+            if (FINAL) {
+                const R v1 = sd2[wib][0][FINAL ? j1 : 0], v2 = sd2[wib][1][FINAL ? j2 : 0], v3 = sd2[wib][2][FINAL ? j3 : 0];
+                f2[0] += v1 * t2 * t3 * ph;
+                f2[1] += t1 * v2 * t3 * ph;
+                f2[2] += t1 * t2 * v3 * ph;
+                f2[3] += u1 * u2 * t3 * ph;
+                f2[4] += u1 * t2 * u3 * ph;
+                f2[5] += t1 * u2 * u3 * ph;
+                pot += t1 * t2 * t3 * ph;
+            }
         }
     }
     double F[3] = {(double) f[0], (double) f[1], (double) f[2]};
@@ -671,7 +811,8 @@ __global__ void __launch_bounds__(256) k_pair_field(Dev dv, int gateDone) {
     const R2* grow = (const R2*) dv.G12 + (size_t) slot * dv.cap;
     const R4* dS = (const R4*) dv.dS;
     const int cnt = dv.listCount[slot];
-    double E0 = 0, E1 = 0, E2 = 0;
+    R a0 = 0, a1 = 0, a2 = 0;   // per-lane sums in R (about cnt / GS terms each), across lanes in double
+#pragma unroll 4
     for (int t = lane; t < cnt; t += GS) {
         const uint32_t e = row[t];
         const R2 G = grow[t];
@@ -685,10 +826,11 @@ __global__ void __launch_bounds__(256) k_pair_field(Dev dv, int gateDone) {
         R c = djx * G.y;
         if (WITHQ)
             c += dj.w * G.x;
-        E0 += (double) (c * x0 - dj.x * G.x);
-        E1 += (double) (c * x1 - dj.y * G.x);
-        E2 += (double) (c * x2 - dj.z * G.x);
+        a0 += c * x0 - dj.x * G.x;
+        a1 += c * x1 - dj.y * G.x;
+        a2 += c * x2 - dj.z * G.x;
     }
+    double E0 = a0, E1 = a1, E2 = a2;
     const unsigned gm = groupMask<GS>();
 #pragma unroll
     for (int o = GS / 2; o > 0; o >>= 1) {
@@ -722,10 +864,10 @@ __global__ void __launch_bounds__(256) k_pair_final(Dev dv) {
     const R4 di = dS[slot];
     const R beta = (R) S.beta;
     const int cnt = dv.listCount[slot];
-    double acc[16];
+    R racc[16];
 #pragma unroll
     for (int k = 0; k < 16; k++)
-        acc[k] = 0.0;   // 0 energy, 1-3 force, 4-6 field, 7-15 strain
+        racc[k] = R(0);   // 0 energy, 1-3 force, 4-6 field, 7-15 strain: per-lane sums in R, across lanes in double
     for (int t = lane; t < cnt; t += GS) {
         const uint32_t e = row[t];
         const int js = entrySlot(e);
@@ -746,17 +888,21 @@ __global__ void __launch_bounds__(256) k_pair_final(Dev dv) {
         const R U = qi * qj * G[0] + (qi * djx - qj * dix) * G[1] + didj * G[1] - dix * djx * G[2];
         const R sc = -qi * qj * G[1] - (qi * djx - qj * dix) * G[2] - didj * G[2] + dix * djx * G[3];
         const R dcomp[3] = {dj.x, dj.y, dj.z}, icomp[3] = {di.x, di.y, di.z};
-        acc[0] += 0.5 * (double) U;
+        racc[0] += R(0.5) * U;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const R dedx = sc * x[k] + (qi * dcomp[k] - qj * icomp[k]) * G[1] - (djx * icomp[k] + dix * dcomp[k]) * G[2];
-            acc[1 + k] -= (double) dedx;
-            acc[4 + k] += (double) (qj * x[k] * G[1] - dcomp[k] * G[1] + djx * x[k] * G[2]);
+            racc[1 + k] -= dedx;
+            racc[4 + k] += qj * x[k] * G[1] - dcomp[k] * G[1] + djx * x[k] * G[2];
 #pragma unroll
             for (int b = 0; b < 3; b++)
-                acc[7 + 3 * k + b] += 0.5 * (double) (dedx * x[b]);
+                racc[7 + 3 * k + b] += R(0.5) * dedx * x[b];
         }
     }
+    double acc[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+        acc[k] = racc[k];
     const unsigned gm = groupMask<GS>();
 #pragma unroll
     for (int o = GS / 2; o > 0; o >>= 1)
