@@ -166,6 +166,56 @@ def algorithmic_bytes(kernel, S, precision, it):
     return None
 
 
+def roofline_table(S, kt, it, precision):
+    """Per-kernel algorithmic bandwidth against the measured HBM copy bandwidth; the dominant kernel is the
+    engine's own kernel with the largest share of an evaluation (the cuFFT chain is listed beside it)."""
+    peak, peak_kind = peaks()
+    share = {k: v * launches_per_eval(k, it) for k, v in kt.items()}
+    total = sum(share.values())
+    per = {}
+    for k, ms in kt.items():
+        alg = algorithmic_bytes(k, S, precision, it)
+        ach = alg / (ms * 1e-3) / 1e9 if alg else None
+        per[k] = {"ms_per_launch": ms, "launches_per_eval": launches_per_eval(k, it), "share": share[k] / total,
+                  "bytes_per_launch": alg, "achieved_gbs": ach, "frac": ach / peak if ach else None}
+    own = {k: v for k, v in share.items() if k != "fft_chain"}
+    dom = max(own, key=own.get)
+    return {"kernel": dom, "bound": "hbm", "achieved": per[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
+            "frac": per[dom]["frac"], "peak_source": peak_kind, "traffic": traffic_of(dom),
+            "bytes_per_launch": per[dom]["bytes_per_launch"], "ms_per_launch": kt[dom],
+            "fft_chain_share": per["fft_chain"]["share"], "per_kernel": per}
+
+
+def md_leg(pkg, S, make, lanes, dev, steps=30):
+    """MD-like use: positions move smoothly every step (amplitude 0.01 nm, period 100 steps, random phases,
+    as the reference harness's moving timing, core/cuda/tests/test_cuda.cpp:351-372), new step every call,
+    mu4 predictor; host call with host positions and forces.  Both precisions."""
+    import torch
+    rng = np.random.default_rng(7)
+    phase = rng.uniform(0, 2 * np.pi, S.pos.shape)
+    out = {}
+    for name, prec in (("mixed", pkg.MIXED), ("fp64", pkg.FP64)):
+        eng = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=TOL, max_iter=200,
+                                      peek=0.65, predictor=2, ke=pkg.systems.KE_DEFAULT, precision=prec,
+                                      device=dev.index or 0))
+        eng.set_system(S)
+        eng.set_pair_lanes(lanes)
+        its = []
+        for st in range(10):
+            eng.compute(S.pos + 0.01 * np.sin(2 * np.pi * st / 100 + phase), S.box)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for st in range(10, 10 + steps):
+            r = eng.compute(S.pos + 0.01 * np.sin(2 * np.pi * st / 100 + phase), S.box)
+            its.append(r.iterations)
+        dt = (time.perf_counter() - t0) / steps
+        out[name] = {"evals_per_s": 1.0 / dt, "mean_cg_iterations": float(np.mean(its))}
+        eng.close()
+    out["mixed_over_fp64"] = out["mixed"]["evals_per_s"] / out["fp64"]["evals_per_s"]
+    out["note"] = "host call incl. position generation on the host; predictor mu4"
+    return out
+
+
 def launches_per_eval(kernel, it):
     return {"pair_list": 1, "pair_field": it + 2, "spread": it + 3, "gather": it + 3, "pair_final": 1,
             "fft_chain": it + 3, "cg_update": it}.get(kernel, 1)
@@ -346,28 +396,23 @@ def main():
     mixed.compute(S.pos, S.box)
     it = mixed.iterations()
     kt = mixed.kernel_times(reps=20)
-    share = {k: v * launches_per_eval(k, it) for k, v in kt.items()}
-    dom = max(share, key=share.get)
-    alg = algorithmic_bytes(dom, S, 1, it)
-    peak, peak_kind = peaks()
-    achieved = alg / (kt[dom] * 1e-3) / 1e9 if alg else None
-    roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
-            "traffic": traffic_of(dom), "bytes_per_launch": alg, "ms_per_launch": kt[dom],
-            "kernel_ms": kt, "kernel_share_of_eval": {k: v / sum(share.values()) for k, v in share.items()}}
+    roof = roofline_table(S, kt, it, 1)
+    fp64.compute(S.pos, S.box)
+    kt64 = fp64.kernel_times(reps=10)
+    md = md_leg(pkg, S, make, lanes, dev)
     line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
             "config": config(S, {"parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                                  "pair_lanes": lanes, "cg_iterations": int(np.median(its_mixed))}),
             "fp64": {"value": fp64_value, "unit": "evals/s", "steps": fsteps,
-                     "cg_iterations": int(np.median(its_fp64))},
+                     "cg_iterations": int(np.median(its_fp64)), "kernel_ms": kt64},
             "mixed_over_fp64": value / fp64_value,
             "ns_per_day_2fs": value / world * 86400 * 2e-6,
             "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": S.n * 3 * 8,
                     "d2h_bytes_per_step": S.n * 3 * 8 + 16 * 8},
             "gpu_launches": mixed.kernel_launches() * args.steps,
-            "roofline": roof, "clocks": clocks}
+            "roofline": roof, "clocks": clocks, "md_moving": md}
     if rank == 0 and not args.no_accuracy:
         line["accuracy"] = accuracy(pkg, S, mixed, fp64)
     mixed.close()

@@ -138,6 +138,15 @@ int pgm_engine_set_history(pgm_engine* e, const void* blob);
  * covalent dipole (ncov).  Any output may be NULL.  No counterpart in the reference. */
 int pgm_engine_param_grad(pgm_engine* e, double* dq, double* dradius, double* dalpha, double* dstrength);
 
+/* Adjoint building blocks (no counterpart in the reference).  evaluate_fixed: energy terms, forces (n*3, may be
+ * NULL) and the total field (n*3, may be NULL) at the given induced dipoles mu (n*3), without a solve; keep_list
+ * reuses the previous evaluation's pair list and box (smooth finite-difference probes).  pgm_engine_param_grad
+ * then gives dE/dtheta at those dipoles.  solve: (alpha^-1 - T) x = rhs on the geometry of the last evaluation,
+ * to tolerance tol; *iterations (may be NULL) gets the CG iterations. */
+int pgm_engine_evaluate_fixed(pgm_engine* e, const double* pos, const double* box, const double* mu, int keep_list,
+                              double* forces, double* field, pgm_terms* terms);
+int pgm_engine_solve(pgm_engine* e, const double* rhs, double* x, double tol, int* iterations);
+
 /* Measurement (no counterpart in the reference): the number of this library's kernels the last evaluation
  * ran (cuFFT transforms not counted); average device durations [ms] over reps launches of the main kernels
  * relaunched alone on the engine's stream after an evaluation: ms[0] pair list build, [1] pair field pass,

@@ -311,6 +311,29 @@ int pgm_engine_param_grad(pgm_engine* e, double* dq, double* dradius, double* da
     return guarded([&] { e->e->paramGrad(dq, dradius, dalpha, dstrength); });
 }
 
+int pgm_engine_evaluate_fixed(pgm_engine* e, const double* pos, const double* box, const double* mu, int keep_list,
+                              double* forces, double* field, pgm_terms* terms) {
+    NEED(e);
+    return guarded([&] {
+        if (!pos || !box || !mu)
+            throw std::invalid_argument("pgm_b200: evaluate_fixed needs positions, box and dipoles");
+        double b[3][3];
+        toBox(box, b);
+        fill(terms, e->e->evaluateFixed(pos, b, mu, keep_list != 0, forces, field));
+    });
+}
+
+int pgm_engine_solve(pgm_engine* e, const double* rhs, double* x, double tol, int* iterations) {
+    NEED(e);
+    return guarded([&] {
+        if (!rhs || !x || !(tol > 0))
+            throw std::invalid_argument("pgm_b200: solve needs rhs, x and tol > 0");
+        const int it = e->e->solve(rhs, x, tol);
+        if (iterations)
+            *iterations = it;
+    });
+}
+
 int pgm_engine_kernel_launches(pgm_engine* e) { return (e && e->e) ? e->e->kernelLaunches() : -1; }
 
 int pgm_engine_kernel_times(pgm_engine* e, int reps, double* ms) {

@@ -41,6 +41,8 @@ struct Ctl {
     int guess;               // 0 alpha b, 1 zero, 2 history[h0], 3 mu3, 4 mu4
     int h[4];                // history slots, newest first
     int histSlot;            // slot the solution is pushed to (-1: none)
+    int customRhs;           // 1: the CG solves for the right-hand side already in b (adjoint solves)
+    int fixedMu;             // 1: the final pass uses the induced dipoles already in mu (no solve)
     int posMode;             // 0 positions in posIn, 1 device float4 posDevice, 2 device double posDevice
     int fixedStride;
     const void* posDevice;

@@ -1386,6 +1386,125 @@ void Engine::paramGrad(double* dq, double* dradius, double* dalpha, double* dstr
         }
 }
 
+Terms Engine::evaluateFixed(const double* pos, const double box[3][3], const double* mu, bool keepList,
+                            double* forces, double* field) {
+    Impl& I = *impl;
+    if (!I.atomsSet || I.nsys != 1)
+        throw std::logic_error("pgm_b200: evaluateFixed needs a single-system engine with atoms set");
+    if (keepList && !I.haveResult)
+        throw std::logic_error("pgm_b200: evaluateFixed with keepList needs a previous evaluation");
+    I.checkPositions(pos, 3 * (size_t) I.n);
+    I.selectDevice();
+    for (int attempt = 0; attempt < 4; attempt++) {
+        if (!keepList)
+            I.setBoxes(&box[0][0]);
+        else
+            for (int a = 0; a < 9; a++)
+                if (I.sysHost[0].H[a] != (&box[0][0])[a])
+                    throw std::invalid_argument("pgm_b200: evaluateFixed with keepList needs the list's box");
+        I.prepareControl(true, 0, nullptr, nullptr, 0, 0.0, nullptr);
+        I.hCtl->histSlot = -1;
+        I.hCtl->fixedMu = 1;
+        I.pendingSlot = -1;
+        std::memcpy(I.hSys, I.sysHost.data(), I.nsys * sizeof(SysDev));
+        CU(cudaMemcpyAsync(I.dSys.p, I.hSys, I.nsys * sizeof(SysDev), cudaMemcpyHostToDevice, I.st));
+        CU(cudaMemcpyAsync(I.dCtl.p, I.hCtl, sizeof(Ctl), cudaMemcpyHostToDevice, I.st));
+        CU(cudaMemcpyAsync(I.dPosIn.p, pos, 3 * (size_t) I.n * 8, cudaMemcpyHostToDevice, I.st));
+        CU(cudaMemcpyAsync(I.dMu.p, mu, 3 * (size_t) I.n * 8, cudaMemcpyHostToDevice, I.st));
+        const Dev d = I.makeDev(false, 0);
+        const int tb = (I.n + 255) / 256;
+        CU(cudaMemsetAsync(d.flags, 0, 16 * sizeof(int), I.st));
+        auto body = [&](auto tag) {
+            typedef decltype(tag) R;
+            if (keepList) {
+                k_refresh_positions<<<tb, 256, 0, I.st>>>(d);
+            } else {
+                CU(cudaMemsetAsync(d.cellCount, 0, (size_t) I.totalCells * sizeof(int), I.st));
+                k_prep<<<tb, 256, 0, I.st>>>(d, I.dPosIn.as<double>());
+                k_cell_scan<<<1, 1024, 0, I.st>>>(d);
+                k_cell_scatter<<<tb, 256, 0, I.st>>>(d);
+                k_cell_sort<<<(I.totalCells + 7) / 8, 256, 0, I.st>>>(d);
+                k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(d);
+                k_pair_kernels<R><<<(I.n + 7) / 8, 256, 0, I.st>>>(d);
+            }
+            k_splines<R><<<(3 * I.n + 255) / 256, 256, 0, I.st>>>(d);
+            k_perm<<<tb, 256, 0, I.st>>>(d);
+            k_influence<R><<<dim3(I.convBlocks, I.nsys), 256, 0, I.st>>>(d);
+            CU(cudaGetLastError());
+            I.enqueuePost<R>(I.st, I.side, d);
+        };
+        if (I.mixed())
+            body(float());
+        else
+            body(double());
+        CU(cudaMemcpyAsync(I.hResults, I.dResults.p, I.nsys * NRES * 8, cudaMemcpyDeviceToHost, I.st));
+        CU(cudaMemcpyAsync(I.hFlags, I.dFlags.p, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
+        if (forces)
+            CU(cudaMemcpyAsync(forces, I.dForces.p, 3 * (size_t) I.n * 8, cudaMemcpyDeviceToHost, I.st));
+        if (field)
+            CU(cudaMemcpyAsync(field, I.dEtot.p, 3 * (size_t) I.n * 8, cudaMemcpyDeviceToHost, I.st));
+        CU(cudaStreamSynchronize(I.st));
+        if (I.hFlags[0] > I.cap) {
+            if (keepList)
+                throw std::logic_error("pgm_b200: list overflow with keepList");
+            I.cap = (I.hFlags[0] + I.hFlags[0] / 4 + 31) / 32 * 32;
+            I.allocList();
+            if (I.exec) {
+                cudaGraphExecDestroy(I.exec);
+                I.exec = nullptr;
+            }
+            continue;
+        }
+        I.lastResults.assign(I.hResults, I.hResults + I.nsys * NRES);
+        I.haveResult = true;
+        I.hCtl->fixedMu = 0;
+        return I.termsOf(0);
+    }
+    throw std::runtime_error("pgm_b200: pair list did not fit after growing it");
+}
+
+int Engine::solve(const double* rhs, double* x, double tol) {
+    Impl& I = *impl;
+    if (!I.haveResult || I.nsys != 1)
+        throw std::logic_error("pgm_b200: solve needs a previous single-system evaluation (its geometry)");
+    I.selectDevice();
+    I.prepareControl(true, 0, nullptr, nullptr, 0, 0.0, nullptr);
+    I.hCtl->histSlot = -1;
+    I.hCtl->customRhs = 1;
+    I.hCtl->guess = 1;
+    I.pendingSlot = -1;
+    CU(cudaMemcpyAsync(I.dCtl.p, I.hCtl, sizeof(Ctl), cudaMemcpyHostToDevice, I.st));
+    CU(cudaMemcpyAsync(I.dB.p, rhs, 3 * (size_t) I.n * 8, cudaMemcpyHostToDevice, I.st));
+    Dev d = I.makeDev(false, 0);
+    d.tol = tol;
+    auto run = [&](auto tag) {
+        typedef decltype(tag) R;
+        CU(cudaMemsetAsync(d.flags, 0, 16 * sizeof(int), I.st));
+        k_cg_b<<<(int) I.chunkSys.size(), CHUNK, 0, I.st>>>(d);
+        CU(cudaMemsetAsync(d.grid, 0, I.gridTotal * I.realSize(), I.st));
+        I.fieldPass<R, false>(I.st, I.side, d, 1, d.x, false);
+        k_cg_init<<<(int) I.chunkSys.size(), CHUNK, 0, I.st>>>(d);
+        CU(cudaMemsetAsync(d.grid, 0, I.gridTotal * I.realSize(), I.st));
+        for (int it = 0; it <= I.s.maxIter + 1; it++) {
+            CU(cudaMemcpyAsync(I.hFlags, d.flags, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
+            CU(cudaStreamSynchronize(I.st));
+            if (I.hFlags[2] >= I.nsys)
+                break;
+            I.enqueueIteration<R>(I.st, I.side, d);
+        }
+    };
+    if (I.mixed())
+        run(float());
+    else
+        run(double());
+    double sc[NSCAL];
+    CU(cudaMemcpyAsync(x, I.dX.p, 3 * (size_t) I.n * 8, cudaMemcpyDeviceToHost, I.st));
+    CU(cudaMemcpyAsync(sc, I.dScal.p, sizeof(sc), cudaMemcpyDeviceToHost, I.st));
+    CU(cudaStreamSynchronize(I.st));
+    I.hCtl->customRhs = 0;
+    return (int) sc[SC_IT];
+}
+
 int Engine::kernelLaunches() const {
     const Impl& I = *impl;
     if (!I.haveResult)

@@ -74,6 +74,33 @@ __global__ void k_prep(Dev dv, double* posCopy) {
     dv.Etot[3 * i + 2] = pw[2];
 }
 
+// New positions on an existing pair list (finite-difference probes of the adjoint): PME base and fraction of
+// the new positions, wrapped positions with the wraps of the list's build (so the list's image shifts still
+// apply), slot-order copies refreshed in place.  The pair set is the build's.
+__global__ void k_refresh_positions(Dev dv) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= dv.nAtoms)
+        return;
+    const int i = dv.slotAtom[slot];
+    const SysDev& S = dv.sys[dv.atomSys[i]];
+    const double r[3] = {dv.posIn[3 * i], dv.posIn[3 * i + 1], dv.posIn[3 * i + 2]};
+    double pw[3] = {r[0], r[1], r[2]};
+    for (int a = 0; a < 3; a++) {
+        const double s = __dadd_rn(__dadd_rn(__dmul_rn(r[0], S.recip[a]), __dmul_rn(r[1], S.recip[3 + a])),
+                                   __dmul_rn(r[2], S.recip[6 + a]));
+        const double t = s - floor(s);
+        const double w = (double) S.K[a] * t;
+        const double base = floor(w);
+        dv.pmeBase[3 * i + a] = (int) base;
+        dv.pmeFr[3 * i + a] = w - base;
+        const double n = (double) dv.wrapN[3 * i + a];
+        for (int k = 0; k < 3; k++)
+            pw[k] -= n * S.H[3 * a + k];
+    }
+    dv.posS[slot] = make_double4(pw[0], pw[1], pw[2], dv.q[i]);
+    dv.origS[slot] = make_double4(r[0], r[1], r[2], dv.radius[i]);
+}
+
 // Exclusive scan of the cell counts (one block; totalCells + 1 entries written).
 __global__ void k_cell_scan(Dev dv) {
     __shared__ int warpSums[32];
@@ -937,8 +964,9 @@ __global__ void __launch_bounds__(CHUNK) k_cg_b(Dev dv) {
         const int gi = dv.globalIndex ? dv.globalIndex[i] : i;
         const size_t hs = (size_t) 3 * dv.numGlobal;
         const int guess = dv.ctl->guess, h0 = dv.ctl->h[0], h1 = dv.ctl->h[1], h2 = dv.ctl->h[2], h3 = dv.ctl->h[3];
+        const bool custom = dv.ctl->customRhs != 0;
         for (int k = 0; k < 3; k++) {
-            const double bk = dv.Epair[3 * i + k] + dv.Erec[3 * i + k] + cs * dv.perm[3 * i + k];
+            const double bk = custom ? dv.b[3 * i + k] : dv.Epair[3 * i + k] + dv.Erec[3 * i + k] + cs * dv.perm[3 * i + k];
             dv.b[3 * i + k] = bk;
             v[0] += fabs(al * bk);
             double x0;
@@ -1102,8 +1130,9 @@ __global__ void k_final_prep(Dev dv, int solved) {
     const double al = dv.alpha[i];
     double m2 = 0.0, d2 = 0.0;
     const int gi = dv.globalIndex ? dv.globalIndex[i] : i;
+    const bool fixedMu = dv.ctl->fixedMu != 0;
     for (int k = 0; k < 3; k++) {
-        const double m = solved ? dv.x[3 * i + k] + dv.peek * al * dv.r[3 * i + k] : 0.0;
+        const double m = fixedMu ? dv.mu[3 * i + k] : solved ? dv.x[3 * i + k] + dv.peek * al * dv.r[3 * i + k] : 0.0;
         dv.mu[3 * i + k] = m;
         const double d = dv.perm[3 * i + k] + m;
         dv.dtot[3 * i + k] = d;

@@ -70,6 +70,13 @@ public:
     void getHistory(void* blob) const;
     void setHistory(const void* blob);
     void paramGrad(double* dq, double* dradius, double* dalpha, double* dstrength);
+    // Energy, forces and total field at given induced dipoles (no solve); keepList: the previous evaluation's
+    // pair list, box and wraps (finite-difference probes).  Then paramGrad gives dE/dtheta at these dipoles.
+    Terms evaluateFixed(const double* pos, const double box[3][3], const double* mu, bool keepList, double* forces,
+                        double* field);
+    // (alpha^-1 - T) x = rhs on the geometry of the last evaluation (rows of non-polarizable atoms: 0);
+    // returns the CG iterations.
+    int solve(const double* rhs, double* x, double tol);
 
     // measurement: own kernels per evaluation; average durations [ms] of the main kernels relaunched
     // alone (0 pair list, 1 pair field pass, 2 spread, 3 gather, 4 final pair pass, 5 FFT chain, 6 CG update)

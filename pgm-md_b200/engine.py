@@ -278,6 +278,27 @@ class Engine:
         _check(self._L.pgm_engine_param_grad(self._h, _d(dq), _d(dR), _d(da), _d(dc)))
         return dict(q=dq, radius=dR, alpha=da, cov_strength=dc[: self.ncov])
 
+    def evaluate_fixed(self, pos, box, mu, keep_list=False):
+        """Energy, forces and total field [e/nm^2] at given induced dipoles, no solve (adjoint probes); with
+        keep_list the previous evaluation's pair list and box are reused.  param_grad() then gives dE/dtheta at
+        these dipoles."""
+        pos, box, mu = _f64(pos), _f64(box), _f64(mu)
+        f = np.zeros((self.n, 3))
+        E = np.zeros((self.n, 3))
+        t = _lib.PgmTerms()
+        _check(self._L.pgm_engine_evaluate_fixed(self._h, _d(pos), _d(box), _d(mu), int(bool(keep_list)), _d(f), _d(E),
+                                                 ctypes.byref(t)))
+        return Result(Terms.from_c(t), f, None, 0, {"field": E})
+
+    def solve(self, rhs, tol=1e-10):
+        """x with (alpha^-1 - T) x = rhs on the geometry of the last evaluation (rows of non-polarizable atoms
+        are 0): the adjoint solve, the same symmetric operator as the induced dipoles'."""
+        rhs = _f64(rhs)
+        x = np.zeros((self.n, 3))
+        it = ctypes.c_int()
+        _check(self._L.pgm_engine_solve(self._h, _d(rhs), _d(x), float(tol), ctypes.byref(it)))
+        return x, it.value
+
     def kernel_launches(self):
         return int(self._L.pgm_engine_kernel_launches(self._h))
 
