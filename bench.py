@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="with --profile")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 1024-system leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 98304-atom leg")
+    ap.add_argument("--no-grad", action="store_true", help="skip the parameter-gradient leg")
     return ap.parse_args()
 
 
@@ -70,56 +71,52 @@ def config(S, extra=None):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    """SM clocks and clock-event (throttle) reasons sampled through NVML every 2 ms during the timed region
+    (read-only queries)."""
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown"}
 
     def __init__(self, index):
         self.index = index
-        self.proc = None
-        self.path = None
+        self.samples = []
+        self.reasons = 0
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
+
+    def _run(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            while not self._stop.is_set():
+                self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                try:
+                    self.reasons |= int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))
+                except Exception:
+                    self.reasons |= int(pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h))
+                self._stop.wait(0.002)
+            pynvml.nvmlShutdown()
+        except Exception:
+            pass
 
     def __enter__(self):
-        try:
-            fd, self.path = tempfile.mkstemp(suffix=".csv")
-            os.close(fd)
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
         return self
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self._stop.set()
+        self._thread.join(timeout=5)
 
     def summary(self):
-        if not self.path or not os.path.exists(self.path):
+        if not self.samples:
             return None
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for k, nm in enumerate(names):
-                if f[5 + k].lower() == "active":
-                    reasons.add(nm)
-        os.unlink(self.path)
-        if not sm:
-            return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(v for k, v in self.REASONS.items() if self.reasons & k), "samples": len(self.samples),
+                "source": "NVML, every 2 ms during the timed region"}
 
 
 def peaks():
@@ -421,6 +418,8 @@ def main():
         line["water98304"] = large_leg(pkg, local, world, dist if world > 1 else None)
     if not args.no_batch:
         line["water_batch1024"] = batch_leg(pkg, local, rank, world, dist if world > 1 else None)
+    if not args.no_grad and rank == 0:
+        line["gradients"] = grad_leg(pkg, local)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pkg, S)
     if world > 1:
@@ -513,6 +512,53 @@ def batch_leg(pkg, local, rank, world, dist):
         out["batched_over_sequential"] = out["systems_per_s"] / world / out["sequential_systems_per_s"]
         for e, _ in engines:
             e.close()
+    return out
+
+
+def grad_leg(pkg, local):
+    """Parameter gradients (dE/d per-atom q, R, alpha and per-dipole strength, the adjoint of the stationary
+    energy) of (a) 256 boxes of 64 waters in one batched evaluation and (b) the 8550-atom liquid, mixed
+    precision; and the force-matching gradient of (b) (one adjoint solve, FP64)."""
+    import torch
+    out = {}
+    boxes = [pkg.systems.waters(64, (64 / 0.0334) ** (1 / 3), seed=5000 + k, grid=(13, 13, 13),
+                                cutoff=min(9.0, (64 / 0.0334) ** (1 / 3) / 2), tol=1e-8, lattice=4) for k in range(256)]
+    eng = pkg.Engine(pkg.Settings(cutoff=0.6, beta=3.5, grid=(13, 13, 13), order=6, tol=1e-8, max_iter=300, peek=0.0,
+                                  predictor=0, ke=pkg.systems.KE_DEFAULT, precision=pkg.MIXED, device=local))
+    eng.set_systems(boxes)
+    pos = np.concatenate([s.pos for s in boxes])
+    bx = np.stack([s.box for s in boxes])
+
+    def batch_grad():
+        eng.compute_batch(pos, bx, forces=True)
+        eng.param_grad()
+
+    dt = _timed(batch_grad, 5, 2)
+    out["water64x256_energy_grad"] = {"systems_per_s": 256 / dt, "ms_per_batch": 1e3 * dt}
+    eng.close()
+    _, S = system()
+    eng = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=6, tol=1e-8, max_iter=300, peek=0.0,
+                                  predictor=0, ke=pkg.systems.KE_DEFAULT, precision=pkg.MIXED, device=local))
+    eng.set_system(S)
+
+    def single_grad():
+        eng.compute(S.pos, S.box)
+        eng.param_grad()
+
+    dt = _timed(single_grad, 5, 2)
+    out["dimethylphenol8550_energy_grad"] = {"evals_per_s": 1.0 / dt, "ms": 1e3 * dt}
+    eng.close()
+    import pgm_md_b200.autograd as ag
+    eng = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=6, tol=1e-8, max_iter=300, peek=0.0,
+                                  predictor=0, ke=pkg.systems.KE_DEFAULT, precision=pkg.FP64, device=local))
+    eng.set_system(S)
+    Sp = pkg.systems.perturbed(S, rel=0.05, seed=4)
+    eng.set_system(Sp)
+    Ft = eng.compute(S.pos, S.box).forces
+    eng.set_system(S)
+    dt = _timed(lambda: ag.force_matching_atom_grads(eng, S, Ft, tol=1e-8), 2, 1)
+    out["dimethylphenol8550_force_matching_grad_fp64"] = {"ms": 1e3 * dt}
+    eng.close()
     return out
 
 

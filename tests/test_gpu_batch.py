@@ -69,3 +69,23 @@ def test_batch_tiny_boxes_half_box_cutoff():
         ora = O.Engine(oracle_topology(S), oracle_settings(S))
         e = ora.compute(S.pos, S.box)
         assert abs(out["energies"][k, :5].sum() - e) <= 1e-9 * abs(e)
+
+
+def test_batch_param_gradients():
+    """Parameter gradients of every system of a batch (one launch) against the oracle's analytic gradient."""
+    systems = PKG.systems.water_batch(nsys=5, seed=21, nmin=8, nmax=40, tol=1e-12)
+    eng = batch_engine(systems, PKG.FP64, tol=1e-12)
+    eng.compute_batch(np.concatenate([s.pos for s in systems]), np.stack([s.box for s in systems]))
+    g = eng.param_grad()
+    off, coff = 0, 0
+    for S in systems:
+        ora = O.Engine(oracle_topology(S), oracle_settings(S, tol=1e-12))
+        ora.compute(S.pos, S.box)
+        go = ora.param_gradients()
+        sl = slice(off, off + S.n)
+        cl = slice(coff, coff + len(S.cov_atom))
+        for k, part in (("q", sl), ("radius", sl), ("alpha", sl), ("cov_strength", cl)):
+            ref = go[k]
+            assert np.linalg.norm(g[k][part] - ref) <= 1e-7 * np.linalg.norm(ref), (k, S.n)
+        off += S.n
+        coff += len(S.cov_atom)
