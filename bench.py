@@ -411,7 +411,14 @@ def main():
             "gpu_launches": mixed.kernel_launches() * args.steps,
             "roofline": roof, "clocks": clocks, "md_moving": md}
     if rank == 0 and not args.no_accuracy:
-        line["accuracy"] = accuracy(pkg, S, mixed, fp64)
+        def make_refined():
+            e = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=TOL,
+                                        max_iter=200, peek=0.65, predictor=0, ke=pkg.systems.KE_DEFAULT,
+                                        precision=pkg.MIXED, device=local, refine=True))
+            e.set_system(S)
+            e.set_pair_lanes(lanes)
+            return e
+        line["accuracy"] = accuracy(pkg, S, mixed, fp64, make_refined)
     mixed.close()
     fp64.close()
     if not args.no_large:
@@ -585,14 +592,22 @@ def _oracle_reference(pkg, S, tol):
     return E, e.forces, "numpy oracle, tol 1e-10"
 
 
-def accuracy(pkg, S, mixed, fp64):
-    """Errors of both GPU paths (at the benchmark tolerance) against the FP64 oracle at tol 1e-10."""
+def accuracy(pkg, S, mixed, fp64, make_refined=None):
+    """Errors of the GPU paths (at the benchmark tolerance) against the FP64 oracle at tol 1e-10; the mixed
+    path with FP64 refinement also timed (host call, direct launches)."""
     E0, F0, kind = _oracle_reference(pkg, S, 1e-10)
     out = {"oracle": kind}
-    for name, eng in (("mixed", mixed), ("fp64", fp64)):
+    engines = [("mixed", mixed), ("fp64", fp64)]
+    if make_refined is not None:
+        engines.append(("mixed_fp64_refined", make_refined()))
+    for name, eng in engines:
         r = eng.compute(S.pos, S.box)
         out[name] = {"force_rel_rms": float(np.linalg.norm(r.forces - F0) / np.linalg.norm(F0)),
                      "energy_rel": float(abs(r.energy - E0) / abs(E0)), "iterations": r.iterations}
+        if name == "mixed_fp64_refined":
+            dt = _timed(lambda: eng.compute(S.pos, S.box), 5, 1)
+            out[name]["evals_per_s_host_call"] = 1.0 / dt
+            eng.close()
     return out
 
 

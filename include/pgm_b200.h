@@ -48,6 +48,9 @@ typedef struct pgm_settings {
     int precision;       /* PGM_PRECISION_FP64 or PGM_PRECISION_MIXED */
     int zero_guess;      /* 1: initial guess mu = 0 when the predictor has no history (instead of alpha E_perm) */
     int polarizable;     /* 0: no induced dipoles (pgmcore::Settings::polarizable) */
+    int refine;          /* mixed precision: 1 = FP64 iterative refinement of the induced dipoles (the residual
+                            E_perm - (alpha^-1 - T) mu recomputed with FP64 pair and PME arithmetic, corrections
+                            solved with the FP32 operator) */
 } pgm_settings;
 
 /* pgmcuda::Terms (core/cuda/pgm_cuda.h:41-45). gvdw is always 0 (combination-rule GVDW is not part of this

@@ -21,7 +21,8 @@ P_LL = ctypes.POINTER(ctypes.c_longlong)
 class PgmSettings(ctypes.Structure):
     _fields_ = [("cutoff", c_double), ("beta", c_double), ("grid", c_int * 3), ("order", c_int), ("tol", c_double),
                 ("max_iter", c_int), ("peek", c_double), ("predictor", c_int), ("ke", c_double), ("device", c_int),
-                ("skin", c_double), ("precision", c_int), ("zero_guess", c_int), ("polarizable", c_int)]
+                ("skin", c_double), ("precision", c_int), ("zero_guess", c_int), ("polarizable", c_int),
+                ("refine", c_int)]
 
 
 class PgmTerms(ctypes.Structure):

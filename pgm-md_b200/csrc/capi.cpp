@@ -55,6 +55,7 @@ pgmb200::Settings toSettings(const pgm_settings* s) {
     o.precision = s->precision;
     o.zeroGuess = s->zero_guess;
     o.polarizable = s->polarizable;
+    o.refine = s->refine;
     return o;
 }
 
@@ -103,6 +104,7 @@ void pgm_settings_default(pgm_settings* s) {
     s->precision = d.precision;
     s->zero_guess = d.zeroGuess;
     s->polarizable = d.polarizable;
+    s->refine = d.refine;
 }
 
 const char* pgm_last_error(void) { return g_lastError.c_str(); }

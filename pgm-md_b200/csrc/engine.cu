@@ -15,6 +15,7 @@
 #include <stdexcept>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 namespace pgmb200 {
@@ -157,6 +158,9 @@ struct Engine::Impl {
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
         dGradQ, dGradR;
+    // FP64 shadow of the mixed path for the iterative refinement
+    Buf dG12d, dDSd, dGridD, dSpecD, dInflD, dSplD, dB64, dXsave;
+    std::vector<std::pair<cufftHandle, cufftHandle>> plans64;
     // pinned host staging
     double* hPos = nullptr;
     float* hPosF = nullptr;
@@ -199,13 +203,19 @@ struct Engine::Impl {
                 cufftDestroy(g.c2r);
         }
         groups.clear();
+        for (auto& pl : plans64) {
+            cufftDestroy(pl.first);
+            cufftDestroy(pl.second);
+        }
+        plans64.clear();
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
                       &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dG12, &dFlags, &dDS,
                       &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
                       &dCovByAtomOff, &dCovByAtom, &dCovByPartnerOff, &dCovByPartner, &dChunkSys, &dChunkBegin,
-                      &dChunkEnd, &dHist, &dGlobal, &dCtl, &dGradQ, &dGradR};
+                      &dChunkEnd, &dHist, &dGlobal, &dCtl, &dGradQ, &dGradR, &dG12d, &dDSd, &dGridD, &dSpecD,
+                      &dInflD, &dSplD, &dB64, &dXsave};
         for (Buf* b : all)
             b->release();
         if (hPos) cudaFreeHost(hPos);
@@ -413,6 +423,11 @@ struct Engine::Impl {
             if (g.c2r) cufftDestroy(g.c2r);
         }
         groups.clear();
+        for (auto& pl : plans64) {
+            cufftDestroy(pl.first);
+            cufftDestroy(pl.second);
+        }
+        plans64.clear();
         // systems grouped by grid shape; grid storage group after group
         std::map<std::array<int, 3>, std::vector<int>> byShape;
         for (int k = 0; k < nsys; k++)
@@ -463,6 +478,12 @@ struct Engine::Impl {
                                 g.count));
             CUFFT(cufftPlanMany(&g.c2r, 3, dims, nullptr, 1, sn, nullptr, 1, gn, mixed() ? CUFFT_C2R : CUFFT_Z2D,
                                 g.count));
+            if (refining()) {
+                cufftHandle a, b;
+                CUFFT(cufftPlanMany(&a, 3, dims, nullptr, 1, gn, nullptr, 1, sn, CUFFT_D2Z, g.count));
+                CUFFT(cufftPlanMany(&b, 3, dims, nullptr, 1, sn, nullptr, 1, gn, CUFFT_Z2D, g.count));
+                plans64.push_back({a, b});
+            }
         }
         if (std::getenv("PGM_B200_TRACE"))
             for (auto& g : groups)
@@ -534,6 +555,15 @@ struct Engine::Impl {
         dGrid.ensure(gridTotal * R);
         dSpec.ensure(specTotal * 2 * R);
         dInfl.ensure(specTotal * R);
+        if (refining()) {
+            dGridD.ensure(gridTotal * 8);
+            dSpecD.ensure(specTotal * 16);
+            dInflD.ensure(specTotal * 8);
+            dDSd.ensure(n * sizeof(double4));
+            dSplD.ensure((size_t) n * 9 * MAXP * 8);
+            dB64.ensure(3 * (size_t) n * 8);
+            dXsave.ensure(3 * (size_t) n * 8);
+        }
         upload(dModuli, moduliHost, st);
         upload(dChunkSys, chunkSys, st);
         upload(dChunkBegin, chunkBegin, st);
@@ -649,6 +679,23 @@ struct Engine::Impl {
     void allocList() {
         dList.ensure((size_t) n * cap * sizeof(uint32_t));
         dG12.ensure((size_t) n * cap * 2 * realSize());
+        if (refining())
+            dG12d.ensure((size_t) n * cap * 16);
+    }
+
+    bool refining() const { return mixed() && s.refine && s.polarizable; }
+
+    // The mixed path's device pointers with the FP64 shadow buffers in place of the R-typed ones.
+    Dev makeDev64() {
+        Dev d = makeDev(false, 0);
+        d.G12 = dG12d.p;
+        d.dS = dDSd.p;
+        d.grid = dGridD.p;
+        d.spec = dSpecD.p;
+        d.infl = dInflD.p;
+        d.spl = dSplD.p;
+        d.gridWords = gridTotal * 2;
+        return d;
     }
 
     Dev makeDev(bool forGraph, cudaGraphConditionalHandle h) {
@@ -743,14 +790,18 @@ struct Engine::Impl {
     // ------------------------------------------------------------------------------------------ launches
     template <typename R> void fftChain(cudaStream_t sm, const Dev& d, bool energy, bool gate) {
         typedef typename CplxT<R>::T C;
-        for (auto& g : groups) {
-            CUFFT(cufftSetStream(g.r2c, sm));
+        constexpr bool dbl = std::is_same<R, double>::value;
+        const bool shadow = dbl && mixed();   // the FP64 refinement's transforms of a mixed engine
+        for (size_t k = 0; k < groups.size(); k++) {
+            auto& g = groups[k];
+            const cufftHandle plan = shadow ? plans64[k].first : g.r2c;
+            CUFFT(cufftSetStream(plan, sm));
             R* gp = (R*) d.grid + g.gridOff;
             C* sp = (C*) d.spec + g.specOff;
-            if (mixed())
-                CUFFT(cufftExecR2C(g.r2c, (cufftReal*) gp, (cufftComplex*) sp));
+            if (!dbl)
+                CUFFT(cufftExecR2C(plan, (cufftReal*) gp, (cufftComplex*) sp));
             else
-                CUFFT(cufftExecD2Z(g.r2c, (cufftDoubleReal*) gp, (cufftDoubleComplex*) sp));
+                CUFFT(cufftExecD2Z(plan, (cufftDoubleReal*) gp, (cufftDoubleComplex*) sp));
         }
         dim3 cg(convBlocks, nsys);
         if (energy)
@@ -758,14 +809,16 @@ struct Engine::Impl {
         else
             k_conv<R, false><<<cg, 256, 0, sm>>>(d, gate ? 1 : 0);
         CU(cudaGetLastError());
-        for (auto& g : groups) {
-            CUFFT(cufftSetStream(g.c2r, sm));
+        for (size_t k = 0; k < groups.size(); k++) {
+            auto& g = groups[k];
+            const cufftHandle plan = shadow ? plans64[k].second : g.c2r;
+            CUFFT(cufftSetStream(plan, sm));
             R* gp = (R*) d.grid + g.gridOff;
             C* sp = (C*) d.spec + g.specOff;
-            if (mixed())
-                CUFFT(cufftExecC2R(g.c2r, (cufftComplex*) sp, (cufftReal*) gp));
+            if (!dbl)
+                CUFFT(cufftExecC2R(plan, (cufftComplex*) sp, (cufftReal*) gp));
             else
-                CUFFT(cufftExecZ2D(g.c2r, (cufftDoubleComplex*) sp, (cufftDoubleReal*) gp));
+                CUFFT(cufftExecZ2D(plan, (cufftDoubleComplex*) sp, (cufftDoubleReal*) gp));
         }
     }
 
@@ -960,6 +1013,70 @@ struct Engine::Impl {
         enqueuePost<R>(st, side, d);
     }
 
+    // Mixed path with FP64 iterative refinement: the FP32-operator CG, then up to three rounds of
+    //   r = E_perm - (alpha^-1 - T) x   with FP64 pair and PME arithmetic (FP64 G1, G2, splines, grids, D2Z/Z2D),
+    //   stop when max|alpha r| / mean|alpha E_perm| <= tol, else solve (alpha^-1 - T) delta = r with the FP32-operator
+    //   CG and x += delta;
+    // the peek step then uses the FP64 residual.  Direct launches (the rounds depend on host-read residuals).
+    void runRefined() {
+        static const bool trace = std::getenv("PGM_B200_TRACE") != nullptr;
+        const Dev d = makeDev(false, 0);
+        const Dev d64 = makeDev64();
+        auto cgLoop = [&]() {
+            for (int it = 0; it <= s.maxIter + 1; it++) {
+                CU(cudaMemcpyAsync(hFlags, d.flags, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));
+                CU(cudaStreamSynchronize(st));
+                if (hFlags[2] >= nsys)
+                    break;
+                enqueueIteration<float>(st, side, d);
+            }
+        };
+        enqueuePre<float>(st, side, d);
+        cgLoop();
+        // FP64 geometry: G1, G2, splines and influence in double
+        k_pair_kernels<double><<<(n + 7) / 8, 256, 0, st>>>(d64);
+        k_splines<double><<<(3 * n + 255) / 256, 256, 0, st>>>(d64);
+        k_influence<double><<<dim3(convBlocks, nsys), 256, 0, st>>>(d64);
+        CU(cudaMemsetAsync(d64.grid, 0, gridTotal * 8, st));
+        fieldPass<double, true>(st, side, d64, 0, d.perm, false);
+        k_refine_b<<<(n + 255) / 256, 256, 0, st>>>(d64, dB64.as<double>());
+        CU(cudaGetLastError());
+        for (int round = 0; round < 4; round++) {
+            CU(cudaMemsetAsync(d64.grid, 0, gridTotal * 8, st));
+            CU(cudaMemsetAsync(d.flags + 2, 0, sizeof(int), st));
+            fieldPass<double, false>(st, side, d64, 1, d.x, false);
+            k_refine_res<<<(int) chunkSys.size(), CHUNK, 0, st>>>(d64, dB64.as<double>());
+            CU(cudaMemcpyAsync(hFlags, d.flags, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            CU(cudaStreamSynchronize(st));
+            if (trace) {
+                double sc[NSCAL];
+                CU(cudaMemcpy(sc, d.scal, sizeof(sc), cudaMemcpyDeviceToHost));
+                fprintf(stderr, "pgm_b200 trace: refinement round %d: FP64 residual %.3e (system 0)\n", round,
+                        sc[SC_ERR]);
+            }
+            if (hFlags[2] >= nsys || round == 3)
+                break;
+            // correction: (alpha^-1 - T) delta = r with the FP32 operator, from delta = 0
+            CU(cudaMemcpyAsync(dXsave.p, d.x, 3 * (size_t) n * 8, cudaMemcpyDeviceToDevice, st));
+            hCtl->customRhs = 1;
+            hCtl->guess = 1;
+            CU(cudaMemcpyAsync(dCtl.p, hCtl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+            CU(cudaMemsetAsync(d.flags, 0, 16 * sizeof(int), st));
+            k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, st>>>(d);
+            CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), st));
+            fieldPass<float, false>(st, side, d, 1, d.x, false);
+            k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, st>>>(d);
+            CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), st));
+            cgLoop();
+            k_refine_add<<<(3 * n + 255) / 256, 256, 0, st>>>(d, dXsave.as<double>());
+            hCtl->customRhs = 0;
+            CU(cudaMemcpyAsync(dCtl.p, hCtl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+            CU(cudaGetLastError());
+        }
+        // r now holds the FP64 residual of x: the final pass's peek uses it
+        enqueuePost<float>(st, side, d);
+    }
+
     // ------------------------------------------------------------------------------------------ evaluation
     void prepareControl(bool newStep, int posMode, const void* posDevice, long long* forceFixed, int stride,
                         double fixedScale, double* forcesOut) {
@@ -1004,7 +1121,9 @@ struct Engine::Impl {
         std::memcpy(hSys, sysHost.data(), nsys * sizeof(SysDev));
         CU(cudaMemcpyAsync(dSys.p, hSys, nsys * sizeof(SysDev), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(dCtl.p, hCtl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
-        if (useGraph) {
+        if (refining()) {
+            runRefined();
+        } else if (useGraph) {
             if (!exec) {
                 try {
                     if (mixed())
@@ -1018,7 +1137,9 @@ struct Engine::Impl {
                 }
             }
         }
-        if (useGraph)
+        if (refining())
+            ;
+        else if (useGraph)
             CU(cudaGraphLaunch(exec, st));
         else if (mixed())
             runDirect<float>();

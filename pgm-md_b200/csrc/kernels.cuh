@@ -1034,6 +1034,55 @@ __global__ void __launch_bounds__(CHUNK) k_cg_init(Dev dv) {
     }
 }
 
+// FP64 refinement, permanent field: b64 = E_pair + E_rec + cs p (all FP64 arithmetic).
+__global__ void k_refine_b(Dev dv, double* b64) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= dv.nAtoms)
+        return;
+    const SysDev& S = dv.sys[dv.atomSys[i]];
+    const double cs = 4.0 * S.beta * S.beta * S.beta / (3.0 * SQRT_PI);
+    for (int k = 0; k < 3; k++)
+        b64[3 * i + k] = dv.Epair[3 * i + k] + dv.Erec[3 * i + k] + cs * dv.perm[3 * i + k];
+}
+
+// FP64 refinement, residual: r = b64 - (x/alpha - T x) with T x from FP64 pair and PME passes (rows of
+// polarizable atoms), written to the CG's right-hand side b and to r; per system err = max|alpha r| /
+// mean|alpha b64| in scal[SC_ERR], the count of systems within tol in flags[2].
+__global__ void __launch_bounds__(CHUNK) k_refine_res(Dev dv, const double* b64) {
+    const int chunk = blockIdx.x;
+    const int s = dv.chunkSys[chunk];
+    const SysDev& S = dv.sys[s];
+    const int i = dv.chunkBegin[chunk] + threadIdx.x;
+    double v[2] = {0.0, 0.0};
+    if (i < dv.chunkEnd[chunk]) {
+        const double cs = 4.0 * S.beta * S.beta * S.beta / (3.0 * SQRT_PI);
+        const double al = dv.alpha[i];
+        for (int k = 0; k < 3; k++) {
+            const double xk = dv.x[3 * i + k];
+            const double Tx = dv.Epair[3 * i + k] + dv.Erec[3 * i + k] + cs * xk;
+            const double rk = (al > 0) ? b64[3 * i + k] - (xk / al - Tx) : 0.0;
+            dv.b[3 * i + k] = rk;
+            dv.r[3 * i + k] = rk;
+            v[0] += fabs(al * b64[3 * i + k]);
+            v[1] = fmax(v[1], fabs(al * rk));
+        }
+    }
+    double tot[2];
+    if (chunkFinish<2>(dv, chunk, s, v, 2u, tot) && threadIdx.x == 0) {
+        const double norm = tot[0] / (3.0 * (S.atomEnd - S.atomBegin)) + 1e-300;
+        dv.scal[s * NSCAL + SC_ERR] = tot[1] / norm;
+        if (tot[1] / norm <= dv.tol)
+            atomicAdd(&dv.flags[2], 1);
+    }
+}
+
+// x = xsave + delta (the correction solved into x).
+__global__ void k_refine_add(Dev dv, const double* xsave) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < 3 * dv.nAtoms)
+        dv.x[t] += xsave[t];
+}
+
 // Ap = p/alpha - T p and p.Ap, then alph = rz / p.Ap per system (core/pgm_core.cpp:363-364).
 __global__ void __launch_bounds__(CHUNK) k_cg_a(Dev dv) {
     const int chunk = blockIdx.x;

@@ -25,6 +25,7 @@ struct Settings {
     int precision = 1;    // 0 FP64, 1 mixed
     int zeroGuess = 0;
     int polarizable = 1;
+    int refine = 0;       // mixed: FP64 iterative refinement of the induced dipoles
 };
 
 // pgmcuda::Terms (core/cuda/pgm_cuda.h:41-45).

@@ -68,6 +68,7 @@ class Settings:
     precision: int = MIXED
     zero_guess: bool = False
     polarizable: bool = True
+    refine: bool = False
 
     def to_c(self):
         s = _lib.PgmSettings()
@@ -77,6 +78,7 @@ class Settings:
         s.order, s.tol, s.max_iter, s.peek = int(self.order), self.tol, int(self.max_iter), self.peek
         s.predictor, s.ke, s.device, s.skin = int(self.predictor), self.ke, int(self.device), self.skin
         s.precision, s.zero_guess, s.polarizable = int(self.precision), int(self.zero_guess), int(self.polarizable)
+        s.refine = int(self.refine)
         return s
 
 
