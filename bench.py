@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run for ncu: only warmup + steps evaluations of one precision, no other legs")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="with --profile")
+    ap.add_argument("--profile-workload", default=WORKLOAD, choices=[WORKLOAD, "water98304"],
+                    help="with --profile: the system evaluated")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 1024-system leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 98304-atom leg")
     ap.add_argument("--no-grad", action="store_true", help="skip the parameter-gradient leg")
@@ -308,6 +310,8 @@ def main():
 
     stream = torch.cuda.current_stream(dev)
     if args.profile:
+        if args.profile_workload == "water98304":
+            S = pkg.systems.water98304(tol=TOL)
         eng = make(pkg.MIXED if args.precision == "mixed" else pkg.FP64)
         pos_p = torch.from_numpy(S.pos).to(dev).contiguous()
         f_p = torch.zeros((S.n, 3), dtype=torch.float64, device=dev)
