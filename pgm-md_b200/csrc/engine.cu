@@ -262,9 +262,9 @@ struct Engine::Impl {
         CU(cudaMallocHost((void**) &hFlags, 16 * sizeof(int)));
         CU(cudaMallocHost((void**) &hCtl, sizeof(Ctl)));
         useGraph = envInt("PGM_B200_NO_GRAPH", 0) == 0;
-        pairGS = envInt("PGM_B200_PAIR_LANES", 8);
+        pairGS = envInt("PGM_B200_PAIR_LANES", 32);
         if (pairGS != 4 && pairGS != 8 && pairGS != 16 && pairGS != 32)
-            pairGS = 8;
+            pairGS = 32;
     }
 
     void selectDevice() {
@@ -852,8 +852,8 @@ struct Engine::Impl {
         switch (pairGS) {
         case 4: k_pair_field<R, WITHQ, 4><<<blocks, 256, 0, sm>>>(d, gate); break;
         case 16: k_pair_field<R, WITHQ, 16><<<blocks, 256, 0, sm>>>(d, gate); break;
-        case 32: k_pair_field<R, WITHQ, 32><<<blocks, 256, 0, sm>>>(d, gate); break;
-        default: k_pair_field<R, WITHQ, 8><<<blocks, 256, 0, sm>>>(d, gate);
+        case 8: k_pair_field<R, WITHQ, 8><<<blocks, 256, 0, sm>>>(d, gate); break;
+        default: k_pair_field<R, WITHQ, 32><<<blocks, 256, 0, sm>>>(d, gate);
         }
         CU(cudaGetLastError());
     }
@@ -880,15 +880,23 @@ struct Engine::Impl {
         k_cell_scan<<<1, 1024, 0, sm>>>(d);
         k_cell_scatter<<<tb, 256, 0, sm>>>(d);
         k_cell_sort<<<(totalCells + 7) / 8, 256, 0, sm>>>(d);
-        k_build_list<<<totalCells, LIST_THREADS, 0, sm>>>(d);
-        k_pair_kernels<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
-        k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
-        k_perm<<<tb, 256, 0, sm>>>(d);
-        k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
         CU(cudaGetLastError());
         if (s.polarizable) {
+            // the pair list (side stream) beside the permanent field's PME half (main stream)
+            CU(cudaEventRecord(evFork, sm));
+            CU(cudaStreamWaitEvent(sd, evFork, 0));
+            k_build_list<<<totalCells, LIST_THREADS, 0, sd>>>(d);
+            k_pair_kernels<R><<<(n + 7) / 8, 256, 0, sd>>>(d);
+            CU(cudaEventRecord(evJoin, sd));
+            k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
+            k_perm<<<tb, 256, 0, sm>>>(d);
+            k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
-            fieldPass<R, true>(sm, sd, d, 0, d.perm, false);
+            launchSpread<R>(sm, d, 0, d.perm);
+            fftChain<R>(sm, d, false, false);
+            CU(cudaStreamWaitEvent(sm, evJoin, 0));
+            pairField<R, true>(sm, d, 0);
+            launchGather<R, false>(sm, d, 0);
             k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
             CU(cudaGetLastError());
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
@@ -897,6 +905,13 @@ struct Engine::Impl {
             CU(cudaGetLastError());
             // the loop's first spread needs a clear grid (each iteration clears it for the next one)
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
+        } else {
+            k_build_list<<<totalCells, LIST_THREADS, 0, sm>>>(d);
+            k_pair_kernels<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
+            k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
+            k_perm<<<tb, 256, 0, sm>>>(d);
+            k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
+            CU(cudaGetLastError());
         }
     }
 
