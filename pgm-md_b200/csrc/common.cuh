@@ -358,14 +358,29 @@ __device__ __forceinline__ bool chunkFinish(const Dev& dv, int chunk, int s, dou
         return false;
     __threadfence();
     const SysDev& S = dv.sys[s];
+    // the system's chunk partials in a fixed order: value k = tid mod 16, chunk group tid / 16 takes chunks
+    // group, group + 16, ...; the groups' sums then in group order (deterministic)
+    __shared__ double sgrp[CHUNK / 16][NV];
+    {
+        const int k = threadIdx.x & 15, grp = threadIdx.x >> 4;
+        if (k < NV) {
+            const bool isMax = (maxMask >> k) & 1u;
+            double acc = 0.0;
+#pragma unroll 4
+            for (int c = grp; c < S.chunkCount; c += CHUNK / 16) {
+                const double val = __ldcg(&dv.partial[(size_t) (S.chunkFirst + c) * 16 + k]);
+                acc = isMax ? fmax(acc, val) : acc + val;
+            }
+            sgrp[grp][k] = acc;
+        }
+    }
+    __syncthreads();
     if (threadIdx.x < NV) {
         const int k = threadIdx.x;
         const bool isMax = (maxMask >> k) & 1u;
         double acc = 0.0;
-        for (int c = 0; c < S.chunkCount; c++) {
-            const double val = __ldcg(&dv.partial[(size_t) (S.chunkFirst + c) * 16 + k]);
-            acc = isMax ? fmax(acc, val) : acc + val;
-        }
+        for (int g = 0; g < CHUNK / 16; g++)
+            acc = isMax ? fmax(acc, sgrp[g][k]) : acc + sgrp[g][k];
         stot[k] = acc;
     }
     __syncthreads();

@@ -149,6 +149,7 @@ struct Engine::Impl {
     int totalCells = 0, cellCapacity = 0;
     int cap = 0;
     int convBlocks = 1;
+    bool usePlanes = false;
     bool configured = false, atomsSet = false;
 
     // device
@@ -175,6 +176,7 @@ struct Engine::Impl {
     cudaGraphExec_t exec = nullptr;
     bool useGraph = true;
     int pairGS = 8;
+    int pairSmem = 0;
 
     // predictor history: NHIST slots, newest at head
     static constexpr int NHIST = 5;
@@ -254,7 +256,11 @@ struct Engine::Impl {
             CU(cudaSetDevice(s.device));
         CU(cudaGetDevice(&devId));
         CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        CU(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        // the side stream (list build, transforms) carries the critical path beside the pair passes: it runs at
+        // the highest priority, in the graph too (node priorities)
+        int prLeast = 0, prGreatest = 0;
+        CU(cudaDeviceGetStreamPriorityRange(&prLeast, &prGreatest));
+        CU(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, prGreatest));
         CU(cudaEventCreateWithFlags(&evFork, cudaEventDisableTiming));
         CU(cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming));
         CU(cudaEventCreateWithFlags(&evCaller, cudaEventDisableTiming));
@@ -263,6 +269,23 @@ struct Engine::Impl {
         CU(cudaMallocHost((void**) &hCtl, sizeof(Ctl)));
         useGraph = envInt("PGM_B200_NO_GRAPH", 0) == 0;
         pairGS = envInt("PGM_B200_PAIR_LANES", 32);
+        // the field pair pass runs beside the transforms of the same pass: at most pairBlocks of its blocks per SM
+        // (a shared-memory reservation it does not use), so the transform kernels find room at once
+        const int pairBlocks = envInt("PGM_B200_PAIR_BLOCKS", 3);
+        int smPerSM = 0, smPerBlock = 0;
+        CU(cudaDeviceGetAttribute(&smPerSM, cudaDevAttrMaxSharedMemoryPerMultiprocessor, devId));
+        CU(cudaDeviceGetAttribute(&smPerBlock, cudaDevAttrMaxSharedMemoryPerBlockOptin, devId));
+        pairSmem = pairBlocks > 0 ? std::min(smPerBlock, smPerSM / (pairBlocks + 1) + 1024) : 0;
+        if (pairSmem > 0)
+            for (auto f : {(const void*) k_pair_field<float, false, 32>, (const void*) k_pair_field<float, true, 32>,
+                           (const void*) k_pair_field<double, false, 32>, (const void*) k_pair_field<double, true, 32>,
+                           (const void*) k_pair_field<float, false, 16>, (const void*) k_pair_field<float, true, 16>,
+                           (const void*) k_pair_field<double, false, 16>, (const void*) k_pair_field<double, true, 16>,
+                           (const void*) k_pair_field<float, false, 8>, (const void*) k_pair_field<float, true, 8>,
+                           (const void*) k_pair_field<double, false, 8>, (const void*) k_pair_field<double, true, 8>,
+                           (const void*) k_pair_field<float, false, 4>, (const void*) k_pair_field<float, true, 4>,
+                           (const void*) k_pair_field<double, false, 4>, (const void*) k_pair_field<double, true, 4>})
+                CU(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, pairSmem));
         if (pairGS != 4 && pairGS != 8 && pairGS != 16 && pairGS != 32)
             pairGS = 32;
     }
@@ -490,6 +513,23 @@ struct Engine::Impl {
                 fprintf(stderr, "pgm_b200 trace: FFT group %dx%dx%d, %d systems from %d, grid offset %lld, spectrum "
                         "offset %lld\n", g.K[0], g.K[1], g.K[2], g.count, g.first, g.gridOff, g.specOff);
         convBlocks = std::max(1, std::min(512, (maxSpec + 255) / 256));
+        // the plane transforms (one system, 2-3-5 grid up to PLANE_MAXK) on request: alone they take less time than
+        // the cuFFT chain, beside the pair pass of the same field pass they take more
+        usePlanes = nsys == 1 && envInt("PGM_B200_PLANE_FFT", 0) != 0;
+        for (int a = 0; a < 3 && usePlanes; a++) {
+            int rad[8];
+            usePlanes = sysK[0][a] <= PLANE_MAXK && fftRadices(sysK[0][a], rad) > 0;
+        }
+        if (usePlanes) {
+            CU(cudaFuncSetAttribute(k_planes_fwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int) planeSmem<float>()));
+            CU(cudaFuncSetAttribute(k_planes_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int) planeSmem<double>()));
+            CU(cudaFuncSetAttribute(k_planes_inv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int) planeSmem<float>()));
+            CU(cudaFuncSetAttribute(k_planes_inv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int) planeSmem<double>()));
+        }
         // chunks
         chunkSys.clear();
         chunkBegin.clear();
@@ -822,6 +862,21 @@ struct Engine::Impl {
         }
     }
 
+    // Shared memory of the plane kernels: two twiddle tables and two transform buffers.
+    template <typename R> static size_t planeSmem() {
+        return (2 * PLANE_MAXK + 2 * PLANE_BUF) * sizeof(typename CplxT<R>::T);
+    }
+
+    // The transform pair with the influence product in three kernels (one system, small 2-3-5 grid).
+    template <typename R> void planeChain(cudaStream_t sm, const Dev& d) {
+        const SysDev& S = sysHost[0];
+        const int lines = S.K[1] * (S.K[2] / 2 + 1);
+        k_planes_fwd<R><<<S.K[0], PLANE_THREADS, planeSmem<R>(), sm>>>(d);
+        k_lines_x<R><<<(lines + PLANE_LINES - 1) / PLANE_LINES, LINES_THREADS, 0, sm>>>(d);
+        k_planes_inv<R><<<S.K[0], PLANE_THREADS, planeSmem<R>(), sm>>>(d);
+        CU(cudaGetLastError());
+    }
+
     template <typename R> void launchSpread(cudaStream_t sm, const Dev& d, int mode, double* vec) {
         const int wb = (n + 7) / 8;
         switch (s.order) {
@@ -849,11 +904,12 @@ struct Engine::Impl {
     template <typename R, bool WITHQ> void pairField(cudaStream_t sm, const Dev& d, int gate) {
         const long long threads = (long long) n * pairGS;
         const int blocks = (int) ((threads + 255) / 256);
+        const int sh = pairSmem;
         switch (pairGS) {
-        case 4: k_pair_field<R, WITHQ, 4><<<blocks, 256, 0, sm>>>(d, gate); break;
-        case 16: k_pair_field<R, WITHQ, 16><<<blocks, 256, 0, sm>>>(d, gate); break;
-        case 8: k_pair_field<R, WITHQ, 8><<<blocks, 256, 0, sm>>>(d, gate); break;
-        default: k_pair_field<R, WITHQ, 32><<<blocks, 256, 0, sm>>>(d, gate);
+        case 4: k_pair_field<R, WITHQ, 4><<<blocks, 256, sh, sm>>>(d, gate); break;
+        case 16: k_pair_field<R, WITHQ, 16><<<blocks, 256, sh, sm>>>(d, gate); break;
+        case 8: k_pair_field<R, WITHQ, 8><<<blocks, 256, sh, sm>>>(d, gate); break;
+        default: k_pair_field<R, WITHQ, 32><<<blocks, 256, sh, sm>>>(d, gate);
         }
         CU(cudaGetLastError());
     }
@@ -865,7 +921,10 @@ struct Engine::Impl {
         launchSpread<R>(sm, d, spreadMode, vec);
         CU(cudaEventRecord(evFork, sm));
         CU(cudaStreamWaitEvent(sd, evFork, 0));
-        fftChain<R>(sd, d, false, gate);
+        if (usePlanes)
+            planeChain<R>(sd, d);
+        else
+            fftChain<R>(sd, d, false, gate);
         pairField<R, WITHQ>(sm, d, gate ? 1 : 0);
         CU(cudaEventRecord(evJoin, sd));
         CU(cudaStreamWaitEvent(sm, evJoin, 0));
@@ -893,7 +952,10 @@ struct Engine::Impl {
             k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
             launchSpread<R>(sm, d, 0, d.perm);
-            fftChain<R>(sm, d, false, false);
+            if (usePlanes)
+                planeChain<R>(sm, d);
+            else
+                fftChain<R>(sm, d, false, false);
             CU(cudaStreamWaitEvent(sm, evJoin, 0));
             pairField<R, true>(sm, d, 0);
             launchGather<R, false>(sm, d, 0);
@@ -1001,7 +1063,7 @@ struct Engine::Impl {
             }
             CU(cudaStreamEndCapture(st, &body));
         }
-        CU(cudaGraphInstantiate(&exec, graph, 0));
+        CU(cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority));
         CU(cudaGraphDestroy(graph));
     }
 
@@ -1646,11 +1708,13 @@ int Engine::kernelLaunches() const {
     if (!I.haveResult)
         return 0;
     // own kernels per evaluation: preparation 10, the two field passes before the loop 3 + 1 + 3 + 1,
-    // 4 per CG iteration, final 7 (the cuFFT transforms are not counted)
+    // 4 per CG iteration, final 7 (the cuFFT transforms are not counted); the plane transforms replace the
+    // influence product of each field pass by three kernels
     int it = 0;
     for (int k = 0; k < I.nsys; k++)
         it = std::max(it, (int) I.lastResults[(size_t) k * NRES + 14]);
-    return 10 + (I.s.polarizable ? 8 + 4 * it : 0) + 7;
+    const int planes = I.usePlanes ? 2 * (2 + it) : 0;
+    return 10 + (I.s.polarizable ? 8 + 4 * it + planes : 0) + 7;
 }
 
 void Engine::kernelTimes(int reps, double* ms) {
@@ -1692,7 +1756,12 @@ void Engine::kernelTimes(int reps, double* ms) {
             default: k_pair_final<R, 8><<<blocks, 256, 0, I.st>>>(d);
             }
         });
-        ms[5] = timeIt([&] { I.fftChain<R>(I.st, d, false, false); });
+        ms[5] = timeIt([&] {
+            if (I.usePlanes)
+                I.planeChain<R>(I.st, d);
+            else
+                I.fftChain<R>(I.st, d, false, false);
+        });
         ms[6] = timeIt([&] { k_cg_a<<<(int) I.chunkSys.size(), CHUNK, 0, I.st>>>(d); });
     };
     if (I.mixed())

@@ -662,6 +662,354 @@ __global__ void __launch_bounds__(256) k_conv(Dev dv, int gateDone) {
     }
 }
 
+// ------------------------------------------------------------------------------------------------ plane transforms
+
+// The 3D real transform pair with the influence product in three kernels for one system whose grid has at most
+// PLANE_MAXK points and only the prime factors 2, 3, 5 per dimension (instead of the cuFFT kernels plus the
+// product): x-planes transform along z (real to half spectrum) and y in shared memory, lines along x transform
+// forward, take the influence product and transform back, x-planes transform back along y and z (half spectrum
+// to real).  Unnormalised, the spectrum layout F[(kx K1 + ky) (K2/2 + 1) + kz] of cuFFT's R2C / C2R, shared with
+// the cuFFT path.  Each line transform is a mixed-radix Stockham FFT (radices 4, 2, 3, 5; ping-pong buffers,
+// no reordering pass) with twiddles W^m = exp(-2 pi i m / K) from sincospi in double.  Real rows are
+// transformed two at a time as one complex row (x + i y) and separated by Hermitian symmetry.
+constexpr int PLANE_MAXK = 64;
+constexpr int PLANE_BUF = 2176;   // >= max(ceil(K1/2) K2, (K2/2+1)(K1+1)) complex for K <= PLANE_MAXK
+constexpr int PLANE_LINES = 8;    // x-lines per block of the line kernel
+
+__host__ __device__ inline int fftRadices(int n, int* r) {
+    int c = 0;
+    while (n % 4 == 0) { r[c++] = 4; n /= 4; }
+    while (n % 2 == 0) { r[c++] = 2; n /= 2; }
+    while (n % 3 == 0) { r[c++] = 3; n /= 3; }
+    while (n % 5 == 0) { r[c++] = 5; n /= 5; }
+    return n == 1 ? c : -1;
+}
+
+template <typename R>
+__device__ __forceinline__ void twiddleTable(typename CplxT<R>::T* w, int K) {
+    for (int m = threadIdx.x; m < K; m += blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * m / K, &sn, &cs);
+        w[m].x = (R) cs;
+        w[m].y = (R) sn;
+    }
+}
+
+// In-register DFT of length RAD, sign DIR (-1 forward, +1 inverse), unnormalised.
+template <typename R, int RAD, int DIR>
+__device__ __forceinline__ void smallDft(R* xr, R* xi) {
+    if (RAD == 2) {
+        const R ar = xr[0] + xr[1], ai = xi[0] + xi[1];
+        xr[1] = xr[0] - xr[1];
+        xi[1] = xi[0] - xi[1];
+        xr[0] = ar;
+        xi[0] = ai;
+    } else if (RAD == 3) {
+        const R s = (R) (DIR * 0.86602540378443864676);   // DIR sin(2 pi / 3)
+        const R tr = xr[1] + xr[2], ti = xi[1] + xi[2];
+        const R ur = xr[0] - (R) 0.5 * tr, ui = xi[0] - (R) 0.5 * ti;
+        const R dr = s * (xr[1] - xr[2]), di = s * (xi[1] - xi[2]);   // i s (v1 - v2) = (-di, dr)
+        xr[0] += tr;
+        xi[0] += ti;
+        xr[1] = ur - di;
+        xi[1] = ui + dr;
+        xr[2] = ur + di;
+        xi[2] = ui - dr;
+    } else if (RAD == 4) {
+        const R ar = xr[0] + xr[2], ai = xi[0] + xi[2], br = xr[0] - xr[2], bi = xi[0] - xi[2];
+        const R cr = xr[1] + xr[3], ci = xi[1] + xi[3];
+        const R er = xr[1] - xr[3], ei = xi[1] - xi[3];
+        const R dr = (R) (-DIR) * ei, di = (R) DIR * er;   // (v1 - v3) DIR i
+        xr[0] = ar + cr;
+        xi[0] = ai + ci;
+        xr[2] = ar - cr;
+        xi[2] = ai - ci;
+        xr[1] = br + dr;
+        xi[1] = bi + di;
+        xr[3] = br - dr;
+        xi[3] = bi - di;
+    } else {   // 5
+        const R c1 = (R) 0.30901699437494742410, c2 = (R) -0.80901699437494742410;   // cos(2 pi/5), cos(4 pi/5)
+        const R s1 = (R) (DIR * 0.95105651629515357212), s2 = (R) (DIR * 0.58778525229247312917);
+        const R a1r = xr[1] + xr[4], a1i = xi[1] + xi[4], a2r = xr[2] + xr[3], a2i = xi[2] + xi[3];
+        const R b1r = xr[1] - xr[4], b1i = xi[1] - xi[4], b2r = xr[2] - xr[3], b2i = xi[2] - xi[3];
+        const R p1r = xr[0] + c1 * a1r + c2 * a2r, p1i = xi[0] + c1 * a1i + c2 * a2i;
+        const R p2r = xr[0] + c2 * a1r + c1 * a2r, p2i = xi[0] + c2 * a1i + c1 * a2i;
+        const R q1r = s1 * b1r + s2 * b2r, q1i = s1 * b1i + s2 * b2i;   // y1 = p1 + i q1, y4 = p1 - i q1
+        const R q2r = s2 * b1r - s1 * b2r, q2i = s2 * b1i - s1 * b2i;   // y2 = p2 + i q2, y3 = p2 - i q2
+        xr[0] += a1r + a2r;
+        xi[0] += a1i + a2i;
+        xr[1] = p1r - q1i;
+        xi[1] = p1i + q1r;
+        xr[4] = p1r + q1i;
+        xi[4] = p1i - q1r;
+        xr[2] = p2r - q2i;
+        xi[2] = p2i + q2r;
+        xr[3] = p2r + q2i;
+        xi[3] = p2i - q2r;
+    }
+}
+
+// e / K for 0 <= e < 2^20, 1 <= K <= 2^10 without an integer division: (e + 1/2) / K lies at least 1/(2K) from
+// an integer and the float product errs by under 2^-22 (e + 1/2) / K, so truncation gives the exact quotient.
+__device__ __forceinline__ int fdiv(int e, float invK) { return __float2int_rz(((float) e + 0.5f) * invK); }
+
+// One Stockham pass of radix RAD over nlines lines of length N (line stride ls): butterfly j of a line reads
+// in[j + r N/RAD], twiddles by W^(r (j mod Ns) N / (Ns RAD)), and writes out[(j / Ns) Ns RAD + j mod Ns + r Ns],
+// Ns the product of the earlier radices.
+template <typename R, int RAD, int DIR>
+__device__ __forceinline__ void stockhamPass(const typename CplxT<R>::T* in, typename CplxT<R>::T* out, int nlines,
+                                             int N, int ls, int Ns, const typename CplxT<R>::T* tw) {
+    typedef typename CplxT<R>::T C;
+    const int nb = N / RAD, step = N / (Ns * RAD);
+    const float invNb = 1.0f / (float) nb, invNs = 1.0f / (float) Ns;
+    for (int t = threadIdx.x; t < nlines * nb; t += blockDim.x) {
+        const int line = fdiv(t, invNb), j = t - line * nb;
+        const int q = fdiv(j, invNs), jn = j - q * Ns;
+        const C* src = in + line * ls + j;
+        R xr[RAD], xi[RAD];
+        C v[RAD];
+#pragma unroll
+        for (int r = 0; r < RAD; r++)
+            v[r] = src[r * nb];
+        xr[0] = v[0].x;
+        xi[0] = v[0].y;
+#pragma unroll
+        for (int r = 1; r < RAD; r++) {
+            const C w = tw[jn * r * step];
+            const R wy = DIR < 0 ? w.y : -w.y;
+            xr[r] = v[r].x * w.x - v[r].y * wy;
+            xi[r] = v[r].x * wy + v[r].y * w.x;
+        }
+        smallDft<R, RAD, DIR>(xr, xi);
+        C* dst = out + line * ls + q * Ns * RAD + jn;
+#pragma unroll
+        for (int r = 0; r < RAD; r++) {
+            C o;
+            o.x = xr[r];
+            o.y = xi[r];
+            dst[r * Ns] = o;
+        }
+    }
+}
+
+// Transforms nlines lines of length N held in a (line stride ls); b is scratch of the same size.  Returns the
+// buffer holding the result.  Every thread of the block calls it (it synchronises after each pass).
+template <typename R, int DIR>
+__device__ typename CplxT<R>::T* fftLines(typename CplxT<R>::T* a, typename CplxT<R>::T* b, int nlines, int N, int ls,
+                                          const typename CplxT<R>::T* tw) {
+    typedef typename CplxT<R>::T C;
+    int n = N, Ns = 1;
+    while (n > 1) {
+        const int rad = (n % 4 == 0) ? 4 : (n % 2 == 0) ? 2 : (n % 3 == 0) ? 3 : 5;
+        switch (rad) {
+        case 4: stockhamPass<R, 4, DIR>(a, b, nlines, N, ls, Ns, tw); break;
+        case 2: stockhamPass<R, 2, DIR>(a, b, nlines, N, ls, Ns, tw); break;
+        case 3: stockhamPass<R, 3, DIR>(a, b, nlines, N, ls, Ns, tw); break;
+        default: stockhamPass<R, 5, DIR>(a, b, nlines, N, ls, Ns, tw);
+        }
+        __syncthreads();
+        C* t = a;
+        a = b;
+        b = t;
+        Ns *= rad;
+        n /= rad;
+    }
+    return a;
+}
+
+constexpr int PLANE_THREADS = 256;
+constexpr int PLANE_PER = (PLANE_MAXK * PLANE_MAXK / 2 + PLANE_THREADS - 1) / PLANE_THREADS;   // row pairs x K2
+
+// blockIdx.x: plane x.  Shared: twiddles W1[K1], W2[K2]; buffers A, B of PLANE_BUF complex.
+template <typename R>
+__global__ void __launch_bounds__(PLANE_THREADS) k_planes_fwd(Dev dv) {
+    typedef typename CplxT<R>::T C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const SysDev& S = dv.sys[0];
+    const int K1 = S.K[1], K2 = S.K[2], K2h = K2 / 2 + 1, P = (K1 + 1) / 2, ly = K1 + 1;
+    const float invK2 = 1.0f / (float) K2, invK2h = 1.0f / (float) K2h;
+    const int x = blockIdx.x;
+    C* W1 = (C*) smraw;
+    C* W2 = W1 + PLANE_MAXK;
+    C* A = W2 + PLANE_MAXK;
+    C* B = A + PLANE_BUF;
+    const R* g = (const R*) dv.grid + S.gridOff + (size_t) x * K1 * K2;
+    {   // rows 2p, 2p+1 as one complex row; all loads issued before the stores
+        R lo[PLANE_PER], hi[PLANE_PER];
+#pragma unroll
+        for (int k = 0; k < PLANE_PER; k++) {
+            const int e = threadIdx.x + k * PLANE_THREADS;
+            lo[k] = hi[k] = 0;
+            if (e < P * K2) {
+                const int p = fdiv(e, invK2), z = e - p * K2;
+                lo[k] = g[2 * p * K2 + z];
+                if (2 * p + 1 < K1)
+                    hi[k] = g[(2 * p + 1) * K2 + z];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < PLANE_PER; k++) {
+            const int e = threadIdx.x + k * PLANE_THREADS;
+            if (e < P * K2) {
+                C v;
+                v.x = lo[k];
+                v.y = hi[k];
+                A[e] = v;
+            }
+        }
+    }
+    twiddleTable<R>(W1, K1);
+    twiddleTable<R>(W2, K2);
+    __syncthreads();
+    C* Z = fftLines<R, -1>(A, B, P, K2, K2, W2);
+    C* O = (Z == A) ? B : A;
+    for (int e = threadIdx.x; e < P * K2h; e += blockDim.x) {   // separate the two rows; y-lines O[kz ly + y]
+        const int p = fdiv(e, invK2h), kz = e - p * K2h;
+        const C zk = Z[p * K2 + kz], zm = Z[p * K2 + (kz == 0 ? 0 : K2 - kz)];
+        C X, Y;   // X = (Z_k + conj Z_-k) / 2, Y = (Z_k - conj Z_-k) / 2i
+        X.x = (R) 0.5 * (zk.x + zm.x);
+        X.y = (R) 0.5 * (zk.y - zm.y);
+        Y.x = (R) 0.5 * (zk.y + zm.y);
+        Y.y = (R) 0.5 * (zm.x - zk.x);
+        O[kz * ly + 2 * p] = X;
+        if (2 * p + 1 < K1)
+            O[kz * ly + 2 * p + 1] = Y;
+    }
+    __syncthreads();
+    const C* F = fftLines<R, -1>(O, Z, K2h, K1, ly, W1);
+    C* spec = (C*) dv.spec + S.specOff + (size_t) x * K1 * K2h;
+    for (int e = threadIdx.x; e < K1 * K2h; e += blockDim.x) {
+        const int ky = fdiv(e, invK2h), kz = e - ky * K2h;
+        spec[e] = F[kz * ly + ky];
+    }
+}
+
+constexpr int LINES_THREADS = 128;
+constexpr int LINES_PER = (PLANE_MAXK * PLANE_LINES + LINES_THREADS - 1) / LINES_THREADS;
+
+// PLANE_LINES consecutive x-lines (ky, kz) per block: forward transform along x, influence product, inverse.
+template <typename R>
+__global__ void __launch_bounds__(LINES_THREADS) k_lines_x(Dev dv) {
+    typedef typename CplxT<R>::T C;
+    __shared__ C W0[PLANE_MAXK];
+    __shared__ C A[PLANE_LINES * (PLANE_MAXK + 1)], B[PLANE_LINES * (PLANE_MAXK + 1)];
+    const SysDev& S = dv.sys[0];
+    const int K0 = S.K[0], nline = S.K[1] * (S.K[2] / 2 + 1), lx = K0 + 1;
+    const size_t stride = (size_t) nline;   // F[(kx K1 + ky) K2h + kz]: line ky K2h + kz, stride K1 K2h in kx
+    const int line0 = blockIdx.x * PLANE_LINES;
+    C* spec = (C*) dv.spec + S.specOff + line0;
+    const R* infl = (const R*) dv.infl + S.specOff + line0;
+    C v[LINES_PER];
+    R gk[LINES_PER];
+#pragma unroll
+    for (int k = 0; k < LINES_PER; k++) {   // element e = kx PLANE_LINES + l; the loads, then the stores
+        const int e = threadIdx.x + k * LINES_THREADS, kx = e / PLANE_LINES, l = e % PLANE_LINES;
+        v[k].x = v[k].y = 0;
+        gk[k] = 0;
+        if (kx < K0 && line0 + l < nline) {
+            v[k] = spec[kx * stride + l];
+            gk[k] = infl[kx * stride + l];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < LINES_PER; k++) {
+        const int e = threadIdx.x + k * LINES_THREADS, kx = e / PLANE_LINES, l = e % PLANE_LINES;
+        if (kx < K0)
+            A[l * lx + kx] = v[k];
+    }
+    twiddleTable<R>(W0, K0);
+    __syncthreads();
+    C* F = fftLines<R, -1>(A, B, PLANE_LINES, K0, lx, W0);
+#pragma unroll
+    for (int k = 0; k < LINES_PER; k++) {
+        const int e = threadIdx.x + k * LINES_THREADS, kx = e / PLANE_LINES, l = e % PLANE_LINES;
+        if (kx < K0) {
+            F[l * lx + kx].x *= gk[k];
+            F[l * lx + kx].y *= gk[k];
+        }
+    }
+    __syncthreads();
+    const C* G = fftLines<R, 1>(F, F == A ? B : A, PLANE_LINES, K0, lx, W0);
+#pragma unroll
+    for (int k = 0; k < LINES_PER; k++) {
+        const int e = threadIdx.x + k * LINES_THREADS, kx = e / PLANE_LINES, l = e % PLANE_LINES;
+        if (kx < K0 && line0 + l < nline)
+            spec[kx * stride + l] = G[l * lx + kx];
+    }
+}
+
+// blockIdx.x: plane x.  Inverse along y, then rows 2p, 2p+1 rebuilt from their half spectra (imaginary parts
+// at kz = 0 and the Nyquist index dropped, as a C2R transform does) as one complex row, inverse along z.
+template <typename R>
+__global__ void __launch_bounds__(PLANE_THREADS) k_planes_inv(Dev dv) {
+    typedef typename CplxT<R>::T C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const SysDev& S = dv.sys[0];
+    const int K1 = S.K[1], K2 = S.K[2], K2h = K2 / 2 + 1, P = (K1 + 1) / 2, ly = K1 + 1;
+    const float invK2 = 1.0f / (float) K2, invK2h = 1.0f / (float) K2h;
+    const int x = blockIdx.x;
+    C* W1 = (C*) smraw;
+    C* W2 = W1 + PLANE_MAXK;
+    C* A = W2 + PLANE_MAXK;
+    C* B = A + PLANE_BUF;
+    const C* spec = (const C*) dv.spec + S.specOff + (size_t) x * K1 * K2h;
+    {
+        C v[PLANE_PER + 1];   // K1 K2h <= PLANE_MAXK (PLANE_MAXK / 2 + 1) elements
+#pragma unroll
+        for (int k = 0; k < PLANE_PER + 1; k++) {
+            const int e = threadIdx.x + k * PLANE_THREADS;
+            if (e < K1 * K2h)
+                v[k] = spec[e];
+        }
+#pragma unroll
+        for (int k = 0; k < PLANE_PER + 1; k++) {
+            const int e = threadIdx.x + k * PLANE_THREADS;
+            if (e < K1 * K2h) {
+                const int ky = fdiv(e, invK2h), kz = e - ky * K2h;
+                A[kz * ly + ky] = v[k];
+            }
+        }
+    }
+    twiddleTable<R>(W1, K1);
+    twiddleTable<R>(W2, K2);
+    __syncthreads();
+    C* G = fftLines<R, 1>(A, B, K2h, K1, ly, W1);   // G[kz ly + y]
+    C* O = (G == A) ? B : A;
+    for (int e = threadIdx.x; e < P * K2; e += blockDim.x) {
+        const int p = fdiv(e, invK2), k = e - p * K2;
+        const bool upper = k >= K2h;
+        const int kk = upper ? K2 - k : k;
+        const bool realOnly = (k == 0) || ((K2 & 1) == 0 && k == K2 / 2);
+        C X = G[kk * ly + 2 * p], Y;
+        Y.x = 0;
+        Y.y = 0;
+        if (2 * p + 1 < K1)
+            Y = G[kk * ly + 2 * p + 1];
+        if (upper) {
+            X.y = -X.y;
+            Y.y = -Y.y;
+        }
+        if (realOnly) {
+            X.y = 0;
+            Y.y = 0;
+        }
+        C Zv;   // X + i Y
+        Zv.x = X.x - Y.y;
+        Zv.y = X.y + Y.x;
+        O[e] = Zv;
+    }
+    __syncthreads();
+    const C* Zt = fftLines<R, 1>(O, G, P, K2, K2, W2);
+    R* g = (R*) dv.grid + S.gridOff + (size_t) x * K1 * K2;
+    for (int e = threadIdx.x; e < P * K2; e += blockDim.x) {
+        const int p = fdiv(e, invK2), z = e - p * K2;
+        g[2 * p * K2 + z] = Zt[e].x;
+        if (2 * p + 1 < K1)
+            g[(2 * p + 1) * K2 + z] = Zt[e].y;
+    }
+}
+
 // Interpolation from the potential grid: f_a = sum (d theta_a) theta theta phi (the field, E_rec = -sum_a K_a
 // recip[:, a] f_a, core/pgm_core.cpp:241-264); FINAL also the second derivatives, the potential and the
 // reciprocal forces -K_a recip[k][a] (q f1_a + sum_b e_b f2_ab) (core/pgm_core.cpp:452-487) and E_rec (x) d.
@@ -1276,13 +1624,24 @@ __global__ void __launch_bounds__(CHUNK) k_final_forces(Dev dv, int iterationsSo
         v[12] = dv.q[i];
     }
     double tot[14];
-    __shared__ double sconv[NCONV];
+    __shared__ double sconv[NCONV], cgrp[CHUNK / 16][NCONV];
     if (!chunkFinish<14>(dv, chunk, s, v, 0u, tot))
         return;
+    {   // the reciprocal-space partials: value k = tid mod 16, block group tid / 16 (fixed order)
+        const int k = threadIdx.x & 15, grp = threadIdx.x >> 4;
+        if (k < NCONV) {
+            double acc = 0.0;
+#pragma unroll 4
+            for (int bk = grp; bk < S.convBlocks; bk += CHUNK / 16)
+                acc += __ldcg(&dv.convPartial[(size_t) (dv.convPartialOff[s] + bk) * NCONV + k]);
+            cgrp[grp][k] = acc;
+        }
+    }
+    __syncthreads();
     if (threadIdx.x < NCONV) {
         double acc = 0.0;
-        for (int bk = 0; bk < S.convBlocks; bk++)
-            acc += __ldcg(&dv.convPartial[(size_t) (dv.convPartialOff[s] + bk) * NCONV + threadIdx.x]);
+        for (int g = 0; g < CHUNK / 16; g++)
+            acc += cgrp[g][threadIdx.x];
         sconv[threadIdx.x] = acc;
     }
     __syncthreads();
