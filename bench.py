@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 1024-system leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 98304-atom leg")
     ap.add_argument("--no-grad", action="store_true", help="skip the parameter-gradient leg")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm: skip the reference GPU engine timed on this GPU")
     return ap.parse_args()
 
 
@@ -255,8 +257,84 @@ def reference_arm(args):
             "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "reference",
                              "sample": f"{steps} steps x {cores} full evaluations of {WORKLOAD}"},
             "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu_leg(pkg, S, steps, max(args.warmup, 3))
     print(json.dumps(line))
     return 0
+
+
+def reference_gpu_leg(pkg, S, steps, warmup):
+    """The reference's own GPU engine (core/cuda/pgm_cuda.cu, unchanged, built into oracle/_ref) on this GPU,
+    with its defaults (mixed precision, CUDA graph, own pair list with a 0.15 nm skin):
+      step: the benchmark step (predictor none, tol 1e-5, peek 0.65, the same positions every call) through its
+        OpenMM path (float4 device positions in, 64-bit fixed-point device forces out, launchDevice + waitDevice
+        on the caller's stream), CUDA events on that stream, L2 flushed before every step.  Its pair list is
+        built at the first call and reused, since the positions do not move (pgm_b200 builds its list in every
+        step);
+      md_moving: as md_leg (host call, mu4 predictor, smooth motions, same phases and steps);
+      accuracy: forces and energy against the FP64 oracle at tol 1e-10."""
+    try:
+        import torch
+        from oracle import ref_cuda as RC
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU"}
+        if not RC.available():
+            return {"unavailable": "oracle/_ref/libpgmcuda_ref.so not built (make -C oracle cuda)"}
+        dev = torch.device("cuda:0")
+        torch.cuda.set_device(dev)
+        stream = torch.cuda.current_stream(dev)
+        ke = pkg.systems.KE_DEFAULT
+        out = {"engine": "reference pgm_cuda (core/cuda/pgm_cuda.cu) built for sm_100a, its default settings"}
+        eng = RC.RefCudaEngine(S, TOL, predictor=0, peek=0.65, ke=ke)
+        posq = torch.zeros((S.n, 4), dtype=torch.float32, device=dev)
+        posq[:, :3] = torch.from_numpy(S.pos).to(dev, torch.float32)
+        ffix = torch.zeros(3 * S.n, dtype=torch.int64, device=dev)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+        def one():
+            while True:
+                eng.launch_device(posq.data_ptr(), S.box, True, ffix.data_ptr(), S.n, 2.0 ** 32, stream.cuda_stream)
+                eng.wait_device(stream.cuda_stream)
+                if eng.finish_device():
+                    return
+        for _ in range(warmup):
+            one()
+        torch.cuda.synchronize()
+        ms, its = 0.0, []
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            one()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms += a.elapsed_time(b)
+            its.append(eng.iterations())
+        out["step"] = {"evals_per_s": steps / (ms / 1e3), "ms_per_eval": ms / steps,
+                       "cg_iterations": int(np.median(its)), "list_builds": eng.list_builds(), "steps": steps}
+        E, F = eng.compute(S.pos, S.box)
+        E0, F0, kind = _oracle_reference(pkg, S, 1e-10)
+        out["accuracy"] = {"oracle": kind, "force_rel_rms": float(np.linalg.norm(F - F0) / np.linalg.norm(F0)),
+                           "energy_rel": float(abs(E - E0) / abs(E0))}
+        eng.close()
+        rng = np.random.default_rng(7)
+        phase = rng.uniform(0, 2 * np.pi, S.pos.shape)
+        eng = RC.RefCudaEngine(S, TOL, predictor=2, peek=0.65, ke=ke)
+        for st in range(10):
+            eng.compute(S.pos + 0.01 * np.sin(2 * np.pi * st / 100 + phase), S.box)
+        md_steps, its = 30, []
+        t0 = time.perf_counter()
+        for st in range(10, 10 + md_steps):
+            eng.compute(S.pos + 0.01 * np.sin(2 * np.pi * st / 100 + phase), S.box)
+            its.append(eng.iterations())
+        dt = (time.perf_counter() - t0) / md_steps
+        out["md_moving"] = {"evals_per_s": 1.0 / dt, "mean_cg_iterations": float(np.mean(its)),
+                            "list_builds": eng.list_builds(),
+                            "note": "host call incl. position generation on the host; predictor mu4"}
+        eng.close()
+        return out
+    except Exception as e:   # the comparison is reported, never fatal to the reference arm
+        return {"unavailable": f"{type(e).__name__}: {e}"}
 
 
 _REF = {}
