@@ -190,7 +190,8 @@ def roofline_table(S, kt, it, precision):
 def md_leg(pkg, S, make, lanes, dev, steps=30):
     """MD-like use: positions move smoothly every step (amplitude 0.01 nm, period 100 steps, random phases,
     as the reference harness's moving timing, core/cuda/tests/test_cuda.cpp:351-372), new step every call,
-    mu4 predictor; host call with host positions and forces.  Both precisions."""
+    mu4 predictor, the Verlet list kept with the default 0.15 nm skin (as the reference engine's); host call with
+    host positions and forces.  Both precisions."""
     import torch
     rng = np.random.default_rng(7)
     phase = rng.uniform(0, 2 * np.pi, S.pos.shape)
@@ -210,10 +211,11 @@ def md_leg(pkg, S, make, lanes, dev, steps=30):
             r = eng.compute(S.pos + 0.01 * np.sin(2 * np.pi * st / 100 + phase), S.box)
             its.append(r.iterations)
         dt = (time.perf_counter() - t0) / steps
-        out[name] = {"evals_per_s": 1.0 / dt, "mean_cg_iterations": float(np.mean(its))}
+        out[name] = {"evals_per_s": 1.0 / dt, "mean_cg_iterations": float(np.mean(its)),
+                     "list_builds": eng.list_builds()}
         eng.close()
     out["mixed_over_fp64"] = out["mixed"]["evals_per_s"] / out["fp64"]["evals_per_s"]
-    out["note"] = "host call incl. position generation on the host; predictor mu4"
+    out["note"] = "host call incl. position generation on the host; predictor mu4; Verlet list, skin 0.15 nm"
     return out
 
 
@@ -380,9 +382,10 @@ def main():
     pkg, S = system()
 
     def make(precision):
+        # skin 0: the pair list is built in every step (a full, independent evaluation)
         eng = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=TOL,
                                       max_iter=200, peek=0.65, predictor=0, ke=pkg.systems.KE_DEFAULT,
-                                      precision=precision, device=local))
+                                      precision=precision, device=local, skin=0.0))
         eng.set_system(S)
         return eng
 
@@ -457,6 +460,21 @@ def main():
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     fp64_value = world * fsteps / (float(t.item()) / 1e3)
+    # the same step with the Verlet list kept (default 0.15 nm skin; the positions do not move, so it is built
+    # once), the protocol of the reference GPU engine's step in the reference arm
+    kept = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=TOL, max_iter=200,
+                                   peek=0.65, predictor=0, ke=pkg.systems.KE_DEFAULT, precision=pkg.MIXED,
+                                   device=local))
+    kept.set_system(S)
+    kept.compute(S.pos, S.box)
+    kept.set_pair_lanes(lanes)
+    ms_kept, _ = timed_resident(kept, fsteps, 3)
+    t = torch.tensor([ms_kept], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    kept_value = world * fsteps / (float(t.item()) / 1e3)
+    kept_builds = kept.list_builds()
+    kept.close()
     # end to end through the C ABI host call (host positions in, host forces out)
     for _ in range(2):
         mixed.compute(S.pos, S.box)
@@ -487,6 +505,9 @@ def main():
             "fp64": {"value": fp64_value, "unit": "evals/s", "steps": fsteps,
                      "cg_iterations": int(np.median(its_fp64)), "kernel_ms": kt64},
             "mixed_over_fp64": value / fp64_value,
+            "kept_list": {"value": kept_value, "unit": "evals/s", "steps": fsteps, "list_builds": kept_builds,
+                          "note": "mixed, Verlet list kept (skin 0.15 nm, positions unchanged): the reference "
+                                  "GPU engine's step protocol"},
             "ns_per_day_2fs": value / world * 86400 * 2e-6,
             "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": S.n * 3 * 8,
                     "d2h_bytes_per_step": S.n * 3 * 8 + 16 * 8},
@@ -496,7 +517,7 @@ def main():
         def make_refined():
             e = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=TOL,
                                         max_iter=200, peek=0.65, predictor=0, ke=pkg.systems.KE_DEFAULT,
-                                        precision=pkg.MIXED, device=local, refine=True))
+                                        precision=pkg.MIXED, device=local, refine=True, skin=0.0))
             e.set_system(S)
             e.set_pair_lanes(lanes)
             return e
@@ -540,7 +561,7 @@ def large_leg(pkg, local, world, dist):
     for tol in (1e-4, 1e-5):
         eng = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=6, tol=tol, max_iter=200,
                                       peek=0.65, predictor=0, ke=pkg.systems.KE_DEFAULT, precision=pkg.MIXED,
-                                      device=local))
+                                      device=local, skin=0.0))
         eng.set_system(S)
         eng.compute(S.pos, S.box)
         out["pair_lanes"] = eng.autotune(S.pos, S.box, reps=3)
@@ -570,7 +591,7 @@ def batch_leg(pkg, local, rank, world, dist):
     mine = [systems[k] for k in parts[rank]]
     eng = pkg.Engine(pkg.Settings(cutoff=0.9, beta=3.5, grid=(24, 24, 24), order=6, tol=1e-5, max_iter=200,
                                   peek=0.65, predictor=0, ke=pkg.systems.KE_DEFAULT, precision=pkg.MIXED,
-                                  device=local))
+                                  device=local, skin=0.0))
     eng.set_systems(mine)
     pos = np.concatenate([s.pos for s in mine])
     boxes = np.stack([s.box for s in mine])
@@ -592,7 +613,7 @@ def batch_leg(pkg, local, rank, world, dist):
         for S in sample:
             e = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=6, tol=1e-5, max_iter=200,
                                         peek=0.65, predictor=0, ke=pkg.systems.KE_DEFAULT, precision=pkg.MIXED,
-                                        device=local))
+                                        device=local, skin=0.0))
             e.set_system(S)
             e.compute(S.pos, S.box)
             engines.append((e, S))

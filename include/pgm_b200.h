@@ -44,7 +44,9 @@ typedef struct pgm_settings {
     int predictor;       /* 0 none (guess alpha E_perm), 1 mu3, 2 mu4 (history in the global order) */
     double ke;           /* Coulomb constant [kJ mol^-1 nm e^-2] */
     int device;          /* CUDA device; < 0: the device current on the calling thread */
-    double skin;         /* accepted for interface parity; the pair list is rebuilt at every evaluation */
+    double skin;         /* Verlet list radius cutoff + skin [nm] (shrunk to stay within half the box); the list is
+                            kept while every atom stays within skin/2 of its position at the build and the box
+                            is unchanged (checked on the GPU at every evaluation); <= 0: built at every evaluation */
     int precision;       /* PGM_PRECISION_FP64 or PGM_PRECISION_MIXED */
     int zero_guess;      /* 1: initial guess mu = 0 when the predictor has no history (instead of alpha E_perm) */
     int polarizable;     /* 0: no induced dipoles (pgmcore::Settings::polarizable) */
@@ -109,7 +111,9 @@ int pgm_engine_compute_device(pgm_engine* e, const void* posq4, const double* bo
 int pgm_engine_launch_resident(pgm_engine* e, const double* pos_dev, const double* box, int new_step,
                                double* forces_dev, void* stream);
 
-/* Getters of pgmcuda::Engine (core/cuda/pgm_cuda.h:112-122). */
+/* Getters of pgmcuda::Engine (core/cuda/pgm_cuda.h:112-122).  list_builds: builds of the Verlet list so far;
+ * late_list_checks: always 0 (the stale test runs on the GPU before the list is used); num_candidates: the
+ * directed pairs within the cutoff at the last evaluation (the reference counts its list's candidates). */
 int pgm_engine_iterations(pgm_engine* e);
 double pgm_engine_residual(pgm_engine* e);
 int pgm_engine_induced_dipoles(pgm_engine* e, double* mu);

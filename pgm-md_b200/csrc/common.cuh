@@ -24,6 +24,8 @@ struct SysDev {
     double H[9];          // box rows a, b, c
     double recip[9];      // recip[k*3+a] = (H^-1)_{k a}
     double volume, cutoff, rc2, beta;
+    double rl2;           // list radius^2: (cutoff + skin)^2, the skin shrunk so that it stays below half the box
+    double skinHalf2;     // (skin / 2)^2: an atom moved further since the list's build makes the list stale
     int K[3];
     int atomBegin, atomEnd;
     int cellN[3], cellM[3];
@@ -49,6 +51,7 @@ struct Ctl {
     long long* forceFixed;   // device 64-bit fixed-point forces (added), or null
     double fixedScale;
     double* forcesOut;       // device double forces (written), or null
+    int forceRebuild;        // 1: build the pair list whatever the displacements (no list, box changed, skin 0)
 };
 
 // Device pointers of one engine (passed by value to every kernel).
@@ -82,11 +85,17 @@ struct Dev {
     double4* origS;           // original position + radius
     int4* wrapS;              // wraps N
     double* radS;
-    // pair list
-    uint32_t* list;           // [slot][cap]
+    // pair lists: the Verlet list of the last build (radius cutoff + skin) and, per evaluation, the pairs of
+    // it within the cutoff with their G1, G2
+    uint32_t* slist;          // [slot][cap] Verlet list (cutoff + skin)
+    int* slistCount;          // per slot
+    double* posBuild;         // 3n positions at the list's build
+    uint32_t* list;           // [slot][cap] pairs within the cutoff
     int* listCount;           // per slot
     void* G12;                // [slot][cap] R2
-    int* flags;               // [0]: list overflow, [1]: shift out of range, [2]: all systems done
+    int* flags;               // [0]: list overflow, [1]: shift out of range, [2]: all systems done, [3]-[5] CG
+                              // bookkeeping, [6]: list stale, [7]: block counter, [8]: list built,
+                              // [9]: a pair changed its image since the build (rebuild and repeat)
     // dipoles
     void* dS;                 // slot-order R4 (dipole xyz, charge w) for the pair passes
     double* perm;             // 3n
@@ -138,7 +147,8 @@ struct Dev {
     const int* globalIndex;
     int numGlobal;
     // graph
-    cudaGraphConditionalHandle cond;
+    cudaGraphConditionalHandle cond;       // CG while loop
+    cudaGraphConditionalHandle listCond;   // pair-list build if stale
     int useCond;
 };
 

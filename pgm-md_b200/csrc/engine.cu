@@ -158,7 +158,7 @@ struct Engine::Impl {
         dScal, dPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
-        dGradQ, dGradR;
+        dGradQ, dGradR, dSList, dSListCount, dPosBuild;
     // FP64 shadow of the mixed path for the iterative refinement
     Buf dG12d, dDSd, dGridD, dSpecD, dInflD, dSplD, dB64, dXsave;
     std::vector<std::pair<cufftHandle, cufftHandle>> plans64;
@@ -183,10 +183,20 @@ struct Engine::Impl {
     int histHead = 0, histCount = 0;
     int pendingSlot = -1;
 
+    // Verlet list state: valid once built; kept while the boxes stay those of the build and no atom has moved by
+    // more than half the skin (checked on the device at every evaluation)
+    bool listValid = false;
+    std::vector<double> buildBoxes;    // nsys * 9, the boxes of the last build
+    std::vector<double> launchBoxes;   // nsys * 9, the boxes of the evaluation in flight
+    cudaGraph_t listBody = nullptr;    // body of the build's conditional node while capturing
+    int graphCells = -1;               // cell count the graph was captured with
+    bool capturing = false;
+
     // last evaluation
     std::vector<double> lastResults;   // nsys * NRES
     bool haveResult = false;
     long builds = 0;
+    bool lastBuilt = false;   // the last evaluation built the Verlet list
     std::vector<double> forcesHostCache;
     bool launched = false;
     int launchedMode = 0;
@@ -217,7 +227,7 @@ struct Engine::Impl {
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
                       &dCovByAtomOff, &dCovByAtom, &dCovByPartnerOff, &dCovByPartner, &dChunkSys, &dChunkBegin,
                       &dChunkEnd, &dHist, &dGlobal, &dCtl, &dGradQ, &dGradR, &dG12d, &dDSd, &dGridD, &dSpecD,
-                      &dInflD, &dSplD, &dB64, &dXsave};
+                      &dInflD, &dSplD, &dB64, &dXsave, &dSList, &dSListCount, &dPosBuild};
         for (Buf* b : all)
             b->release();
         if (hPos) cudaFreeHost(hPos);
@@ -572,6 +582,8 @@ struct Engine::Impl {
         dWrapS.ensure(n * sizeof(int4));
         dRadS.ensure(n * 8);
         dListCount.ensure(n * sizeof(int));
+        dSListCount.ensure(n * sizeof(int));
+        dPosBuild.ensure(3 * (size_t) n * 8);
         dFlags.ensure(16 * sizeof(int));
         dDS.ensure(n * 4 * R);
         for (Buf* b : {&dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dEpair, &dErec, &dFpair, &dFrec, &dEtot,
@@ -639,6 +651,7 @@ struct Engine::Impl {
         // no covalent dipoles until setCovalent
         uploadCovalent();
         haveResult = false;
+        listValid = false;
         configured = true;
     }
 
@@ -663,12 +676,22 @@ struct Engine::Impl {
             if (!(S.cutoff > 0) || !(S.beta > 0))
                 throw std::invalid_argument("pgm_b200: cutoff and Ewald coefficient must be positive");
             S.cellOff = cells;
+            // the Verlet list radius: cutoff + skin, the skin shrunk so that the radius stays within half the
+            // smallest plane spacing (minimum image), as core/cuda/pgm_cuda.cu:1930-1940
+            double colMax = 0.0;
+            for (int a = 0; a < 3; a++)
+                colMax = std::max(colMax, std::sqrt(S.recip[a] * S.recip[a] + S.recip[3 + a] * S.recip[3 + a] +
+                                                    S.recip[6 + a] * S.recip[6 + a]));
+            const double skin = std::max(0.0, std::min(s.skin, 0.5 / colMax - S.cutoff));
+            const double rl = S.cutoff + skin;
+            S.rl2 = rl * rl;
+            S.skinHalf2 = 0.25 * skin * skin;
             for (int a = 0; a < 3; a++) {
                 const double col = std::sqrt(S.recip[a] * S.recip[a] + S.recip[3 + a] * S.recip[3 + a] +
                                              S.recip[6 + a] * S.recip[6 + a]);
-                const double rho = S.cutoff * col;   // fractional extent of the cutoff along a
-                if (rho > 0.5 * (1.0 + 1e-12))
+                if (S.cutoff * col > 0.5 * (1.0 + 1e-12))
                     throw std::invalid_argument("pgm_b200: cut-off beyond half the box");
+                const double rho = std::min(rl * col, 0.5);   // fractional extent of the list radius along a
                 int nc = (int) std::floor(2.0 / rho);
                 nc = std::max(1, std::min(nc, 1024));
                 S.cellN[a] = nc;
@@ -686,7 +709,7 @@ struct Engine::Impl {
             for (int a = 0; a < 3; a++) {
                 const double col = std::sqrt(S.recip[a] * S.recip[a] + S.recip[3 + a] * S.recip[3 + a] +
                                              S.recip[6 + a] * S.recip[6 + a]);
-                S.cellM[a] = std::max(1, (int) std::ceil(S.cutoff * col * S.cellN[a] * (1.0 + 1e-12)));
+                S.cellM[a] = std::max(1, (int) std::ceil(rl * col * S.cellN[a] * (1.0 + 1e-12)));
             }
             S.cellCount = S.cellN[0] * S.cellN[1] * S.cellN[2];
             cells += S.cellCount;
@@ -706,7 +729,7 @@ struct Engine::Impl {
             double maxNb = 0;
             for (int k = 0; k < nsys; k++) {
                 const int na = atomBegin[k + 1] - atomBegin[k];
-                const double nb = 4.0 / 3.0 * PI_D * std::pow(sysCutoff[k], 3) * (na / sysHost[k].volume);
+                const double nb = 4.0 / 3.0 * PI_D * std::pow(std::sqrt(sysHost[k].rl2), 3) * (na / sysHost[k].volume);
                 maxNb = std::max(maxNb, std::min(nb * 1.5 + 64.0, (double) na * 27));
             }
             cap = ((int) maxNb + 31) / 32 * 32;
@@ -717,7 +740,9 @@ struct Engine::Impl {
     }
 
     void allocList() {
+        listValid = false;
         dList.ensure((size_t) n * cap * sizeof(uint32_t));
+        dSList.ensure((size_t) n * cap * sizeof(uint32_t));
         dG12.ensure((size_t) n * cap * 2 * realSize());
         if (refining())
             dG12d.ensure((size_t) n * cap * 16);
@@ -738,9 +763,10 @@ struct Engine::Impl {
         return d;
     }
 
-    Dev makeDev(bool forGraph, cudaGraphConditionalHandle h) {
+    Dev makeDev(bool forGraph, cudaGraphConditionalHandle h, cudaGraphConditionalHandle listHandle = 0) {
         Dev d;
         std::memset(&d, 0, sizeof(d));
+        d.listCond = listHandle;
         d.nAtoms = n;
         d.nSys = nsys;
         d.nChunks = (int) chunkSys.size();
@@ -777,6 +803,9 @@ struct Engine::Impl {
         d.radS = dRadS.as<double>();
         d.list = dList.as<uint32_t>();
         d.listCount = dListCount.as<int>();
+        d.slist = dSList.as<uint32_t>();
+        d.slistCount = dSListCount.as<int>();
+        d.posBuild = dPosBuild.as<double>();
         d.G12 = dG12.p;
         d.flags = dFlags.as<int>();
         d.dS = dDS.p;
@@ -931,21 +960,60 @@ struct Engine::Impl {
         launchGather<R, false>(sm, d, gate ? 1 : 0);
     }
 
-    template <typename R> void enqueuePre(cudaStream_t sm, cudaStream_t sd, const Dev& d) {
+    // The Verlet list's build: cells, slots, the list at cutoff + skin (positions already in posIn).
+    void enqueueBuild(cudaStream_t sm, const Dev& d) {
         const int tb = (n + 255) / 256;
-        CU(cudaMemsetAsync(d.cellCount, 0, (size_t) totalCells * sizeof(int), sm));
-        CU(cudaMemsetAsync(d.flags, 0, 16 * sizeof(int), sm));
-        k_prep<<<tb, 256, 0, sm>>>(d, dPosIn.as<double>());
+        k_prep<<<tb, 256, 0, sm>>>(d, nullptr, 2);
         k_cell_scan<<<1, 1024, 0, sm>>>(d);
         k_cell_scatter<<<tb, 256, 0, sm>>>(d);
         k_cell_sort<<<(totalCells + 7) / 8, 256, 0, sm>>>(d);
+        k_build_list<<<totalCells, LIST_THREADS, 0, sm>>>(d);
         CU(cudaGetLastError());
+    }
+
+    // The pair-list step of an evaluation: positions in (PME base and fraction), the stale test, the build when
+    // stale (a conditional node of the graph, its body captured after the main capture; without graphs a host
+    // decision), the slot-order positions with the build's wraps.
+    void enqueueListStep(cudaStream_t sm, const Dev& d) {
+        const int tb = (n + 255) / 256;
+        k_prep<<<tb, 256, 0, sm>>>(d, dPosIn.as<double>(), 1);
+        k_displace<<<tb, 256, 0, sm>>>(d);
+        CU(cudaGetLastError());
+        if (capturing) {
+            cudaStreamCaptureStatus status;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t numDeps = 0;
+            cudaGraph_t g;
+            CU(cudaStreamGetCaptureInfo(sm, &status, nullptr, &g, &deps, &numDeps));
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = d.listCond;
+            cp.conditional.type = cudaGraphCondTypeIf;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            CU(cudaGraphAddNode(&node, g, deps, numDeps, &cp));
+            listBody = cp.conditional.phGraph_out[0];
+            CU(cudaStreamUpdateCaptureDependencies(sm, &node, 1, cudaStreamSetCaptureDependencies));
+        } else {
+            CU(cudaMemcpyAsync(hFlags, d.flags, 16 * sizeof(int), cudaMemcpyDeviceToHost, sm));
+            CU(cudaStreamSynchronize(sm));
+            if (hFlags[6])
+                enqueueBuild(sm, d);
+        }
+        k_refresh_positions<<<tb, 256, 0, sm>>>(d);
+        CU(cudaGetLastError());
+    }
+
+    template <typename R> void enqueuePre(cudaStream_t sm, cudaStream_t sd, const Dev& d) {
+        const int tb = (n + 255) / 256;
+        CU(cudaMemsetAsync(d.flags, 0, 16 * sizeof(int), sm));
+        enqueueListStep(sm, d);
         if (s.polarizable) {
-            // the pair list (side stream) beside the permanent field's PME half (main stream)
+            // the pairs within the cutoff and their G1, G2 (side stream) beside the permanent field's PME half
+            // (main stream)
             CU(cudaEventRecord(evFork, sm));
             CU(cudaStreamWaitEvent(sd, evFork, 0));
-            k_build_list<<<totalCells, LIST_THREADS, 0, sd>>>(d);
-            k_pair_kernels<R><<<(n + 7) / 8, 256, 0, sd>>>(d);
+            k_pair_compact<R><<<(n + 7) / 8, 256, 0, sd>>>(d);
             CU(cudaEventRecord(evJoin, sd));
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
             k_perm<<<tb, 256, 0, sm>>>(d);
@@ -968,8 +1036,7 @@ struct Engine::Impl {
             // the loop's first spread needs a clear grid (each iteration clears it for the next one)
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
         } else {
-            k_build_list<<<totalCells, LIST_THREADS, 0, sm>>>(d);
-            k_pair_kernels<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
+            k_pair_compact<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
             k_perm<<<tb, 256, 0, sm>>>(d);
             k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
@@ -1017,12 +1084,15 @@ struct Engine::Impl {
         }
         cudaGraph_t graph;
         CU(cudaGraphCreate(&graph, 0));
-        cudaGraphConditionalHandle handle = 0;
+        cudaGraphConditionalHandle handle = 0, listHandle = 0;
         if (s.polarizable)
             CU(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
-        const Dev d = makeDev(true, handle);
+        CU(cudaGraphConditionalHandleCreate(&listHandle, graph, 0, cudaGraphCondAssignDefault));
+        const Dev d = makeDev(true, handle, listHandle);
         CU(cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
         cudaGraph_t body = nullptr;
+        capturing = true;
+        listBody = nullptr;
         try {
             enqueuePre<R>(st, side, d);
             if (s.polarizable) {
@@ -1043,6 +1113,7 @@ struct Engine::Impl {
             }
             enqueuePost<R>(st, side, d);
         } catch (...) {
+            capturing = false;
             cudaGraph_t g = nullptr;
             cudaStreamEndCapture(st, &g);
             if (g)
@@ -1050,7 +1121,20 @@ struct Engine::Impl {
             cudaGraphDestroy(graph);
             throw;
         }
+        capturing = false;
         CU(cudaStreamEndCapture(st, &graph));
+        {
+            CU(cudaStreamBeginCaptureToGraph(st, listBody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueueBuild(st, d);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(st, &g);
+                cudaGraphDestroy(graph);
+                throw;
+            }
+            CU(cudaStreamEndCapture(st, &listBody));
+        }
         if (body) {
             CU(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
             try {
@@ -1064,6 +1148,7 @@ struct Engine::Impl {
             CU(cudaStreamEndCapture(st, &body));
         }
         CU(cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority));
+        graphCells = totalCells;
         CU(cudaGraphDestroy(graph));
     }
 
@@ -1191,10 +1276,16 @@ struct Engine::Impl {
         if (!configured || !atomsSet)
             throw std::logic_error("pgm_b200: compute before setAtoms");
         const bool grew = setBoxes(boxes);
-        if (grew && exec) {
+        // the graph's launch shapes hold the cell count (another box can change it without growing the storage)
+        if ((grew || totalCells != graphCells) && exec) {
             cudaGraphExecDestroy(exec);
             exec = nullptr;
         }
+        // the Verlet list is built anew when there is none, the boxes changed or the skin is 0; else the device
+        // decides from the displacements
+        launchBoxes.assign(boxes, boxes + 9 * (size_t) nsys);
+        const bool sameBoxes = listValid && buildBoxes == launchBoxes;
+        hCtl->forceRebuild = (!sameBoxes || grew || s.skin <= 0) ? 1 : 0;
         std::memcpy(hSys, sysHost.data(), nsys * sizeof(SysDev));
         CU(cudaMemcpyAsync(dSys.p, hSys, nsys * sizeof(SysDev), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(dCtl.p, hCtl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
@@ -1225,7 +1316,6 @@ struct Engine::Impl {
         CU(cudaMemcpyAsync(hResults, dResults.p, nsys * NRES * 8, cudaMemcpyDeviceToHost, st));
         CU(cudaMemcpyAsync(hFlags, dFlags.p, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));
         CU(cudaEventRecord(evDone, st));
-        builds++;
         launched = true;
     }
 
@@ -1235,6 +1325,12 @@ struct Engine::Impl {
         launched = false;
         if (hFlags[1])
             throw std::runtime_error("pgm_b200: pair image shift beyond 3 boxes (positions far outside the box?)");
+        lastBuilt = hFlags[8] != 0;
+        if (hFlags[8]) {
+            builds++;
+            buildBoxes = launchBoxes;
+            listValid = true;
+        }
         if (hFlags[0] > cap) {
             cap = (hFlags[0] + hFlags[0] / 4 + 31) / 32 * 32;
             allocList();
@@ -1242,6 +1338,10 @@ struct Engine::Impl {
                 cudaGraphExecDestroy(exec);
                 exec = nullptr;
             }
+            return false;
+        }
+        if (hFlags[9]) {   // a pair within the cutoff changed its image since the build: rebuild and repeat
+            listValid = false;
             return false;
         }
         lastResults.assign(hResults, hResults + nsys * NRES);
@@ -1489,20 +1589,21 @@ void Engine::field(const double* pos, const double box[3][3], const double* qf, 
         const int tb = (I.n + 255) / 256;
         CU(cudaMemsetAsync(dv.cellCount, 0, (size_t) I.totalCells * sizeof(int), I.st));
         CU(cudaMemsetAsync(dv.flags, 0, 16 * sizeof(int), I.st));
-        k_prep<<<tb, 256, 0, I.st>>>(dv, I.dPosIn.as<double>());
+        I.listValid = false;   // the list below is this call's
+        k_prep<<<tb, 256, 0, I.st>>>(dv, I.dPosIn.as<double>(), 3);
         k_cell_scan<<<1, 1024, 0, I.st>>>(dv);
         k_cell_scatter<<<tb, 256, 0, I.st>>>(dv);
         k_cell_sort<<<(I.totalCells + 7) / 8, 256, 0, I.st>>>(dv);
         if (I.mixed()) {
             k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(dv);
-            k_pair_kernels<float><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
+            k_pair_compact<float><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
             k_splines<float><<<(3 * I.n + 255) / 256, 256, 0, I.st>>>(dv);
             k_influence<float><<<dim3(I.convBlocks, I.nsys), 256, 0, I.st>>>(dv);
             CU(cudaMemsetAsync(dv.grid, 0, I.gridTotal * I.realSize(), I.st));
             I.fieldPass<float, true>(I.st, I.side, dv, 0, dv.dtot, false);
         } else {
             k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(dv);
-            k_pair_kernels<double><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
+            k_pair_compact<double><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
             k_splines<double><<<(3 * I.n + 255) / 256, 256, 0, I.st>>>(dv);
             k_influence<double><<<dim3(I.convBlocks, I.nsys), 256, 0, I.st>>>(dv);
             CU(cudaMemsetAsync(dv.grid, 0, I.gridTotal * I.realSize(), I.st));
@@ -1617,13 +1718,14 @@ Terms Engine::evaluateFixed(const double* pos, const double box[3][3], const dou
             if (keepList) {
                 k_refresh_positions<<<tb, 256, 0, I.st>>>(d);
             } else {
+                I.listValid = false;   // the list below is this call's
                 CU(cudaMemsetAsync(d.cellCount, 0, (size_t) I.totalCells * sizeof(int), I.st));
-                k_prep<<<tb, 256, 0, I.st>>>(d, I.dPosIn.as<double>());
+                k_prep<<<tb, 256, 0, I.st>>>(d, I.dPosIn.as<double>(), 3);
                 k_cell_scan<<<1, 1024, 0, I.st>>>(d);
                 k_cell_scatter<<<tb, 256, 0, I.st>>>(d);
                 k_cell_sort<<<(I.totalCells + 7) / 8, 256, 0, I.st>>>(d);
                 k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(d);
-                k_pair_kernels<R><<<(I.n + 7) / 8, 256, 0, I.st>>>(d);
+                k_pair_compact<R><<<(I.n + 7) / 8, 256, 0, I.st>>>(d);
             }
             k_splines<R><<<(3 * I.n + 255) / 256, 256, 0, I.st>>>(d);
             k_perm<<<tb, 256, 0, I.st>>>(d);
@@ -1707,14 +1809,14 @@ int Engine::kernelLaunches() const {
     const Impl& I = *impl;
     if (!I.haveResult)
         return 0;
-    // own kernels per evaluation: preparation 10, the two field passes before the loop 3 + 1 + 3 + 1,
-    // 4 per CG iteration, final 7 (the cuFFT transforms are not counted); the plane transforms replace the
-    // influence product of each field pass by three kernels
+    // own kernels per evaluation (the cuFFT transforms not counted): preparation 7, the Verlet list's build 5
+    // when it ran; a field pass fp = 4 (spread, influence product, pair pass, gather; 6 with the plane
+    // transforms); polarizable: two field passes + 2 before the loop, fp + 2 per CG iteration; final 7
     int it = 0;
     for (int k = 0; k < I.nsys; k++)
         it = std::max(it, (int) I.lastResults[(size_t) k * NRES + 14]);
-    const int planes = I.usePlanes ? 2 * (2 + it) : 0;
-    return 10 + (I.s.polarizable ? 8 + 4 * it + planes : 0) + 7;
+    const int fp = I.usePlanes ? 6 : 4;
+    return 7 + (I.lastBuilt ? 5 : 0) + (I.s.polarizable ? 2 * fp + 2 + (fp + 2) * it : 0) + 7;
 }
 
 void Engine::kernelTimes(int reps, double* ms) {
@@ -1742,7 +1844,7 @@ void Engine::kernelTimes(int reps, double* ms) {
         typedef decltype(tag) R;
         ms[0] = timeIt([&] {
             k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(d);
-            k_pair_kernels<R><<<(I.n + 7) / 8, 256, 0, I.st>>>(d);
+            k_pair_compact<R><<<(I.n + 7) / 8, 256, 0, I.st>>>(d);
         });
         ms[1] = timeIt([&] { I.pairField<R, false>(I.st, d, 0); });
         ms[2] = timeIt([&] { I.launchSpread<R>(I.st, d, 1, d.x); });
@@ -1889,6 +1991,7 @@ int pairListNoAlloc(int n, const double* posDev, const double* box, double cutof
     boxInverse(box, S.recip, S.volume);
     S.cutoff = cutoff;
     S.rc2 = cutoff * cutoff;
+    S.rl2 = S.rc2;   // the list at the cutoff itself (no skin)
     S.beta = 1.0;
     S.K[0] = S.K[1] = S.K[2] = 1;
     S.atomBegin = 0;
@@ -1954,8 +2057,8 @@ int pairListNoAlloc(int n, const double* posDev, const double* box, double cutof
     if (off > NOALLOC_BYTES)
         throw std::length_error("pgm_b200: pair_list_noalloc scratch layout exceeds its array");
     d.slotAtom = slotAtomOut;
-    d.listCount = countsOut;
-    d.list = (uint32_t*) neighborsOut;
+    d.slistCount = countsOut;
+    d.slist = (uint32_t*) neighborsOut;
     Ctl c;
     std::memset(&c, 0, sizeof(c));
     c.posMode = 0;
@@ -1969,7 +2072,7 @@ int pairListNoAlloc(int n, const double* posDev, const double* box, double cutof
     CU(cudaMemsetAsync((void*) d.radius, 0, n * 8, st));
     CU(cudaMemsetAsync(d.cellCount, 0, S.cellCount * sizeof(int), st));
     const int tb = (n + 255) / 256;
-    k_prep<<<tb, 256, 0, st>>>(d, nullptr);
+    k_prep<<<tb, 256, 0, st>>>(d, nullptr, 3);
     k_cell_scan<<<1, 1024, 0, st>>>(d);
     k_cell_scatter<<<tb, 256, 0, st>>>(d);
     k_cell_sort<<<(S.cellCount + 7) / 8, 256, 0, st>>>(d);

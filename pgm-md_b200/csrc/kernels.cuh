@@ -17,16 +17,17 @@ __device__ __forceinline__ int wrapIndex(int g, int K) {
 
 // ------------------------------------------------------------------------------------------------ prep
 
-// Per atom: fractional coordinates, wrap into the primary cell, cell index (with a within-cell rank from an
-// atomic counter, made deterministic by k_cell_sort), PME base index and fraction
-// (core/pgm_core.cpp:134-152: t = s - floor(s), w = K t, base = floor(w), fr = w - base).
+// Per atom, what & 1: the positions copied in from the caller's device array, the PME base index and fraction
+// (core/pgm_core.cpp:134-152: t = s - floor(s), w = K t, base = floor(w), fr = w - base); what & 2 (a pair-list
+// build, positions already in posIn): wrap into the primary cell, cell index (with a within-cell rank from an
+// atomic counter, made deterministic by k_cell_sort) and the positions of the build.
 // posMode 0: dv.posIn (double 3n); 1: device float4 posq4 (dv.posDevice); 2: device double 3n (dv.posDevice).
-__global__ void k_prep(Dev dv, double* posCopy) {
+__global__ void k_prep(Dev dv, double* posCopy, int what) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= dv.nAtoms)
         return;
     const SysDev& S = dv.sys[dv.atomSys[i]];
-    const int posMode = dv.ctl->posMode;
+    const int posMode = (what & 1) ? dv.ctl->posMode : 0;
     double r[3];
     if (posMode == 1) {
         const float4 v = ((const float4*) dv.ctl->posDevice)[i];
@@ -55,23 +56,66 @@ __global__ void k_prep(Dev dv, double* posCopy) {
                                    __dmul_rn(r[2], S.recip[6 + a]));
         const double fl = floor(s);
         const double t = s - fl;
-        const double w = (double) S.K[a] * t;
-        const double base = floor(w);
-        dv.pmeBase[3 * i + a] = (int) base;
-        dv.pmeFr[3 * i + a] = w - base;
-        dv.wrapN[3 * i + a] = (int) fl;
-        int c = (int) floor(t * S.cellN[a]);
-        cell[a] = min(max(c, 0), S.cellN[a] - 1);
-        for (int k = 0; k < 3; k++)
-            pw[k] -= fl * S.H[3 * a + k];
+        if (what & 1) {
+            const double w = (double) S.K[a] * t;
+            const double base = floor(w);
+            dv.pmeBase[3 * i + a] = (int) base;
+            dv.pmeFr[3 * i + a] = w - base;
+        }
+        if (what & 2) {
+            dv.wrapN[3 * i + a] = (int) fl;
+            int c = (int) floor(t * S.cellN[a]);
+            cell[a] = min(max(c, 0), S.cellN[a] - 1);
+            for (int k = 0; k < 3; k++)
+                pw[k] -= fl * S.H[3 * a + k];
+        }
     }
-    const int lin = S.cellOff + (cell[0] * S.cellN[1] + cell[1]) * S.cellN[2] + cell[2];
-    dv.cellOf[i] = lin;
-    dv.cellRank[i] = atomicAdd(&dv.cellCount[lin], 1);
-    // wrapped position kept per atom until the slot copy
-    dv.Etot[3 * i] = pw[0];
-    dv.Etot[3 * i + 1] = pw[1];
-    dv.Etot[3 * i + 2] = pw[2];
+    if (what & 2) {
+        const int lin = S.cellOff + (cell[0] * S.cellN[1] + cell[1]) * S.cellN[2] + cell[2];
+        dv.cellOf[i] = lin;
+        dv.cellRank[i] = atomicAdd(&dv.cellCount[lin], 1);
+        // wrapped position kept per atom until the slot copy
+        dv.Etot[3 * i] = pw[0];
+        dv.Etot[3 * i + 1] = pw[1];
+        dv.Etot[3 * i + 2] = pw[2];
+        if (dv.posBuild)
+            for (int a = 0; a < 3; a++)
+                dv.posBuild[3 * i + a] = r[a];
+        if (i == 0)
+            dv.flags[8] = 1;   // a build
+    }
+}
+
+// Stale test of the Verlet list (core/cuda/pgm_cuda.cu:1914-1928 decides the same on the host): an atom that has
+// moved by more than half the skin since the build, or the host's request (no list yet, another box, skin 0),
+// makes flags[6] = 1; the last block then sets the build's conditional node.  Also clears the cell counters for
+// a build.
+__global__ void k_displace(Dev dv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool stale = false;
+    if (i < dv.nAtoms) {
+        const SysDev& S = dv.sys[dv.atomSys[i]];
+        double d2 = 0.0;
+        for (int a = 0; a < 3; a++) {
+            const double dx = dv.posIn[3 * i + a] - dv.posBuild[3 * i + a];
+            d2 += dx * dx;
+        }
+        stale = !(d2 <= S.skinHalf2);
+    }
+    for (int c = i; c < dv.totalCells; c += gridDim.x * blockDim.x)
+        dv.cellCount[c] = 0;
+    if (__syncthreads_or(stale) && threadIdx.x == 0)
+        atomicOr(&dv.flags[6], 1);
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&dv.flags[7], 1) == (int) gridDim.x - 1) {
+            const int st = (atomicOr(&dv.flags[6], 0) != 0 || dv.ctl->forceRebuild != 0) ? 1 : 0;
+            dv.flags[6] = st;
+            dv.flags[7] = 0;
+            if (dv.useCond)
+                cudaGraphSetConditional(dv.listCond, st ? 1u : 0u);
+        }
+    }
 }
 
 // New positions on an existing pair list (finite-difference probes of the adjoint): PME base and fraction of
@@ -211,9 +255,10 @@ __device__ __forceinline__ int systemOfCell(const Dev& dv, int c) {
 // consecutive slots with one image shift each (cells along the last dimension merged); their atoms are
 // staged through shared memory in chunks (wrapped position, original position and radius, wraps) and every
 // warp tests them against the cell's atoms it owns: a prefilter on the wrapped positions, then the
-// reference's exact test (minimum image of the original positions, r^2 < rc^2, core/pgm_core.cpp:64-87),
-// keeping a candidate only at the image that test chose, so every pair enters once.  Accepted pairs are
-// appended in candidate order (deterministic); k_pair_kernels then gives them G1, G2.
+// reference's exact test (minimum image of the original positions, core/pgm_core.cpp:64-87) at the list
+// radius (cutoff + skin), keeping a candidate only at the image that test chose, so every pair enters once.
+// Accepted pairs are appended to the Verlet list in candidate order (deterministic); k_pair_compact then takes
+// the ones within the cutoff at every evaluation.
 __global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
     __shared__ int runSlot[MAX_RUNS], runOff[MAX_RUNS + 1], runShift[MAX_RUNS];
     __shared__ double4 cPos[LIST_CHUNK], cOrig[LIST_CHUNK];
@@ -280,10 +325,10 @@ __global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
             runOff[nr] = carry;
     }
     for (int ii = cb + tid; ii < ce; ii += LIST_THREADS)
-        dv.listCount[ii] = 0;
+        dv.slistCount[ii] = 0;
     __syncthreads();
     const int total = runOff[nr];
-    const double pre = S.rc2 * (1.0 + 1e-10) + 1e-300, preLo = S.rc2 * (1.0 - 1e-10);
+    const double pre = S.rl2 * (1.0 + 1e-10) + 1e-300, preLo = S.rl2 * (1.0 - 1e-10);
     const double half0 = 0.5 * S.H[0] * (1.0 - 1e-10), half1 = 0.5 * S.H[4] * (1.0 - 1e-10),
                  half2 = 0.5 * S.H[8] * (1.0 - 1e-10);
     const double invDiag[3] = {1.0 / S.H[0], 1.0 / S.H[4], 1.0 / S.H[8]};
@@ -315,8 +360,8 @@ __global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
             const double4 pwi = dv.posS[ii];
             const double4 oi = dv.origS[ii];
             const int4 wi = dv.wrapS[ii];
-            uint32_t* row = dv.list + (size_t) ii * dv.cap;
-            int count = dv.listCount[ii];
+            uint32_t* row = dv.slist + (size_t) ii * dv.cap;
+            int count = dv.slistCount[ii];
             int qn = 0;   // prefilter survivors queued (candidate order) for the exact test
             for (int t0 = 0; t0 < nc; t0 += 32) {
                 const int t = t0 + lane;
@@ -356,7 +401,7 @@ __global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
                         double x[3] = {__dsub_rn(oi.x, oj.x), __dsub_rn(oi.y, oj.y), __dsub_rn(oi.z, oj.z)};
                         int kk[3];
                         minImageFast(x, S.H, invDiag, kk);
-                        if (dot3exact(x) < S.rc2)   // image of the exact test relative to the wrapped positions
+                        if (dot3exact(x) < S.rl2)   // image of the exact test relative to the wrapped positions
                             acc = (kk[0] - (wi.x - cw.x) == w0 && kk[1] - (wi.y - cw.y) == w1 &&
                                    kk[2] - (wi.z - cw.z) == w2);
                     }
@@ -380,15 +425,15 @@ __global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
                 }
             }
             if (lane == 0)
-                dv.listCount[ii] = count;
+                dv.slistCount[ii] = count;
         }
         __syncthreads();
     }
     for (int ii = cb + tid; ii < ce; ii += LIST_THREADS) {
-        const int cnt = dv.listCount[ii];
+        const int cnt = dv.slistCount[ii];
         if (cnt > dv.cap) {
             atomicMax(&dv.flags[0], cnt);
-            dv.listCount[ii] = dv.cap;
+            dv.slistCount[ii] = dv.cap;
         }
     }
 }
@@ -426,6 +471,90 @@ __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
         g.y = G[2];
         grow[t] = g;
     }
+}
+
+// The pairs of the Verlet list within the cutoff at this evaluation's positions, with their G1, G2 in precision
+// R (core/pgm_math.h:77-93 via pairKernels): one warp per slot, the list's row in candidate order over the
+// lanes, compacted by ballot into the row of the evaluation's list (same order, deterministic).  The test is
+// the list build's at the cutoff: a prefilter on the wrapped positions, the reference's exact test
+// (core/pgm_core.cpp:64-87) only near the cutoff or near half a box edge.  A pair within the cutoff whose exact
+// image is not the one stored at the build sets flags[9]: the list is rebuilt and the evaluation repeated.
+template <typename R>
+__global__ void __launch_bounds__(256) k_pair_compact(Dev dv) {
+    typedef typename V2T<R>::T R2;
+    const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (slot >= dv.nAtoms)
+        return;
+    const SysDev& S = dv.sys[dv.atomSys[dv.slotAtom[slot]]];
+    const double4 pwi = dv.posS[slot];
+    const double4 oi = dv.origS[slot];
+    const int4 wi = dv.wrapS[slot];
+    const double Ri = dv.radS[slot];
+    const uint32_t* srow = dv.slist + (size_t) slot * dv.cap;
+    uint32_t* row = dv.list + (size_t) slot * dv.cap;
+    R2* grow = (R2*) dv.G12 + (size_t) slot * dv.cap;
+    const int cnt = dv.slistCount[slot];
+    const R beta = (R) S.beta;
+    const double pre = S.rc2 * (1.0 + 1e-10) + 1e-300, preLo = S.rc2 * (1.0 - 1e-10);
+    const double half0 = 0.5 * S.H[0] * (1.0 - 1e-10), half1 = 0.5 * S.H[4] * (1.0 - 1e-10),
+                 half2 = 0.5 * S.H[8] * (1.0 - 1e-10);
+    const double invDiag[3] = {1.0 / S.H[0], 1.0 / S.H[4], 1.0 / S.H[8]};
+    int count = 0;
+    for (int t0 = 0; t0 < cnt; t0 += 32) {
+        const int t = t0 + lane;
+        bool acc = false;
+        uint32_t e = 0;
+        double x0 = 0, x1 = 0, x2 = 0;
+        int js = 0;
+        if (t < cnt) {
+            e = srow[t];
+            js = entrySlot(e);
+            double sh[3];
+            entryShift(e, S.H, sh);
+            const double4 pwj = dv.posS[js];
+            x0 = pwi.x - pwj.x - sh[0];
+            x1 = pwi.y - pwj.y - sh[1];
+            x2 = pwi.z - pwj.z - sh[2];
+            const double r2 = x0 * x0 + x1 * x1 + x2 * x2;
+            if (r2 < pre) {
+                if (r2 < preLo && fabs(x0) < half0 && fabs(x1) < half1 && fabs(x2) < half2) {
+                    acc = true;
+                } else {
+                    const double4 oj = dv.origS[js];
+                    const int4 wj = dv.wrapS[js];
+                    double x[3] = {__dsub_rn(oi.x, oj.x), __dsub_rn(oi.y, oj.y), __dsub_rn(oi.z, oj.z)};
+                    int kk[3];
+                    minImageFast(x, S.H, invDiag, kk);
+                    if (dot3exact(x) < S.rc2) {
+                        const int w0 = (int) ((e >> 23) & 7u) - 4, w1 = (int) ((e >> 26) & 7u) - 4,
+                                  w2 = (int) ((e >> 29) & 7u) - 4;
+                        acc = (kk[0] - (wi.x - wj.x) == w0 && kk[1] - (wi.y - wj.y) == w1 &&
+                               kk[2] - (wi.z - wj.z) == w2);
+                        if (!acc)
+                            atomicOr(&dv.flags[9], 1);
+                    }
+                }
+            }
+        }
+        const unsigned ma = __ballot_sync(0xffffffffu, acc);
+        if (acc) {
+            const int pos = count + __popc(ma & ((1u << lane) - 1u));
+            row[pos] = e;
+            const R Rj = (R) dv.radS[js], Rr = (R) Ri;
+            const R xr0 = (R) x0, xr1 = (R) x1, xr2 = (R) x2;
+            const R r = fsqrt(xr0 * xr0 + xr1 * xr1 + xr2 * xr2);
+            const R a = R(1) / fsqrt(R(2) * (Rr * Rr + Rj * Rj));
+            R G[3];
+            pairKernels<R, 3>(a, beta, r, G);
+            R2 g;
+            g.x = G[1];
+            g.y = G[2];
+            grow[pos] = g;
+        }
+        count += __popc(ma);
+    }
+    if (lane == 0)
+        dv.listCount[slot] = count;
 }
 
 // ------------------------------------------------------------------------------------------------ dipoles
