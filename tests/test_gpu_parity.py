@@ -216,3 +216,18 @@ def test_mixed_fp64_refinement():
     assert err_ref <= 1e-8 and err_ref < err_plain / 10, (err_plain, err_ref)
     assert abs(rr.energy - float(d["energy"])) <= 1e-7 * abs(float(d["energy"]))
     assert rel_rms(rr.forces, d["forces"]) <= 1e-5
+
+
+@pytest.mark.parametrize("order", [4, 5, 7, 8])
+def test_other_spline_orders(order):
+    """Spline orders other than 6: the kernels with the order as a compile-time constant (4, 5, 8) and with the
+    order at run time (7) against the oracle (FP64: 1e-7 energy, 1e-6 forces)."""
+    S = PKG.systems.tiny_triclinic(nmol=16, seed=21)
+    S.order = order
+    eng = make_engine(S, PKG.FP64)
+    r = eng.compute(S.pos, S.box)
+    ora = O.Engine(oracle_topology(S), oracle_settings(S))
+    e = ora.compute(S.pos, S.box)
+    assert abs(r.energy - e) <= 1e-7 * abs(e)
+    assert rel_rms(r.forces, ora.forces) <= 1e-6
+
