@@ -92,7 +92,8 @@ struct Dev {
     double* posBuild;         // 3n positions at the list's build
     uint32_t* list;           // [slot][cap] pairs within the cutoff
     int* listCount;           // per slot
-    void* G12;                // [slot][cap] R2
+    void* pairA;              // [slot][cap] R4: pair geometry x = r_i - r_j (image) and G1, per evaluation
+    void* pairB;              // [slot][cap] R2: G2 and the slot of j (as the bits of an R)
     int* flags;               // [0]: list overflow, [1]: shift out of range, [2]: all systems done, [3]-[5] CG
                               // bookkeeping, [6]: list stale, [7]: block counter, [8]: list built,
                               // [9]: a pair changed its image since the build (rebuild and repeat)
@@ -158,6 +159,11 @@ template <> struct V4T<double> { typedef double4 T; };
 template <typename R> struct V2T;
 template <> struct V2T<float> { typedef float2 T; };
 template <> struct V2T<double> { typedef double2 T; };
+// The slot of j carried in a pair record's R lane: the int's bits in a float, its value in a double.
+__device__ __forceinline__ float slotAsReal(int js, float) { return __int_as_float(js); }
+__device__ __forceinline__ double slotAsReal(int js, double) { return (double) js; }
+__device__ __forceinline__ int realAsSlot(float v) { return __float_as_int(v); }
+__device__ __forceinline__ int realAsSlot(double v) { return (int) v; }
 template <typename R> struct CplxT;
 template <> struct CplxT<float> { typedef cufftComplex T; };
 template <> struct CplxT<double> { typedef cufftDoubleComplex T; };

@@ -154,13 +154,13 @@ struct Engine::Impl {
 
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
-        dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dG12, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
+        dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dPairA, dPairB, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
         dScal, dPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
         dGradQ, dGradR, dSList, dSListCount, dPosBuild;
     // FP64 shadow of the mixed path for the iterative refinement
-    Buf dG12d, dDSd, dGridD, dSpecD, dInflD, dSplD, dB64, dXsave;
+    Buf dPairBd, dDSd, dGridD, dSpecD, dInflD, dSplD, dB64, dXsave;
     std::vector<std::pair<cufftHandle, cufftHandle>> plans64;
     // pinned host staging
     double* hPos = nullptr;
@@ -221,12 +221,12 @@ struct Engine::Impl {
         }
         plans64.clear();
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
-                      &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dG12, &dFlags, &dDS,
+                      &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dPairA, &dPairB, &dFlags, &dDS,
                       &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
                       &dCovByAtomOff, &dCovByAtom, &dCovByPartnerOff, &dCovByPartner, &dChunkSys, &dChunkBegin,
-                      &dChunkEnd, &dHist, &dGlobal, &dCtl, &dGradQ, &dGradR, &dG12d, &dDSd, &dGridD, &dSpecD,
+                      &dChunkEnd, &dHist, &dGlobal, &dCtl, &dGradQ, &dGradR, &dPairBd, &dDSd, &dGridD, &dSpecD,
                       &dInflD, &dSplD, &dB64, &dXsave, &dSList, &dSListCount, &dPosBuild};
         for (Buf* b : all)
             b->release();
@@ -743,9 +743,11 @@ struct Engine::Impl {
         listValid = false;
         dList.ensure((size_t) n * cap * sizeof(uint32_t));
         dSList.ensure((size_t) n * cap * sizeof(uint32_t));
-        dG12.ensure((size_t) n * cap * 2 * realSize());
+        if (mixed())   // pair records: (x, G1) + (G2, slot of j) in float; FP64 (G1, G2) only
+            dPairA.ensure((size_t) n * cap * 16);
+        dPairB.ensure((size_t) n * cap * 2 * realSize());
         if (refining())
-            dG12d.ensure((size_t) n * cap * 16);
+            dPairBd.ensure((size_t) n * cap * 16);
     }
 
     bool refining() const { return mixed() && s.refine && s.polarizable; }
@@ -753,7 +755,8 @@ struct Engine::Impl {
     // The mixed path's device pointers with the FP64 shadow buffers in place of the R-typed ones.
     Dev makeDev64() {
         Dev d = makeDev(false, 0);
-        d.G12 = dG12d.p;
+        d.pairA = nullptr;
+        d.pairB = dPairBd.p;
         d.dS = dDSd.p;
         d.grid = dGridD.p;
         d.spec = dSpecD.p;
@@ -806,7 +809,8 @@ struct Engine::Impl {
         d.slist = dSList.as<uint32_t>();
         d.slistCount = dSListCount.as<int>();
         d.posBuild = dPosBuild.as<double>();
-        d.G12 = dG12.p;
+        d.pairA = dPairA.p;
+        d.pairB = dPairB.p;
         d.flags = dFlags.as<int>();
         d.dS = dDS.p;
         d.perm = dPerm.as<double>();

@@ -438,11 +438,20 @@ __global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
     }
 }
 
-// G1, G2 of every listed pair in precision R (core/pgm_math.h:77-93 via pairKernels), one warp per slot, the
-// pairs of its row over the lanes: separate from the list build so that every lane of a warp evaluates one.
+// Pair records.  Mixed precision (float): pairA = (x, G1) with x = pw_i - pw_j - w.H rounded to float,
+// pairB = (G2, slot of j), so that the field passes stream them and gather only (d_j, q_j).  FP64: pairB =
+// (G1, G2), the field passes form x from the slot-order positions (streaming 48-byte double records is slower
+// there than the L1-resident position gathers).
+template <typename R> struct PairRec { static constexpr bool storeX = false; };
+template <> struct PairRec<float> { static constexpr bool storeX = true; };
+
+// The pair records of every listed pair (the list of the evaluation) in precision R with G1, G2 by
+// core/pgm_math.h:77-93 via pairKernels, one warp per slot, the pairs of its row over the lanes.
 template <typename R>
 __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
     typedef typename V2T<R>::T R2;
+    typedef typename V4T<R>::T R4;
+    constexpr bool STORE_X = PairRec<R>::storeX;
     const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (slot >= dv.nAtoms)
         return;
@@ -450,7 +459,8 @@ __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
     const double4 pwi = dv.posS[slot];
     const double Ri = dv.radS[slot];
     const uint32_t* row = dv.list + (size_t) slot * dv.cap;
-    R2* grow = (R2*) dv.G12 + (size_t) slot * dv.cap;
+    R4* arow = (R4*) dv.pairA + (size_t) slot * dv.cap;
+    R2* brow = (R2*) dv.pairB + (size_t) slot * dv.cap;
     const int cnt = dv.listCount[slot];
     const R beta = (R) S.beta;
     for (int t = lane; t < cnt; t += 32) {
@@ -466,22 +476,36 @@ __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
         const R a = R(1) / fsqrt(R(2) * (Rr * Rr + Rj * Rj));
         R G[3];
         pairKernels<R, 3>(a, beta, r, G);
-        R2 g;
-        g.x = G[1];
-        g.y = G[2];
-        grow[t] = g;
+        R2 vb;
+        if constexpr (STORE_X) {
+            R4 va;
+            va.x = xr0;
+            va.y = xr1;
+            va.z = xr2;
+            va.w = G[1];
+            arow[t] = va;
+            vb.x = G[2];
+            vb.y = slotAsReal(js, R(0));
+        } else {
+            vb.x = G[1];
+            vb.y = G[2];
+        }
+        brow[t] = vb;
     }
 }
 
-// The pairs of the Verlet list within the cutoff at this evaluation's positions, with their G1, G2 in precision
-// R (core/pgm_math.h:77-93 via pairKernels): one warp per slot, the list's row in candidate order over the
-// lanes, compacted by ballot into the row of the evaluation's list (same order, deterministic).  The test is
+// The pairs of the Verlet list within the cutoff at this evaluation's positions with their records (x rounded to
+// R, G1, G2 in precision R by core/pgm_math.h:77-93 via pairKernels, the slot of j): one warp per slot, the
+// list's row in candidate order over the lanes, compacted by ballot into the row of the evaluation's list
+// (same order, deterministic), then the radial kernels over the kept pairs.  The test is
 // the list build's at the cutoff: a prefilter on the wrapped positions, the reference's exact test
 // (core/pgm_core.cpp:64-87) only near the cutoff or near half a box edge.  A pair within the cutoff whose exact
 // image is not the one stored at the build sets flags[9]: the list is rebuilt and the evaluation repeated.
 template <typename R>
 __global__ void __launch_bounds__(256) k_pair_compact(Dev dv) {
     typedef typename V2T<R>::T R2;
+    typedef typename V4T<R>::T R4;
+    constexpr bool STORE_X = PairRec<R>::storeX;
     const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (slot >= dv.nAtoms)
         return;
@@ -492,7 +516,8 @@ __global__ void __launch_bounds__(256) k_pair_compact(Dev dv) {
     const double Ri = dv.radS[slot];
     const uint32_t* srow = dv.slist + (size_t) slot * dv.cap;
     uint32_t* row = dv.list + (size_t) slot * dv.cap;
-    R2* grow = (R2*) dv.G12 + (size_t) slot * dv.cap;
+    R4* arow = (R4*) dv.pairA + (size_t) slot * dv.cap;
+    R2* brow = (R2*) dv.pairB + (size_t) slot * dv.cap;
     const int cnt = dv.slistCount[slot];
     const R beta = (R) S.beta;
     const double pre = S.rc2 * (1.0 + 1e-10) + 1e-300, preLo = S.rc2 * (1.0 - 1e-10);
@@ -540,21 +565,57 @@ __global__ void __launch_bounds__(256) k_pair_compact(Dev dv) {
         if (acc) {
             const int pos = count + __popc(ma & ((1u << lane) - 1u));
             row[pos] = e;
-            const R Rj = (R) dv.radS[js], Rr = (R) Ri;
-            const R xr0 = (R) x0, xr1 = (R) x1, xr2 = (R) x2;
-            const R r = fsqrt(xr0 * xr0 + xr1 * xr1 + xr2 * xr2);
-            const R a = R(1) / fsqrt(R(2) * (Rr * Rr + Rj * Rj));
-            R G[3];
-            pairKernels<R, 3>(a, beta, r, G);
-            R2 g;
-            g.x = G[1];
-            g.y = G[2];
-            grow[pos] = g;
+            if constexpr (STORE_X) {
+                R4 va;
+                va.x = (R) x0;
+                va.y = (R) x1;
+                va.z = (R) x2;
+                va.w = (R) 0;
+                arow[pos] = va;
+            }
         }
         count += __popc(ma);
     }
     if (lane == 0)
         dv.listCount[slot] = count;
+    __syncwarp();
+    // G1, G2 of the kept pairs, every lane busy (the radial kernels branch per pair)
+    const R Rr = (R) Ri;
+    for (int t = lane; t < count; t += 32) {
+        const uint32_t e = row[t];
+        const int js = entrySlot(e);
+        R xr0, xr1, xr2;
+        R4 va;
+        if constexpr (STORE_X) {
+            va = arow[t];
+            xr0 = va.x;
+            xr1 = va.y;
+            xr2 = va.z;
+        } else {
+            double sh[3];
+            entryShift(e, S.H, sh);
+            const double4 pwj = dv.posS[js];
+            xr0 = (R) (pwi.x - pwj.x - sh[0]);
+            xr1 = (R) (pwi.y - pwj.y - sh[1]);
+            xr2 = (R) (pwi.z - pwj.z - sh[2]);
+        }
+        const R Rj = (R) dv.radS[js];
+        const R r = fsqrt(xr0 * xr0 + xr1 * xr1 + xr2 * xr2);
+        const R a = R(1) / fsqrt(R(2) * (Rr * Rr + Rj * Rj));
+        R G[3];
+        pairKernels<R, 3>(a, beta, r, G);
+        R2 vb;
+        if constexpr (STORE_X) {
+            va.w = G[1];
+            arow[t] = va;
+            vb.x = G[2];
+            vb.y = slotAsReal(js, R(0));
+        } else {
+            vb.x = G[1];
+            vb.y = G[2];
+        }
+        brow[t] = vb;
+    }
 }
 
 // ------------------------------------------------------------------------------------------------ dipoles
@@ -1297,6 +1358,8 @@ __global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
 
 // Direct field at slot's atom of the dipoles (and with WITHQ the charges) of its list: E_i += q_j x G1 - d_j G1
 // + (d_j . x) x G2 (core/pgm_core.cpp:274-284), products in precision R, sums in double.  GS lanes per atom.
+// Mixed: the pair records (x, G1, G2, slot of j) stream from the evaluation's list and only (d_j, q_j) is
+// gathered; FP64: x from the gathered slot-order positions, (G1, G2) streamed.
 template <typename R, bool WITHQ, int GS>
 __global__ void __launch_bounds__(256) k_pair_field(Dev dv, int gateDone) {
     typedef typename V4T<R>::T R4;
@@ -1309,30 +1372,47 @@ __global__ void __launch_bounds__(256) k_pair_field(Dev dv, int gateDone) {
     const int s = dv.atomSys[i];
     if (gateDone && dv.scal[s * NSCAL + SC_DONE] != 0.0)
         return;
-    const SysDev& S = dv.sys[s];
-    const double4 pwi = dv.posS[slot];
-    const uint32_t* row = dv.list + (size_t) slot * dv.cap;
-    const R2* grow = (const R2*) dv.G12 + (size_t) slot * dv.cap;
+    const R4* arow = (const R4*) dv.pairA + (size_t) slot * dv.cap;
+    const R2* brow = (const R2*) dv.pairB + (size_t) slot * dv.cap;
     const R4* dS = (const R4*) dv.dS;
     const int cnt = dv.listCount[slot];
     R a0 = 0, a1 = 0, a2 = 0;   // per-lane sums in R (about cnt / GS terms each), across lanes in double
+    if constexpr (PairRec<R>::storeX) {
 #pragma unroll 4
-    for (int t = lane; t < cnt; t += GS) {
-        const uint32_t e = row[t];
-        const R2 G = grow[t];
-        const int js = entrySlot(e);
-        double sh[3];
-        entryShift(e, S.H, sh);
-        const double4 pwj = dv.posS[js];
-        const R x0 = (R) (pwi.x - pwj.x - sh[0]), x1 = (R) (pwi.y - pwj.y - sh[1]), x2 = (R) (pwi.z - pwj.z - sh[2]);
-        const R4 dj = dS[js];
-        const R djx = dj.x * x0 + dj.y * x1 + dj.z * x2;
-        R c = djx * G.y;
-        if (WITHQ)
-            c += dj.w * G.x;
-        a0 += c * x0 - dj.x * G.x;
-        a1 += c * x1 - dj.y * G.x;
-        a2 += c * x2 - dj.z * G.x;
+        for (int t = lane; t < cnt; t += GS) {
+            const R4 xg = arow[t];
+            const R2 gb = brow[t];
+            const R4 dj = dS[realAsSlot(gb.y)];
+            const R djx = dj.x * xg.x + dj.y * xg.y + dj.z * xg.z;
+            R c = djx * gb.x;
+            if (WITHQ)
+                c += dj.w * xg.w;
+            a0 += c * xg.x - dj.x * xg.w;
+            a1 += c * xg.y - dj.y * xg.w;
+            a2 += c * xg.z - dj.z * xg.w;
+        }
+    } else {
+        const SysDev& S = dv.sys[s];
+        const double4 pwi = dv.posS[slot];
+        const uint32_t* row = dv.list + (size_t) slot * dv.cap;
+#pragma unroll 4
+        for (int t = lane; t < cnt; t += GS) {
+            const uint32_t e = row[t];
+            const R2 G = brow[t];
+            const int js = entrySlot(e);
+            double sh[3];
+            entryShift(e, S.H, sh);
+            const double4 pwj = dv.posS[js];
+            const R x0 = (R) (pwi.x - pwj.x - sh[0]), x1 = (R) (pwi.y - pwj.y - sh[1]), x2 = (R) (pwi.z - pwj.z - sh[2]);
+            const R4 dj = dS[js];
+            const R djx = dj.x * x0 + dj.y * x1 + dj.z * x2;
+            R c = djx * G.y;
+            if (WITHQ)
+                c += dj.w * G.x;
+            a0 += c * x0 - dj.x * G.x;
+            a1 += c * x1 - dj.y * G.x;
+            a2 += c * x2 - dj.z * G.x;
+        }
     }
     double E0 = a0, E1 = a1, E2 = a2;
     const unsigned gm = groupMask<GS>();
