@@ -35,6 +35,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "pGM E+F evals/s, 8550-atom PME, mixed vs FP64 GPU at force relRMS≤1e-5"
 WORKLOAD = "dimethylphenol8550"
 TOL = 1e-5
+TRANSFORMS = {0: "cuFFT + influence product", 1: "cluster kernel"}
 
 
 def parse():
@@ -49,7 +50,7 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run for ncu: only warmup + steps evaluations of one precision, no other legs")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="with --profile")
-    ap.add_argument("--profile-workload", default=WORKLOAD, choices=[WORKLOAD, "water98304"],
+    ap.add_argument("--profile-workload", default=WORKLOAD, choices=[WORKLOAD, "water98304", "water_batch1024"],
                     help="with --profile: the system evaluated")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 1024-system leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 98304-atom leg")
@@ -391,6 +392,23 @@ def main():
 
     stream = torch.cuda.current_stream(dev)
     if args.profile:
+        if args.profile_workload == "water_batch1024":
+            systems = pkg.systems.water_batch(nsys=1024, seed=1024, tol=1e-5)
+            eng = pkg.Engine(pkg.Settings(cutoff=0.9, beta=3.5, grid=(24, 24, 24), order=6, tol=1e-5, max_iter=200,
+                                          peek=0.65, predictor=0, ke=pkg.systems.KE_DEFAULT,
+                                          precision=pkg.MIXED if args.precision == "mixed" else pkg.FP64,
+                                          device=local, skin=0.0))
+            eng.set_systems(systems)
+            pos = np.concatenate([s.pos for s in systems])
+            boxes = np.stack([s.box for s in systems])
+            eng.set_pair_lanes(16)
+            for _ in range(args.warmup + args.steps):
+                r = eng.compute_batch(pos, boxes)
+            print(json.dumps({"profile": args.precision, "workload": "water_batch1024",
+                              "evaluations": args.warmup + args.steps, "max_iterations": int(r["iterations"].max()),
+                              "launches_per_eval": eng.kernel_launches()}))
+            eng.close()
+            return 0
         if args.profile_workload == "water98304":
             S = pkg.systems.water98304(tol=TOL)
         eng = make(pkg.MIXED if args.precision == "mixed" else pkg.FP64)
@@ -453,7 +471,7 @@ def main():
     # FP64 path on the same input (the metric's denominator)
     fp64 = make(pkg.FP64)
     fp64.compute(S.pos, S.box)
-    fp64.set_pair_lanes(lanes)
+    lanes64 = fp64.autotune(S.pos, S.box)
     fsteps = max(3, min(args.steps, 20))
     ms_fp64, its_fp64 = timed_resident(fp64, fsteps, 3)
     t = torch.tensor([ms_fp64], dtype=torch.float64, device=dev)
@@ -468,6 +486,7 @@ def main():
     kept.set_system(S)
     kept.compute(S.pos, S.box)
     kept.set_pair_lanes(lanes)
+    kept.set_transforms(mixed.transforms())
     ms_kept, _ = timed_resident(kept, fsteps, 3)
     t = torch.tensor([ms_kept], dtype=torch.float64, device=dev)
     if world > 1:
@@ -501,8 +520,10 @@ def main():
             "warmup": max(args.warmup, 3), "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
             "config": config(S, {"parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                                 "pair_lanes": lanes, "cg_iterations": int(np.median(its_mixed))}),
-            "fp64": {"value": fp64_value, "unit": "evals/s", "steps": fsteps,
+                                 "pair_lanes": lanes, "transforms": TRANSFORMS[mixed.transforms()],
+                                 "cg_iterations": int(np.median(its_mixed))}),
+            "fp64": {"value": fp64_value, "unit": "evals/s", "steps": fsteps, "pair_lanes": lanes64,
+                     "transforms": TRANSFORMS[fp64.transforms()],
                      "cg_iterations": int(np.median(its_fp64)), "kernel_ms": kt64},
             "mixed_over_fp64": value / fp64_value,
             "kept_list": {"value": kept_value, "unit": "evals/s", "steps": fsteps, "list_builds": kept_builds,
@@ -581,7 +602,8 @@ def large_leg(pkg, local, world, dist):
 
 
 def batch_leg(pkg, local, rank, world, dist):
-    """1024 independent water boxes of 8..512 molecules (0.0334 / A^3, ~1 A grids, cutoff min(9 A, L/2),
+    """1024 independent water boxes of 8..512 molecules (0.0334 / A^3, grids <= 1 A spacing with 2-3-5 sizes,
+    cutoff min(9 A, L/2),
     tol 1e-5, mixed) in one launch per rank (systems partitioned by atom count across ranks), against the same
     systems evaluated one after the other by single-system engines (a sample of 64, on rank 0)."""
     import torch
@@ -595,16 +617,28 @@ def batch_leg(pkg, local, rank, world, dist):
     eng.set_systems(mine)
     pos = np.concatenate([s.pos for s in mine])
     boxes = np.stack([s.box for s in mine])
+    lanes = eng.autotune(pos, boxes, reps=3)
+    chosen = eng.transforms()
     res = {}
-    dt = _timed(lambda: res.__setitem__("r", eng.compute_batch(pos, boxes)), 5, 2)
-    t = torch.tensor([dt], dtype=torch.float64, device=f"cuda:{local}")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dt = float(t.item())
+    per_mode = {}
+    for mode in (0, 1):   # both kinds of transforms timed (every rank the same steps); the autotuned one reported
+        eng.set_transforms(mode)
+        if eng.transforms() != mode:
+            continue
+        dt = _timed(lambda: res.__setitem__("r", eng.compute_batch(pos, boxes)), 5, 2)
+        t = torch.tensor([dt], dtype=torch.float64, device=f"cuda:{local}")
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        per_mode[mode] = float(t.item())
+    eng.set_transforms(chosen)
+    res["r"] = eng.compute_batch(pos, boxes)
+    dt = per_mode[chosen]
     energies = sh.gather_energies(parts[rank], res["r"]["energies"], len(systems))
     out = {"workload": "water_batch1024", "systems": len(systems), "atoms": int(sum(s.n for s in systems)),
            "systems_per_s": len(systems) / dt, "ms_per_batch": 1e3 * dt,
            "max_cg_iterations": int(res["r"]["iterations"].max()), "partition": "atom-balanced, one launch per rank",
+           "pair_lanes": lanes, "transforms": TRANSFORMS[chosen],
+           "ms_per_batch_by_transforms": {TRANSFORMS[m]: 1e3 * v for m, v in per_mode.items()},
            "energies_finite": bool(np.isfinite(energies).all())}
     eng.close()
     if rank == 0:

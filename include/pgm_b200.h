@@ -163,6 +163,12 @@ int pgm_engine_kernel_launches(pgm_engine* e);
 int pgm_engine_kernel_times(pgm_engine* e, int reps, double* ms);
 int pgm_engine_set_pair_lanes(pgm_engine* e, int lanes);
 int pgm_engine_pair_lanes(pgm_engine* e);
+/* Field-pass transforms (the autotuner's second knob; no counterpart in the reference, which calls cuFFT):
+ * 0 cuFFT R2C / C2R plans with an influence-product kernel, 1 one kernel per pass in which a thread-block
+ * cluster per system holds the half spectrum in distributed shared memory (grids up to 64 points per dimension
+ * with prime factors 2, 3, 5).  pgm_engine_transforms: the kind in use (1 only where the grids allow it). */
+int pgm_engine_set_transforms(pgm_engine* e, int mode);
+int pgm_engine_transforms(pgm_engine* e);
 
 /* Batched evaluation: nsys independent systems of uneven sizes in one launch.  Atom arrays are the systems'
  * arrays concatenated; atom_count[s] atoms per system; per-system cutoff, beta and grid (3 ints); covalent

@@ -70,6 +70,8 @@ SIGNATURES = {
     "pgm_engine_kernel_times": (c_int, [c_void_p, c_int, P_D]),
     "pgm_engine_set_pair_lanes": (c_int, [c_void_p, c_int]),
     "pgm_engine_pair_lanes": (c_int, [c_void_p]),
+    "pgm_engine_set_transforms": (c_int, [c_void_p, c_int]),
+    "pgm_engine_transforms": (c_int, [c_void_p]),
     "pgm_engine_set_systems": (c_int, [c_void_p, c_int, P_I, P_D, P_D, P_I, P_D, P_D, P_D, P_I, P_I, P_I, P_D]),
     "pgm_engine_compute_batch": (c_int, [c_void_p, P_D, P_D, P_D, P_D, P_D, P_I]),
     "pgm_pair_list_noalloc": (c_int, [c_int, c_void_p, P_D, c_double, c_int, c_void_p, c_void_p, c_void_p, c_void_p,

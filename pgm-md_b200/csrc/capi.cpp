@@ -354,6 +354,13 @@ int pgm_engine_set_pair_lanes(pgm_engine* e, int lanes) {
 
 int pgm_engine_pair_lanes(pgm_engine* e) { return (e && e->e) ? e->e->pairLanes() : -1; }
 
+int pgm_engine_set_transforms(pgm_engine* e, int mode) {
+    NEED(e);
+    return guarded([&] { e->e->setTransforms(mode); });
+}
+
+int pgm_engine_transforms(pgm_engine* e) { return (e && e->e) ? e->e->transforms() : -1; }
+
 int pgm_engine_set_systems(pgm_engine* e, int nsys, const int* atom_count, const double* cutoff, const double* beta,
                            const int* grid, const double* q, const double* radius, const double* alpha,
                            const int* cov_count, const int* cov_atom, const int* cov_partner, const double* strength) {

@@ -36,6 +36,7 @@ struct SysDev {
     int chunkFirst, chunkCount;
     int convBlocks;
     int covBegin, covEnd;
+    int twOff[3];         // offsets of the twiddle tables of K[0..2] in the engine's table (cluster transforms)
 };
 
 // Per-call control, read by the kernels from device memory so that one captured graph serves every call.
@@ -129,6 +130,9 @@ struct Dev {
     void* grid;               // R, gridTotal
     void* spec;               // complex R
     void* infl;               // R, spec size
+    const void* twiddle;      // complex R tables exp(-2 pi i m / K), m < K, per distinct K (cluster transforms)
+    int fftcBuf;              // complex elements per transform buffer of a cluster block
+    int fftcC;                // blocks per cluster
     const double* moduli;
     // covalent
     int ncov;

@@ -149,14 +149,18 @@ struct Engine::Impl {
     int totalCells = 0, cellCapacity = 0;
     int cap = 0;
     int convBlocks = 1;
-    bool usePlanes = false;
+    bool useCluster = false;   // field-pass transforms by the cluster kernel (else cuFFT + influence product)
+    bool wantCluster = false;  // the caller's choice (setTransforms)
+    bool clusterOk = false;    // the systems' grids and the GPU allow the cluster kernel
+    int fftcBuf = 0, fftcC = 16;
+    size_t fftcSmem = 0;
     bool configured = false, atomsSet = false;
 
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
         dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dPairA, dPairB, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
         dScal, dPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
-        dConvPartial, dConvOff, dGrid, dSpec, dInfl, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
+        dConvPartial, dConvOff, dGrid, dSpec, dInfl, dTwiddle, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
         dGradQ, dGradR, dSList, dSListCount, dPosBuild;
     // FP64 shadow of the mixed path for the iterative refinement
@@ -224,7 +228,7 @@ struct Engine::Impl {
                       &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dPairA, &dPairB, &dFlags, &dDS,
                       &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
-                      &dConvOff, &dGrid, &dSpec, &dInfl, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
+                      &dConvOff, &dGrid, &dSpec, &dInfl, &dTwiddle, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
                       &dCovByAtomOff, &dCovByAtom, &dCovByPartnerOff, &dCovByPartner, &dChunkSys, &dChunkBegin,
                       &dChunkEnd, &dHist, &dGlobal, &dCtl, &dGradQ, &dGradR, &dPairBd, &dDSd, &dGridD, &dSpecD,
                       &dInflD, &dSplD, &dB64, &dXsave, &dSList, &dSListCount, &dPosBuild};
@@ -279,9 +283,10 @@ struct Engine::Impl {
         CU(cudaMallocHost((void**) &hCtl, sizeof(Ctl)));
         useGraph = envInt("PGM_B200_NO_GRAPH", 0) == 0;
         pairGS = envInt("PGM_B200_PAIR_LANES", 32);
-        // the field pair pass runs beside the transforms of the same pass: at most pairBlocks of its blocks per SM
-        // (a shared-memory reservation it does not use), so the transform kernels find room at once
-        const int pairBlocks = envInt("PGM_B200_PAIR_BLOCKS", 3);
+        wantCluster = envInt("PGM_B200_CLUSTER_FFT", 0) != 0;
+        // the field pair pass runs beside the transforms of the same pass: optionally at most pairBlocks of its
+        // blocks per SM (a shared-memory reservation it does not use), so that the transform kernels find room
+        const int pairBlocks = envInt("PGM_B200_PAIR_BLOCKS", 0);
         int smPerSM = 0, smPerBlock = 0;
         CU(cudaDeviceGetAttribute(&smPerSM, cudaDevAttrMaxSharedMemoryPerMultiprocessor, devId));
         CU(cudaDeviceGetAttribute(&smPerBlock, cudaDevAttrMaxSharedMemoryPerBlockOptin, devId));
@@ -523,23 +528,69 @@ struct Engine::Impl {
                 fprintf(stderr, "pgm_b200 trace: FFT group %dx%dx%d, %d systems from %d, grid offset %lld, spectrum "
                         "offset %lld\n", g.K[0], g.K[1], g.K[2], g.count, g.first, g.gridOff, g.specOff);
         convBlocks = std::max(1, std::min(512, (maxSpec + 255) / 256));
-        // the plane transforms (one system, 2-3-5 grid up to PLANE_MAXK) on request: alone they take less time than
-        // the cuFFT chain, beside the pair pass of the same field pass they take more
-        usePlanes = nsys == 1 && envInt("PGM_B200_PLANE_FFT", 0) != 0;
-        for (int a = 0; a < 3 && usePlanes; a++) {
-            int rad[8];
-            usePlanes = sysK[0][a] <= PLANE_MAXK && fftRadices(sysK[0][a], rad) > 0;
+        // the field passes' transform pair with the influence product as one cluster kernel (a cluster per
+        // system) when chosen (setTransforms, the autotuner) and every grid has at most FFT_MAXK points per
+        // dimension with the prime factors 2, 3, 5 only; else cuFFT plans and the product kernel.  Cluster size:
+        // 16 for few systems (parallelism), down to the smallest that fits shared memory for many
+        clusterOk = true;
+        for (int k = 0; k < nsys && clusterOk; k++)
+            for (int a = 0; a < 3; a++) {
+                int rad[16];
+                const int K = sysK[k][a];
+                if (K > FFT_MAXK || fftRadices(K, rad) < 0)
+                    clusterOk = false;
+            }
+        if (clusterOk) {
+            const size_t csz = mixed() ? 8 : 16;
+            int optin = 0;
+            CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, devId));
+            auto smemFor = [&](int C) {
+                int m = 0;
+                for (int k = 0; k < nsys; k++)
+                    m = std::max(m, fftcBufferElems(sysHost[k].K, C));
+                return std::make_pair(m, (3 * (size_t) FFT_MAXK + 3 * (size_t) m) * csz);
+            };
+            int cfit = 1;
+            while (cfit < FFTC_MAXC && smemFor(cfit).second > (size_t) optin)
+                cfit *= 2;
+            int cwant = 1;
+            while (cwant < FFTC_MAXC && cwant * nsys < 148)
+                cwant *= 2;
+            fftcC = std::max(cfit, cwant);
+            const auto mb = smemFor(fftcC);
+            fftcBuf = mb.first;
+            fftcSmem = mb.second;
+            clusterOk = fftcSmem <= (size_t) optin;
         }
-        if (usePlanes) {
-            CU(cudaFuncSetAttribute(k_planes_fwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int) planeSmem<float>()));
-            CU(cudaFuncSetAttribute(k_planes_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int) planeSmem<double>()));
-            CU(cudaFuncSetAttribute(k_planes_inv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int) planeSmem<float>()));
-            CU(cudaFuncSetAttribute(k_planes_inv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int) planeSmem<double>()));
+        if (clusterOk) {
+            std::map<int, int> twOff;
+            std::vector<double> tw;
+            for (int k = 0; k < nsys; k++) {
+                SysDev& S = sysHost[k];
+                for (int a = 0; a < 3; a++) {
+                    const int K = S.K[a];
+                    if (!twOff.count(K)) {
+                        twOff[K] = (int) (tw.size() / 2);
+                        for (int m = 0; m < K; m++) {   // exp(-2 pi i m / K), the angle reduced to [-pi, pi]
+                            const int mm = (2 * m <= K) ? m : m - K;
+                            const double ang = -2.0 * PI_D * mm / K;
+                            tw.push_back(std::cos(ang));
+                            tw.push_back(std::sin(ang));
+                        }
+                    }
+                    S.twOff[a] = twOff[K];
+                }
+            }
+            if (mixed()) {
+                std::vector<float> tf(tw.begin(), tw.end());
+                upload(dTwiddle, tf, st);
+                clusterOk = prepareCluster<float>();
+            } else {
+                upload(dTwiddle, tw, st);
+                clusterOk = prepareCluster<double>();
+            }
         }
+        useCluster = clusterOk && wantCluster;
         // chunks
         chunkSys.clear();
         chunkBegin.clear();
@@ -840,6 +891,9 @@ struct Engine::Impl {
         d.grid = dGrid.p;
         d.spec = dSpec.p;
         d.infl = dInfl.p;
+        d.twiddle = dTwiddle.p;
+        d.fftcBuf = fftcBuf;
+        d.fftcC = fftcC;
         d.moduli = dModuli.as<double>();
         d.ncov = (int) covAtom.size();
         d.covAtom = dCovAtom.as<int>();
@@ -895,19 +949,51 @@ struct Engine::Impl {
         }
     }
 
-    // Shared memory of the plane kernels: two twiddle tables and two transform buffers.
-    template <typename R> static size_t planeSmem() {
-        return (2 * PLANE_MAXK + 2 * PLANE_BUF) * sizeof(typename CplxT<R>::T);
+    // Attributes of the cluster transform kernel; false when no cluster of its size fits on this GPU.
+    template <typename R> bool prepareCluster() {
+        const void* f = (const void*) k_fft_cluster<R>;
+        CU(cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        CU(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fftcSmem));
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = fftcC;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(fftcC * nsys);
+        cfg.blockDim = dim3(FftcThreads<R>::n);
+        cfg.dynamicSmemBytes = fftcSmem;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, k_fft_cluster<R>, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return clusters > 0;
     }
 
-    // The transform pair with the influence product in three kernels (one system, small 2-3-5 grid).
-    template <typename R> void planeChain(cudaStream_t sm, const Dev& d) {
-        const SysDev& S = sysHost[0];
-        const int lines = S.K[1] * (S.K[2] / 2 + 1);
-        k_planes_fwd<R><<<S.K[0], PLANE_THREADS, planeSmem<R>(), sm>>>(d);
-        k_lines_x<R><<<(lines + PLANE_LINES - 1) / PLANE_LINES, LINES_THREADS, 0, sm>>>(d);
-        k_planes_inv<R><<<S.K[0], PLANE_THREADS, planeSmem<R>(), sm>>>(d);
-        CU(cudaGetLastError());
+    // The transform pair with the influence product of a field pass: one cluster kernel (all systems), or
+    // cuFFT plans and the product kernel.  The FP64 shadow of a mixed engine takes the cuFFT path.
+    template <typename R> void transformPair(cudaStream_t sm, const Dev& d, bool gate) {
+        constexpr bool dbl = std::is_same<R, double>::value;
+        if (!useCluster || dbl == mixed()) {
+            fftChain<R>(sm, d, false, gate);
+            return;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = fftcC;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(fftcC * nsys);
+        cfg.blockDim = dim3(FftcThreads<R>::n);
+        cfg.dynamicSmemBytes = fftcSmem;
+        cfg.stream = sm;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        CU(cudaLaunchKernelEx(&cfg, k_fft_cluster<R>, d, gate ? 1 : 0));
     }
 
     template <typename R> void launchSpread(cudaStream_t sm, const Dev& d, int mode, double* vec) {
@@ -954,10 +1040,7 @@ struct Engine::Impl {
         launchSpread<R>(sm, d, spreadMode, vec);
         CU(cudaEventRecord(evFork, sm));
         CU(cudaStreamWaitEvent(sd, evFork, 0));
-        if (usePlanes)
-            planeChain<R>(sd, d);
-        else
-            fftChain<R>(sd, d, false, gate);
+        transformPair<R>(sd, d, gate);
         pairField<R, WITHQ>(sm, d, gate ? 1 : 0);
         CU(cudaEventRecord(evJoin, sd));
         CU(cudaStreamWaitEvent(sm, evJoin, 0));
@@ -1024,10 +1107,7 @@ struct Engine::Impl {
             k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
             launchSpread<R>(sm, d, 0, d.perm);
-            if (usePlanes)
-                planeChain<R>(sm, d);
-            else
-                fftChain<R>(sm, d, false, false);
+            transformPair<R>(sm, d, false);
             CU(cudaStreamWaitEvent(sm, evJoin, 0));
             pairField<R, true>(sm, d, 0);
             launchGather<R, false>(sm, d, 0);
@@ -1814,12 +1894,12 @@ int Engine::kernelLaunches() const {
     if (!I.haveResult)
         return 0;
     // own kernels per evaluation (the cuFFT transforms not counted): preparation 7, the Verlet list's build 5
-    // when it ran; a field pass fp = 4 (spread, influence product, pair pass, gather; 6 with the plane
-    // transforms); polarizable: two field passes + 2 before the loop, fp + 2 per CG iteration; final 7
+    // when it ran; a field pass fp = 4 (spread, the cluster transform kernel or the influence product, pair
+    // pass, gather); polarizable: two field passes + 2 before the loop, fp + 2 per CG iteration; final 7
     int it = 0;
     for (int k = 0; k < I.nsys; k++)
         it = std::max(it, (int) I.lastResults[(size_t) k * NRES + 14]);
-    const int fp = I.usePlanes ? 6 : 4;
+    const int fp = 4;
     return 7 + (I.lastBuilt ? 5 : 0) + (I.s.polarizable ? 2 * fp + 2 + (fp + 2) * it : 0) + 7;
 }
 
@@ -1863,10 +1943,7 @@ void Engine::kernelTimes(int reps, double* ms) {
             }
         });
         ms[5] = timeIt([&] {
-            if (I.usePlanes)
-                I.planeChain<R>(I.st, d);
-            else
-                I.fftChain<R>(I.st, d, false, false);
+            I.transformPair<R>(I.st, d, false);
         });
         ms[6] = timeIt([&] { k_cg_a<<<(int) I.chunkSys.size(), CHUNK, 0, I.st>>>(d); });
     };
@@ -1891,6 +1968,21 @@ void Engine::setPairLanes(int lanes) {
 }
 
 int Engine::pairLanes() const { return impl->pairGS; }
+
+void Engine::setTransforms(int mode) {
+    if (mode != 0 && mode != 1)
+        throw std::invalid_argument("pgm_b200: transforms must be 0 (cuFFT) or 1 (cluster kernel)");
+    Impl& I = *impl;
+    I.wantCluster = mode == 1;
+    const bool use = I.clusterOk && I.wantCluster;
+    if (use != I.useCluster && I.exec) {
+        cudaGraphExecDestroy(I.exec);
+        I.exec = nullptr;
+    }
+    I.useCluster = use;
+}
+
+int Engine::transforms() const { return impl->useCluster ? 1 : 0; }
 
 void Engine::setSystems(int nsys, const int* atomCount, const double* cutoff, const double* beta, const int* grid,
                         const double* q, const double* radius, const double* alpha, const int* covCount,

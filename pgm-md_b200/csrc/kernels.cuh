@@ -7,6 +7,8 @@
 
 #include "common.cuh"
 
+#include <cooperative_groups.h>
+
 namespace pgmb200 {
 
 __device__ __forceinline__ int wrapIndex(int g, int K) {
@@ -852,19 +854,24 @@ __global__ void __launch_bounds__(256) k_conv(Dev dv, int gateDone) {
     }
 }
 
-// ------------------------------------------------------------------------------------------------ plane transforms
+// ------------------------------------------------------------------------------------------------ cluster transforms
 
-// The 3D real transform pair with the influence product in three kernels for one system whose grid has at most
-// PLANE_MAXK points and only the prime factors 2, 3, 5 per dimension (instead of the cuFFT kernels plus the
-// product): x-planes transform along z (real to half spectrum) and y in shared memory, lines along x transform
-// forward, take the influence product and transform back, x-planes transform back along y and z (half spectrum
-// to real).  Unnormalised, the spectrum layout F[(kx K1 + ky) (K2/2 + 1) + kz] of cuFFT's R2C / C2R, shared with
-// the cuFFT path.  Each line transform is a mixed-radix Stockham FFT (radices 4, 2, 3, 5; ping-pong buffers,
-// no reordering pass) with twiddles W^m = exp(-2 pi i m / K) from sincospi in double.  Real rows are
-// transformed two at a time as one complex row (x + i y) and separated by Hermitian symmetry.
-constexpr int PLANE_MAXK = 64;
-constexpr int PLANE_BUF = 2176;   // >= max(ceil(K1/2) K2, (K2/2+1)(K1+1)) complex for K <= PLANE_MAXK
-constexpr int PLANE_LINES = 8;    // x-lines per block of the line kernel
+// The 3D real transform pair with the influence product of a field pass in ONE kernel: a cluster of C thread
+// blocks per system (C = 1 .. 16, the same for every system of a launch) holds the system's half spectrum in
+// its distributed shared memory (grids up to FFT_MAXK points per dimension with only the prime factors 2, 3, 5).  Block `rank` of the cluster owns
+// x-planes [rank ppc, rank ppc + ppc):
+//   1. its planes' real rows, two at a time as one complex row (x + i y), transform along z (real to half
+//      spectrum, separated by Hermitian symmetry) and along y in shared memory;
+//   2. (cluster barrier) x-lines (ky, kz), numbered kz K1 + ky, are split over the blocks: each gathers its lines
+//      from the owners' shared memory, transforms forward along x, multiplies by the influence function,
+//      transforms back and scatters the lines to the owners;
+//   3. (cluster barrier) its planes transform back along y and z (half spectrum to real; imaginary parts at
+//      kz = 0 and the Nyquist index dropped, as a C2R transform does) into the real grid.
+// Unnormalised, the spectrum in cuFFT's R2C / C2R layout F[(kx K1 + ky) (K2/2 + 1) + kz].  Each line transform is
+// a mixed-radix Stockham FFT (radices 4, 2, 3, 5; ping-pong buffers, no reordering pass) with twiddles
+// W^m = exp(-2 pi i m / K) from a table built on the host.
+constexpr int FFT_MAXK = 64;
+constexpr int FFTC_MAXC = 16;      // the largest cluster (a non-portable cluster size on sm_100)
 
 __host__ __device__ inline int fftRadices(int n, int* r) {
     int c = 0;
@@ -873,16 +880,6 @@ __host__ __device__ inline int fftRadices(int n, int* r) {
     while (n % 3 == 0) { r[c++] = 3; n /= 3; }
     while (n % 5 == 0) { r[c++] = 5; n /= 5; }
     return n == 1 ? c : -1;
-}
-
-template <typename R>
-__device__ __forceinline__ void twiddleTable(typename CplxT<R>::T* w, int K) {
-    for (int m = threadIdx.x; m < K; m += blockDim.x) {
-        double sn, cs;
-        sincospi(-2.0 * m / K, &sn, &cs);
-        w[m].x = (R) cs;
-        w[m].y = (R) sn;
-    }
 }
 
 // In-register DFT of length RAD, sign DIR (-1 forward, +1 inverse), unnormalised.
@@ -940,8 +937,9 @@ __device__ __forceinline__ void smallDft(R* xr, R* xi) {
     }
 }
 
-// e / K for 0 <= e < 2^20, 1 <= K <= 2^10 without an integer division: (e + 1/2) / K lies at least 1/(2K) from
-// an integer and the float product errs by under 2^-22 (e + 1/2) / K, so truncation gives the exact quotient.
+// e / K for 0 <= e < 2^20, K >= 1 without an integer division: (e + 1/2) / K lies at least 1/(2K) from an
+// integer and the float product errs by at most about 2^-23 (e + 1/2) / K < 1/(8K), so truncation gives the
+// exact quotient.
 __device__ __forceinline__ int fdiv(int e, float invK) { return __float2int_rz(((float) e + 0.5f) * invK); }
 
 // One Stockham pass of radix RAD over nlines lines of length N (line stride ls): butterfly j of a line reads
@@ -984,7 +982,8 @@ __device__ __forceinline__ void stockhamPass(const typename CplxT<R>::T* in, typ
 }
 
 // Transforms nlines lines of length N held in a (line stride ls); b is scratch of the same size.  Returns the
-// buffer holding the result.  Every thread of the block calls it (it synchronises after each pass).
+// buffer holding the result (which of the two depends on N only).  Every thread of the block calls it (it
+// synchronises after each pass).
 template <typename R, int DIR>
 __device__ typename CplxT<R>::T* fftLines(typename CplxT<R>::T* a, typename CplxT<R>::T* b, int nlines, int N, int ls,
                                           const typename CplxT<R>::T* tw) {
@@ -1008,174 +1007,130 @@ __device__ typename CplxT<R>::T* fftLines(typename CplxT<R>::T* a, typename Cplx
     return a;
 }
 
-constexpr int PLANE_THREADS = 256;
-constexpr int PLANE_PER = (PLANE_MAXK * PLANE_MAXK / 2 + PLANE_THREADS - 1) / PLANE_THREADS;   // row pairs x K2
+// Complex elements of each of the three transform buffers of a block of a cluster of C blocks for grid K (max
+// of the plane rows, the y-lines and the x-lines it holds).
+__host__ __device__ inline int fftcBufferElems(const int* K, int C) {
+    const int K2h = K[2] / 2 + 1, P = (K[1] + 1) / 2, ly = K[1] + 1;
+    const int ppc = (K[0] + C - 1) / C, lpc = (K[1] * K2h + C - 1) / C;
+    int m = ppc * P * K[2];
+    m = m > ppc * K2h * ly ? m : ppc * K2h * ly;
+    m = m > lpc * (K[0] + 1) ? m : lpc * (K[0] + 1);
+    return (m + 1) / 2 * 2;   // 16-byte multiples
+}
 
-// blockIdx.x: plane x.  Shared: twiddles W1[K1], W2[K2]; buffers A, B of PLANE_BUF complex.
+// Threads per cluster block: 1024 in float (64 registers), 512 in double.
+template <typename R> struct FftcThreads { static constexpr int n = 512; };
+template <> struct FftcThreads<float> { static constexpr int n = 1024; };
+
 template <typename R>
-__global__ void __launch_bounds__(PLANE_THREADS) k_planes_fwd(Dev dv) {
+__global__ void __launch_bounds__(FftcThreads<R>::n) k_fft_cluster(Dev dv, int gateDone) {
     typedef typename CplxT<R>::T C;
+    namespace cgx = cooperative_groups;
+    cgx::cluster_group cl = cgx::this_cluster();
+    const int rank = (int) cl.block_rank();
+    const int csize = dv.fftcC;
+    const int s = blockIdx.x / csize;
+    if (gateDone && dv.scal[s * NSCAL + SC_DONE] != 0.0)
+        return;   // the whole cluster (one system)
+    const SysDev& S = dv.sys[s];
+    const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2], K2h = K2 / 2 + 1, P = (K1 + 1) / 2, ly = K1 + 1, lx = K0 + 1;
+    const int ppc = (K0 + csize - 1) / csize, x0 = rank * ppc;
+    const int np = max(0, min(K0, x0 + ppc) - x0);                    // my planes
+    const int L = K1 * K2h, lpc = (L + csize - 1) / csize, l0 = rank * lpc;
+    const int nl = max(0, min(L, l0 + lpc) - l0);                      // my x-lines
+    const int nT = blockDim.x, tid = threadIdx.x;
+    // reciprocals for the index maps (fdiv: exact quotients below 2^20)
+    const float iK1 = 1.0f / (float) K1, iK2 = 1.0f / (float) K2, iK2h = 1.0f / (float) K2h;
+    const float iPK2 = 1.0f / (float) (P * K2), iPK2h = 1.0f / (float) (P * K2h), iNl = 1.0f / (float) max(nl, 1);
+    const float iPpc = 1.0f / (float) ppc;
     extern __shared__ __align__(16) unsigned char smraw[];
-    const SysDev& S = dv.sys[0];
-    const int K1 = S.K[1], K2 = S.K[2], K2h = K2 / 2 + 1, P = (K1 + 1) / 2, ly = K1 + 1;
-    const float invK2 = 1.0f / (float) K2, invK2h = 1.0f / (float) K2h;
-    const int x = blockIdx.x;
-    C* W1 = (C*) smraw;
-    C* W2 = W1 + PLANE_MAXK;
-    C* A = W2 + PLANE_MAXK;
-    C* B = A + PLANE_BUF;
-    const R* g = (const R*) dv.grid + S.gridOff + (size_t) x * K1 * K2;
-    {   // rows 2p, 2p+1 as one complex row; all loads issued before the stores
-        R lo[PLANE_PER], hi[PLANE_PER];
-#pragma unroll
-        for (int k = 0; k < PLANE_PER; k++) {
-            const int e = threadIdx.x + k * PLANE_THREADS;
-            lo[k] = hi[k] = 0;
-            if (e < P * K2) {
-                const int p = fdiv(e, invK2), z = e - p * K2;
-                lo[k] = g[2 * p * K2 + z];
-                if (2 * p + 1 < K1)
-                    hi[k] = g[(2 * p + 1) * K2 + z];
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < PLANE_PER; k++) {
-            const int e = threadIdx.x + k * PLANE_THREADS;
-            if (e < P * K2) {
-                C v;
-                v.x = lo[k];
-                v.y = hi[k];
-                A[e] = v;
-            }
-        }
+    C* W0 = (C*) smraw;
+    C* W1 = W0 + FFT_MAXK;
+    C* W2 = W1 + FFT_MAXK;
+    C* const b0 = W2 + FFT_MAXK;
+    C* const b1 = b0 + dv.fftcBuf;
+    C* const b2 = b1 + dv.fftcBuf;
+    const C* tw = (const C*) dv.twiddle;
+    for (int m = tid; m < K0; m += nT)
+        W0[m] = tw[S.twOff[0] + m];
+    for (int m = tid; m < K1; m += nT)
+        W1[m] = tw[S.twOff[1] + m];
+    for (int m = tid; m < K2; m += nT)
+        W2[m] = tw[S.twOff[2] + m];
+    R* g = (R*) dv.grid + S.gridOff;
+    // 1. my planes: rows 2p, 2p + 1 as one complex row, [plane][pair][z]
+    const int rowsN = np * P * K2;
+    for (int e = tid; e < rowsN; e += nT) {
+        const int pl = fdiv(e, iPK2), rem = e - pl * (P * K2), pr = fdiv(rem, iK2), z = rem - pr * K2;
+        const R* gp = g + ((size_t) (x0 + pl) * K1 + 2 * pr) * K2 + z;
+        C v;
+        v.x = gp[0];
+        v.y = (2 * pr + 1 < K1) ? gp[K2] : (R) 0;
+        b0[e] = v;
     }
-    twiddleTable<R>(W1, K1);
-    twiddleTable<R>(W2, K2);
     __syncthreads();
-    C* Z = fftLines<R, -1>(A, B, P, K2, K2, W2);
-    C* O = (Z == A) ? B : A;
-    for (int e = threadIdx.x; e < P * K2h; e += blockDim.x) {   // separate the two rows; y-lines O[kz ly + y]
-        const int p = fdiv(e, invK2h), kz = e - p * K2h;
-        const C zk = Z[p * K2 + kz], zm = Z[p * K2 + (kz == 0 ? 0 : K2 - kz)];
+    C* Z = fftLines<R, -1>(b0, b1, np * P, K2, K2, W2);
+    C* O = (Z == b0) ? b1 : b0;
+    for (int e = tid; e < np * P * K2h; e += nT) {   // separate the two rows; y-lines O[(plane K2h + kz) ly + y]
+        const int pl = fdiv(e, iPK2h), rem = e - pl * (P * K2h), pr = fdiv(rem, iK2h), kz = rem - pr * K2h;
+        const C* zr = Z + (pl * P + pr) * K2;
+        const C zk = zr[kz], zm = zr[kz == 0 ? 0 : K2 - kz];
         C X, Y;   // X = (Z_k + conj Z_-k) / 2, Y = (Z_k - conj Z_-k) / 2i
         X.x = (R) 0.5 * (zk.x + zm.x);
         X.y = (R) 0.5 * (zk.y - zm.y);
         Y.x = (R) 0.5 * (zk.y + zm.y);
         Y.y = (R) 0.5 * (zm.x - zk.x);
-        O[kz * ly + 2 * p] = X;
-        if (2 * p + 1 < K1)
-            O[kz * ly + 2 * p + 1] = Y;
+        C* o = O + (pl * K2h + kz) * ly + 2 * pr;
+        o[0] = X;
+        if (2 * pr + 1 < K1)
+            o[1] = Y;
     }
     __syncthreads();
-    const C* F = fftLines<R, -1>(O, Z, K2h, K1, ly, W1);
-    C* spec = (C*) dv.spec + S.specOff + (size_t) x * K1 * K2h;
-    for (int e = threadIdx.x; e < K1 * K2h; e += blockDim.x) {
-        const int ky = fdiv(e, invK2h), kz = e - ky * K2h;
-        spec[e] = F[kz * ly + ky];
-    }
-}
-
-constexpr int LINES_THREADS = 128;
-constexpr int LINES_PER = (PLANE_MAXK * PLANE_LINES + LINES_THREADS - 1) / LINES_THREADS;
-
-// PLANE_LINES consecutive x-lines (ky, kz) per block: forward transform along x, influence product, inverse.
-template <typename R>
-__global__ void __launch_bounds__(LINES_THREADS) k_lines_x(Dev dv) {
-    typedef typename CplxT<R>::T C;
-    __shared__ C W0[PLANE_MAXK];
-    __shared__ C A[PLANE_LINES * (PLANE_MAXK + 1)], B[PLANE_LINES * (PLANE_MAXK + 1)];
-    const SysDev& S = dv.sys[0];
-    const int K0 = S.K[0], nline = S.K[1] * (S.K[2] / 2 + 1), lx = K0 + 1;
-    const size_t stride = (size_t) nline;   // F[(kx K1 + ky) K2h + kz]: line ky K2h + kz, stride K1 K2h in kx
-    const int line0 = blockIdx.x * PLANE_LINES;
-    C* spec = (C*) dv.spec + S.specOff + line0;
-    const R* infl = (const R*) dv.infl + S.specOff + line0;
-    C v[LINES_PER];
-    R gk[LINES_PER];
-#pragma unroll
-    for (int k = 0; k < LINES_PER; k++) {   // element e = kx PLANE_LINES + l; the loads, then the stores
-        const int e = threadIdx.x + k * LINES_THREADS, kx = e / PLANE_LINES, l = e % PLANE_LINES;
-        v[k].x = v[k].y = 0;
-        gk[k] = 0;
-        if (kx < K0 && line0 + l < nline) {
-            v[k] = spec[kx * stride + l];
-            gk[k] = infl[kx * stride + l];
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < LINES_PER; k++) {
-        const int e = threadIdx.x + k * LINES_THREADS, kx = e / PLANE_LINES, l = e % PLANE_LINES;
-        if (kx < K0)
-            A[l * lx + kx] = v[k];
-    }
-    twiddleTable<R>(W0, K0);
-    __syncthreads();
-    C* F = fftLines<R, -1>(A, B, PLANE_LINES, K0, lx, W0);
-#pragma unroll
-    for (int k = 0; k < LINES_PER; k++) {
-        const int e = threadIdx.x + k * LINES_THREADS, kx = e / PLANE_LINES, l = e % PLANE_LINES;
-        if (kx < K0) {
-            F[l * lx + kx].x *= gk[k];
-            F[l * lx + kx].y *= gk[k];
-        }
+    C* F = fftLines<R, -1>(O, Z, np * K2h, K1, ly, W1);
+    C* const Fb = (F == b0) ? b0 : b1;   // the same buffer in every block (the pass counts depend on K only)
+    C* const Yb = (F == b0) ? b1 : b0;
+    cl.sync();
+    // 2. my x-lines l = kz K1 + ky: gather, forward along x, influence product, inverse, scatter
+    C* const Xb = b2;
+    for (int e = tid; e < nl * K0; e += nT) {
+        const int x = fdiv(e, iNl), li = e - x * nl, l = l0 + li, kz = fdiv(l, iK1), ky = l - kz * K1;
+        const int ow = fdiv(x, iPpc), xp = x - ow * ppc;
+        const C* src = cl.map_shared_rank(Fb, ow);
+        Xb[li * lx + x] = src[(xp * K2h + kz) * ly + ky];
     }
     __syncthreads();
-    const C* G = fftLines<R, 1>(F, F == A ? B : A, PLANE_LINES, K0, lx, W0);
-#pragma unroll
-    for (int k = 0; k < LINES_PER; k++) {
-        const int e = threadIdx.x + k * LINES_THREADS, kx = e / PLANE_LINES, l = e % PLANE_LINES;
-        if (kx < K0 && line0 + l < nline)
-            spec[kx * stride + l] = G[l * lx + kx];
+    C* Fx = fftLines<R, -1>(Xb, Yb, nl, K0, lx, W0);
+    const R* infl = (const R*) dv.infl + S.specOff;
+    for (int e = tid; e < nl * K0; e += nT) {
+        const int x = fdiv(e, iNl), li = e - x * nl, l = l0 + li, kz = fdiv(l, iK1), ky = l - kz * K1;
+        const R gk = infl[((size_t) x * K1 + ky) * K2h + kz];
+        C& v = Fx[li * lx + x];
+        v.x *= gk;
+        v.y *= gk;
     }
-}
-
-// blockIdx.x: plane x.  Inverse along y, then rows 2p, 2p+1 rebuilt from their half spectra (imaginary parts
-// at kz = 0 and the Nyquist index dropped, as a C2R transform does) as one complex row, inverse along z.
-template <typename R>
-__global__ void __launch_bounds__(PLANE_THREADS) k_planes_inv(Dev dv) {
-    typedef typename CplxT<R>::T C;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    const SysDev& S = dv.sys[0];
-    const int K1 = S.K[1], K2 = S.K[2], K2h = K2 / 2 + 1, P = (K1 + 1) / 2, ly = K1 + 1;
-    const float invK2 = 1.0f / (float) K2, invK2h = 1.0f / (float) K2h;
-    const int x = blockIdx.x;
-    C* W1 = (C*) smraw;
-    C* W2 = W1 + PLANE_MAXK;
-    C* A = W2 + PLANE_MAXK;
-    C* B = A + PLANE_BUF;
-    const C* spec = (const C*) dv.spec + S.specOff + (size_t) x * K1 * K2h;
-    {
-        C v[PLANE_PER + 1];   // K1 K2h <= PLANE_MAXK (PLANE_MAXK / 2 + 1) elements
-#pragma unroll
-        for (int k = 0; k < PLANE_PER + 1; k++) {
-            const int e = threadIdx.x + k * PLANE_THREADS;
-            if (e < K1 * K2h)
-                v[k] = spec[e];
-        }
-#pragma unroll
-        for (int k = 0; k < PLANE_PER + 1; k++) {
-            const int e = threadIdx.x + k * PLANE_THREADS;
-            if (e < K1 * K2h) {
-                const int ky = fdiv(e, invK2h), kz = e - ky * K2h;
-                A[kz * ly + ky] = v[k];
-            }
-        }
-    }
-    twiddleTable<R>(W1, K1);
-    twiddleTable<R>(W2, K2);
     __syncthreads();
-    C* G = fftLines<R, 1>(A, B, K2h, K1, ly, W1);   // G[kz ly + y]
-    C* O = (G == A) ? B : A;
-    for (int e = threadIdx.x; e < P * K2; e += blockDim.x) {
-        const int p = fdiv(e, invK2), k = e - p * K2;
+    C* Gx = fftLines<R, 1>(Fx, Fx == Xb ? Yb : Xb, nl, K0, lx, W0);
+    for (int e = tid; e < nl * K0; e += nT) {
+        const int x = fdiv(e, iNl), li = e - x * nl, l = l0 + li, kz = fdiv(l, iK1), ky = l - kz * K1;
+        const int ow = fdiv(x, iPpc), xp = x - ow * ppc;
+        C* dst = cl.map_shared_rank(Fb, ow);
+        dst[(xp * K2h + kz) * ly + ky] = Gx[li * lx + x];
+    }
+    cl.sync();
+    // 3. my planes back along y, then z (two real rows from one complex row)
+    C* Gy = fftLines<R, 1>(Fb, Yb, np * K2h, K1, ly, W1);
+    C* O2 = (Gy == Fb) ? Yb : Fb;
+    for (int e = tid; e < rowsN; e += nT) {
+        const int pl = fdiv(e, iPK2), rem = e - pl * (P * K2), pr = fdiv(rem, iK2), k = rem - pr * K2;
         const bool upper = k >= K2h;
         const int kk = upper ? K2 - k : k;
         const bool realOnly = (k == 0) || ((K2 & 1) == 0 && k == K2 / 2);
-        C X = G[kk * ly + 2 * p], Y;
+        const C* gy = Gy + (pl * K2h + kk) * ly + 2 * pr;
+        C X = gy[0], Y;
         Y.x = 0;
         Y.y = 0;
-        if (2 * p + 1 < K1)
-            Y = G[kk * ly + 2 * p + 1];
+        if (2 * pr + 1 < K1)
+            Y = gy[1];
         if (upper) {
             X.y = -X.y;
             Y.y = -Y.y;
@@ -1187,16 +1142,16 @@ __global__ void __launch_bounds__(PLANE_THREADS) k_planes_inv(Dev dv) {
         C Zv;   // X + i Y
         Zv.x = X.x - Y.y;
         Zv.y = X.y + Y.x;
-        O[e] = Zv;
+        O2[e] = Zv;
     }
     __syncthreads();
-    const C* Zt = fftLines<R, 1>(O, G, P, K2, K2, W2);
-    R* g = (R*) dv.grid + S.gridOff + (size_t) x * K1 * K2;
-    for (int e = threadIdx.x; e < P * K2; e += blockDim.x) {
-        const int p = fdiv(e, invK2), z = e - p * K2;
-        g[2 * p * K2 + z] = Zt[e].x;
-        if (2 * p + 1 < K1)
-            g[(2 * p + 1) * K2 + z] = Zt[e].y;
+    const C* Zt = fftLines<R, 1>(O2, Gy, np * P, K2, K2, W2);
+    for (int e = tid; e < rowsN; e += nT) {
+        const int pl = fdiv(e, iPK2), rem = e - pl * (P * K2), pr = fdiv(rem, iK2), z = rem - pr * K2;
+        R* gp = g + ((size_t) (x0 + pl) * K1 + 2 * pr) * K2 + z;
+        gp[0] = Zt[e].x;
+        if (2 * pr + 1 < K1)
+            gp[K2] = Zt[e].y;
     }
 }
 

@@ -84,6 +84,10 @@ public:
     int kernelLaunches() const;
     void kernelTimes(int reps, double* ms);
     void setPairLanes(int lanes);
+    // field-pass transforms: 0 cuFFT plans + influence product kernel, 1 one cluster kernel per launch (when
+    // the grids allow it; transforms() tells which runs)
+    void setTransforms(int mode);
+    int transforms() const;
     int pairLanes() const;
 
     // batched systems

@@ -319,17 +319,35 @@ class Engine:
     def pair_lanes(self):
         return int(self._L.pgm_engine_pair_lanes(self._h))
 
+    def set_transforms(self, mode):
+        """Field-pass transforms: 0 cuFFT plans + influence product, 1 one cluster kernel per pass."""
+        _check(self._L.pgm_engine_set_transforms(self._h, int(mode)))
+
+    def transforms(self):
+        return int(self._L.pgm_engine_transforms(self._h))
+
     def autotune(self, pos, box, reps=10, candidates=(4, 8, 16, 32)):
-        """Picks the lanes per atom of the pair passes by timing each candidate on this system."""
+        """Picks the lanes per atom of the pair passes and the kind of field-pass transforms by timing each
+        candidate on this system (batched engines: pass the batch's positions and boxes).  Returns the lanes."""
+        batched = getattr(self, "nsys", 1) > 1
+        run = (lambda: self.compute_batch(pos, box)) if batched else (lambda: self.compute(pos, box, new_step=False))
         best, best_t = None, None
         for lanes in candidates:
             self.set_pair_lanes(lanes)
-            self.compute(pos, box, new_step=False)
+            run()
             kt = self.kernel_times(reps)
             t = kt["pair_field"] + kt["pair_final"] / max(1, self.iterations() + 2)
             if best_t is None or t < best_t:
                 best, best_t = lanes, t
         self.set_pair_lanes(best)
+        ft = {}
+        for mode in (0, 1):
+            self.set_transforms(mode)
+            if self.transforms() != mode:
+                continue
+            run()
+            ft[mode] = self.kernel_times(reps)["fft_chain"]
+        self.set_transforms(min(ft, key=ft.get))
         return best
 
     # ---------------------------------------------------------------- batched

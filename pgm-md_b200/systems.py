@@ -11,7 +11,7 @@ Workloads
   dimethylphenol8550
                 450 rigid 19-atom C8H10O molecules (8550 atoms), 44.5 A box, 48^3, order 6, tol 1e-5
   water98304    32768 waters, 99.4 A box, 104^3, order 6
-  water_batch   independent water boxes of 8..512 molecules at 0.0334 molecules/A^3, ~1 A grids
+  water_batch   independent water boxes of 8..512 molecules at 0.0334 molecules/A^3, grids <= 1 A (2-3-5 sizes)
 """
 
 from __future__ import annotations
@@ -211,15 +211,29 @@ def dimethylphenol8550(seed=8550, tol=1e-5):
                   cov_types=np.tile(np.arange(len(bonds)), nmol), meta=dict(seed=seed, nmol=nmol, L_A=L))
 
 
+def fft_size(x):
+    """The smallest integer >= x with no prime factor above 5 (a PME grid size the transforms handle best)."""
+    n = max(1, int(math.ceil(x)))
+    while True:
+        m = n
+        for p in (2, 3, 5):
+            while m % p == 0:
+                m //= p
+        if m == 1:
+            return n
+        n += 1
+
+
 def water_batch(nsys=1024, seed=1024, nmin=8, nmax=512, density=0.0334, tol=1e-5):
-    """``nsys`` independent water boxes, molecule counts U{nmin..nmax}, L = (n/density)^(1/3) A, grid
-    ceil(L / 1 A) (at least the order), cutoff min(9 A, L/2), beta 0.35/A."""
+    """``nsys`` independent water boxes, molecule counts U{nmin..nmax}, L = (n/density)^(1/3) A, grid the
+    smallest size >= L / 1 A without a prime factor above 5 (at least the order; spacing <= 1 A), cutoff
+    min(9 A, L/2), beta 0.35/A."""
     rng = np.random.default_rng(seed)
     counts = rng.integers(nmin, nmax + 1, size=nsys)
     out = []
     for k, nm in enumerate(counts):
         L = (nm / density) ** (1.0 / 3.0)
-        K = max(6, int(math.ceil(L / 1.0)))
+        K = max(6, fft_size(L / 1.0))
         rc = min(9.0, L / 2.0)
         out.append(waters(int(nm), L, seed=seed * 100003 + k, grid=(K, K, K), cutoff=rc, tol=tol,
                           name=f"water_batch[{k}]"))
