@@ -237,7 +237,7 @@ __device__ __forceinline__ void minImageFast(double* v, const double* H, const d
 }
 
 constexpr int LIST_THREADS = 256;
-constexpr int LIST_CHUNK = 512;   // candidates staged in shared memory at a time
+constexpr int LIST_CHUNK = 1024;  // candidates staged in shared memory at a time
 constexpr int MAX_RUNS = 343;     // (2m+1)^3 with m <= 3
 
 // System of a global cell index (binary search over the systems' first cells).
@@ -255,17 +255,22 @@ __device__ __forceinline__ int systemOfCell(const Dev& dv, int c) {
 
 // One block per cell.  The neighbour cells (offsets -m..m per dimension) become at most (2m+1)^3 runs of
 // consecutive slots with one image shift each (cells along the last dimension merged); their atoms are
-// staged through shared memory in chunks (wrapped position, original position and radius, wraps) and every
-// warp tests them against the cell's atoms it owns: a prefilter on the wrapped positions, then the
-// reference's exact test (minimum image of the original positions, core/pgm_core.cpp:64-87) at the list
-// radius (cutoff + skin), keeping a candidate only at the image that test chose, so every pair enters once.
-// Accepted pairs are appended to the Verlet list in candidate order (deterministic); k_pair_compact then takes
-// the ones within the cutoff at every evaluation.
-__global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
+// staged through shared memory in chunks (the image's wrapped position relative to the cell's first atom, in
+// float, and the pair entry) and every warp tests them against the cell's atoms it owns, 32 candidates at a
+// time:
+//   - float prefilter: outside (1 + 1e-5) rl^2 is out, inside (1 - 1e-5) rl^2 with every component inside half a
+//     box edge is in (the float differences of positions within a few nm of the cell err by < 1e-6 nm^2, and
+//     a pair clearly inside the radius with its cell image inside half a box edge provably gets the same image
+//     and side from the reference's rounding);
+//   - the rest (a thin shell, or near half a box edge) takes the reference's exact test: minimum image of the
+//     original positions, r^2 < rl^2 in double without contraction (core/pgm_core.cpp:64-87), keeping the
+//     candidate only at the image that test chose, so every pair enters once.
+// Accepted pairs are appended to the Verlet list (radius rl = cutoff + skin) in candidate order
+// (deterministic); k_pair_compact then takes the ones within the cutoff at every evaluation.
+__global__ void __launch_bounds__(LIST_THREADS, 4) k_build_list(Dev dv) {
     __shared__ int runSlot[MAX_RUNS], runOff[MAX_RUNS + 1], runShift[MAX_RUNS];
-    __shared__ double4 cPos[LIST_CHUNK], cOrig[LIST_CHUNK];
-    __shared__ int4 cWrap[LIST_CHUNK];
-    __shared__ int wq[LIST_THREADS / 32][64];
+    __shared__ float4 cPos[LIST_CHUNK];
+    __shared__ uint32_t cEntry[LIST_CHUNK];
     const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     constexpr int NW = LIST_THREADS / 32;
     if (c >= dv.totalCells)
@@ -330,9 +335,10 @@ __global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
         dv.slistCount[ii] = 0;
     __syncthreads();
     const int total = runOff[nr];
-    const double pre = S.rl2 * (1.0 + 1e-10) + 1e-300, preLo = S.rl2 * (1.0 - 1e-10);
-    const double half0 = 0.5 * S.H[0] * (1.0 - 1e-10), half1 = 0.5 * S.H[4] * (1.0 - 1e-10),
-                 half2 = 0.5 * S.H[8] * (1.0 - 1e-10);
+    const double4 org = dv.posS[cb];   // the block's origin for the float positions
+    const float preF = (float) (S.rl2 * (1.0 + 1e-5)), preLoF = (float) (S.rl2 * (1.0 - 1e-5));
+    const float hf0 = (float) (0.5 * S.H[0] * (1.0 - 1e-5)), hf1 = (float) (0.5 * S.H[4] * (1.0 - 1e-5)),
+                hf2 = (float) (0.5 * S.H[8] * (1.0 - 1e-5));
     const double invDiag[3] = {1.0 / S.H[0], 1.0 / S.H[4], 1.0 / S.H[8]};
     for (int base = 0; base < total; base += LIST_CHUNK) {
         const int nc = min(LIST_CHUNK, total - base);
@@ -349,82 +355,56 @@ __global__ void __launch_bounds__(LIST_THREADS) k_build_list(Dev dv) {
             const int js = runSlot[lo] + (k - runOff[lo]);
             const int code = runShift[lo];
             const int w0 = (code & 7) - 4, w1 = ((code >> 3) & 7) - 4, w2 = ((code >> 6) & 7) - 4;
-            // the candidate's image: wrapped position + w.H, staged once for all atoms of the cell
+            // the candidate's image (wrapped position + w.H) relative to the origin, staged once for the cell
             const double4 pw = dv.posS[js];
-            cPos[t] = make_double4(pw.x + (w0 * S.H[0] + w1 * S.H[3] + w2 * S.H[6]), pw.y + (w1 * S.H[4] + w2 * S.H[7]),
-                                   pw.z + w2 * S.H[8], 0.0);
-            cOrig[t] = dv.origS[js];
-            const int4 w = dv.wrapS[js];
-            cWrap[t] = make_int4(w.x, w.y, w.z, js | (code << 23));
+            cPos[t] = make_float4((float) (pw.x + (w0 * S.H[0] + w1 * S.H[3] + w2 * S.H[6]) - org.x),
+                                  (float) (pw.y + (w1 * S.H[4] + w2 * S.H[7]) - org.y),
+                                  (float) (pw.z + w2 * S.H[8] - org.z), 0.0f);
+            cEntry[t] = (uint32_t) (js | (code << 23));
         }
         __syncthreads();
         for (int ii = cb + wid; ii < ce; ii += NW) {
             const double4 pwi = dv.posS[ii];
-            const double4 oi = dv.origS[ii];
-            const int4 wi = dv.wrapS[ii];
+            const float xi = (float) (pwi.x - org.x), yi = (float) (pwi.y - org.y), zi = (float) (pwi.z - org.z);
             uint32_t* row = dv.slist + (size_t) ii * dv.cap;
             int count = dv.slistCount[ii];
-            int qn = 0;   // prefilter survivors queued (candidate order) for the exact test
             for (int t0 = 0; t0 < nc; t0 += 32) {
                 const int t = t0 + lane;
-                bool pass = false;
-                int qv = t;
+                bool acc = false, unsure = false;
+                uint32_t entry = 0;
                 if (t < nc) {
-                    const double4 pj = cPos[t];
-                    const double y0 = pwi.x - pj.x, y1 = pwi.y - pj.y, y2 = pwi.z - pj.z;
-                    const double r2 = y0 * y0 + y1 * y1 + y2 * y2;
-                    pass = ((cWrap[t].w & 0x7FFFFF) != ii) && (r2 < pre);
-                    // clearly inside the cutoff with every component of the cell image inside half a box edge:
-                    // the reference's rounding then picks this very image and the same side of the cutoff,
-                    // so the exact test can be skipped
-                    if (pass && r2 < preLo && fabs(y0) < half0 && fabs(y1) < half1 && fabs(y2) < half2)
-                        qv = t | (1 << 30);
-                }
-                const unsigned m = __ballot_sync(0xffffffffu, pass);
-                if (pass)
-                    wq[wid][qn + __popc(m & ((1u << lane) - 1u))] = qv;
-                qn += __popc(m);
-                __syncwarp();
-                const bool last = (t0 + 32 >= nc);
-                while (qn >= 32 || (last && qn > 0)) {
-                    const int nb = min(qn, 32);
-                    bool acc = false;
-                    uint32_t entry = 0;
-                    if (lane < nb && (wq[wid][lane] & (1 << 30))) {
-                        entry = (uint32_t) cWrap[wq[wid][lane] & 0xFFFF].w;
-                        acc = true;
-                    } else if (lane < nb) {
-                        const int tq = wq[wid][lane];
-                        const int4 cw = cWrap[tq];
-                        entry = (uint32_t) cw.w;
-                        const int w0 = (int) ((entry >> 23) & 7u) - 4, w1 = (int) ((entry >> 26) & 7u) - 4,
-                                  w2 = (int) ((entry >> 29) & 7u) - 4;
-                        const double4 oj = cOrig[tq];
-                        double x[3] = {__dsub_rn(oi.x, oj.x), __dsub_rn(oi.y, oj.y), __dsub_rn(oi.z, oj.z)};
-                        int kk[3];
-                        minImageFast(x, S.H, invDiag, kk);
-                        if (dot3exact(x) < S.rl2)   // image of the exact test relative to the wrapped positions
-                            acc = (kk[0] - (wi.x - cw.x) == w0 && kk[1] - (wi.y - cw.y) == w1 &&
-                                   kk[2] - (wi.z - cw.z) == w2);
+                    const float4 pj = cPos[t];
+                    entry = cEntry[t];
+                    const float y0 = xi - pj.x, y1 = yi - pj.y, y2 = zi - pj.z;
+                    const float r2 = y0 * y0 + y1 * y1 + y2 * y2;
+                    if ((int) (entry & 0x7FFFFFu) != ii && r2 < preF) {
+                        if (r2 < preLoF && fabsf(y0) < hf0 && fabsf(y1) < hf1 && fabsf(y2) < hf2)
+                            acc = true;
+                        else
+                            unsure = true;
                     }
-                    const unsigned ma = __ballot_sync(0xffffffffu, acc);
-                    if (acc) {
-                        const int pos = count + __popc(ma & ((1u << lane) - 1u));
-                        if (pos < dv.cap)
-                            row[pos] = entry;
-                    }
-                    count += __popc(ma);
-                    // move the queue's remainder to its front
-                    const int rest = qn - nb;
-                    int moved = 0;
-                    if (lane < rest)
-                        moved = wq[wid][nb + lane];
-                    __syncwarp();
-                    if (lane < rest)
-                        wq[wid][lane] = moved;
-                    __syncwarp();
-                    qn = rest;
                 }
+                if (__any_sync(0xffffffffu, unsure) && unsure) {
+                    // the reference's exact test on the original positions; kept only at the image it chooses
+                    const int js = (int) (entry & 0x7FFFFFu);
+                    const int w0 = (int) ((entry >> 23) & 7u) - 4, w1 = (int) ((entry >> 26) & 7u) - 4,
+                              w2 = (int) ((entry >> 29) & 7u) - 4;
+                    const double4 oi = dv.origS[ii], oj = dv.origS[js];
+                    const int4 wi = dv.wrapS[ii], cw = dv.wrapS[js];
+                    double x[3] = {__dsub_rn(oi.x, oj.x), __dsub_rn(oi.y, oj.y), __dsub_rn(oi.z, oj.z)};
+                    int kk[3];
+                    minImageFast(x, S.H, invDiag, kk);
+                    if (dot3exact(x) < S.rl2)
+                        acc = (kk[0] - (wi.x - cw.x) == w0 && kk[1] - (wi.y - cw.y) == w1 &&
+                               kk[2] - (wi.z - cw.z) == w2);
+                }
+                const unsigned ma = __ballot_sync(0xffffffffu, acc);
+                if (acc) {
+                    const int pos = count + __popc(ma & ((1u << lane) - 1u));
+                    if (pos < dv.cap)
+                        row[pos] = entry;
+                }
+                count += __popc(ma);
             }
             if (lane == 0)
                 dv.slistCount[ii] = count;
