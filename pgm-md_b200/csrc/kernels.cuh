@@ -484,7 +484,7 @@ __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
 // (core/pgm_core.cpp:64-87) only near the cutoff or near half a box edge.  A pair within the cutoff whose exact
 // image is not the one stored at the build sets flags[9]: the list is rebuilt and the evaluation repeated.
 template <typename R>
-__global__ void __launch_bounds__(256) k_pair_compact(Dev dv) {
+__global__ void __launch_bounds__(256, 3) k_pair_compact(Dev dv) {
     typedef typename V2T<R>::T R2;
     typedef typename V4T<R>::T R4;
     constexpr bool STORE_X = PairRec<R>::storeX;
@@ -493,8 +493,6 @@ __global__ void __launch_bounds__(256) k_pair_compact(Dev dv) {
         return;
     const SysDev& S = dv.sys[dv.atomSys[dv.slotAtom[slot]]];
     const double4 pwi = dv.posS[slot];
-    const double4 oi = dv.origS[slot];
-    const int4 wi = dv.wrapS[slot];
     const double Ri = dv.radS[slot];
     const uint32_t* srow = dv.slist + (size_t) slot * dv.cap;
     uint32_t* row = dv.list + (size_t) slot * dv.cap;
@@ -505,58 +503,63 @@ __global__ void __launch_bounds__(256) k_pair_compact(Dev dv) {
     const double pre = S.rc2 * (1.0 + 1e-10) + 1e-300, preLo = S.rc2 * (1.0 - 1e-10);
     const double half0 = 0.5 * S.H[0] * (1.0 - 1e-10), half1 = 0.5 * S.H[4] * (1.0 - 1e-10),
                  half2 = 0.5 * S.H[8] * (1.0 - 1e-10);
-    const double invDiag[3] = {1.0 / S.H[0], 1.0 / S.H[4], 1.0 / S.H[8]};
+    // test of list entry t (t < cnt): pair geometry x and whether the pair is within the cutoff
+    auto test = [&](int t, uint32_t e, double4 pwj, double* x) -> bool {
+        double sh[3];
+        entryShift(e, S.H, sh);
+        x[0] = pwi.x - pwj.x - sh[0];
+        x[1] = pwi.y - pwj.y - sh[1];
+        x[2] = pwi.z - pwj.z - sh[2];
+        const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        if (!(r2 < pre))
+            return false;
+        if (r2 < preLo && fabs(x[0]) < half0 && fabs(x[1]) < half1 && fabs(x[2]) < half2)
+            return true;
+        const int js = entrySlot(e);
+        const double4 oi = dv.origS[slot], oj = dv.origS[js];
+        const int4 wi = dv.wrapS[slot], wj = dv.wrapS[js];
+        const double invDiag[3] = {1.0 / S.H[0], 1.0 / S.H[4], 1.0 / S.H[8]};
+        double xe[3] = {__dsub_rn(oi.x, oj.x), __dsub_rn(oi.y, oj.y), __dsub_rn(oi.z, oj.z)};
+        int kk[3];
+        minImageFast(xe, S.H, invDiag, kk);
+        if (!(dot3exact(xe) < S.rc2))
+            return false;
+        const int w0 = (int) ((e >> 23) & 7u) - 4, w1 = (int) ((e >> 26) & 7u) - 4, w2 = (int) ((e >> 29) & 7u) - 4;
+        const bool same = kk[0] - (wi.x - wj.x) == w0 && kk[1] - (wi.y - wj.y) == w1 && kk[2] - (wi.z - wj.z) == w2;
+        if (!same)
+            atomicOr(&dv.flags[9], 1);
+        return same;
+    };
+    // append the accepted lanes of a 32-entry chunk in lane (candidate) order
     int count = 0;
-    for (int t0 = 0; t0 < cnt; t0 += 32) {
-        const int t = t0 + lane;
-        bool acc = false;
-        uint32_t e = 0;
-        double x0 = 0, x1 = 0, x2 = 0;
-        int js = 0;
-        if (t < cnt) {
-            e = srow[t];
-            js = entrySlot(e);
-            double sh[3];
-            entryShift(e, S.H, sh);
-            const double4 pwj = dv.posS[js];
-            x0 = pwi.x - pwj.x - sh[0];
-            x1 = pwi.y - pwj.y - sh[1];
-            x2 = pwi.z - pwj.z - sh[2];
-            const double r2 = x0 * x0 + x1 * x1 + x2 * x2;
-            if (r2 < pre) {
-                if (r2 < preLo && fabs(x0) < half0 && fabs(x1) < half1 && fabs(x2) < half2) {
-                    acc = true;
-                } else {
-                    const double4 oj = dv.origS[js];
-                    const int4 wj = dv.wrapS[js];
-                    double x[3] = {__dsub_rn(oi.x, oj.x), __dsub_rn(oi.y, oj.y), __dsub_rn(oi.z, oj.z)};
-                    int kk[3];
-                    minImageFast(x, S.H, invDiag, kk);
-                    if (dot3exact(x) < S.rc2) {
-                        const int w0 = (int) ((e >> 23) & 7u) - 4, w1 = (int) ((e >> 26) & 7u) - 4,
-                                  w2 = (int) ((e >> 29) & 7u) - 4;
-                        acc = (kk[0] - (wi.x - wj.x) == w0 && kk[1] - (wi.y - wj.y) == w1 &&
-                               kk[2] - (wi.z - wj.z) == w2);
-                        if (!acc)
-                            atomicOr(&dv.flags[9], 1);
-                    }
-                }
-            }
-        }
+    auto append = [&](bool acc, uint32_t e, const double* x) {
         const unsigned ma = __ballot_sync(0xffffffffu, acc);
         if (acc) {
             const int pos = count + __popc(ma & ((1u << lane) - 1u));
             row[pos] = e;
             if constexpr (STORE_X) {
                 R4 va;
-                va.x = (R) x0;
-                va.y = (R) x1;
-                va.z = (R) x2;
+                va.x = (R) x[0];
+                va.y = (R) x[1];
+                va.z = (R) x[2];
                 va.w = (R) 0;
                 arow[pos] = va;
             }
         }
         count += __popc(ma);
+    };
+    // two chunks per step: both chunks' entries and partner positions are loaded before either is tested
+    for (int t0 = 0; t0 < cnt; t0 += 64) {
+        const int ta = t0 + lane, tb = t0 + 32 + lane;
+        const uint32_t ea = ta < cnt ? srow[ta] : 0u, eb = tb < cnt ? srow[tb] : 0u;
+        const double4 pa = dv.posS[ta < cnt ? entrySlot(ea) : slot];
+        const double4 pb = dv.posS[tb < cnt ? entrySlot(eb) : slot];
+        double xa[3] = {0, 0, 0}, xb[3] = {0, 0, 0};
+        const bool acca = ta < cnt && test(ta, ea, pa, xa);
+        const bool accb = tb < cnt && test(tb, eb, pb, xb);
+        append(acca, ea, xa);
+        if (t0 + 32 < cnt)
+            append(accb, eb, xb);
     }
     if (lane == 0)
         dv.listCount[slot] = count;
