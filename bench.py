@@ -155,12 +155,17 @@ def algorithmic_bytes(kernel, S, precision, it):
         return n * (7 * s + p ** 3 * s)
     if kernel == "gather":           # splines in, p^3 grid reads, 3 field values out
         return n * (7 * s + 3 * 8 + p ** 3 * s)
-    if kernel == "pair_field":       # per directed pair: 4 B entry + 2 s (G1, G2); per atom: position, dipole, field
+    if kernel == "pair_field":       # mixed: per directed pair a 24 B record (x, G1 | G2, slot of j); FP64: 4 B entry
+        # + (G1, G2); per atom: (d, q) in R (gathered, each once), position (FP64), field out (24 B)
+        if precision:
+            return P * 24 + n * (4 * s + 24)
         return P * (4 + 2 * s) + n * (32 + 4 * s + 24)
     if kernel == "fft_chain":        # r2c + convolution (read F, G, write F) + c2r
         return 2 * (G * s + Gc * 2 * s) + Gc * (2 * s + s + 2 * s)
-    if kernel == "pair_list":        # candidates' positions, list entries + G1, G2 written
-        return n * 32 * 125 // 4 + P * (4 + 2 * s)
+    if kernel == "pair_list":        # build + compaction (skin 0): slot-order positions, wraps and radii read, the
+        # list written and read back, the entries and pair records of the evaluation written
+        rec = 24 if precision else 2 * s
+        return n * (32 + 32 + 16 + 8) + P * (4 + 4 + 4 + rec)
     if kernel == "pair_final":
         return P * 4 + n * (32 + 4 * s + 8 * 16)
     if kernel == "cg_update":
