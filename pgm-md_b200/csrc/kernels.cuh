@@ -753,22 +753,37 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
     if (P > 0) {
         // lane -> (j2, j3), loop over j1: consecutive lanes hit consecutive grid points of one row, and
         // w = t1 (q t2 t3 + e1 u2 t3 + e2 t2 u3) + u1 (e0 t2 t3) costs two products per point
-        constexpr int NPAIR = P * P, ROUNDS = (P * P + 31) / 32;
+        // full rounds: lane -> column (j2, j3), loop over j1; the columns left over (P^2 mod 32) then have their
+        // points spread over the lanes (p = 6: 6 + 1 iterations instead of 2 x 6 with 4 lanes busy in the second)
+        constexpr int PP = P > 0 ? P : 1;
+        constexpr int NPAIR = PP * PP, FULL = NPAIR / 32, LEFT = NPAIR % 32, LROUNDS = (LEFT * PP + 31) / 32;
         const size_t plane = (size_t) K1 * K2;
 #pragma unroll
-        for (int rd = 0; rd < ROUNDS; rd++) {
+        for (int rd = 0; rd < FULL; rd++) {
             const int pr = lane + 32 * rd;
-            if (pr < NPAIR) {
-                const int j2 = pr / (P > 0 ? P : 1), j3 = pr % (P > 0 ? P : 1);
+            const int j2 = pr / PP, j3 = pr % PP;
+            const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
+            const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+            const R c23 = t2 * t3;
+            const R a = qr * c23 + e1 * u2 * t3 + e2 * t2 * u3;
+            const R b = e0 * c23;
+            R* col = grid + (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2);
+#pragma unroll
+            for (int j1 = 0; j1 < PP; j1++)
+                atomicAdd(col + (size_t) wrapIndex(b0 - j1, K0) * plane, a * sth[wib][0][j1] + b * sdth[wib][0][j1]);
+        }
+#pragma unroll
+        for (int lr = 0; lr < LROUNDS; lr++) {
+            const int k = lane + 32 * lr;
+            if (k < LEFT * PP) {
+                const int pr = 32 * FULL + k % LEFT, j1 = k / LEFT;
+                const int j2 = pr / PP, j3 = pr % PP;
                 const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
                 const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
                 const R c23 = t2 * t3;
-                const R a = qr * c23 + e1 * u2 * t3 + e2 * t2 * u3;
-                const R b = e0 * c23;
-                R* col = grid + (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2);
-#pragma unroll
-                for (int j1 = 0; j1 < PM; j1++)
-                    atomicAdd(col + (size_t) wrapIndex(b0 - j1, K0) * plane, a * sth[wib][0][j1] + b * sdth[wib][0][j1]);
+                const R w = (qr * c23 + e1 * u2 * t3 + e2 * t2 * u3) * sth[wib][0][j1] + e0 * c23 * sdth[wib][0][j1];
+                atomicAdd(grid + (size_t) wrapIndex(b0 - j1, K0) * plane + (size_t) wrapIndex(b1 - j2, K1) * K2 +
+                              wrapIndex(b2 - j3, K2), w);
             }
         }
     } else {
@@ -1194,37 +1209,64 @@ __global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
     if (P > 0) {
         // lane -> (j2, j3), loop over j1: sums S_t = sum t1 phi, S_u = sum u1 phi (S_v = sum v1 phi), then the
         // products with the lane's t2, t3, u2, u3 (v2, v3)
-        constexpr int NPAIR = P * P, ROUNDS = (P * P + 31) / 32;
+        // full rounds: lane -> column (j2, j3), loop over j1; the leftover columns' points over the lanes
+        constexpr int PP = P > 0 ? P : 1;
+        constexpr int NPAIR = PP * PP, FULL = NPAIR / 32, LEFT = NPAIR % 32, LROUNDS = (LEFT * PP + 31) / 32;
         const size_t plane = (size_t) K1 * K2;
 #pragma unroll
-        for (int rd = 0; rd < ROUNDS; rd++) {
+        for (int rd = 0; rd < FULL; rd++) {
             const int pr = lane + 32 * rd;
-            if (pr < NPAIR) {
-                const int j2 = pr / (P > 0 ? P : 1), j3 = pr % (P > 0 ? P : 1);
-                const R* col = grid + (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2);
-                R St = 0, Su = 0, Sv = 0;
+            const int j2 = pr / PP, j3 = pr % PP;
+            const R* col = grid + (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2);
+            R St = 0, Su = 0, Sv = 0;
 #pragma unroll
-                for (int j1 = 0; j1 < PM; j1++) {
-                    const R ph = col[(size_t) wrapIndex(b0 - j1, K0) * plane];
-                    St += sth[wib][0][j1] * ph;
-                    Su += sdth[wib][0][j1] * ph;
-                    if (FINAL)
-                        Sv += sd2[wib][0][FINAL ? j1 : 0] * ph;
-                }
+            for (int j1 = 0; j1 < PP; j1++) {
+                const R ph = col[(size_t) wrapIndex(b0 - j1, K0) * plane];
+                St += sth[wib][0][j1] * ph;
+                Su += sdth[wib][0][j1] * ph;
+                if (FINAL)
+                    Sv += sd2[wib][0][FINAL ? j1 : 0] * ph;
+            }
+            const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
+            const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+            f[0] += Su * t2 * t3;
+            f[1] += St * u2 * t3;
+            f[2] += St * t2 * u3;
+            if (FINAL) {
+                const R v2 = sd2[wib][1][FINAL ? j2 : 0], v3 = sd2[wib][2][FINAL ? j3 : 0];
+                f2[0] += Sv * t2 * t3;
+                f2[1] += St * v2 * t3;
+                f2[2] += St * t2 * v3;
+                f2[3] += Su * u2 * t3;
+                f2[4] += Su * t2 * u3;
+                f2[5] += St * u2 * u3;
+                pot += St * t2 * t3;
+            }
+        }
+#pragma unroll
+        for (int lr = 0; lr < LROUNDS; lr++) {
+            const int k = lane + 32 * lr;
+            if (k < LEFT * PP) {
+                const int pr = 32 * FULL + k % LEFT, j1 = k / LEFT;
+                const int j2 = pr / PP, j3 = pr % PP;
+                const R ph = grid[(size_t) wrapIndex(b0 - j1, K0) * plane + (size_t) wrapIndex(b1 - j2, K1) * K2 +
+                                  wrapIndex(b2 - j3, K2)];
+                const R t1 = sth[wib][0][j1], u1 = sdth[wib][0][j1];
                 const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
                 const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
-                f[0] += Su * t2 * t3;
-                f[1] += St * u2 * t3;
-                f[2] += St * t2 * u3;
+                f[0] += u1 * t2 * t3 * ph;
+                f[1] += t1 * u2 * t3 * ph;
+                f[2] += t1 * t2 * u3 * ph;
                 if (FINAL) {
-                    const R v2 = sd2[wib][1][FINAL ? j2 : 0], v3 = sd2[wib][2][FINAL ? j3 : 0];
-                    f2[0] += Sv * t2 * t3;
-                    f2[1] += St * v2 * t3;
-                    f2[2] += St * t2 * v3;
-                    f2[3] += Su * u2 * t3;
-                    f2[4] += Su * t2 * u3;
-                    f2[5] += St * u2 * u3;
-                    pot += St * t2 * t3;
+                    const R v1 = sd2[wib][0][FINAL ? j1 : 0], v2 = sd2[wib][1][FINAL ? j2 : 0],
+                            v3 = sd2[wib][2][FINAL ? j3 : 0];
+                    f2[0] += v1 * t2 * t3 * ph;
+                    f2[1] += t1 * v2 * t3 * ph;
+                    f2[2] += t1 * t2 * v3 * ph;
+                    f2[3] += u1 * u2 * t3 * ph;
+                    f2[4] += u1 * t2 * u3 * ph;
+                    f2[5] += t1 * u2 * u3 * ph;
+                    pot += t1 * t2 * t3 * ph;
                 }
             }
         }
