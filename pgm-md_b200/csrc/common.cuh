@@ -95,6 +95,7 @@ struct Dev {
     int* listCount;           // per slot
     void* pairA;              // [slot][cap] R4: pair geometry x = r_i - r_j (image) and G1, per evaluation
     void* pairB;              // [slot][cap] R2: G2 and the slot of j (as the bits of an R)
+    void* pairC;              // [slot][cap] R2: G0, G3 (the final pass), per evaluation
     int* flags;               // [0]: list overflow, [1]: shift out of range, [2]: all systems done, [3]-[5] CG
                               // bookkeeping, [6]: list stale, [7]: block counter, [8]: list built,
                               // [9]: a pair changed its image since the build (rebuild and repeat)

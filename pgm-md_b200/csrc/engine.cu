@@ -158,7 +158,7 @@ struct Engine::Impl {
 
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
-        dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dPairA, dPairB, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
+        dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dPairA, dPairB, dPairC, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
         dScal, dPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dTwiddle, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
@@ -225,7 +225,7 @@ struct Engine::Impl {
         }
         plans64.clear();
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
-                      &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dPairA, &dPairB, &dFlags, &dDS,
+                      &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dPairA, &dPairB, &dPairC, &dFlags, &dDS,
                       &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dTwiddle, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
@@ -797,6 +797,7 @@ struct Engine::Impl {
         if (mixed())   // pair records: (x, G1) + (G2, slot of j) in float; FP64 (G1, G2) only
             dPairA.ensure((size_t) n * cap * 16);
         dPairB.ensure((size_t) n * cap * 2 * realSize());
+        dPairC.ensure((size_t) n * cap * 2 * realSize());
         if (refining())
             dPairBd.ensure((size_t) n * cap * 16);
     }
@@ -808,6 +809,7 @@ struct Engine::Impl {
         Dev d = makeDev(false, 0);
         d.pairA = nullptr;
         d.pairB = dPairBd.p;
+        d.pairC = nullptr;
         d.dS = dDSd.p;
         d.grid = dGridD.p;
         d.spec = dSpecD.p;
@@ -862,6 +864,7 @@ struct Engine::Impl {
         d.posBuild = dPosBuild.as<double>();
         d.pairA = dPairA.p;
         d.pairB = dPairB.p;
+        d.pairC = dPairC.p;
         d.flags = dFlags.as<int>();
         d.dS = dDS.p;
         d.perm = dPerm.as<double>();
@@ -1801,6 +1804,7 @@ Terms Engine::evaluateFixed(const double* pos, const double box[3][3], const dou
             typedef decltype(tag) R;
             if (keepList) {
                 k_refresh_positions<<<tb, 256, 0, I.st>>>(d);
+                k_pair_kernels<R><<<(I.n + 7) / 8, 256, 0, I.st>>>(d);   // records at the new positions
             } else {
                 I.listValid = false;   // the list below is this call's
                 CU(cudaMemsetAsync(d.cellCount, 0, (size_t) I.totalCells * sizeof(int), I.st));

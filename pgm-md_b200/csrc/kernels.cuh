@@ -427,8 +427,9 @@ __global__ void __launch_bounds__(LIST_THREADS, 4) k_build_list(Dev dv) {
 template <typename R> struct PairRec { static constexpr bool storeX = false; };
 template <> struct PairRec<float> { static constexpr bool storeX = true; };
 
-// The pair records of every listed pair (the list of the evaluation) in precision R with G1, G2 by
-// core/pgm_math.h:77-93 via pairKernels, one warp per slot, the pairs of its row over the lanes.
+// The pair records of every listed pair (the list of the evaluation) in precision R with G0..G3 by
+// core/pgm_math.h:77-93 via pairKernels, from the current slot-order positions (also after new positions on a
+// kept list), one warp per slot, the pairs of its row over the lanes.
 template <typename R>
 __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
     typedef typename V2T<R>::T R2;
@@ -443,6 +444,7 @@ __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
     const uint32_t* row = dv.list + (size_t) slot * dv.cap;
     R4* arow = (R4*) dv.pairA + (size_t) slot * dv.cap;
     R2* brow = (R2*) dv.pairB + (size_t) slot * dv.cap;
+    R2* crow = dv.pairC ? (R2*) dv.pairC + (size_t) slot * dv.cap : nullptr;
     const int cnt = dv.listCount[slot];
     const R beta = (R) S.beta;
     for (int t = lane; t < cnt; t += 32) {
@@ -456,8 +458,8 @@ __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
         const R xr0 = (R) x0, xr1 = (R) x1, xr2 = (R) x2;
         const R r = fsqrt(xr0 * xr0 + xr1 * xr1 + xr2 * xr2);
         const R a = R(1) / fsqrt(R(2) * (Rr * Rr + Rj * Rj));
-        R G[3];
-        pairKernels<R, 3>(a, beta, r, G);
+        R G[4];
+        pairKernels<R, 4>(a, beta, r, G);
         R2 vb;
         if constexpr (STORE_X) {
             R4 va;
@@ -473,11 +475,17 @@ __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
             vb.y = G[2];
         }
         brow[t] = vb;
+        if (crow) {
+            R2 vc;
+            vc.x = G[0];
+            vc.y = G[3];
+            crow[t] = vc;
+        }
     }
 }
 
 // The pairs of the Verlet list within the cutoff at this evaluation's positions with their records (x rounded to
-// R, G1, G2 in precision R by core/pgm_math.h:77-93 via pairKernels, the slot of j): one warp per slot, the
+// R, G0..G3 in precision R by core/pgm_math.h:77-93 via pairKernels, the slot of j): one warp per slot, the
 // list's row in candidate order over the lanes, compacted by ballot into the row of the evaluation's list
 // (same order, deterministic), then the radial kernels over the kept pairs.  The test is
 // the list build's at the cutoff: a prefilter on the wrapped positions, the reference's exact test
@@ -498,6 +506,7 @@ __global__ void __launch_bounds__(256, 3) k_pair_compact(Dev dv) {
     uint32_t* row = dv.list + (size_t) slot * dv.cap;
     R4* arow = (R4*) dv.pairA + (size_t) slot * dv.cap;
     R2* brow = (R2*) dv.pairB + (size_t) slot * dv.cap;
+    R2* crow = (R2*) dv.pairC + (size_t) slot * dv.cap;
     const int cnt = dv.slistCount[slot];
     const R beta = (R) S.beta;
     const double pre = S.rc2 * (1.0 + 1e-10) + 1e-300, preLo = S.rc2 * (1.0 - 1e-10);
@@ -587,8 +596,8 @@ __global__ void __launch_bounds__(256, 3) k_pair_compact(Dev dv) {
         const R Rj = (R) dv.radS[js];
         const R r = fsqrt(xr0 * xr0 + xr1 * xr1 + xr2 * xr2);
         const R a = R(1) / fsqrt(R(2) * (Rr * Rr + Rj * Rj));
-        R G[3];
-        pairKernels<R, 3>(a, beta, r, G);
+        R G[4];
+        pairKernels<R, 4>(a, beta, r, G);
         R2 vb;
         if constexpr (STORE_X) {
             va.w = G[1];
@@ -600,6 +609,10 @@ __global__ void __launch_bounds__(256, 3) k_pair_compact(Dev dv) {
             vb.y = G[2];
         }
         brow[t] = vb;
+        R2 vc;
+        vc.x = G[0];
+        vc.y = G[3];
+        crow[t] = vc;
     }
 }
 
@@ -1410,11 +1423,12 @@ __global__ void __launch_bounds__(256) k_pair_field(Dev dv, int gateDone) {
 }
 
 // Final pair pass at fixed d (core/pgm_core.cpp:422-440), per directed pair from i's side: half the pair
-// energy, the force on i (-dE/dx), the field at i and half the strain dE/dx (x) x.  G_0..G_3 recomputed in
-// precision R.
+// energy, the force on i (-dE/dx), the field at i and half the strain dE/dx (x) x.  G_0..G_3 from the
+// evaluation's pair records (x from the records in mixed precision, from the slot-order positions in FP64).
 template <typename R, int GS>
 __global__ void __launch_bounds__(256) k_pair_final(Dev dv) {
     typedef typename V4T<R>::T R4;
+    typedef typename V2T<R>::T R2;
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) / GS, lane = threadIdx.x % GS;
     if (g >= dv.nAtoms)
         return;
@@ -1422,29 +1436,46 @@ __global__ void __launch_bounds__(256) k_pair_final(Dev dv) {
     const int i = dv.slotAtom[slot];
     const SysDev& S = dv.sys[dv.atomSys[i]];
     const double4 pwi = dv.posS[slot];
-    const R Ri = (R) dv.radS[slot];
     const uint32_t* row = dv.list + (size_t) slot * dv.cap;
+    const R4* arow = (const R4*) dv.pairA + (size_t) slot * dv.cap;
+    const R2* brow = (const R2*) dv.pairB + (size_t) slot * dv.cap;
+    const R2* crow = (const R2*) dv.pairC + (size_t) slot * dv.cap;
     const R4* dS = (const R4*) dv.dS;
     const R4 di = dS[slot];
-    const R beta = (R) S.beta;
     const int cnt = dv.listCount[slot];
     R racc[16];
 #pragma unroll
     for (int k = 0; k < 16; k++)
         racc[k] = R(0);   // 0 energy, 1-3 force, 4-6 field, 7-15 strain: per-lane sums in R, across lanes in double
     for (int t = lane; t < cnt; t += GS) {
-        const uint32_t e = row[t];
-        const int js = entrySlot(e);
-        double sh[3];
-        entryShift(e, S.H, sh);
-        const double4 pwj = dv.posS[js];
-        const R x[3] = {(R) (pwi.x - pwj.x - sh[0]), (R) (pwi.y - pwj.y - sh[1]), (R) (pwi.z - pwj.z - sh[2])};
+        R x[3], G[4];
+        int js;
+        const R2 gc = crow[t];
+        G[0] = gc.x;
+        G[3] = gc.y;
+        if constexpr (PairRec<R>::storeX) {
+            const R4 xg = arow[t];
+            const R2 gb = brow[t];
+            x[0] = xg.x;
+            x[1] = xg.y;
+            x[2] = xg.z;
+            G[1] = xg.w;
+            G[2] = gb.x;
+            js = realAsSlot(gb.y);
+        } else {
+            const uint32_t e = row[t];
+            js = entrySlot(e);
+            double sh[3];
+            entryShift(e, S.H, sh);
+            const double4 pwj = dv.posS[js];
+            x[0] = (R) (pwi.x - pwj.x - sh[0]);
+            x[1] = (R) (pwi.y - pwj.y - sh[1]);
+            x[2] = (R) (pwi.z - pwj.z - sh[2]);
+            const R2 gb = brow[t];
+            G[1] = gb.x;
+            G[2] = gb.y;
+        }
         const R4 dj = dS[js];
-        const R Rj = (R) dv.radS[js];
-        const R r = fsqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
-        const R a = R(1) / fsqrt(R(2) * (Ri * Ri + Rj * Rj));
-        R G[4];
-        pairKernels<R, 4>(a, beta, r, G);
         const R qi = di.w, qj = dj.w;
         const R dix = di.x * x[0] + di.y * x[1] + di.z * x[2];
         const R djx = dj.x * x[0] + dj.y * x[1] + dj.z * x[2];
