@@ -142,6 +142,7 @@ struct Engine::Impl {
         int first, count;   // systems (contiguous in grid storage)
         long long gridOff, specOff;
         cufftHandle r2c = 0, c2r = 0;
+        cufftHandle r2c2d = 0, c2r2d = 0;   // 2D plans over the x-planes (split transforms)
     };
     std::vector<FftGroup> groups;
     std::vector<int> sysOrder;   // unused (systems stored in caller order within their group)
@@ -149,10 +150,15 @@ struct Engine::Impl {
     int totalCells = 0, cellCapacity = 0;
     int cap = 0;
     int convBlocks = 1;
-    bool useCluster = false;   // field-pass transforms by the cluster kernel (else cuFFT + influence product)
-    bool wantCluster = false;  // the caller's choice (setTransforms)
+    // field-pass transforms: TF_CUFFT cuFFT 3D plans + influence product; TF_CLUSTER one cluster kernel;
+    // TF_SPLIT cuFFT 2D plans over the x-planes + one kernel for the x-lines with the influence product
+    enum { TF_CUFFT = 0, TF_CLUSTER = 1, TF_SPLIT = 2 };
+    int tfMode = TF_CUFFT;     // in use
+    int tfWant = TF_CUFFT;     // the caller's choice (setTransforms)
     bool clusterOk = false;    // the systems' grids and the GPU allow the cluster kernel
+    bool splitOk = false;      // the systems' x extents allow the x-line kernel
     int fftcBuf = 0, fftcC = 16;
+    int maxLineBlocks = 0;
     size_t fftcSmem = 0;
     bool configured = false, atomsSet = false;
 
@@ -217,6 +223,10 @@ struct Engine::Impl {
                 cufftDestroy(g.r2c);
             if (g.c2r)
                 cufftDestroy(g.c2r);
+            if (g.r2c2d)
+                cufftDestroy(g.r2c2d);
+            if (g.c2r2d)
+                cufftDestroy(g.c2r2d);
         }
         groups.clear();
         for (auto& pl : plans64) {
@@ -283,7 +293,7 @@ struct Engine::Impl {
         CU(cudaMallocHost((void**) &hCtl, sizeof(Ctl)));
         useGraph = envInt("PGM_B200_NO_GRAPH", 0) == 0;
         pairGS = envInt("PGM_B200_PAIR_LANES", 32);
-        wantCluster = envInt("PGM_B200_CLUSTER_FFT", 0) != 0;
+        tfWant = envInt("PGM_B200_TRANSFORMS", TF_CUFFT);
         // the field pair pass runs beside the transforms of the same pass: optionally at most pairBlocks of its
         // blocks per SM (a shared-memory reservation it does not use), so that the transform kernels find room
         const int pairBlocks = envInt("PGM_B200_PAIR_BLOCKS", 0);
@@ -459,6 +469,8 @@ struct Engine::Impl {
         for (auto& g : groups) {
             if (g.r2c) cufftDestroy(g.r2c);
             if (g.c2r) cufftDestroy(g.c2r);
+            if (g.r2c2d) cufftDestroy(g.r2c2d);
+            if (g.c2r2d) cufftDestroy(g.c2r2d);
         }
         groups.clear();
         for (auto& pl : plans64) {
@@ -532,14 +544,17 @@ struct Engine::Impl {
         // system) when chosen (setTransforms, the autotuner) and every grid has at most FFT_MAXK points per
         // dimension with the prime factors 2, 3, 5 only; else cuFFT plans and the product kernel.  Cluster size:
         // 16 for few systems (parallelism), down to the smallest that fits shared memory for many
+        auto smallK = [](int K) {
+            int rad[16];
+            return K <= FFT_MAXK && fftRadices(K, rad) >= 0;
+        };
         clusterOk = true;
-        for (int k = 0; k < nsys && clusterOk; k++)
-            for (int a = 0; a < 3; a++) {
-                int rad[16];
-                const int K = sysK[k][a];
-                if (K > FFT_MAXK || fftRadices(K, rad) < 0)
-                    clusterOk = false;
-            }
+        splitOk = true;
+        for (int k = 0; k < nsys; k++) {
+            splitOk = splitOk && smallK(sysK[k][0]);
+            for (int a = 0; a < 3; a++)
+                clusterOk = clusterOk && smallK(sysK[k][a]);
+        }
         if (clusterOk) {
             const size_t csz = mixed() ? 8 : 16;
             int optin = 0;
@@ -562,13 +577,16 @@ struct Engine::Impl {
             fftcSmem = mb.second;
             clusterOk = fftcSmem <= (size_t) optin;
         }
-        if (clusterOk) {
+        if (clusterOk || splitOk) {   // twiddle tables of every grid size the kernels transform
             std::map<int, int> twOff;
             std::vector<double> tw;
             for (int k = 0; k < nsys; k++) {
                 SysDev& S = sysHost[k];
                 for (int a = 0; a < 3; a++) {
                     const int K = S.K[a];
+                    S.twOff[a] = -1;
+                    if (!smallK(K))
+                        continue;
                     if (!twOff.count(K)) {
                         twOff[K] = (int) (tw.size() / 2);
                         for (int m = 0; m < K; m++) {   // exp(-2 pi i m / K), the angle reduced to [-pi, pi]
@@ -584,13 +602,27 @@ struct Engine::Impl {
             if (mixed()) {
                 std::vector<float> tf(tw.begin(), tw.end());
                 upload(dTwiddle, tf, st);
-                clusterOk = prepareCluster<float>();
+                if (clusterOk)
+                    clusterOk = prepareCluster<float>();
             } else {
                 upload(dTwiddle, tw, st);
-                clusterOk = prepareCluster<double>();
+                if (clusterOk)
+                    clusterOk = prepareCluster<double>();
             }
         }
-        useCluster = clusterOk && wantCluster;
+        if (splitOk)
+            for (auto& g : groups) {   // 2D transforms of the x-planes: [x][y][z] -> [x][ky][kz]
+                int dims[2] = {g.K[1], g.K[2]};
+                const int pn = g.K[1] * g.K[2], sn = g.K[1] * (g.K[2] / 2 + 1);
+                CUFFT(cufftPlanMany(&g.r2c2d, 2, dims, nullptr, 1, pn, nullptr, 1, sn,
+                                    mixed() ? CUFFT_R2C : CUFFT_D2Z, g.count * g.K[0]));
+                CUFFT(cufftPlanMany(&g.c2r2d, 2, dims, nullptr, 1, sn, nullptr, 1, pn,
+                                    mixed() ? CUFFT_C2R : CUFFT_Z2D, g.count * g.K[0]));
+            }
+        maxLineBlocks = 0;
+        for (int k = 0; k < nsys; k++)
+            maxLineBlocks = std::max(maxLineBlocks, (sysK[k][1] * (sysK[k][2] / 2 + 1) + XL_LINES - 1) / XL_LINES);
+        selectTransforms();
         // chunks
         chunkSys.clear();
         chunkBegin.clear();
@@ -978,10 +1010,55 @@ struct Engine::Impl {
 
     // The transform pair with the influence product of a field pass: one cluster kernel (all systems), or
     // cuFFT plans and the product kernel.  The FP64 shadow of a mixed engine takes the cuFFT path.
+    // The transform mode in use: the caller's choice where the systems' grids allow it, else cuFFT.
+    void selectTransforms() {
+        int m = TF_CUFFT;
+        if (tfWant == TF_CLUSTER && clusterOk)
+            m = TF_CLUSTER;
+        if (tfWant == TF_SPLIT && splitOk)
+            m = TF_SPLIT;
+        if (m != tfMode && exec) {
+            cudaGraphExecDestroy(exec);
+            exec = nullptr;
+        }
+        tfMode = m;
+    }
+
+    // Split transforms: 2D R2C of every x-plane (cuFFT), the x-lines with the influence product (one kernel, all
+    // systems), 2D C2R.
+    template <typename R> void splitChain(cudaStream_t sm, const Dev& d, bool gate) {
+        typedef typename CplxT<R>::T C;
+        constexpr bool dbl = std::is_same<R, double>::value;
+        for (auto& g : groups) {
+            CUFFT(cufftSetStream(g.r2c2d, sm));
+            R* gp = (R*) d.grid + g.gridOff;
+            C* sp = (C*) d.spec + g.specOff;
+            if (!dbl)
+                CUFFT(cufftExecR2C(g.r2c2d, (cufftReal*) gp, (cufftComplex*) sp));
+            else
+                CUFFT(cufftExecD2Z(g.r2c2d, (cufftDoubleReal*) gp, (cufftDoubleComplex*) sp));
+        }
+        k_xlines<R><<<dim3(maxLineBlocks, nsys), XL_THREADS, 0, sm>>>(d, gate ? 1 : 0);
+        CU(cudaGetLastError());
+        for (auto& g : groups) {
+            CUFFT(cufftSetStream(g.c2r2d, sm));
+            R* gp = (R*) d.grid + g.gridOff;
+            C* sp = (C*) d.spec + g.specOff;
+            if (!dbl)
+                CUFFT(cufftExecC2R(g.c2r2d, (cufftComplex*) sp, (cufftReal*) gp));
+            else
+                CUFFT(cufftExecZ2D(g.c2r2d, (cufftDoubleComplex*) sp, (cufftDoubleReal*) gp));
+        }
+    }
+
     template <typename R> void transformPair(cudaStream_t sm, const Dev& d, bool gate) {
         constexpr bool dbl = std::is_same<R, double>::value;
-        if (!useCluster || dbl == mixed()) {
+        if (dbl == mixed() || tfMode == TF_CUFFT) {   // (the FP64 shadow of a mixed engine: cuFFT)
             fftChain<R>(sm, d, false, gate);
+            return;
+        }
+        if (tfMode == TF_SPLIT) {
+            splitChain<R>(sm, d, gate);
             return;
         }
         cudaLaunchConfig_t cfg = {};
@@ -1974,19 +2051,14 @@ void Engine::setPairLanes(int lanes) {
 int Engine::pairLanes() const { return impl->pairGS; }
 
 void Engine::setTransforms(int mode) {
-    if (mode != 0 && mode != 1)
-        throw std::invalid_argument("pgm_b200: transforms must be 0 (cuFFT) or 1 (cluster kernel)");
-    Impl& I = *impl;
-    I.wantCluster = mode == 1;
-    const bool use = I.clusterOk && I.wantCluster;
-    if (use != I.useCluster && I.exec) {
-        cudaGraphExecDestroy(I.exec);
-        I.exec = nullptr;
-    }
-    I.useCluster = use;
+    if (mode < 0 || mode > 2)
+        throw std::invalid_argument("pgm_b200: transforms must be 0 (cuFFT), 1 (cluster kernel) or 2 (2D cuFFT + "
+                                    "x-line kernel)");
+    impl->tfWant = mode;
+    impl->selectTransforms();
 }
 
-int Engine::transforms() const { return impl->useCluster ? 1 : 0; }
+int Engine::transforms() const { return impl->tfMode; }
 
 void Engine::setSystems(int nsys, const int* atomCount, const double* cutoff, const double* beta, const int* grid,
                         const double* q, const double* radius, const double* alpha, const int* covCount,

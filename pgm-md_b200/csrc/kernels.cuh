@@ -1166,6 +1166,57 @@ __global__ void __launch_bounds__(FftcThreads<R>::n) k_fft_cluster(Dev dv, int g
     }
 }
 
+// The x-lines of the split transforms: after 2D R2C transforms of every x-plane (cuFFT, spectrum layout
+// F[(x K1 + ky) (K2/2 + 1) + kz]), XL_LINES consecutive lines (ky, kz) per block transform forward along x,
+// take the influence product and transform back (mixed-radix Stockham passes in shared memory, host-built
+// twiddles); 2D C2R transforms of the planes follow.  blockIdx.y: the system.
+constexpr int XL_LINES = 16;
+constexpr int XL_THREADS = 256;
+
+template <typename R>
+__global__ void __launch_bounds__(XL_THREADS) k_xlines(Dev dv, int gateDone) {
+    typedef typename CplxT<R>::T C;
+    __shared__ C W0[FFT_MAXK];
+    __shared__ C A[XL_LINES * (FFT_MAXK + 1)], B[XL_LINES * (FFT_MAXK + 1)];
+    const int s = blockIdx.y;
+    if (gateDone && dv.scal[s * NSCAL + SC_DONE] != 0.0)
+        return;
+    const SysDev& S = dv.sys[s];
+    const int K0 = S.K[0], nline = S.K[1] * (S.K[2] / 2 + 1), lx = K0 + 1;
+    const int line0 = blockIdx.x * XL_LINES;
+    if (line0 >= nline)
+        return;
+    const int nl = min(XL_LINES, nline - line0);
+    C* spec = (C*) dv.spec + S.specOff + line0;
+    const R* infl = (const R*) dv.infl + S.specOff + line0;
+    const C* tw = (const C*) dv.twiddle + S.twOff[0];
+    for (int m = threadIdx.x; m < K0; m += blockDim.x)
+        W0[m] = tw[m];
+    for (int e = threadIdx.x; e < K0 * XL_LINES; e += blockDim.x) {   // consecutive threads: consecutive lines
+        const int x = e / XL_LINES, l = e % XL_LINES;
+        if (l < nl)
+            A[l * lx + x] = spec[(size_t) x * nline + l];
+    }
+    __syncthreads();
+    C* F = fftLines<R, -1>(A, B, nl, K0, lx, W0);
+    for (int e = threadIdx.x; e < K0 * XL_LINES; e += blockDim.x) {
+        const int x = e / XL_LINES, l = e % XL_LINES;
+        if (l < nl) {
+            const R g = infl[(size_t) x * nline + l];
+            C& v = F[l * lx + x];
+            v.x *= g;
+            v.y *= g;
+        }
+    }
+    __syncthreads();
+    const C* G = fftLines<R, 1>(F, F == A ? B : A, nl, K0, lx, W0);
+    for (int e = threadIdx.x; e < K0 * XL_LINES; e += blockDim.x) {
+        const int x = e / XL_LINES, l = e % XL_LINES;
+        if (l < nl)
+            spec[(size_t) x * nline + l] = G[l * lx + x];
+    }
+}
+
 // Interpolation from the potential grid: f_a = sum (d theta_a) theta theta phi (the field, E_rec = -sum_a K_a
 // recip[:, a] f_a, core/pgm_core.cpp:241-264); FINAL also the second derivatives, the potential and the
 // reciprocal forces -K_a recip[k][a] (q f1_a + sum_b e_b f2_ab) (core/pgm_core.cpp:452-487) and E_rec (x) d.

@@ -84,8 +84,9 @@ public:
     int kernelLaunches() const;
     void kernelTimes(int reps, double* ms);
     void setPairLanes(int lanes);
-    // field-pass transforms: 0 cuFFT plans + influence product kernel, 1 one cluster kernel per launch (when
-    // the grids allow it; transforms() tells which runs)
+    // field-pass transforms: 0 cuFFT 3D plans + influence product kernel, 1 one cluster kernel per launch,
+    // 2 cuFFT 2D plans over the x-planes + one x-line kernel with the influence product (1 and 2 where the grids
+    // allow them; transforms() tells which runs)
     void setTransforms(int mode);
     int transforms() const;
     int pairLanes() const;

@@ -321,7 +321,8 @@ class Engine:
         return int(self._L.pgm_engine_pair_lanes(self._h))
 
     def set_transforms(self, mode):
-        """Field-pass transforms: 0 cuFFT plans + influence product, 1 one cluster kernel per pass."""
+        """Field-pass transforms: 0 cuFFT 3D plans + influence product, 1 one cluster kernel per pass, 2 cuFFT 2D
+        plans over the x-planes + one x-line kernel with the influence product."""
         _check(self._L.pgm_engine_set_transforms(self._h, int(mode)))
 
     def transforms(self):
@@ -342,7 +343,7 @@ class Engine:
                 best, best_t = lanes, t
         self.set_pair_lanes(best)
         ft = {}
-        for mode in (0, 1):   # whole evaluations: the transforms run beside the pair passes
+        for mode in (0, 1, 2):   # whole evaluations: the transforms run beside the pair passes
             self.set_transforms(mode)
             if self.transforms() != mode:
                 continue

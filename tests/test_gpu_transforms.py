@@ -1,8 +1,9 @@
 """The field passes' transforms by the cluster kernel (a thread-block cluster per system holding its half
-spectrum in distributed shared memory) against the cuFFT plans + influence product path: the same energies and
-forces (FP64 within 1e-12 relative, mixed within 1e-6 in energy and 1e-5 relative RMS in forces), for one
-system (16 blocks per cluster) and a batch of many small systems (smaller clusters); grids with a prime factor
-above 5 or beyond 64 points stay on cuFFT."""
+spectrum in distributed shared memory) and by the split path (cuFFT 2D plans over the x-planes, one kernel for
+the x-lines with the influence product) against the cuFFT 3D plans + influence product path: the same
+energies and forces (FP64 within 1e-12 relative, mixed within 1e-6 in energy and 1e-5 relative RMS in
+forces), for one system (16 blocks per cluster) and a batch of many small systems (smaller clusters); grids
+with a prime factor above 5 or beyond 64 points stay on cuFFT."""
 
 import numpy as np
 import pytest
@@ -21,15 +22,16 @@ def settings(S, precision):
                         predictor=0, ke=PKG.systems.KE_DEFAULT, precision=precision)
 
 
+@pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_cluster_transforms_single_system(precision):
+def test_transforms_single_system(precision, mode):
     S = PKG.systems.water216()   # 20^3 grid
     out = []
-    for mode in (0, 1):
+    for m in (0, mode):
         eng = PKG.Engine(settings(S, precision))
         eng.set_system(S)
-        eng.set_transforms(mode)
-        assert eng.transforms() == mode
+        eng.set_transforms(m)
+        assert eng.transforms() == m
         out.append(eng.compute(S.pos, S.box))
         eng.close()
     a, b = out
@@ -39,8 +41,9 @@ def test_cluster_transforms_single_system(precision):
     assert a.iterations == b.iterations or precision == 1
 
 
+@pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_cluster_transforms_batch(precision):
+def test_transforms_batch(precision, mode):
     systems = []
     for k, (nm, K) in enumerate([(8, 8), (20, 9), (40, 12), (64, 15), (100, 16), (150, 18), (220, 20), (300, 24)]):
         L = (nm / 0.0334) ** (1 / 3)
@@ -48,12 +51,12 @@ def test_cluster_transforms_batch(precision):
     pos = np.concatenate([s.pos for s in systems])
     boxes = np.stack([s.box for s in systems])
     out = []
-    for mode in (0, 1):
+    for m in (0, mode):
         eng = PKG.Engine(PKG.Settings(cutoff=0.9, beta=3.5, grid=(24, 24, 24), order=6, tol=1e-10, max_iter=1000,
                                       peek=0.0, predictor=0, ke=PKG.systems.KE_DEFAULT, precision=precision))
         eng.set_systems(systems)
-        eng.set_transforms(mode)
-        assert eng.transforms() == mode
+        eng.set_transforms(m)
+        assert eng.transforms() == m
         out.append(eng.compute_batch(pos, boxes))
         eng.close()
     a, b = out
@@ -62,10 +65,22 @@ def test_cluster_transforms_batch(precision):
     assert rel_rms(b["forces"], a["forces"]) <= (1e-12 if precision == 0 else 1e-5)
 
 
-def test_cluster_transforms_need_small_235_grids():
+def test_transforms_need_small_235_grids():
     S = PKG.systems.waters(64, 12.4, seed=3, grid=(14, 14, 14), cutoff=6.0, tol=1e-6)   # 14 = 2 * 7
     eng = PKG.Engine(settings(S, PKG.FP64))
     eng.set_system(S)
-    eng.set_transforms(1)
-    assert eng.transforms() == 0
+    for mode in (1, 2):
+        eng.set_transforms(mode)
+        assert eng.transforms() == 0
     assert np.isfinite(eng.compute(S.pos, S.box).energy)
+    S2 = PKG.systems.waters(64, 12.4, seed=3, grid=(12, 14, 14), cutoff=6.0, tol=1e-6)   # x extent 12: split only
+    eng2 = PKG.Engine(settings(S2, PKG.FP64))
+    eng2.set_system(S2)
+    eng2.set_transforms(1)
+    assert eng2.transforms() == 0
+    eng2.set_transforms(2)
+    assert eng2.transforms() == 2
+    ref = PKG.Engine(settings(S2, PKG.FP64))
+    ref.set_system(S2)
+    a, b = eng2.compute(S2.pos, S2.box), ref.compute(S2.pos, S2.box)
+    assert abs(a.energy - b.energy) <= 1e-12 * abs(b.energy)
