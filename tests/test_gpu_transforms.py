@@ -1,6 +1,7 @@
 """The field passes' transforms by the cluster kernel (a thread-block cluster per system holding its half
 spectrum in distributed shared memory) and by the split path (cuFFT 2D plans over the x-planes, one kernel for
-the x-lines with the influence product) against the cuFFT 3D plans + influence product path: the same
+the x-lines with the influence product) against the cuFFT 3D plans +
+influence product path: the same
 energies and forces (FP64 within 1e-12 relative, mixed within 1e-6 in energy and 1e-5 relative RMS in
 forces), for one system (16 blocks per cluster) and a batch of many small systems (smaller clusters); grids
 with a prime factor above 5 or beyond 64 points stay on cuFFT."""
@@ -24,8 +25,10 @@ def settings(S, precision):
 
 @pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_transforms_single_system(precision, mode):
-    S = PKG.systems.water216()   # 20^3 grid
+@pytest.mark.parametrize("name", ["water216", "tiny_triclinic"])
+def test_transforms_single_system(precision, mode, name):
+    # 20^3 and 48^3 grids
+    S = PKG.systems.water216() if name == "water216" else PKG.systems.tiny_triclinic(nmol=20, seed=9)
     out = []
     for m in (0, mode):
         eng = PKG.Engine(settings(S, precision))
