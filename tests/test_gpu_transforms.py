@@ -1,10 +1,9 @@
 """The field passes' transforms by the cluster kernel (a thread-block cluster per system holding its half
 spectrum in distributed shared memory) and by the split path (cuFFT 2D plans over the x-planes, one kernel for
-the x-lines with the influence product) against the cuFFT 3D plans +
-influence product path: the same
-energies and forces (FP64 within 1e-12 relative, mixed within 1e-6 in energy and 1e-5 relative RMS in
-forces), for one system (16 blocks per cluster) and a batch of many small systems (smaller clusters); grids
-with a prime factor above 5 or beyond 64 points stay on cuFFT."""
+the x-lines with the influence product) against the cuFFT 3D plans + influence product path: the same energies
+and forces (FP64 within 1e-12 relative, mixed within 1e-6 in energy and 1e-5 relative RMS in forces), for one
+system (16 blocks per cluster) and a batch of many small systems (smaller clusters); grids with a prime factor
+above 5 or beyond 64 points stay on cuFFT."""
 
 import numpy as np
 import pytest
