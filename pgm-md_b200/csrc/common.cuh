@@ -98,7 +98,8 @@ struct Dev {
     void* pairC;              // [slot][cap] R2: G0, G3 (the final pass), per evaluation
     int* flags;               // [0]: list overflow, [1]: shift out of range, [2]: all systems done, [3]-[5] CG
                               // bookkeeping, [6]: list stale, [7]: block counter, [8]: list built,
-                              // [9]: a pair changed its image since the build (rebuild and repeat)
+                              // [9]: a pair changed its image since the build (rebuild and repeat),
+                              // [10]: block counter of the CG gather
     // dipoles
     void* dS;                 // slot-order R4 (dipole xyz, charge w) for the pair passes
     double* perm;             // 3n
@@ -113,6 +114,7 @@ struct Dev {
     double* Ap;
     double* scal;             // nSys * NSCAL
     double* partial;          // nChunks * 16
+    double* gpartial;         // per gather block: p . A p partials (the CG gather of a single-system engine)
     int* sysCounter;          // nSys
     // fields / forces
     double* Epair;            // 3n

@@ -155,6 +155,7 @@ struct Engine::Impl {
     enum { TF_CUFFT = 0, TF_CLUSTER = 1, TF_SPLIT = 2 };
     int tfMode = TF_CUFFT;     // in use
     int tfWant = TF_CUFFT;     // the caller's choice (setTransforms)
+    bool fuseCgA = true;       // single system: A p and alph in the CG gather's epilogue (else a separate kernel)
     bool clusterOk = false;    // the systems' grids and the GPU allow the cluster kernel
     bool splitOk = false;      // the systems' x extents allow the x-line kernel
     int fftcBuf = 0, fftcC = 16;
@@ -165,7 +166,7 @@ struct Engine::Impl {
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
         dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dPairA, dPairB, dPairC, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
-        dScal, dPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
+        dScal, dPartial, dGPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dTwiddle, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
         dGradQ, dGradR, dSList, dSListCount, dPosBuild;
@@ -236,7 +237,7 @@ struct Engine::Impl {
         plans64.clear();
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
                       &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dPairA, &dPairB, &dPairC, &dFlags, &dDS,
-                      &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dSysCounter, &dEpair,
+                      &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dGPartial, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dTwiddle, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
                       &dCovByAtomOff, &dCovByAtom, &dCovByPartnerOff, &dCovByPartner, &dChunkSys, &dChunkBegin,
@@ -294,6 +295,7 @@ struct Engine::Impl {
         useGraph = envInt("PGM_B200_NO_GRAPH", 0) == 0;
         pairGS = envInt("PGM_B200_PAIR_LANES", 32);
         tfWant = envInt("PGM_B200_TRANSFORMS", TF_CUFFT);
+        fuseCgA = envInt("PGM_B200_FUSED_CG", 1) != 0;
         // the field pair pass runs beside the transforms of the same pass: optionally at most pairBlocks of its
         // blocks per SM (a shared-memory reservation it does not use), so that the transform kernels find room
         const int pairBlocks = envInt("PGM_B200_PAIR_BLOCKS", 0);
@@ -679,6 +681,7 @@ struct Engine::Impl {
         dGradR.ensure(n * 8);
         dScal.ensure(nsys * NSCAL * 8);
         dPartial.ensure(chunkSys.size() * 16 * 8);
+        dGPartial.ensure(((size_t) n + 7) / 8 * 8);
         dSysCounter.ensure(nsys * sizeof(int));
         CU(cudaMemset(dSysCounter.p, 0, nsys * sizeof(int)));
         dResults.ensure(nsys * NRES * 8);
@@ -910,6 +913,7 @@ struct Engine::Impl {
         d.Ap = dAp.as<double>();
         d.scal = dScal.as<double>();
         d.partial = dPartial.as<double>();
+        d.gpartial = dGPartial.as<double>();
         d.sysCounter = dSysCounter.as<int>();
         d.Epair = dEpair.as<double>();
         d.Erec = dErec.as<double>();
@@ -1088,14 +1092,15 @@ struct Engine::Impl {
         CU(cudaGetLastError());
     }
 
-    template <typename R, bool FINAL> void launchGather(cudaStream_t sm, const Dev& d, int gate) {
+    // CGA: the CG iteration's gather of a single-system engine, with A p and alph in its epilogue.
+    template <typename R, bool FINAL, bool CGA = false> void launchGather(cudaStream_t sm, const Dev& d, int gate) {
         const int wb = (n + 7) / 8;
         switch (s.order) {
-        case 4: k_gather<R, FINAL, 4><<<wb, 256, 0, sm>>>(d, gate); break;
-        case 5: k_gather<R, FINAL, 5><<<wb, 256, 0, sm>>>(d, gate); break;
-        case 6: k_gather<R, FINAL, 6><<<wb, 256, 0, sm>>>(d, gate); break;
-        case 8: k_gather<R, FINAL, 8><<<wb, 256, 0, sm>>>(d, gate); break;
-        default: k_gather<R, FINAL, 0><<<wb, 256, 0, sm>>>(d, gate);
+        case 4: k_gather<R, FINAL, 4, CGA><<<wb, 256, 0, sm>>>(d, gate); break;
+        case 5: k_gather<R, FINAL, 5, CGA><<<wb, 256, 0, sm>>>(d, gate); break;
+        case 6: k_gather<R, FINAL, 6, CGA><<<wb, 256, 0, sm>>>(d, gate); break;
+        case 8: k_gather<R, FINAL, 8, CGA><<<wb, 256, 0, sm>>>(d, gate); break;
+        default: k_gather<R, FINAL, 0, CGA><<<wb, 256, 0, sm>>>(d, gate);
         }
         CU(cudaGetLastError());
     }
@@ -1115,7 +1120,7 @@ struct Engine::Impl {
 
     // field of (q?, vec) at every atom into Epair / Erec: spread on sm, then the pair pass on sm beside the
     // FFT chain on the side stream; joined on sm.
-    template <typename R, bool WITHQ>
+    template <typename R, bool WITHQ, bool CGA = false>
     void fieldPass(cudaStream_t sm, cudaStream_t sd, const Dev& d, int spreadMode, double* vec, bool gate) {
         launchSpread<R>(sm, d, spreadMode, vec);
         CU(cudaEventRecord(evFork, sm));
@@ -1124,7 +1129,7 @@ struct Engine::Impl {
         pairField<R, WITHQ>(sm, d, gate ? 1 : 0);
         CU(cudaEventRecord(evJoin, sd));
         CU(cudaStreamWaitEvent(sm, evJoin, 0));
-        launchGather<R, false>(sm, d, gate ? 1 : 0);
+        launchGather<R, false, CGA>(sm, d, gate ? 1 : 0);
     }
 
     // The Verlet list's build: cells, slots, the list at cutoff + skin (positions already in posIn).
@@ -1209,8 +1214,12 @@ struct Engine::Impl {
     }
 
     template <typename R> void enqueueIteration(cudaStream_t sm, cudaStream_t sd, const Dev& d) {
-        fieldPass<R, false>(sm, sd, d, 2, d.p, true);
-        k_cg_a<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+        if (nsys == 1 && fuseCgA) {   // A p and alph in the gather's epilogue
+            fieldPass<R, false, true>(sm, sd, d, 2, d.p, true);
+        } else {
+            fieldPass<R, false>(sm, sd, d, 2, d.p, true);
+            k_cg_a<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+        }
         k_cg_upd<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
         CU(cudaGetLastError());
     }
@@ -1976,12 +1985,14 @@ int Engine::kernelLaunches() const {
         return 0;
     // own kernels per evaluation (the cuFFT transforms not counted): preparation 7, the Verlet list's build 5
     // when it ran; a field pass fp = 4 (spread, the cluster transform kernel or the influence product, pair
-    // pass, gather); polarizable: two field passes + 2 before the loop, fp + 2 per CG iteration; final 7
+    // pass, gather); polarizable: two field passes + 2 before the loop, fp + 2 per CG iteration (fp + 1 for one
+    // system); final 7
     int it = 0;
     for (int k = 0; k < I.nsys; k++)
         it = std::max(it, (int) I.lastResults[(size_t) k * NRES + 14]);
     const int fp = 4;
-    return 7 + (I.lastBuilt ? 5 : 0) + (I.s.polarizable ? 2 * fp + 2 + (fp + 2) * it : 0) + 7;
+    const int perIt = fp + (I.nsys == 1 && I.fuseCgA ? 1 : 2);   // single system: A p in the gather
+    return 7 + (I.lastBuilt ? 5 : 0) + (I.s.polarizable ? 2 * fp + 2 + perIt * it : 0) + 7;
 }
 
 void Engine::kernelTimes(int reps, double* ms) {

@@ -1220,19 +1220,13 @@ __global__ void __launch_bounds__(XL_THREADS) k_xlines(Dev dv, int gateDone) {
 // Interpolation from the potential grid: f_a = sum (d theta_a) theta theta phi (the field, E_rec = -sum_a K_a
 // recip[:, a] f_a, core/pgm_core.cpp:241-264); FINAL also the second derivatives, the potential and the
 // reciprocal forces -K_a recip[k][a] (q f1_a + sum_b e_b f2_ab) (core/pgm_core.cpp:452-487) and E_rec (x) d.
+// The gather of slot's atom i (system S) by its warp: E_rec (and with FINAL the reciprocal forces, E_rec (x) d
+// and the potential); sth / sdth / sd2 are the warp's shared spline rows.
 template <typename R, bool FINAL, int P>
-__global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
+__device__ __forceinline__ void gatherSlot(const Dev& dv, const SysDev& S, int slot, int i, int wib, int lane,
+                                           R (*sth)[3][P > 0 ? P : MAXP], R (*sdth)[3][P > 0 ? P : MAXP],
+                                           R (*sd2)[3][FINAL ? (P > 0 ? P : MAXP) : 1]) {
     constexpr int PM = P > 0 ? P : MAXP;
-    __shared__ R sth[8][3][PM], sdth[8][3][PM], sd2[8][3][FINAL ? PM : 1];
-    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int slot = blockIdx.x * 8 + wib;
-    if (slot >= dv.nAtoms)
-        return;
-    const int i = dv.slotAtom[slot];
-    const int s = dv.atomSys[i];
-    if (gateDone && dv.scal[s * NSCAL + SC_DONE] != 0.0)
-        return;
-    const SysDev& S = dv.sys[s];
     const int p = P > 0 ? P : dv.order;
     int bl = 0;
     if (lane < 3) {
@@ -1396,6 +1390,78 @@ __global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
     }
     if (FINAL && lane == 0)
         dv.potRec[i] = F2[6];
+}
+
+// A warp per slot, reads from the grid (L2).  CGA (the CG iterations of a single-system engine): each atom's
+// row of A p = p / alpha - (E_pair + E_rec + cs p) (core/pgm_core.cpp:363) in the epilogue, block partials of
+// p . A p, and the last block to finish sums them in block order (deterministic) and sets alph = rz / p.Ap.
+template <typename R, bool FINAL, int P, bool CGA>
+__global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
+    constexpr int PM = P > 0 ? P : MAXP;
+    __shared__ R sth[8][3][PM], sdth[8][3][PM], sd2[8][3][FINAL ? PM : 1];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = blockIdx.x * 8 + wib;
+    if constexpr (!CGA) {
+        if (slot >= dv.nAtoms)
+            return;
+        const int i = dv.slotAtom[slot];
+        const int s = dv.atomSys[i];
+        if (gateDone && dv.scal[s * NSCAL + SC_DONE] != 0.0)
+            return;
+        gatherSlot<R, FINAL, P>(dv, dv.sys[s], slot, i, wib, lane, sth, sdth, sd2);
+    } else {
+        double* sc = dv.scal;   // system 0
+        if (sc[SC_DONE] != 0.0)
+            return;   // every block alike
+        const SysDev& S = dv.sys[0];
+        double v = 0.0;
+        if (slot < dv.nAtoms) {
+            const int i = dv.slotAtom[slot];
+            gatherSlot<R, FINAL, P>(dv, S, slot, i, wib, lane, sth, sdth, sd2);
+            if (lane < 3) {
+                const double cs = 4.0 * S.beta * S.beta * S.beta / (3.0 * SQRT_PI);
+                const double al = dv.alpha[i];
+                const int k = lane;
+                const double pk = dv.p[3 * i + k];
+                const double Tp = dv.Epair[3 * i + k] + dv.Erec[3 * i + k] + cs * pk;
+                const double apk = (al > 0) ? pk / al - Tp : 0.0;
+                dv.Ap[3 * i + k] = apk;
+                v = pk * apk;
+            }
+        }
+        v += __shfl_down_sync(0xffffffffu, v, 2);
+        v += __shfl_down_sync(0xffffffffu, v, 1);   // lane 0: its atom's p . A p (lanes 0, 1, 2; fixed order)
+        __shared__ double wsum[8];
+        __shared__ int isLast;
+        if (lane == 0)
+            wsum[wib] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b = 0.0;
+            for (int w = 0; w < 8; w++)
+                b += wsum[w];
+            dv.gpartial[blockIdx.x] = b;
+            __threadfence();
+            isLast = atomicAdd(&dv.flags[10], 1) == (int) gridDim.x - 1;
+        }
+        __syncthreads();
+        if (!isLast)
+            return;
+        __threadfence();
+        __shared__ double tsum[256];
+        double acc = 0.0;
+        for (int b = threadIdx.x; b < (int) gridDim.x; b += blockDim.x)
+            acc += __ldcg(&dv.gpartial[b]);
+        tsum[threadIdx.x] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int t = 0; t < (int) blockDim.x; t++)
+                tot += tsum[t];
+            sc[SC_ALPH] = sc[SC_RZ] / fmax(tot, 1e-300);
+            dv.flags[10] = 0;
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------------------ pair passes

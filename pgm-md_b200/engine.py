@@ -343,15 +343,17 @@ class Engine:
                 best, best_t = lanes, t
         self.set_pair_lanes(best)
         ft = {}
-        for mode in (0, 1, 2):   # whole evaluations: the transforms run beside the pair passes
+        for mode in (0, 1, 2):   # whole evaluations (the transforms run beside the pair passes), median of calls
             self.set_transforms(mode)
             if self.transforms() != mode:
                 continue
             run()
-            t0 = time.perf_counter()
-            for _ in range(max(2, reps // 3)):
+            ts = []
+            for _ in range(max(5, reps)):
+                t0 = time.perf_counter()
                 run()
-            ft[mode] = time.perf_counter() - t0
+                ts.append(time.perf_counter() - t0)
+            ft[mode] = float(np.median(ts))
         self.set_transforms(min(ft, key=ft.get))
         return best
 
