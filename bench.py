@@ -608,9 +608,9 @@ def large_leg(pkg, local, world, dist):
 
 def batch_leg(pkg, local, rank, world, dist):
     """1024 independent water boxes of 8..512 molecules (0.0334 / A^3, grids <= 1 A spacing with 2-3-5 sizes,
-    cutoff min(9 A, L/2),
-    tol 1e-5, mixed) in one launch per rank (systems partitioned by atom count across ranks), against the same
-    systems evaluated one after the other by single-system engines (a sample of 64, on rank 0)."""
+    cutoff min(9 A, L/2), tol 1e-5, mixed) in one launch per rank (systems partitioned by atom count across
+    ranks), against the same systems evaluated one after the other by single-system engines (a sample of 64, on
+    rank 0); with the main kernels' times and the field pair pass against the HBM roofline."""
     import torch
     import pgm_md_b200.shard as sh
     systems = pkg.systems.water_batch(nsys=1024, seed=1024, tol=1e-5)
@@ -638,12 +638,21 @@ def batch_leg(pkg, local, rank, world, dist):
     eng.set_transforms(chosen)
     res["r"] = eng.compute_batch(pos, boxes)
     dt = per_mode[chosen]
+    # main kernels relaunched alone; the field pair pass streams P x 24-byte pair records (mixed) from HBM here
+    kt = eng.kernel_times(reps=3)
+    npairs = eng.num_candidates()
+    peak, peak_kind = peaks()
+    pf_bytes = npairs * 24 + eng.n * 40
+    pf_gbs = pf_bytes / (kt["pair_field"] * 1e-3) / 1e9
     energies = sh.gather_energies(parts[rank], res["r"]["energies"], len(systems))
     out = {"workload": "water_batch1024", "systems": len(systems), "atoms": int(sum(s.n for s in systems)),
            "systems_per_s": len(systems) / dt, "ms_per_batch": 1e3 * dt,
            "max_cg_iterations": int(res["r"]["iterations"].max()), "partition": "atom-balanced, one launch per rank",
            "pair_lanes": lanes, "transforms": TRANSFORMS[chosen],
            "ms_per_batch_by_transforms": {TRANSFORMS[m]: 1e3 * v for m, v in per_mode.items()},
+           "directed_pairs": npairs, "kernel_ms": kt,
+           "pair_field_roofline": {"bound": "hbm", "bytes_per_launch": pf_bytes, "achieved": pf_gbs, "peak": peak,
+                                   "unit": "GB/s", "frac": pf_gbs / peak, "peak_source": peak_kind},
            "energies_finite": bool(np.isfinite(energies).all())}
     eng.close()
     if rank == 0:
