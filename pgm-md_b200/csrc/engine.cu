@@ -896,6 +896,10 @@ struct Engine::Impl {
         d.listCount = dListCount.as<int>();
         d.slist = dSList.as<uint32_t>();
         d.slistCount = dSListCount.as<int>();
+        if (s.skin <= 0) {   // no skin: the build writes the evaluation's list itself (no compaction)
+            d.slist = d.list;
+            d.slistCount = d.listCount;
+        }
         d.posBuild = dPosBuild.as<double>();
         d.pairA = dPairA.p;
         d.pairB = dPairB.p;
@@ -1132,6 +1136,16 @@ struct Engine::Impl {
         launchGather<R, false, CGA>(sm, d, gate ? 1 : 0);
     }
 
+    // The evaluation's pair list with its records: the Verlet list compacted to the cutoff, or, without a skin
+    // (the build wrote the evaluation's list), the records of every listed pair.
+    template <typename R> void pairRecords(cudaStream_t sm, const Dev& d) {
+        if (s.skin <= 0)
+            k_pair_kernels<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
+        else
+            k_pair_compact<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
+        CU(cudaGetLastError());
+    }
+
     // The Verlet list's build: cells, slots, the list at cutoff + skin (positions already in posIn).
     void enqueueBuild(cudaStream_t sm, const Dev& d) {
         const int tb = (n + 255) / 256;
@@ -1185,7 +1199,7 @@ struct Engine::Impl {
             // (main stream)
             CU(cudaEventRecord(evFork, sm));
             CU(cudaStreamWaitEvent(sd, evFork, 0));
-            k_pair_compact<R><<<(n + 7) / 8, 256, 0, sd>>>(d);
+            pairRecords<R>(sd, d);
             CU(cudaEventRecord(evJoin, sd));
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
             k_perm<<<tb, 256, 0, sm>>>(d);
@@ -1205,7 +1219,7 @@ struct Engine::Impl {
             // the loop's first spread needs a clear grid (each iteration clears it for the next one)
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
         } else {
-            k_pair_compact<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
+            pairRecords<R>(sm, d);
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
             k_perm<<<tb, 256, 0, sm>>>(d);
             k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
@@ -2020,7 +2034,7 @@ void Engine::kernelTimes(int reps, double* ms) {
         typedef decltype(tag) R;
         ms[0] = timeIt([&] {
             k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(d);
-            k_pair_compact<R><<<(I.n + 7) / 8, 256, 0, I.st>>>(d);
+            I.pairRecords<R>(I.st, d);
         });
         ms[1] = timeIt([&] { I.pairField<R, false>(I.st, d, 0); });
         ms[2] = timeIt([&] { I.launchSpread<R>(I.st, d, 1, d.x); });
