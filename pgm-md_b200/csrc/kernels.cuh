@@ -363,71 +363,51 @@ __global__ void __launch_bounds__(LIST_THREADS, 4) k_build_list(Dev dv) {
             cEntry[t] = (uint32_t) (js | (code << 23));
         }
         __syncthreads();
-        // each warp tests its two atoms (ii and ii + NW) against every staged candidate in one pass
-        for (int ib = cb + wid; ib < ce; ib += 2 * NW) {
-            const int ia[2] = {ib, ib + NW};
-            const bool has1 = ia[1] < ce;
-            float xi[2][3];
-            int count[2];
-#pragma unroll
-            for (int u = 0; u < 2; u++) {
-                const int ii = (u == 0 || has1) ? ia[u] : ia[0];
-                const double4 pwi = dv.posS[ii];
-                xi[u][0] = (float) (pwi.x - org.x);
-                xi[u][1] = (float) (pwi.y - org.y);
-                xi[u][2] = (float) (pwi.z - org.z);
-                count[u] = dv.slistCount[ii];
-            }
+        for (int ii = cb + wid; ii < ce; ii += NW) {
+            const double4 pwi = dv.posS[ii];
+            const float xi = (float) (pwi.x - org.x), yi = (float) (pwi.y - org.y), zi = (float) (pwi.z - org.z);
+            uint32_t* row = dv.slist + (size_t) ii * dv.cap;
+            int count = dv.slistCount[ii];
             for (int t0 = 0; t0 < nc; t0 += 32) {
                 const int t = t0 + lane;
-                bool acc[2] = {false, false}, unsure[2] = {false, false};
+                bool acc = false, unsure = false;
                 uint32_t entry = 0;
                 if (t < nc) {
                     const float4 pj = cPos[t];
                     entry = cEntry[t];
-#pragma unroll
-                    for (int u = 0; u < 2; u++) {
-                        const float y0 = xi[u][0] - pj.x, y1 = xi[u][1] - pj.y, y2 = xi[u][2] - pj.z;
-                        const float r2 = y0 * y0 + y1 * y1 + y2 * y2;
-                        if ((u == 0 || has1) && (int) (entry & 0x7FFFFFu) != ia[u] && r2 < preF) {
-                            if (r2 < preLoF && fabsf(y0) < hf0 && fabsf(y1) < hf1 && fabsf(y2) < hf2)
-                                acc[u] = true;
-                            else
-                                unsure[u] = true;
-                        }
+                    const float y0 = xi - pj.x, y1 = yi - pj.y, y2 = zi - pj.z;
+                    const float r2 = y0 * y0 + y1 * y1 + y2 * y2;
+                    if ((int) (entry & 0x7FFFFFu) != ii && r2 < preF) {
+                        if (r2 < preLoF && fabsf(y0) < hf0 && fabsf(y1) < hf1 && fabsf(y2) < hf2)
+                            acc = true;
+                        else
+                            unsure = true;
                     }
                 }
-#pragma unroll
-                for (int u = 0; u < 2; u++) {
-                    if (__any_sync(0xffffffffu, unsure[u]) && unsure[u]) {
-                        // the reference's exact test on the original positions; kept only at the image it chooses
-                        const int ii = ia[u];
-                        const int js = (int) (entry & 0x7FFFFFu);
-                        const int w0 = (int) ((entry >> 23) & 7u) - 4, w1 = (int) ((entry >> 26) & 7u) - 4,
-                                  w2 = (int) ((entry >> 29) & 7u) - 4;
-                        const double4 oi = dv.origS[ii], oj = dv.origS[js];
-                        const int4 wi = dv.wrapS[ii], cw = dv.wrapS[js];
-                        double x[3] = {__dsub_rn(oi.x, oj.x), __dsub_rn(oi.y, oj.y), __dsub_rn(oi.z, oj.z)};
-                        int kk[3];
-                        minImageFast(x, S.H, invDiag, kk);
-                        if (dot3exact(x) < S.rl2)
-                            acc[u] = (kk[0] - (wi.x - cw.x) == w0 && kk[1] - (wi.y - cw.y) == w1 &&
-                                      kk[2] - (wi.z - cw.z) == w2);
-                    }
-                    const unsigned ma = __ballot_sync(0xffffffffu, acc[u]);
-                    if (acc[u]) {
-                        const int pos = count[u] + __popc(ma & ((1u << lane) - 1u));
-                        if (pos < dv.cap)
-                            dv.slist[(size_t) ia[u] * dv.cap + pos] = entry;
-                    }
-                    count[u] += __popc(ma);
+                if (__any_sync(0xffffffffu, unsure) && unsure) {
+                    // the reference's exact test on the original positions; kept only at the image it chooses
+                    const int js = (int) (entry & 0x7FFFFFu);
+                    const int w0 = (int) ((entry >> 23) & 7u) - 4, w1 = (int) ((entry >> 26) & 7u) - 4,
+                              w2 = (int) ((entry >> 29) & 7u) - 4;
+                    const double4 oi = dv.origS[ii], oj = dv.origS[js];
+                    const int4 wi = dv.wrapS[ii], cw = dv.wrapS[js];
+                    double x[3] = {__dsub_rn(oi.x, oj.x), __dsub_rn(oi.y, oj.y), __dsub_rn(oi.z, oj.z)};
+                    int kk[3];
+                    minImageFast(x, S.H, invDiag, kk);
+                    if (dot3exact(x) < S.rl2)
+                        acc = (kk[0] - (wi.x - cw.x) == w0 && kk[1] - (wi.y - cw.y) == w1 &&
+                               kk[2] - (wi.z - cw.z) == w2);
                 }
+                const unsigned ma = __ballot_sync(0xffffffffu, acc);
+                if (acc) {
+                    const int pos = count + __popc(ma & ((1u << lane) - 1u));
+                    if (pos < dv.cap)
+                        row[pos] = entry;
+                }
+                count += __popc(ma);
             }
-            if (lane == 0) {
-                dv.slistCount[ia[0]] = count[0];
-                if (has1)
-                    dv.slistCount[ia[1]] = count[1];
-            }
+            if (lane == 0)
+                dv.slistCount[ii] = count;
         }
         __syncthreads();
     }
