@@ -35,7 +35,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "pGM E+F evals/s, 8550-atom PME, mixed vs FP64 GPU at force relRMS≤1e-5"
 WORKLOAD = "dimethylphenol8550"
 TOL = 1e-5
-TRANSFORMS = {0: "cuFFT + influence product", 1: "cluster kernel", 2: "cuFFT 2D + x-line kernel"}
+TRANSFORMS = {0: "cuFFT + influence product", 1: "cluster kernel", 2: "cuFFT 2D + x-line kernel",
+              3: "grid kernel (block per x-plane)"}
 
 
 def parse():
@@ -626,7 +627,7 @@ def batch_leg(pkg, local, rank, world, dist):
     chosen = eng.transforms()
     res = {}
     per_mode = {}
-    for mode in (0, 1, 2):   # every kind of transforms timed (every rank the same steps); the autotuned one reported
+    for mode in (0, 1, 2, 3):   # every kind of transforms timed (every rank the same steps); the autotuned one reported
         eng.set_transforms(mode)
         if eng.transforms() != mode:
             continue

@@ -167,8 +167,10 @@ int pgm_engine_pair_lanes(pgm_engine* e);
  * 0 cuFFT R2C / C2R 3D plans with an influence-product kernel; 1 one kernel per pass in which a thread-block
  * cluster per system holds the half spectrum in distributed shared memory (grids up to 64 points per dimension
  * with prime factors 2, 3, 5); 2 cuFFT 2D plans over the x-planes with one kernel for the x-lines and the
- * influence product (x extents up to 64 with prime factors 2, 3, 5).  pgm_engine_transforms: the kind in use
- * (1 and 2 only where the grids allow them). */
+ * influence product (x extents up to 64 with prime factors 2, 3, 5); 3 one cooperative kernel per pass with a
+ * thread block per x-plane of every system, the planes and the x-lines exchanged through L2 between two bounded
+ * barriers (grids as for 1, every system's blocks resident together).  pgm_engine_transforms: the kind in use
+ * (1, 2 and 3 only where the grids allow them). */
 int pgm_engine_set_transforms(pgm_engine* e, int mode);
 int pgm_engine_transforms(pgm_engine* e);
 

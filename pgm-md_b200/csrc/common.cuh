@@ -99,7 +99,8 @@ struct Dev {
     int* flags;               // [0]: list overflow, [1]: shift out of range, [2]: all systems done, [3]-[5] CG
                               // bookkeeping, [6]: list stale, [7]: block counter, [8]: list built,
                               // [9]: a pair changed its image since the build (rebuild and repeat),
-                              // [10]: block counter of the CG gather
+                              // [10]: block counter of the CG gather, [11]: a grid-transform barrier gave up;
+                              // followed by the grid transforms' barriers (2 per system)
     // dipoles
     void* dS;                 // slot-order R4 (dipole xyz, charge w) for the pair passes
     double* perm;             // 3n
@@ -136,6 +137,8 @@ struct Dev {
     const void* twiddle;      // complex R tables exp(-2 pi i m / K), m < K, per distinct K (cluster transforms)
     int fftcBuf;              // complex elements per transform buffer of a cluster block
     int fftcC;                // blocks per cluster
+    int fftgBuf;              // complex elements per transform buffer of a grid-transform block
+    unsigned* fftgBar;        // per system: arrivals and generation of the grid transforms' barrier
     const double* moduli;
     // covalent
     int ncov;

@@ -151,14 +151,18 @@ struct Engine::Impl {
     int cap = 0;
     int convBlocks = 1;
     // field-pass transforms: TF_CUFFT cuFFT 3D plans + influence product; TF_CLUSTER one cluster kernel;
-    // TF_SPLIT cuFFT 2D plans over the x-planes + one kernel for the x-lines with the influence product
-    enum { TF_CUFFT = 0, TF_CLUSTER = 1, TF_SPLIT = 2 };
+    // TF_SPLIT cuFFT 2D plans over the x-planes + one kernel for the x-lines with the influence product;
+    // TF_GRID one cooperative kernel, a block per x-plane
+    enum { TF_CUFFT = 0, TF_CLUSTER = 1, TF_SPLIT = 2, TF_GRID = 3 };
     int tfMode = TF_CUFFT;     // in use
     int tfWant = TF_CUFFT;     // the caller's choice (setTransforms)
     bool fuseCgA = true;       // single system: A p and alph in the CG gather's epilogue (else a separate kernel)
     bool clusterOk = false;    // the systems' grids and the GPU allow the cluster kernel
     bool splitOk = false;      // the systems' x extents allow the x-line kernel
-    int fftcBuf = 0, fftcC = 16;
+    bool gridOk = false;       // the systems' grids and the GPU allow the grid-transform kernel
+    int fftcBuf = 0, fftcC = 16, fftgBuf = 0, maxK0 = 0;
+    int fftgKc = 0;            // the grid transforms' compile-time size (every grid fftgKc^3), or 0
+    size_t fftgSmem = 0;
     int maxLineBlocks = 0;
     size_t fftcSmem = 0;
     bool configured = false, atomsSet = false;
@@ -552,10 +556,26 @@ struct Engine::Impl {
         };
         clusterOk = true;
         splitOk = true;
+        maxK0 = 0;
         for (int k = 0; k < nsys; k++) {
             splitOk = splitOk && smallK(sysK[k][0]);
             for (int a = 0; a < 3; a++)
                 clusterOk = clusterOk && smallK(sysK[k][a]);
+            maxK0 = std::max(maxK0, sysK[k][0]);
+        }
+        const bool allSmall = clusterOk;
+        gridOk = allSmall;
+        if (gridOk) {   // the grid transforms: a block per x-plane of every system, all resident at once
+            fftgBuf = 0;
+            for (int k = 0; k < nsys; k++)
+                fftgBuf = std::max(fftgBuf, fftgBufferElems(sysHost[k].K));
+            fftgSmem = (3 * (size_t) FFT_MAXK + 2 * (size_t) fftgBuf) * (mixed() ? 8 : 16);
+            fftgKc = sysK[0][0];
+            for (int k = 0; k < nsys; k++)
+                for (int a = 0; a < 3; a++)
+                    fftgKc = sysK[k][a] == fftgKc ? fftgKc : 0;
+            if (fftgKc != 32 && fftgKc != 40 && fftgKc != 48 && fftgKc != 64)
+                fftgKc = 0;
         }
         if (clusterOk) {
             const size_t csz = mixed() ? 8 : 16;
@@ -579,7 +599,7 @@ struct Engine::Impl {
             fftcSmem = mb.second;
             clusterOk = fftcSmem <= (size_t) optin;
         }
-        if (clusterOk || splitOk) {   // twiddle tables of every grid size the kernels transform
+        if (allSmall || splitOk) {   // twiddle tables of every grid size the kernels transform
             std::map<int, int> twOff;
             std::vector<double> tw;
             for (int k = 0; k < nsys; k++) {
@@ -606,10 +626,14 @@ struct Engine::Impl {
                 upload(dTwiddle, tf, st);
                 if (clusterOk)
                     clusterOk = prepareCluster<float>();
+                if (gridOk)
+                    gridOk = prepareGrid<float>();
             } else {
                 upload(dTwiddle, tw, st);
                 if (clusterOk)
                     clusterOk = prepareCluster<double>();
+                if (gridOk)
+                    gridOk = prepareGrid<double>();
             }
         }
         if (splitOk)
@@ -669,7 +693,7 @@ struct Engine::Impl {
         dListCount.ensure(n * sizeof(int));
         dSListCount.ensure(n * sizeof(int));
         dPosBuild.ensure(3 * (size_t) n * 8);
-        dFlags.ensure(16 * sizeof(int));
+        dFlags.ensure((16 + 2 * (size_t) nsys) * sizeof(int));
         dDS.ensure(n * 4 * R);
         for (Buf* b : {&dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dEpair, &dErec, &dFpair, &dFrec, &dEtot,
                        &dForces})
@@ -937,6 +961,8 @@ struct Engine::Impl {
         d.twiddle = dTwiddle.p;
         d.fftcBuf = fftcBuf;
         d.fftcC = fftcC;
+        d.fftgBuf = fftgBuf;
+        d.fftgBar = (unsigned*) (dFlags.as<int>() + 16);
         d.moduli = dModuli.as<double>();
         d.ncov = (int) covAtom.size();
         d.covAtom = dCovAtom.as<int>();
@@ -1016,6 +1042,34 @@ struct Engine::Impl {
         return clusters > 0;
     }
 
+    // The grid-transform kernel: compiled for one cubic grid size (32, 40, 48, 64), or for any grid.
+    template <typename R> static void (*fftgKernel(int kc))(Dev, int) {
+        switch (kc) {
+        case 32: return k_fft_grid<R, 32>;
+        case 40: return k_fft_grid<R, 40>;
+        case 48: return k_fft_grid<R, 48>;
+        case 64: return k_fft_grid<R, 64>;
+        default: return k_fft_grid<R, 0>;
+        }
+    }
+
+    // Attributes of the grid-transform kernel; false when its blocks (a block per x-plane of every system) cannot
+    // all be resident at once on this GPU or a block's shared memory does not fit.
+    template <typename R> bool prepareGrid() {
+        int optin = 0, sms = 0, coop = 0;
+        CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, devId));
+        CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, devId));
+        CU(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, devId));
+        if (!coop || fftgSmem > (size_t) optin)
+            return false;
+        CU(cudaFuncSetAttribute((const void*) fftgKernel<R>(fftgKc), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int) fftgSmem));
+        int perSm = 0;
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fftgKernel<R>(fftgKc), FftgThreads<R>::n,
+                                                         fftgSmem));
+        return (long long) perSm * sms >= (long long) maxK0 * nsys;
+    }
+
     // The transform pair with the influence product of a field pass: one cluster kernel (all systems), or
     // cuFFT plans and the product kernel.  The FP64 shadow of a mixed engine takes the cuFFT path.
     // The transform mode in use: the caller's choice where the systems' grids allow it, else cuFFT.
@@ -1025,6 +1079,8 @@ struct Engine::Impl {
             m = TF_CLUSTER;
         if (tfWant == TF_SPLIT && splitOk)
             m = TF_SPLIT;
+        if (tfWant == TF_GRID && gridOk)
+            m = TF_GRID;
         if (m != tfMode && exec) {
             cudaGraphExecDestroy(exec);
             exec = nullptr;
@@ -1067,6 +1123,20 @@ struct Engine::Impl {
         }
         if (tfMode == TF_SPLIT) {
             splitChain<R>(sm, d, gate);
+            return;
+        }
+        if (tfMode == TF_GRID) {   // cooperative: the blocks of a system meet at two barriers
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeCooperative;
+            at[0].val.cooperative = 1;
+            cfg.gridDim = dim3(maxK0, nsys);
+            cfg.blockDim = dim3(FftgThreads<R>::n);
+            cfg.dynamicSmemBytes = fftgSmem;
+            cfg.stream = sm;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            CU(cudaLaunchKernelEx(&cfg, fftgKernel<R>(fftgKc), d, gate ? 1 : 0));
             return;
         }
         cudaLaunchConfig_t cfg = {};
@@ -1163,6 +1233,20 @@ struct Engine::Impl {
     void enqueueListStep(cudaStream_t sm, const Dev& d) {
         const int tb = (n + 255) / 256;
         k_prep<<<tb, 256, 0, sm>>>(d, dPosIn.as<double>(), 1);
+        if (s.skin <= 0) {   // no skin: a build at every evaluation, without the stale test or a conditional node
+            CU(cudaMemsetAsync(d.cellCount, 0, (size_t) totalCells * sizeof(int), sm));
+            enqueueBuild(sm, d);
+        } else {
+            enqueueStaleBuild(sm, d);
+        }
+        k_refresh_positions<<<tb, 256, 0, sm>>>(d);
+        CU(cudaGetLastError());
+    }
+
+    // The stale test and the build when stale (a conditional node of the graph, its body captured after the main
+    // capture; without graphs a host decision).
+    void enqueueStaleBuild(cudaStream_t sm, const Dev& d) {
+        const int tb = (n + 255) / 256;
         k_displace<<<tb, 256, 0, sm>>>(d);
         CU(cudaGetLastError());
         if (capturing) {
@@ -1186,13 +1270,11 @@ struct Engine::Impl {
             if (hFlags[6])
                 enqueueBuild(sm, d);
         }
-        k_refresh_positions<<<tb, 256, 0, sm>>>(d);
-        CU(cudaGetLastError());
     }
 
     template <typename R> void enqueuePre(cudaStream_t sm, cudaStream_t sd, const Dev& d) {
         const int tb = (n + 255) / 256;
-        CU(cudaMemsetAsync(d.flags, 0, 16 * sizeof(int), sm));
+        CU(cudaMemsetAsync(d.flags, 0, flagBytes(), sm));
         enqueueListStep(sm, d);
         if (s.polarizable) {
             // the pairs within the cutoff and their G1, G2 (side stream) beside the permanent field's PME half
@@ -1274,7 +1356,8 @@ struct Engine::Impl {
         cudaGraphConditionalHandle handle = 0, listHandle = 0;
         if (s.polarizable)
             CU(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
-        CU(cudaGraphConditionalHandleCreate(&listHandle, graph, 0, cudaGraphCondAssignDefault));
+        if (s.skin > 0)   // (a handle without its conditional node makes the instantiation fail)
+            CU(cudaGraphConditionalHandleCreate(&listHandle, graph, 0, cudaGraphCondAssignDefault));
         const Dev d = makeDev(true, handle, listHandle);
         CU(cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
         cudaGraph_t body = nullptr;
@@ -1310,7 +1393,7 @@ struct Engine::Impl {
         }
         capturing = false;
         CU(cudaStreamEndCapture(st, &graph));
-        {
+        if (listBody) {   // (no skin: the build is part of the main graph)
             CU(cudaStreamBeginCaptureToGraph(st, listBody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
             try {
                 enqueueBuild(st, d);
@@ -1410,7 +1493,7 @@ struct Engine::Impl {
             hCtl->customRhs = 1;
             hCtl->guess = 1;
             CU(cudaMemcpyAsync(dCtl.p, hCtl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
-            CU(cudaMemsetAsync(d.flags, 0, 16 * sizeof(int), st));
+            CU(cudaMemsetAsync(d.flags, 0, flagBytes(), st));
             k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, st>>>(d);
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), st));
             fieldPass<float, false>(st, side, d, 1, d.x, false);
@@ -1506,12 +1589,24 @@ struct Engine::Impl {
         launched = true;
     }
 
+    // The flags and the grid transforms' barrier words (cleared together at the start of every call).
+    size_t flagBytes() const { return (16 + 2 * (size_t) nsys) * sizeof(int); }
+
+    // After the flags came back: a grid-transform barrier that gave up leaves the evaluation's results
+    // undefined (the barrier words are reset at the next evaluation's start).
+    void barrierCheck() const {
+        if (hFlags[11])
+            throw std::runtime_error("pgm_b200: a grid-transform barrier gave up waiting (blocks not resident "
+                                     "together?)");
+    }
+
     // Waits for the launched evaluation; false if it must be repeated (pair-list capacity grown).
     bool finish() {
         CU(cudaEventSynchronize(evDone));
         launched = false;
         if (hFlags[1])
             throw std::runtime_error("pgm_b200: pair image shift beyond 3 boxes (positions far outside the box?)");
+        barrierCheck();
         lastBuilt = hFlags[8] != 0;
         if (hFlags[8]) {
             builds++;
@@ -1775,7 +1870,7 @@ void Engine::field(const double* pos, const double box[3][3], const double* qf, 
         const Dev dv = I.makeDev(false, 0);
         const int tb = (I.n + 255) / 256;
         CU(cudaMemsetAsync(dv.cellCount, 0, (size_t) I.totalCells * sizeof(int), I.st));
-        CU(cudaMemsetAsync(dv.flags, 0, 16 * sizeof(int), I.st));
+        CU(cudaMemsetAsync(dv.flags, 0, I.flagBytes(), I.st));
         I.listValid = false;   // the list below is this call's
         k_prep<<<tb, 256, 0, I.st>>>(dv, I.dPosIn.as<double>(), 3);
         k_cell_scan<<<1, 1024, 0, I.st>>>(dv);
@@ -1803,6 +1898,7 @@ void Engine::field(const double* pos, const double box[3][3], const double* qf, 
         CU(cudaMemcpyAsync(I.hFlags, I.dFlags.p, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
         CU(cudaMemcpyAsync(I.dQ.p, I.q.data(), (size_t) I.n * 8, cudaMemcpyHostToDevice, I.st));
         CU(cudaStreamSynchronize(I.st));
+        I.barrierCheck();
         if (I.hFlags[0] > I.cap) {
             I.cap = (I.hFlags[0] + I.hFlags[0] / 4 + 31) / 32 * 32;
             I.allocList();
@@ -1899,7 +1995,7 @@ Terms Engine::evaluateFixed(const double* pos, const double box[3][3], const dou
         CU(cudaMemcpyAsync(I.dMu.p, mu, 3 * (size_t) I.n * 8, cudaMemcpyHostToDevice, I.st));
         const Dev d = I.makeDev(false, 0);
         const int tb = (I.n + 255) / 256;
-        CU(cudaMemsetAsync(d.flags, 0, 16 * sizeof(int), I.st));
+        CU(cudaMemsetAsync(d.flags, 0, I.flagBytes(), I.st));
         auto body = [&](auto tag) {
             typedef decltype(tag) R;
             if (keepList) {
@@ -1932,6 +2028,7 @@ Terms Engine::evaluateFixed(const double* pos, const double box[3][3], const dou
         if (field)
             CU(cudaMemcpyAsync(field, I.dEtot.p, 3 * (size_t) I.n * 8, cudaMemcpyDeviceToHost, I.st));
         CU(cudaStreamSynchronize(I.st));
+        I.barrierCheck();
         if (I.hFlags[0] > I.cap) {
             if (keepList)
                 throw std::logic_error("pgm_b200: list overflow with keepList");
@@ -1967,7 +2064,7 @@ int Engine::solve(const double* rhs, double* x, double tol) {
     d.tol = tol;
     auto run = [&](auto tag) {
         typedef decltype(tag) R;
-        CU(cudaMemsetAsync(d.flags, 0, 16 * sizeof(int), I.st));
+        CU(cudaMemsetAsync(d.flags, 0, I.flagBytes(), I.st));
         k_cg_b<<<(int) I.chunkSys.size(), CHUNK, 0, I.st>>>(d);
         CU(cudaMemsetAsync(d.grid, 0, I.gridTotal * I.realSize(), I.st));
         I.fieldPass<R, false>(I.st, I.side, d, 1, d.x, false);
@@ -1976,6 +2073,7 @@ int Engine::solve(const double* rhs, double* x, double tol) {
         for (int it = 0; it <= I.s.maxIter + 1; it++) {
             CU(cudaMemcpyAsync(I.hFlags, d.flags, 16 * sizeof(int), cudaMemcpyDeviceToHost, I.st));
             CU(cudaStreamSynchronize(I.st));
+            I.barrierCheck();
             if (I.hFlags[2] >= I.nsys)
                 break;
             I.enqueueIteration<R>(I.st, I.side, d);
@@ -2076,9 +2174,9 @@ void Engine::setPairLanes(int lanes) {
 int Engine::pairLanes() const { return impl->pairGS; }
 
 void Engine::setTransforms(int mode) {
-    if (mode < 0 || mode > 2)
-        throw std::invalid_argument("pgm_b200: transforms must be 0 (cuFFT), 1 (cluster kernel) or 2 (2D cuFFT + "
-                                    "x-line kernel)");
+    if (mode < 0 || mode > 3)
+        throw std::invalid_argument("pgm_b200: transforms must be 0 (cuFFT), 1 (cluster kernel), 2 (2D cuFFT + "
+                                    "x-line kernel) or 3 (grid kernel)");
     impl->tfWant = mode;
     impl->selectTransforms();
 }

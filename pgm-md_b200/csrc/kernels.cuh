@@ -953,42 +953,49 @@ __device__ __forceinline__ void smallDft(R* xr, R* xi) {
 // exact quotient.
 __device__ __forceinline__ int fdiv(int e, float invK) { return __float2int_rz(((float) e + 0.5f) * invK); }
 
-// One Stockham pass of radix RAD over nlines lines of length N (line stride ls): butterfly j of a line reads
-// in[j + r N/RAD], twiddles by W^(r (j mod Ns) N / (Ns RAD)), and writes out[(j / Ns) Ns RAD + j mod Ns + r Ns],
-// Ns the product of the earlier radices.
+// Butterfly j of a Stockham pass of radix RAD (src = in + line start + j, dst = out + line start + (j / Ns) Ns RAD
+// + j mod Ns): reads src[r nb], twiddles by W^(r tws) (tws = (j mod Ns) N / (Ns RAD)), writes dst[r Ns].
+template <typename R, int RAD, int DIR>
+__device__ __forceinline__ void stockhamButterfly(const typename CplxT<R>::T* src, typename CplxT<R>::T* dst, int nb,
+                                                  int Ns, int tws, const typename CplxT<R>::T* tw) {
+    typedef typename CplxT<R>::T C;
+    R xr[RAD], xi[RAD];
+    C v[RAD];
+#pragma unroll
+    for (int r = 0; r < RAD; r++)
+        v[r] = src[r * nb];
+    xr[0] = v[0].x;
+    xi[0] = v[0].y;
+#pragma unroll
+    for (int r = 1; r < RAD; r++) {
+        const C w = tw[tws * r];
+        const R wy = DIR < 0 ? w.y : -w.y;
+        xr[r] = v[r].x * w.x - v[r].y * wy;
+        xi[r] = v[r].x * wy + v[r].y * w.x;
+    }
+    smallDft<R, RAD, DIR>(xr, xi);
+#pragma unroll
+    for (int r = 0; r < RAD; r++) {
+        C o;
+        o.x = xr[r];
+        o.y = xi[r];
+        dst[r * Ns] = o;
+    }
+}
+
+// One Stockham pass of radix RAD over nlines lines of length N (line stride ls), Ns the product of the earlier
+// radices and n = N / Ns the length still to transform: butterfly j of a line reads in[j + r N/RAD], twiddles by
+// W^(r (j mod Ns) N / (Ns RAD)), and writes out[(j / Ns) Ns RAD + j mod Ns + r Ns].
 template <typename R, int RAD, int DIR>
 __device__ __forceinline__ void stockhamPass(const typename CplxT<R>::T* in, typename CplxT<R>::T* out, int nlines,
-                                             int N, int ls, int Ns, const typename CplxT<R>::T* tw) {
-    typedef typename CplxT<R>::T C;
-    const int nb = N / RAD, step = N / (Ns * RAD);
-    const float invNb = 1.0f / (float) nb, invNs = 1.0f / (float) Ns;
+                                             int N, int ls, int Ns, int n, const typename CplxT<R>::T* tw) {
+    const int nb = N / RAD, step = n / RAD;
+    const float invNb = __frcp_rn((float) nb), invNs = __frcp_rn((float) Ns);
     for (int t = threadIdx.x; t < nlines * nb; t += blockDim.x) {
         const int line = fdiv(t, invNb), j = t - line * nb;
         const int q = fdiv(j, invNs), jn = j - q * Ns;
-        const C* src = in + line * ls + j;
-        R xr[RAD], xi[RAD];
-        C v[RAD];
-#pragma unroll
-        for (int r = 0; r < RAD; r++)
-            v[r] = src[r * nb];
-        xr[0] = v[0].x;
-        xi[0] = v[0].y;
-#pragma unroll
-        for (int r = 1; r < RAD; r++) {
-            const C w = tw[jn * r * step];
-            const R wy = DIR < 0 ? w.y : -w.y;
-            xr[r] = v[r].x * w.x - v[r].y * wy;
-            xi[r] = v[r].x * wy + v[r].y * w.x;
-        }
-        smallDft<R, RAD, DIR>(xr, xi);
-        C* dst = out + line * ls + q * Ns * RAD + jn;
-#pragma unroll
-        for (int r = 0; r < RAD; r++) {
-            C o;
-            o.x = xr[r];
-            o.y = xi[r];
-            dst[r * Ns] = o;
-        }
+        stockhamButterfly<R, RAD, DIR>(in + line * ls + j, out + line * ls + q * Ns * RAD + jn, nb, Ns, jn * step,
+                                       tw);
     }
 }
 
@@ -1001,21 +1008,63 @@ __device__ typename CplxT<R>::T* fftLines(typename CplxT<R>::T* a, typename Cplx
     typedef typename CplxT<R>::T C;
     int n = N, Ns = 1;
     while (n > 1) {
-        const int rad = (n % 4 == 0) ? 4 : (n % 2 == 0) ? 2 : (n % 3 == 0) ? 3 : 5;
-        switch (rad) {
-        case 4: stockhamPass<R, 4, DIR>(a, b, nlines, N, ls, Ns, tw); break;
-        case 2: stockhamPass<R, 2, DIR>(a, b, nlines, N, ls, Ns, tw); break;
-        case 3: stockhamPass<R, 3, DIR>(a, b, nlines, N, ls, Ns, tw); break;
-        default: stockhamPass<R, 5, DIR>(a, b, nlines, N, ls, Ns, tw);
+        if (n % 4 == 0) {
+            stockhamPass<R, 4, DIR>(a, b, nlines, N, ls, Ns, n, tw);
+            Ns *= 4;
+            n /= 4;
+        } else if (n % 2 == 0) {
+            stockhamPass<R, 2, DIR>(a, b, nlines, N, ls, Ns, n, tw);
+            Ns *= 2;
+            n /= 2;
+        } else if (n % 3 == 0) {
+            stockhamPass<R, 3, DIR>(a, b, nlines, N, ls, Ns, n, tw);
+            Ns *= 3;
+            n /= 3;
+        } else {
+            stockhamPass<R, 5, DIR>(a, b, nlines, N, ls, Ns, n, tw);
+            Ns *= 5;
+            n /= 5;
         }
         __syncthreads();
         C* t = a;
         a = b;
         b = t;
-        Ns *= rad;
-        n /= rad;
     }
     return a;
+}
+
+// The same passes for a compile-time length N: the radix sequence, strides and twiddle steps are constants and
+// the index divisions become multiplications.  NREM: the length still to transform, NS the earlier radices.
+template <typename R, int DIR, int N, int NREM, int NS>
+struct FftPassesC {
+    typedef typename CplxT<R>::T C;
+    static __device__ __forceinline__ C* run(C* a, C* b, int nlines, int ls, const C* tw) {
+        constexpr int RAD = NREM % 4 == 0 ? 4 : NREM % 2 == 0 ? 2 : NREM % 3 == 0 ? 3 : 5;
+        constexpr int nb = N / RAD, step = NREM / RAD;
+        for (int t = threadIdx.x; t < nlines * nb; t += blockDim.x) {
+            const int line = t / nb, j = t - line * nb;
+            const int q = j / NS, jn = j - q * NS;
+            stockhamButterfly<R, RAD, DIR>(a + line * ls + j, b + line * ls + q * NS * RAD + jn, nb, NS, jn * step,
+                                           tw);
+        }
+        __syncthreads();
+        return FftPassesC<R, DIR, N, NREM / RAD, NS * RAD>::run(b, a, nlines, ls, tw);
+    }
+};
+template <typename R, int DIR, int N, int NS>
+struct FftPassesC<R, DIR, N, 1, NS> {
+    typedef typename CplxT<R>::T C;
+    static __device__ __forceinline__ C* run(C* a, C*, int, int, const C*) { return a; }
+};
+
+// Line transforms of length N (the compile-time passes when KC > 0, which then equals N).
+template <typename R, int DIR, int KC>
+__device__ __forceinline__ typename CplxT<R>::T* fftLinesK(typename CplxT<R>::T* a, typename CplxT<R>::T* b,
+                                                           int nlines, int N, int ls, const typename CplxT<R>::T* tw) {
+    if constexpr (KC > 0)
+        return FftPassesC<R, DIR, KC, KC, 1>::run(a, b, nlines, ls, tw);
+    else
+        return fftLines<R, DIR>(a, b, nlines, N, ls, tw);
 }
 
 // Complex elements of each of the three transform buffers of a block of a cluster of C blocks for grid K (max
@@ -1214,6 +1263,206 @@ __global__ void __launch_bounds__(XL_THREADS) k_xlines(Dev dv, int gateDone) {
         const int x = e / XL_LINES, l = e % XL_LINES;
         if (l < nl)
             spec[(size_t) x * nline + l] = G[l * lx + x];
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ grid transforms
+
+// The transform pair with the influence product of a field pass as ONE cooperative kernel: block x of system s
+// (blockIdx.y; K0 blocks per system) owns x-plane x and, between two barriers of the system's blocks, a run of
+// the x-lines:
+//   1. plane x: its real rows two at a time as one complex row (x + i y), forward along z (real to half
+//      spectrum, separated by Hermitian symmetry) and along y in shared memory, stored to the spectrum
+//      F[(x K1 + ky) (K2/2 + 1) + kz];
+//   2. (barrier) lines l = ky (K2/2 + 1) + kz in [x lpb, x lpb + lpb): forward along x, the influence product,
+//      back along x, in place in the spectrum;
+//   3. (barrier) plane x back along y and z (imaginary parts at kz = 0 and the Nyquist index dropped, as a C2R
+//      transform does) into the real grid.
+// The same Stockham line transforms as the cluster kernel, with the exchange through L2 instead of distributed
+// shared memory, so a 48^3 grid spreads over 48 SMs.  Loads of what other blocks wrote bypass L1 (__ldcg).
+// Each barrier waits at most FFTG_SPIN_LIMIT polls; a block that gives up sets flags[11] and returns, and the
+// host reports the evaluation as failed.
+// Threads per block: 512 in float (64 registers, 2 blocks per SM), 256 in double (84 registers, 3 per SM).
+template <typename R> struct FftgThreads { static constexpr int n = 256; };
+template <> struct FftgThreads<float> { static constexpr int n = 512; };
+constexpr unsigned FFTG_SPIN_LIMIT = 1u << 22;   // polls of an L2 word (a few hundred ns each): about 1 s
+
+// Complex elements of each of the two transform buffers of a block for grid K (max of its plane rows, its
+// y-lines and its x-lines).
+__host__ __device__ inline int fftgBufferElems(const int* K) {
+    const int K2h = K[2] / 2 + 1, P = (K[1] + 1) / 2, ly = K[1] + 1, lx = K[0] + 1;
+    const int lpb = (K[1] * K2h + K[0] - 1) / K[0];
+    int m = P * K[2];
+    m = m > K2h * ly ? m : K2h * ly;
+    m = m > lpb * lx ? m : lpb * lx;
+    return (m + 1) / 2 * 2;   // 16-byte multiples
+}
+
+__device__ __forceinline__ unsigned ldAcquireGpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Barrier of nb blocks over an arrival counter that only grows between resets (the flags and barrier words are
+// cleared at the start of every call): the blocks of barrier k arrive as numbers k nb .. k nb + nb - 1 and leave
+// once the counter has reached (k + 1) nb.  The wait is bounded: false, with flags[11] set, when it gave up.
+__device__ __forceinline__ bool fftgBarrier(unsigned* bar, unsigned nb, int* flags) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        __threadfence();
+        const unsigned old = atomicAdd(bar, 1u);
+        const unsigned target = (old / nb + 1) * nb;
+        if (old + 1 != target)
+            for (unsigned it = 0; (int) (ldAcquireGpu(bar) - target) < 0; it++)
+                if (it >= FFTG_SPIN_LIMIT) {
+                    ok = 0;
+                    atomicExch(flags + 11, 1);
+                    break;
+                }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// KC > 0: every grid of the launch is KC^3 (compile-time passes and index maps); 0: any grid.
+template <typename R, int KC>
+__global__ void __launch_bounds__(FftgThreads<R>::n) k_fft_grid(Dev dv, int gateDone) {
+    typedef typename CplxT<R>::T C;
+    const int s = blockIdx.y;
+    if (gateDone && dv.scal[s * NSCAL + SC_DONE] != 0.0)
+        return;   // every block of the system
+    const SysDev& S = dv.sys[s];
+    const int K0 = KC > 0 ? KC : S.K[0], K1 = KC > 0 ? KC : S.K[1], K2 = KC > 0 ? KC : S.K[2];
+    const int K2h = K2 / 2 + 1, P = (K1 + 1) / 2, ly = K1 + 1, lx = K0 + 1;
+    const int x = blockIdx.x;
+    if (x >= K0)
+        return;   // (a smaller grid than the launch's largest)
+    const int nline = K1 * K2h, lpb = (nline + K0 - 1) / K0, l0 = x * lpb;
+    const int nl = max(0, min(nline, l0 + lpb) - l0);
+    const int nT = blockDim.x, tid = threadIdx.x;
+    const float iK2 = __frcp_rn((float) K2), iK2h = __frcp_rn((float) K2h), iLpb = __frcp_rn((float) lpb);
+    // e / d: by a constant when the grid is one (the compiler multiplies), else through the float reciprocal
+    auto qd = [](int e, int d, float inv) { return KC > 0 ? e / d : fdiv(e, inv); };
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* W0 = (C*) smraw;
+    C* W1 = W0 + FFT_MAXK;
+    C* W2 = W1 + FFT_MAXK;
+    C* const b0 = W2 + FFT_MAXK;
+    C* const b1 = b0 + dv.fftgBuf;
+    const C* tw = (const C*) dv.twiddle;
+    for (int m = tid; m < K0; m += nT)
+        W0[m] = tw[S.twOff[0] + m];
+    for (int m = tid; m < K1; m += nT)
+        W1[m] = tw[S.twOff[1] + m];
+    for (int m = tid; m < K2; m += nT)
+        W2[m] = tw[S.twOff[2] + m];
+    R* const gx = (R*) dv.grid + S.gridOff + (size_t) x * K1 * K2;
+    C* const spec = (C*) dv.spec + S.specOff;
+    C* const plane = spec + (size_t) x * nline;
+    unsigned* const bar = dv.fftgBar + 2 * s;
+    // 1. plane x: rows 2p, 2p + 1 as one complex row [pair][z]; z; separation into y-lines [kz][y]; y
+    for (int e = tid; e < P * K2; e += nT) {
+        const int pr = qd(e, K2, iK2), z = e - pr * K2;
+        C v;
+        v.x = gx[2 * pr * K2 + z];
+        v.y = (2 * pr + 1 < K1) ? gx[(2 * pr + 1) * K2 + z] : (R) 0;
+        b0[e] = v;
+    }
+    __syncthreads();
+    C* Z = fftLinesK<R, -1, KC>(b0, b1, P, K2, K2, W2);
+    C* O = (Z == b0) ? b1 : b0;
+    for (int e = tid; e < P * K2h; e += nT) {
+        const int pr = qd(e, K2h, iK2h), kz = e - pr * K2h;
+        const C* zr = Z + pr * K2;
+        const C zk = zr[kz], zm = zr[kz == 0 ? 0 : K2 - kz];
+        C X, Y;   // X = (Z_k + conj Z_-k) / 2, Y = (Z_k - conj Z_-k) / 2i
+        X.x = (R) 0.5 * (zk.x + zm.x);
+        X.y = (R) 0.5 * (zk.y - zm.y);
+        Y.x = (R) 0.5 * (zk.y + zm.y);
+        Y.y = (R) 0.5 * (zm.x - zk.x);
+        C* o = O + kz * ly + 2 * pr;
+        o[0] = X;
+        if (2 * pr + 1 < K1)
+            o[1] = Y;
+    }
+    __syncthreads();
+    const C* F = fftLinesK<R, -1, KC>(O, Z, K2h, K1, ly, W1);
+    for (int e = tid; e < nline; e += nT) {
+        const int ky = qd(e, K2h, iK2h), kz = e - ky * K2h;
+        plane[e] = F[kz * ly + ky];
+    }
+    if (!fftgBarrier(bar, (unsigned) K0, dv.flags))
+        return;
+    // 2. my x-lines: forward along x, influence product, back
+    for (int e = tid; e < lpb * K0; e += nT) {   // consecutive threads: consecutive lines of a plane
+        const int xx = qd(e, lpb, iLpb), li = e - xx * lpb;
+        if (li < nl)
+            b0[li * lx + xx] = __ldcg(spec + (size_t) xx * nline + l0 + li);
+    }
+    __syncthreads();
+    C* Fx = fftLinesK<R, -1, KC>(b0, b1, nl, K0, lx, W0);
+    const R* infl = (const R*) dv.infl + S.specOff;
+    for (int e = tid; e < lpb * K0; e += nT) {
+        const int xx = qd(e, lpb, iLpb), li = e - xx * lpb;
+        if (li < nl) {
+            const R gk = infl[(size_t) xx * nline + l0 + li];
+            C& v = Fx[li * lx + xx];
+            v.x *= gk;
+            v.y *= gk;
+        }
+    }
+    __syncthreads();
+    const C* Gx = fftLinesK<R, 1, KC>(Fx, Fx == b0 ? b1 : b0, nl, K0, lx, W0);
+    for (int e = tid; e < lpb * K0; e += nT) {
+        const int xx = qd(e, lpb, iLpb), li = e - xx * lpb;
+        if (li < nl)
+            spec[(size_t) xx * nline + l0 + li] = Gx[li * lx + xx];
+    }
+    if (!fftgBarrier(bar, (unsigned) K0, dv.flags))
+        return;
+    // 3. plane x back: y-lines [kz][y]; y; two real rows from one complex row; z
+    for (int e = tid; e < nline; e += nT) {
+        const int ky = qd(e, K2h, iK2h), kz = e - ky * K2h;
+        b0[kz * ly + ky] = __ldcg(plane + e);
+    }
+    __syncthreads();
+    C* Gy = fftLinesK<R, 1, KC>(b0, b1, K2h, K1, ly, W1);
+    C* O2 = (Gy == b0) ? b1 : b0;
+    for (int e = tid; e < P * K2; e += nT) {
+        const int pr = qd(e, K2, iK2), k = e - pr * K2;
+        const bool upper = k >= K2h;
+        const int kk = upper ? K2 - k : k;
+        const bool realOnly = (k == 0) || ((K2 & 1) == 0 && k == K2 / 2);
+        const C* gy = Gy + kk * ly + 2 * pr;
+        C X = gy[0], Y;
+        Y.x = 0;
+        Y.y = 0;
+        if (2 * pr + 1 < K1)
+            Y = gy[1];
+        if (upper) {
+            X.y = -X.y;
+            Y.y = -Y.y;
+        }
+        if (realOnly) {
+            X.y = 0;
+            Y.y = 0;
+        }
+        C Zv;   // X + i Y
+        Zv.x = X.x - Y.y;
+        Zv.y = X.y + Y.x;
+        O2[e] = Zv;
+    }
+    __syncthreads();
+    const C* Zt = fftLinesK<R, 1, KC>(O2, Gy, P, K2, K2, W2);
+    for (int e = tid; e < P * K2; e += nT) {
+        const int pr = qd(e, K2, iK2), z = e - pr * K2;
+        gx[2 * pr * K2 + z] = Zt[e].x;
+        if (2 * pr + 1 < K1)
+            gx[(2 * pr + 1) * K2 + z] = Zt[e].y;
     }
 }
 
@@ -1448,17 +1697,12 @@ __global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
         if (!isLast)
             return;
         __threadfence();
-        __shared__ double tsum[256];
-        double acc = 0.0;
+        double acc[1] = {0.0};   // thread t: blocks t, t + 256, ... in order; then the fixed block tree
         for (int b = threadIdx.x; b < (int) gridDim.x; b += blockDim.x)
-            acc += __ldcg(&dv.gpartial[b]);
-        tsum[threadIdx.x] = acc;
-        __syncthreads();
+            acc[0] += __ldcg(&dv.gpartial[b]);
+        blockReduce<1>(acc, 0u);
         if (threadIdx.x == 0) {
-            double tot = 0.0;
-            for (int t = 0; t < (int) blockDim.x; t++)
-                tot += tsum[t];
-            sc[SC_ALPH] = sc[SC_RZ] / fmax(tot, 1e-300);
+            sc[SC_ALPH] = sc[SC_RZ] / fmax(acc[0], 1e-300);
             dv.flags[10] = 0;
         }
     }
@@ -1835,6 +2079,11 @@ __global__ void __launch_bounds__(CHUNK) k_cg_upd(Dev dv) {
         if (!more) {
             sc[SC_DONE] = 1.0;
             atomicAdd(&dv.flags[2], 1);
+        }
+        if (dv.nSys == 1) {   // the only system decides alone
+            if (dv.useCond)
+                cudaGraphSetConditional(dv.cond, more ? 1u : 0u);
+            return;
         }
         __threadfence();
         // the last active system of this iteration to finish decides whether the loop goes on (the count of

@@ -85,8 +85,8 @@ public:
     void kernelTimes(int reps, double* ms);
     void setPairLanes(int lanes);
     // field-pass transforms: 0 cuFFT 3D plans + influence product kernel, 1 one cluster kernel per launch,
-    // 2 cuFFT 2D plans over the x-planes + one x-line kernel with the influence product (1 and 2 where the grids
-    // allow them; transforms() tells which runs)
+    // 2 cuFFT 2D plans over the x-planes + one x-line kernel with the influence product, 3 one cooperative kernel
+    // with a block per x-plane (1, 2 and 3 where the grids allow them; transforms() tells which runs)
     void setTransforms(int mode);
     int transforms() const;
     int pairLanes() const;

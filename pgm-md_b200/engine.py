@@ -322,7 +322,8 @@ class Engine:
 
     def set_transforms(self, mode):
         """Field-pass transforms: 0 cuFFT 3D plans + influence product, 1 one cluster kernel per pass, 2 cuFFT 2D
-        plans over the x-planes + one x-line kernel with the influence product."""
+        plans over the x-planes + one x-line kernel with the influence product, 3 one cooperative kernel with a
+        block per x-plane."""
         _check(self._L.pgm_engine_set_transforms(self._h, int(mode)))
 
     def transforms(self):
@@ -343,7 +344,7 @@ class Engine:
                 best, best_t = lanes, t
         self.set_pair_lanes(best)
         ft = {}
-        for mode in (0, 1, 2):   # whole evaluations (the transforms run beside the pair passes), fastest call
+        for mode in (0, 1, 2, 3):   # whole evaluations (the transforms run beside the pair passes), fastest call
             self.set_transforms(mode)
             if self.transforms() != mode:
                 continue

@@ -1,9 +1,11 @@
 """The field passes' transforms by the cluster kernel (a thread-block cluster per system holding its half
-spectrum in distributed shared memory) and by the split path (cuFFT 2D plans over the x-planes, one kernel for
-the x-lines with the influence product) against the cuFFT 3D plans + influence product path: the same energies
-and forces (FP64 within 1e-12 relative, mixed within 1e-6 in energy and 1e-5 relative RMS in forces), for one
-system (16 blocks per cluster) and a batch of many small systems (smaller clusters); grids with a prime factor
-above 5 or beyond 64 points stay on cuFFT."""
+spectrum in distributed shared memory), by the split path (cuFFT 2D plans over the x-planes, one kernel for
+the x-lines with the influence product) and by the grid kernel (one cooperative kernel, a block per x-plane,
+planes and x-lines exchanged through L2 between two barriers) against the cuFFT 3D plans + influence product
+path: the same energies and forces (FP64 within 1e-12 relative, mixed within 1e-6 in energy and 1e-5 relative
+RMS in forces), for one system (16 blocks per cluster) and a batch of small systems (smaller clusters; grid
+kernel blocks of several grid shapes in one launch); grids with a prime factor above 5 or beyond 64 points
+stay on cuFFT."""
 
 import numpy as np
 import pytest
@@ -22,7 +24,7 @@ def settings(S, precision):
                         predictor=0, ke=PKG.systems.KE_DEFAULT, precision=precision)
 
 
-@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("mode", [1, 2, 3])
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("name", ["water216", "tiny_triclinic"])
 def test_transforms_single_system(precision, mode, name):
@@ -43,7 +45,7 @@ def test_transforms_single_system(precision, mode, name):
     assert a.iterations == b.iterations or precision == 1
 
 
-@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("mode", [1, 2, 3])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_transforms_batch(precision, mode):
     systems = []
@@ -71,15 +73,16 @@ def test_transforms_need_small_235_grids():
     S = PKG.systems.waters(64, 12.4, seed=3, grid=(14, 14, 14), cutoff=6.0, tol=1e-6)   # 14 = 2 * 7
     eng = PKG.Engine(settings(S, PKG.FP64))
     eng.set_system(S)
-    for mode in (1, 2):
+    for mode in (1, 2, 3):
         eng.set_transforms(mode)
         assert eng.transforms() == 0
     assert np.isfinite(eng.compute(S.pos, S.box).energy)
     S2 = PKG.systems.waters(64, 12.4, seed=3, grid=(12, 14, 14), cutoff=6.0, tol=1e-6)   # x extent 12: split only
     eng2 = PKG.Engine(settings(S2, PKG.FP64))
     eng2.set_system(S2)
-    eng2.set_transforms(1)
-    assert eng2.transforms() == 0
+    for mode in (1, 3):
+        eng2.set_transforms(mode)
+        assert eng2.transforms() == 0
     eng2.set_transforms(2)
     assert eng2.transforms() == 2
     ref = PKG.Engine(settings(S2, PKG.FP64))
