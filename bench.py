@@ -90,32 +90,50 @@ class ClockSampler:
         self._stop = None
         self._thread = None
 
+    def _sample(self):
+        import pynvml
+        self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(self._h, pynvml.NVML_CLOCK_SM)))
+        try:
+            self.reasons |= int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(self._h))
+        except Exception:
+            self.reasons |= int(pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(self._h))
+
     def _run(self):
         try:
-            import pynvml
-            pynvml.nvmlInit()
-            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
-            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
-            while not self._stop.is_set():
-                self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
-                try:
-                    self.reasons |= int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))
-                except Exception:
-                    self.reasons |= int(pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h))
-                self._stop.wait(0.002)
-            pynvml.nvmlShutdown()
+            while not self._stop.wait(0.002):
+                self._sample()
         except Exception:
             pass
 
     def __enter__(self):
+        # NVML is set up before the timed region starts (it can take longer than a short region lasts); one
+        # sample as the region opens, the thread's every 2 ms, one as it closes
+        self._h = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM))
+            self._sample()
+        except Exception:
+            self._h = None
         self._stop = threading.Event()
-        self._thread = threading.Thread(target=self._run, daemon=True)
-        self._thread.start()
+        if self._h is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._thread.join(timeout=5)
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
+        if self._h is not None:
+            try:
+                import pynvml
+                self._sample()
+                pynvml.nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
         if not self.samples:
