@@ -41,3 +41,15 @@ def load_golden_system(name):
                            cutoff=float(d["cutoff"]), beta=float(d["beta"]), grid=tuple(int(g) for g in d["grid"]),
                            order=int(d["order"]))
     return S, d
+
+
+def load_dmp_real():
+    """The reference's real 8550-atom dimethylphenol liquid with pgm_core's outputs (tests/golden/dmp8550_real.npz):
+    (System, fixture).  The molecule's parameters are tiled by the generator's own function."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("pgm_b200_make_golden", GOLDEN / "make_golden.py")
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    d = np.load(GOLDEN / "dmp8550_real.npz")
+    mol = {k[4:]: d[k] for k in d.files if k.startswith("mol_")}
+    return mg.dmp_system(mol, d["pos"], d["box"], PKG.systems), d

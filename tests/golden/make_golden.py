@@ -10,6 +10,13 @@ the fixtures travel, the reference does not):
                     into oracle/_ref by oracle/Makefile) on the seeded synthetic systems: energy terms,
                     forces, strain derivative, induced and permanent dipoles, iterations, tol 1e-10,
                     predictor none, peek 0.
+  dmp8550_real.npz  the reference's real 8550-atom dimethylphenol liquid (amber/test/dmp: pGM parameters from
+                    the POL_GAUSS_* sections of prmtop.gz, coordinates and box from the NetCDF restart restrt0)
+                    with the benchmark's settings (cutoff 0.9 nm, beta 3.5 / nm, 48^3, order 6), and pgm_core's
+                    outputs on it at tol 1e-10 (predictor none, peek 0).  The 450 molecules carry identical
+                    parameters, so one molecule's 19 atoms and 38 covalent dipoles are stored (the system tiles
+                    them); coordinates, forces and dipoles as float32 (the coordinates are the inputs of both
+                    the reference run and the tests, so their rounding is part of the case).
 
     make -C oracle && python tests/golden/make_golden.py
 """
@@ -95,6 +102,69 @@ def w512():
     print("w512_pgmjax.npz", {k: np.shape(v) for k, v in out.items()})
 
 
+def dmp8550_real():
+    import gzip
+    import tempfile
+    from scipy.io import netcdf_file
+    from oracle import pgm_oracle as O
+    from oracle import ref as R
+    systems = load_systems()
+    with tempfile.NamedTemporaryFile("w", suffix=".prmtop") as t:
+        t.write(gzip.open(REF / "amber/test/dmp/prmtop.gz", "rt").read())
+        t.flush()
+        sec = read_prmtop_sections(t.name, {"POL_GAUSS_MONOPOLES_LIST", "POL_GAUSS_RADII_LIST",
+                                            "POL_GAUSS_POLARIZABILITY_LIST", "POL_GAUSS_COVALENT_POINTERS_LIST",
+                                            "POL_GAUSS_COVALENT_ATOMS_LIST", "POL_GAUSS_COVALENT_DIPOLES_LIST"})
+    nat, nmol = 19, 450
+    q, rad, alp = (sec[k] for k in ("POL_GAUSS_MONOPOLES_LIST", "POL_GAUSS_RADII_LIST",
+                                    "POL_GAUSS_POLARIZABILITY_LIST"))
+    ptr = sec["POL_GAUSS_COVALENT_POINTERS_LIST"].astype(np.int64)
+    catom = np.repeat(np.arange(len(ptr)), ptr)
+    cpart = sec["POL_GAUSS_COVALENT_ATOMS_LIST"].astype(np.int64) - 1
+    cstr = sec["POL_GAUSS_COVALENT_DIPOLES_LIST"]
+    ncov = int(ptr[:nat].sum())
+    mol = dict(q=q[:nat], radius=rad[:nat] * 0.1, alpha=alp[:nat] * 1e-3, cov_atom=catom[:ncov].astype(np.int32),
+               cov_partner=cpart[:ncov].astype(np.int32), cov_strength=cstr[:ncov] * 0.1)
+    for m in range(nmol):   # the tiling is exact
+        a = slice(nat * m, nat * m + nat)
+        c = slice(ncov * m, ncov * m + ncov)
+        assert np.array_equal(q[a], q[:nat]) and np.array_equal(rad[a], rad[:nat]) and np.array_equal(alp[a], alp[:nat])
+        assert np.array_equal(catom[c] - nat * m, catom[:ncov]) and np.array_equal(cpart[c] - nat * m, cpart[:ncov])
+        assert np.array_equal(cstr[c], cstr[:ncov])
+    nc = netcdf_file(str(REF / "amber/test/dmp/restrt0"), "r", mmap=False)
+    assert np.allclose(nc.variables["cell_angles"][:], 90.0)
+    pos = (np.array(nc.variables["coordinates"][:], dtype=np.float64) * 0.1).astype(np.float32)
+    box = np.diag(np.array(nc.variables["cell_lengths"][:], dtype=np.float64) * 0.1)
+    S = dmp_system(mol, pos, box, systems)
+    top = O.Topology(S.q, S.radius, S.alpha, S.cov_atom, S.cov_partner, S.cov_strength)
+    st = O.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=1e-10, max_iter=500, peek=0.0,
+                    predictor=0, ke=systems.KE_DEFAULT)
+    eng = R.RefEngine(top, st)
+    e = eng.compute(S.pos, S.box)
+    t = eng.terms()
+    np.savez_compressed(
+        OUT / "dmp8550_real.npz", nmol=nmol, pos=pos, box=box, cutoff=S.cutoff, beta=S.beta, grid=np.array(S.grid),
+        order=S.order, ke=systems.KE_DEFAULT, tol=1e-10, energy=e,
+        terms=np.array([t[k] for k in ("direct", "reciprocal", "self", "background", "polarization")]),
+        forces=eng.forces.astype(np.float32), strain=eng.strain(), mu=eng.induced().astype(np.float32),
+        iterations=eng.iterations(), **{"mol_" + k: v for k, v in mol.items()})
+    print("dmp8550_real.npz", S.n, "atoms", e, eng.iterations(), "iterations")
+
+
+def dmp_system(mol, pos, box, systems):
+    """The DMP liquid as a System: the molecule's parameters and covalent dipoles tiled over the molecules
+    (the same construction as tests/conftest.py's loader)."""
+    nat, ncov, nmol = len(mol["q"]), len(mol["cov_atom"]), len(pos) // len(mol["q"])
+    off = np.repeat(np.arange(nmol) * nat, ncov)
+    return systems.System(name="dmp8550_real", pos=np.asarray(pos, dtype=np.float64), box=box,
+                          q=np.tile(mol["q"], nmol), radius=np.tile(mol["radius"], nmol),
+                          alpha=np.tile(mol["alpha"], nmol),
+                          cov_atom=(np.tile(mol["cov_atom"], nmol) + off).astype(np.int32),
+                          cov_partner=(np.tile(mol["cov_partner"], nmol) + off).astype(np.int32),
+                          cov_strength=np.tile(mol["cov_strength"], nmol), cutoff=0.9, beta=3.5, grid=(48, 48, 48),
+                          order=6)
+
+
 def ref_outputs():
     from oracle import pgm_oracle as O
     from oracle import ref as R
@@ -119,5 +189,10 @@ def ref_outputs():
 
 
 if __name__ == "__main__":
-    w512()
-    ref_outputs()
+    which = sys.argv[1:] or ["w512", "ref", "dmp"]
+    if "w512" in which:
+        w512()
+    if "ref" in which:
+        ref_outputs()
+    if "dmp" in which:
+        dmp8550_real()

@@ -8,7 +8,7 @@ against the FP64 oracle at tol 1e-10, the pair set bit-exact in both.
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, PKG, load_golden_system, oracle_settings, oracle_topology
+from conftest import GOLDEN, PKG, load_dmp_real, load_golden_system, oracle_settings, oracle_topology
 from oracle import pgm_oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -98,6 +98,22 @@ def test_fp64_matches_pgmjax_goldens(level):
     assert rel_rms(r.forces, g[f"{level}_forces"]) <= 1e-6
     if "i" in level:
         assert np.abs(eng.induced_dipoles() - g[f"{level}_mu"]).max() <= 1e-6 * np.abs(g[f"{level}_mu"]).max()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_real_dmp_liquid_matches_reference(precision):
+    """The reference's real 8550-atom dimethylphenol liquid (amber/test/dmp) with the benchmark's settings against
+    pgm_core at tol 1e-10 (tests/golden/dmp8550_real.npz): FP64 within 1e-7 relative in energy and 1e-6 relative
+    RMS in forces, mixed within 1e-6 and 1e-5; induced dipoles alike."""
+    S, d = load_dmp_real()
+    eng = make_engine(S, precision)
+    r = eng.compute(S.pos, S.box)
+    e = float(d["energy"])
+    lim_e, lim_f = (1e-7, 1e-6) if precision == 0 else (1e-6, 1e-5)
+    assert abs(r.energy - e) <= lim_e * abs(e)
+    assert rel_rms(r.forces, d["forces"].astype(np.float64)) <= lim_f
+    mu = d["mu"].astype(np.float64)
+    assert np.abs(eng.induced_dipoles() - mu).max() <= 10 * lim_f * np.abs(mu).max()
 
 
 @pytest.mark.parametrize("precision", [0, 1])

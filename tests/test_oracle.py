@@ -5,7 +5,7 @@ built here) the reference library live."""
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, PKG, load_golden_system, oracle_settings, oracle_topology
+from conftest import GOLDEN, PKG, load_dmp_real, load_golden_system, oracle_settings, oracle_topology
 from oracle import pgm_oracle as O
 from oracle import ref as R
 
@@ -45,6 +45,20 @@ def test_oracle_matches_pgmjax_goldens(level):
     assert np.linalg.norm(eng.forces - F) <= 1e-12 * np.linalg.norm(F)
     assert np.abs(eng.mu - g[f"{level}_mu"]).max() <= 1e-12
     assert eng.iterations == int(g[f"{level}_iterations"])
+
+
+def test_oracle_matches_reference_on_real_dmp_liquid():
+    """The numpy oracle on the reference's real 8550-atom dimethylphenol liquid (amber/test/dmp, the system the
+    benchmark's synthetic stand-in imitates) against pgm_core's outputs at tol 1e-10: energy and iteration count;
+    forces and induced dipoles to the float32 storage of the fixture."""
+    S, d = load_dmp_real()
+    eng = O.Engine(oracle_topology(S), oracle_settings(S))
+    e = eng.compute(S.pos, S.box)
+    assert abs(e - float(d["energy"])) <= 1e-12 * abs(float(d["energy"]))
+    assert eng.iterations == int(d["iterations"])
+    F = d["forces"].astype(np.float64)
+    assert np.linalg.norm(eng.forces - F) <= 2e-7 * np.linalg.norm(F)
+    assert np.abs(eng.mu - d["mu"]).max() <= 2e-7 * np.abs(d["mu"]).max()
 
 
 def test_oracle_finite_differences():
