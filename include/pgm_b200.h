@@ -78,6 +78,13 @@ int pgm_engine_set_atoms(pgm_engine* e, int n, const double* q, const double* ra
                          const int* global_index, int num_global);
 /* pgmcuda::Engine::setCovalent (core/cuda/pgm_cuda.h:67): p_atom += strength unit(r_partner - r_atom). */
 int pgm_engine_set_covalent(pgm_engine* e, int ncov, const int* atom, const int* partner, const double* strength);
+/* pgmcuda::Engine::setCandidates (core/cuda/pgm_cuda.h:68-73): the caller's pair candidates in place of the
+ * engine's own pair search, until the next set_atoms.  Segment s holds the pairs (seg_i[s], cand_j[k]),
+ * k in [seg_begin[s], seg_begin[s+1]) (seg_begin has nseg+1 entries, seg_begin[0] = 0), with
+ * x = r_i + t.box - r_j, t = seg_shift[3s .. 3s+2] integer box vectors (|t| <= 127); every pair at most once;
+ * the pairs beyond the cutoff are left out at every evaluation.  Single-system engines. */
+int pgm_engine_set_candidates(pgm_engine* e, int nseg, const int* seg_i, const int* seg_shift, const int* seg_begin,
+                              const int* cand_j);
 
 /* pgmcuda::Engine::compute (core/cuda/pgm_cuda.h:79): positions pos (n*3, host), box (9); forces ADDED to
  * f (n*3, may be NULL), strain derivative ADDED to strain (9, may be NULL); terms (may be NULL).

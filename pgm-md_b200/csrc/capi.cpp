@@ -157,6 +157,12 @@ int pgm_engine_set_covalent(pgm_engine* e, int ncov, const int* atom, const int*
     });
 }
 
+int pgm_engine_set_candidates(pgm_engine* e, int nseg, const int* seg_i, const int* seg_shift, const int* seg_begin,
+                              const int* cand_j) {
+    NEED(e);
+    return guarded([&] { e->e->setCandidates(nseg, seg_i, seg_shift, seg_begin, cand_j); });
+}
+
 int pgm_engine_compute(pgm_engine* e, const double* pos, const double* box, int new_step, double* f, double* strain,
                        pgm_terms* terms) {
     NEED(e);

@@ -90,6 +90,13 @@ struct Dev {
     // it within the cutoff with their G1, G2
     uint32_t* slist;          // [slot][cap] Verlet list (cutoff + skin)
     int* slistCount;          // per slot
+    int* atomSlot;            // slot of each atom at the last build
+    // the caller's pair candidates (setCandidates), per atom i in both directions: partners candJ[k] and
+    // integer box shifts candT[k] (8 bits per component, offset 128) for k in [candStart[i], candStart[i + 1]),
+    // x = r_i + t.H - r_j; null: the engine's own cell search
+    const int* candStart;
+    const int* candJ;
+    const int* candT;
     double* posBuild;         // 3n positions at the list's build
     uint32_t* list;           // [slot][cap] pairs within the cutoff
     int* listCount;           // per slot

@@ -173,7 +173,7 @@ struct Engine::Impl {
         dScal, dPartial, dGPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dTwiddle, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
-        dGradQ, dGradR, dSList, dSListCount, dPosBuild;
+        dGradQ, dGradR, dSList, dSListCount, dPosBuild, dAtomSlot, dCandStart, dCandJ, dCandT;
     // FP64 shadow of the mixed path for the iterative refinement
     Buf dPairBd, dDSd, dGridD, dSpecD, dInflD, dSplD, dB64, dXsave;
     std::vector<std::pair<cufftHandle, cufftHandle>> plans64;
@@ -201,6 +201,7 @@ struct Engine::Impl {
     // Verlet list state: valid once built; kept while the boxes stay those of the build and no atom has moved by
     // more than half the skin (checked on the device at every evaluation)
     bool listValid = false;
+    bool externalList = false;   // the caller's candidates (setCandidates) in place of the cell search
     std::vector<double> buildBoxes;    // nsys * 9, the boxes of the last build
     std::vector<double> launchBoxes;   // nsys * 9, the boxes of the evaluation in flight
     cudaGraph_t listBody = nullptr;    // body of the build's conditional node while capturing
@@ -246,7 +247,8 @@ struct Engine::Impl {
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dTwiddle, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
                       &dCovByAtomOff, &dCovByAtom, &dCovByPartnerOff, &dCovByPartner, &dChunkSys, &dChunkBegin,
                       &dChunkEnd, &dHist, &dGlobal, &dCtl, &dGradQ, &dGradR, &dPairBd, &dDSd, &dGridD, &dSpecD,
-                      &dInflD, &dSplD, &dB64, &dXsave, &dSList, &dSListCount, &dPosBuild};
+                      &dInflD, &dSplD, &dB64, &dXsave, &dSList, &dSListCount, &dPosBuild, &dAtomSlot, &dCandStart,
+                      &dCandJ, &dCandT};
         for (Buf* b : all)
             b->release();
         if (hPos) cudaFreeHost(hPos);
@@ -331,6 +333,7 @@ struct Engine::Impl {
         if (nAt <= 0 || nAt >= (1 << 23))
             throw std::invalid_argument("pgm_b200: setAtoms needs 1 .. 8388607 atoms");
         const bool sameCount = atomsSet && nsys == 1 && n == nAt;
+        externalList = false;   // the candidates hold until the next setAtoms
         n = nAt;
         nsys = 1;
         atomBegin = {0, n};
@@ -370,6 +373,7 @@ struct Engine::Impl {
         if (ns <= 0)
             throw std::invalid_argument("pgm_b200: setSystems needs at least one system");
         nsys = ns;
+        externalList = false;
         atomBegin.assign(ns + 1, 0);
         for (int k = 0; k < ns; k++) {
             if (count[k] <= 0)
@@ -692,6 +696,7 @@ struct Engine::Impl {
         dRadS.ensure(n * 8);
         dListCount.ensure(n * sizeof(int));
         dSListCount.ensure(n * sizeof(int));
+        dAtomSlot.ensure(n * sizeof(int));
         dPosBuild.ensure(3 * (size_t) n * 8);
         dFlags.ensure((16 + 2 * (size_t) nsys) * sizeof(int));
         dDS.ensure(n * 4 * R);
@@ -795,7 +800,7 @@ struct Engine::Impl {
             const double skin = std::max(0.0, std::min(s.skin, 0.5 / colMax - S.cutoff));
             const double rl = S.cutoff + skin;
             S.rl2 = rl * rl;
-            S.skinHalf2 = 0.25 * skin * skin;
+            S.skinHalf2 = externalList ? 1e300 : 0.25 * skin * skin;   // (the caller's candidates: never stale)
             for (int a = 0; a < 3; a++) {
                 const double col = std::sqrt(S.recip[a] * S.recip[a] + S.recip[3 + a] * S.recip[3 + a] +
                                              S.recip[6 + a] * S.recip[6 + a]);
@@ -863,6 +868,10 @@ struct Engine::Impl {
 
     bool refining() const { return mixed() && s.refine && s.polarizable; }
 
+    // A list kept between builds and compacted to the cutoff at every evaluation: a skin, or the caller's
+    // candidates.
+    bool verletList() const { return s.skin > 0 || externalList; }
+
     // The mixed path's device pointers with the FP64 shadow buffers in place of the R-typed ones.
     Dev makeDev64() {
         Dev d = makeDev(false, 0);
@@ -920,7 +929,13 @@ struct Engine::Impl {
         d.listCount = dListCount.as<int>();
         d.slist = dSList.as<uint32_t>();
         d.slistCount = dSListCount.as<int>();
-        if (s.skin <= 0) {   // no skin: the build writes the evaluation's list itself (no compaction)
+        d.atomSlot = dAtomSlot.as<int>();
+        if (externalList) {
+            d.candStart = dCandStart.as<int>();
+            d.candJ = dCandJ.as<int>();
+            d.candT = dCandT.as<int>();
+        }
+        if (!verletList()) {   // no skin: the build writes the evaluation's list itself (no compaction)
             d.slist = d.list;
             d.slistCount = d.listCount;
         }
@@ -1209,7 +1224,7 @@ struct Engine::Impl {
     // The evaluation's pair list with its records: the Verlet list compacted to the cutoff, or, without a skin
     // (the build wrote the evaluation's list), the records of every listed pair.
     template <typename R> void pairRecords(cudaStream_t sm, const Dev& d) {
-        if (s.skin <= 0)
+        if (!verletList())
             k_pair_kernels<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
         else
             k_pair_compact<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
@@ -1223,7 +1238,10 @@ struct Engine::Impl {
         k_cell_scan<<<1, 1024, 0, sm>>>(d);
         k_cell_scatter<<<tb, 256, 0, sm>>>(d);
         k_cell_sort<<<(totalCells + 7) / 8, 256, 0, sm>>>(d);
-        k_build_list<<<totalCells, LIST_THREADS, 0, sm>>>(d);
+        if (externalList)
+            k_list_from_candidates<<<(n + 7) / 8, 256, 0, sm>>>(d);
+        else
+            k_build_list<<<totalCells, LIST_THREADS, 0, sm>>>(d);
         CU(cudaGetLastError());
     }
 
@@ -1233,7 +1251,7 @@ struct Engine::Impl {
     void enqueueListStep(cudaStream_t sm, const Dev& d) {
         const int tb = (n + 255) / 256;
         k_prep<<<tb, 256, 0, sm>>>(d, dPosIn.as<double>(), 1);
-        if (s.skin <= 0) {   // no skin: a build at every evaluation, without the stale test or a conditional node
+        if (!verletList()) {   // no skin: a build at every evaluation, without the stale test or a conditional node
             CU(cudaMemsetAsync(d.cellCount, 0, (size_t) totalCells * sizeof(int), sm));
             enqueueBuild(sm, d);
         } else {
@@ -1356,7 +1374,7 @@ struct Engine::Impl {
         cudaGraphConditionalHandle handle = 0, listHandle = 0;
         if (s.polarizable)
             CU(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
-        if (s.skin > 0)   // (a handle without its conditional node makes the instantiation fail)
+        if (verletList())   // (a handle without its conditional node makes the instantiation fail)
             CU(cudaGraphConditionalHandleCreate(&listHandle, graph, 0, cudaGraphCondAssignDefault));
         const Dev d = makeDev(true, handle, listHandle);
         CU(cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
@@ -1555,7 +1573,7 @@ struct Engine::Impl {
         // decides from the displacements
         launchBoxes.assign(boxes, boxes + 9 * (size_t) nsys);
         const bool sameBoxes = listValid && buildBoxes == launchBoxes;
-        hCtl->forceRebuild = (!sameBoxes || grew || s.skin <= 0) ? 1 : 0;
+        hCtl->forceRebuild = (!sameBoxes || grew || !verletList()) ? 1 : 0;
         std::memcpy(hSys, sysHost.data(), nsys * sizeof(SysDev));
         CU(cudaMemcpyAsync(dSys.p, hSys, nsys * sizeof(SysDev), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(dCtl.p, hCtl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
@@ -1690,6 +1708,74 @@ void Engine::setAtoms(int n, const double* q, const double* radius, const double
                       int numGlobal) {
     impl->selectDevice();
     impl->setAtomsSingle(n, q, radius, alpha, globalIndex, numGlobal);
+}
+
+// The caller's pair candidates (core/cuda/pgm_cuda.h:68-73): segment sg holds the pairs (segI[sg], candJ[k]),
+// k in [segBegin[sg], segBegin[sg + 1]), with x = r_i + t.box - r_j, t = segShift[3 sg .. 3 sg + 2] integer box
+// vectors; every pair at most once.  Kept per atom in both directions ((i, j, t) and (j, i, -t)), in the
+// caller's order; they replace the engine's cell search until the next setAtoms, and the pairs beyond the
+// cutoff are left out at every evaluation.
+void Engine::setCandidates(int nseg, const int* segI, const int* segShift, const int* segBegin, const int* candJ) {
+    Impl& I = *impl;
+    if (!I.atomsSet || I.nsys != 1)
+        throw std::logic_error("pgm_b200: setCandidates needs a single-system engine with atoms set");
+    if (nseg < 0 || (nseg > 0 && (!segI || !segShift || !segBegin)))
+        throw std::invalid_argument("pgm_b200: setCandidates: bad segment arrays");
+    I.selectDevice();
+    const int n = I.n;
+    std::vector<int> start(n + 1, 0);
+    const int total = nseg > 0 ? segBegin[nseg] : 0;
+    if (nseg > 0 && (segBegin[0] != 0 || total < 0 || (total > 0 && !candJ)))
+        throw std::invalid_argument("pgm_b200: setCandidates: segBegin must start at 0 and candJ hold its total");
+    for (int sg = 0; sg < nseg; sg++) {
+        const int i = segI[sg];
+        if (i < 0 || i >= n || segBegin[sg + 1] < segBegin[sg])
+            throw std::invalid_argument("pgm_b200: setCandidates: atom index or segment bounds out of range");
+        for (int a = 0; a < 3; a++)
+            if (segShift[3 * sg + a] < -127 || segShift[3 * sg + a] > 127)
+                throw std::invalid_argument("pgm_b200: setCandidates: box shift out of range");
+        for (int k = segBegin[sg]; k < segBegin[sg + 1]; k++) {
+            const int j = candJ[k];
+            if (j < 0 || j >= n)
+                throw std::invalid_argument("pgm_b200: setCandidates: partner index out of range");
+            start[i + 1]++;
+            start[j + 1]++;
+        }
+    }
+    for (int i = 0; i < n; i++)
+        start[i + 1] += start[i];
+    std::vector<int> fill(start.begin(), start.end() - 1), jj(std::max(1, start[n])), tt(std::max(1, start[n]));
+    auto pack = [](int a, int b, int c) { return (a + 128) | ((b + 128) << 8) | ((c + 128) << 16); };
+    int longest = 0;
+    for (int sg = 0; sg < nseg; sg++) {
+        const int i = segI[sg], *t = segShift + 3 * sg;
+        for (int k = segBegin[sg]; k < segBegin[sg + 1]; k++) {
+            const int j = candJ[k];
+            int q = fill[i]++;
+            jj[q] = j;
+            tt[q] = pack(t[0], t[1], t[2]);
+            q = fill[j]++;
+            jj[q] = i;
+            tt[q] = pack(-t[0], -t[1], -t[2]);
+        }
+    }
+    for (int i = 0; i < n; i++)
+        longest = std::max(longest, start[i + 1] - start[i]);
+    CU(cudaStreamSynchronize(I.st));
+    upload(I.dCandStart, start, I.st);
+    upload(I.dCandJ, jj, I.st);
+    upload(I.dCandT, tt, I.st);
+    CU(cudaStreamSynchronize(I.st));
+    if (longest > I.cap) {   // rows for the longest candidate row
+        I.cap = (longest + 31) / 32 * 32;
+        I.allocList();
+    }
+    I.externalList = true;
+    I.listValid = false;
+    if (I.exec) {   // the graph holds the list's shape
+        cudaGraphExecDestroy(I.exec);
+        I.exec = nullptr;
+    }
 }
 
 void Engine::setCovalent(int ncov, const int* atom, const int* partner, const double* strength) {

@@ -214,6 +214,8 @@ __global__ void k_cell_sort(Dev dv) {
             dv.origS[sl] = make_double4(dv.posIn[3 * v], dv.posIn[3 * v + 1], dv.posIn[3 * v + 2], dv.radius[v]);
             dv.wrapS[sl] = make_int4(dv.wrapN[3 * v], dv.wrapN[3 * v + 1], dv.wrapN[3 * v + 2], 0);
             dv.radS[sl] = dv.radius[v];
+            if (dv.atomSlot)
+                dv.atomSlot[v] = sl;
         }
     }
 }
@@ -417,6 +419,40 @@ __global__ void __launch_bounds__(LIST_THREADS, 4) k_build_list(Dev dv) {
             atomicMax(&dv.flags[0], cnt);
             dv.slistCount[ii] = dv.cap;
         }
+    }
+}
+
+// The Verlet list from the caller's candidates (setCandidates, core/cuda/pgm_cuda.h:68-73) in place of the cell
+// search: one warp per slot, the row of atom i = slotAtom[slot] in the caller's order, the entry of candidate
+// (j, t) with the image shift w = N_j - N_i - t of the build's wraps N (r = pw + N.H), so that
+// x = pw_i - pw_j - w.H = r_i + t.H - r_j.  A shift outside the entry's range (-4..3 per component) sets
+// flags[1]; a row beyond the capacity sets flags[0] (the host grows the rows and repeats).  The evaluations'
+// compaction then keeps the candidates within the cutoff.
+__global__ void k_list_from_candidates(Dev dv) {
+    const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (slot >= dv.nAtoms)
+        return;
+    const int i = dv.slotAtom[slot];
+    const int4 ni = dv.wrapS[slot];
+    const int b = dv.candStart[i], cnt = dv.candStart[i + 1] - b;
+    uint32_t* row = dv.slist + (size_t) slot * dv.cap;
+    for (int k = lane; k < cnt && k < dv.cap; k += 32) {
+        const int j = dv.candJ[b + k], tp = dv.candT[b + k];
+        const int js = dv.atomSlot[j];
+        const int4 nj = dv.wrapS[js];
+        const int w0 = nj.x - ni.x - ((tp & 255) - 128), w1 = nj.y - ni.y - (((tp >> 8) & 255) - 128),
+                  w2 = nj.z - ni.z - (((tp >> 16) & 255) - 128);
+        if (w0 < -4 || w0 > 3 || w1 < -4 || w1 > 3 || w2 < -4 || w2 > 3) {
+            atomicOr(&dv.flags[1], 1);
+            row[k] = packEntry(slot, 0, 0, 0);   // (never used: the host raises)
+        } else {
+            row[k] = packEntry(js, w0, w1, w2);
+        }
+    }
+    if (lane == 0) {
+        dv.slistCount[slot] = min(cnt, dv.cap);
+        if (cnt > dv.cap)
+            atomicMax(&dv.flags[0], cnt);
     }
 }
 

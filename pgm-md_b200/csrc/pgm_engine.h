@@ -44,6 +44,8 @@ public:
     void setAtoms(int n, const double* q, const double* radius, const double* alpha, const int* globalIndex,
                   int numGlobal);
     void setCovalent(int ncov, const int* atom, const int* partner, const double* strength);
+    // the caller's pair candidates in place of the own pair search, until the next setAtoms
+    void setCandidates(int nseg, const int* segI, const int* segShift, const int* segBegin, const int* candJ);
     Terms compute(const double* pos, const double box[3][3], bool newStep, double* f, double* strain);
     Terms computeF(const float* pos, const double box[3][3], bool newStep, double* strain);
     void releasePositions() {}

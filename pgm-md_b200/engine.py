@@ -160,6 +160,17 @@ class Engine:
         _check(self._L.pgm_engine_set_covalent(self._h, len(atom), _i(atom), _i(partner), _d(strength)))
         self.ncov = len(atom)
 
+    def set_candidates(self, seg_i, seg_shift, seg_begin, cand_j):
+        """pgmcuda::Engine::setCandidates (core/cuda/pgm_cuda.h:68-73): the caller's pair candidates in place of the
+        own pair search, until the next set_atoms.  Segment s: pairs (seg_i[s], cand_j[k]) for k in
+        [seg_begin[s], seg_begin[s + 1]), x = r_i + t.box - r_j with t = seg_shift[s] (integer box vectors)."""
+        seg_i, seg_begin, cand_j = _i32(seg_i), _i32(seg_begin), _i32(cand_j)
+        seg_shift = np.ascontiguousarray(np.asarray(seg_shift, dtype=np.int32).reshape(-1, 3))
+        if len(seg_begin) != len(seg_i) + 1 or len(seg_shift) != len(seg_i):
+            raise ValueError("set_candidates: seg_begin needs len(seg_i) + 1 entries and seg_shift len(seg_i) rows")
+        _check(self._L.pgm_engine_set_candidates(self._h, len(seg_i), _i(seg_i), _i(seg_shift), _i(seg_begin),
+                                                 _i(cand_j)))
+
     def set_system(self, system):
         """set_atoms + set_covalent from a ``systems.System``."""
         self.set_atoms(system.q, system.radius, system.alpha)
