@@ -85,6 +85,15 @@ int pgm_engine_set_covalent(pgm_engine* e, int ncov, const int* atom, const int*
  * the pairs beyond the cutoff are left out at every evaluation.  Single-system engines. */
 int pgm_engine_set_candidates(pgm_engine* e, int nseg, const int* seg_i, const int* seg_shift, const int* seg_begin,
                               const int* cand_j);
+/* pgmcuda::Engine::setGvdw (core/cuda/pgm_cuda.h:57-65): the combination-rule GVDW van der Waals
+ * (core/gvdw_kernel.h) for the pairs within rvdw except the skipped ones: per atom sqrt_a = sqrt(A) [kJ/mol]^1/2,
+ * sqrt_c6 = sqrt(C6) [kJ/mol nm^6]^1/2, b (zeros: no term), repulsion 0 Gaussian A exp(-B y^2), 1 Slater
+ * A exp(-B y) with y = r / sqrt(2 (R_i^2 + R_j^2)); skipped pairs (skip_i[k], skip_j[k]) once each.  Its energy is
+ * pgm_terms.gvdw, its forces and strain are added to the evaluation's.  rvdw <= cutoff (the pass runs over the
+ * evaluation's pair list).  Single-system engines, until the next set_atoms; parameter gradients (param_grad)
+ * are refused while it is set. */
+int pgm_engine_set_gvdw(pgm_engine* e, int repulsion, double rvdw, const double* sqrt_a, const double* sqrt_c6,
+                        const double* b, int nskip, const int* skip_i, const int* skip_j);
 
 /* pgmcuda::Engine::compute (core/cuda/pgm_cuda.h:79): positions pos (n*3, host), box (9); forces ADDED to
  * f (n*3, may be NULL), strain derivative ADDED to strain (9, may be NULL); terms (may be NULL).

@@ -157,6 +157,12 @@ int pgm_engine_set_covalent(pgm_engine* e, int ncov, const int* atom, const int*
     });
 }
 
+int pgm_engine_set_gvdw(pgm_engine* e, int repulsion, double rvdw, const double* sqrt_a, const double* sqrt_c6,
+                        const double* b, int nskip, const int* skip_i, const int* skip_j) {
+    NEED(e);
+    return guarded([&] { e->e->setGvdw(repulsion, rvdw, sqrt_a, sqrt_c6, b, nskip, skip_i, skip_j); });
+}
+
 int pgm_engine_set_candidates(pgm_engine* e, int nseg, const int* seg_i, const int* seg_shift, const int* seg_begin,
                               const int* cand_j) {
     NEED(e);

@@ -15,8 +15,9 @@ constexpr int CHUNK = 256;                     // atoms per chunk of the per-sys
 constexpr int NSCAL = 16;                      // per-system CG scalars
 // per-system scalar slots
 enum { SC_NORM = 0, SC_RZ, SC_ALPH, SC_BETA, SC_ERR, SC_IT, SC_DONE, SC_PAP };
-constexpr int NRES = 16;                       // per-system results: 5 terms, 9 strain, iterations, residual
-constexpr int NFIN = 14;                       // per-atom final sums: epair, eself, epol, strain[9], q, unused
+constexpr int NRES = 17;                       // per-system results: 5 terms, 9 strain, iterations, residual, GVDW
+constexpr int GVDW_TERMS = 15;                 // terms of the GVDW G(y) series
+constexpr int NFIN = 14;                       // per-atom final sums: epair, eself, epol, strain[9], q, GVDW
 constexpr int NCONV = 10;                      // reciprocal energy + 9 strain per conv block
 
 // Per-system constants (host-computed at every evaluation; box-dependent parts included).
@@ -160,6 +161,14 @@ struct Dev {
     const int* chunkSys;
     const int* chunkBegin;
     const int* chunkEnd;
+    // the combination-rule GVDW (setGvdw): per atom (sqrt A, sqrt C6, b, 0), caller order; skipped partners per
+    // atom (sorted, both directions); pairs within rvdw2 of the evaluation's list; G(y) series coefficients
+    int gvdwOn, gvdwSlater;
+    double rvdw2;
+    const double4* gv;
+    const int* skipStart;
+    const int* skipJ;
+    double gvC[GVDW_TERMS];
     // history (global order)
     double* hist;             // 4 * 3 * numGlobal
     const int* globalIndex;

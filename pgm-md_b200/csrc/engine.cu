@@ -173,7 +173,7 @@ struct Engine::Impl {
         dScal, dPartial, dGPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dTwiddle, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
-        dGradQ, dGradR, dSList, dSListCount, dPosBuild, dAtomSlot, dCandStart, dCandJ, dCandT;
+        dGradQ, dGradR, dSList, dSListCount, dPosBuild, dAtomSlot, dCandStart, dCandJ, dCandT, dGv, dSkipStart, dSkipJ;
     // FP64 shadow of the mixed path for the iterative refinement
     Buf dPairBd, dDSd, dGridD, dSpecD, dInflD, dSplD, dB64, dXsave;
     std::vector<std::pair<cufftHandle, cufftHandle>> plans64;
@@ -202,6 +202,10 @@ struct Engine::Impl {
     // more than half the skin (checked on the device at every evaluation)
     bool listValid = false;
     bool externalList = false;   // the caller's candidates (setCandidates) in place of the cell search
+    // the combination-rule GVDW (setGvdw)
+    bool gvdwOn = false, gvdwSlater = false;
+    double rvdw = 0.0;
+    double gvC[GVDW_TERMS] = {};
     std::vector<double> buildBoxes;    // nsys * 9, the boxes of the last build
     std::vector<double> launchBoxes;   // nsys * 9, the boxes of the evaluation in flight
     cudaGraph_t listBody = nullptr;    // body of the build's conditional node while capturing
@@ -248,7 +252,7 @@ struct Engine::Impl {
                       &dCovByAtomOff, &dCovByAtom, &dCovByPartnerOff, &dCovByPartner, &dChunkSys, &dChunkBegin,
                       &dChunkEnd, &dHist, &dGlobal, &dCtl, &dGradQ, &dGradR, &dPairBd, &dDSd, &dGridD, &dSpecD,
                       &dInflD, &dSplD, &dB64, &dXsave, &dSList, &dSListCount, &dPosBuild, &dAtomSlot, &dCandStart,
-                      &dCandJ, &dCandT};
+                      &dCandJ, &dCandT, &dGv, &dSkipStart, &dSkipJ};
         for (Buf* b : all)
             b->release();
         if (hPos) cudaFreeHost(hPos);
@@ -333,7 +337,8 @@ struct Engine::Impl {
         if (nAt <= 0 || nAt >= (1 << 23))
             throw std::invalid_argument("pgm_b200: setAtoms needs 1 .. 8388607 atoms");
         const bool sameCount = atomsSet && nsys == 1 && n == nAt;
-        externalList = false;   // the candidates hold until the next setAtoms
+        externalList = false;   // the candidates and the GVDW parameters hold until the next setAtoms
+        gvdwOn = false;
         n = nAt;
         nsys = 1;
         atomBegin = {0, n};
@@ -374,6 +379,7 @@ struct Engine::Impl {
             throw std::invalid_argument("pgm_b200: setSystems needs at least one system");
         nsys = ns;
         externalList = false;
+        gvdwOn = false;
         atomBegin.assign(ns + 1, 0);
         for (int k = 0; k < ns; k++) {
             if (count[k] <= 0)
@@ -930,6 +936,16 @@ struct Engine::Impl {
         d.slist = dSList.as<uint32_t>();
         d.slistCount = dSListCount.as<int>();
         d.atomSlot = dAtomSlot.as<int>();
+        d.gvdwOn = gvdwOn ? 1 : 0;
+        if (gvdwOn) {
+            d.gvdwSlater = gvdwSlater ? 1 : 0;
+            d.rvdw2 = rvdw * rvdw;
+            d.gv = dGv.as<double4>();
+            d.skipStart = dSkipStart.as<int>();
+            d.skipJ = dSkipJ.as<int>();
+            for (int k = 0; k < GVDW_TERMS; k++)
+                d.gvC[k] = gvC[k];
+        }
         if (externalList) {
             d.candStart = dCandStart.as<int>();
             d.candJ = dCandJ.as<int>();
@@ -1356,6 +1372,8 @@ struct Engine::Impl {
             default: k_pair_final<R, 8><<<blocks, 256, 0, sm>>>(d);
             }
         }
+        if (gvdwOn)   // (adds to the final pair pass's force and strain)
+            k_gvdw<R><<<(n + 7) / 8, 256, 0, sm>>>(d);
         CU(cudaEventRecord(evJoin, sd));
         CU(cudaStreamWaitEvent(sm, evJoin, 0));
         launchGather<R, true>(sm, d, 0);
@@ -1662,6 +1680,7 @@ struct Engine::Impl {
         t.self = r[2];
         t.background = r[3];
         t.polarization = r[4];
+        t.gvdw = r[16];
         return t;
     }
 
@@ -1773,6 +1792,90 @@ void Engine::setCandidates(int nseg, const int* segI, const int* segShift, const
     I.externalList = true;
     I.listValid = false;
     if (I.exec) {   // the graph holds the list's shape
+        cudaGraphExecDestroy(I.exec);
+        I.exec = nullptr;
+    }
+}
+
+// The combination-rule GVDW (core/cuda/pgm_cuda.h:57-65): per atom sqrt(A), sqrt(C6), b (zeros: none),
+// repulsion 0 Gaussian, 1 Slater; the pairs within rvdw except the skipped ones (once each), added in the final
+// pass (energy Terms::gvdw, forces and strain added to the evaluation's).  rvdw may not exceed the cutoff (the
+// pass runs over the evaluation's pair list).  Until the next setAtoms.
+void Engine::setGvdw(int repulsion, double rvdw, const double* sqrtA, const double* sqrtC6, const double* b, int nskip,
+                     const int* skipI, const int* skipJ) {
+    Impl& I = *impl;
+    if (!I.atomsSet || I.nsys != 1)
+        throw std::logic_error("pgm_b200: setGvdw needs a single-system engine with atoms set");
+    if (repulsion != 0 && repulsion != 1)
+        throw std::invalid_argument("pgm_b200: GVDW repulsion must be 0 (Gaussian) or 1 (Slater)");
+    if (!(rvdw > 0) || rvdw > I.s.cutoff * (1.0 + 1e-12))
+        throw std::invalid_argument("pgm_b200: GVDW radius must be positive and at most the cutoff (the pass runs "
+                                    "over the evaluation's pair list)");
+    const int n = I.n;
+    if (!sqrtA || !sqrtC6 || !b || nskip < 0 || (nskip > 0 && (!skipI || !skipJ)))
+        throw std::invalid_argument("pgm_b200: setGvdw arguments");
+    std::vector<double> gv(4 * (size_t) n);
+    for (int i = 0; i < n; i++) {
+        if (!std::isfinite(sqrtA[i]) || !std::isfinite(sqrtC6[i]) || !std::isfinite(b[i]))
+            throw std::invalid_argument("pgm_b200: non-finite GVDW parameter");
+        gv[4 * i] = sqrtA[i];
+        gv[4 * i + 1] = sqrtC6[i];
+        gv[4 * i + 2] = b[i];
+        gv[4 * i + 3] = 0.0;
+    }
+    std::vector<int> start(n + 1, 0);
+    for (int k = 0; k < nskip; k++) {
+        if (skipI[k] < 0 || skipI[k] >= n || skipJ[k] < 0 || skipJ[k] >= n)
+            throw std::invalid_argument("pgm_b200: GVDW skipped pair index out of range");
+        start[skipI[k] + 1]++;
+        start[skipJ[k] + 1]++;
+    }
+    for (int i = 0; i < n; i++)
+        start[i + 1] += start[i];
+    std::vector<int> fill(start.begin(), start.end() - 1), part(std::max(1, start[n]));
+    for (int k = 0; k < nskip; k++) {
+        part[fill[skipI[k]]++] = skipJ[k];
+        part[fill[skipJ[k]]++] = skipI[k];
+    }
+    for (int i = 0; i < n; i++)
+        std::sort(part.begin() + start[i], part.begin() + start[i + 1]);
+    // the series of G(y) / G(0) in y^2: A(y) = (2/sqrt(pi)) sum a_n y^(2n+1) from the series of erf and exp
+    // (a_0 = a_1 = 0), G pi/4 = y^4 (sum_{n>=2} a_n y^(2n-4))^2 + (2/9) e^(-2 y^2)
+    {
+        const int K = GVDW_TERMS;
+        std::vector<double> a(K + 3), coef(K);
+        double fact = 1.0;   // n!
+        for (int n2 = 0; n2 < K + 3; n2++) {
+            if (n2 > 0)
+                fact *= n2;
+            const double sg = (n2 % 2) ? -1.0 : 1.0;
+            double t = sg / (fact * (2 * n2 + 1)) - sg / fact;
+            if (n2 >= 1)
+                t -= (2.0 / 3.0) * (-sg) / (fact / n2);
+            a[n2] = t;
+        }
+        fact = 1.0;
+        for (int k = 0; k < K; k++) {
+            if (k > 0)
+                fact *= k;
+            coef[k] = (2.0 / 9.0) * std::pow(-2.0, k) / fact;
+        }
+        for (int m1 = 0; m1 < K; m1++)
+            for (int m2 = 0; m1 + m2 + 2 < K; m2++)
+                coef[m1 + m2 + 2] += a[m1 + 2] * a[m2 + 2];
+        for (int k = 0; k < K; k++)
+            I.gvC[k] = coef[k] / coef[0];
+    }
+    I.selectDevice();
+    CU(cudaStreamSynchronize(I.st));
+    upload(I.dGv, gv, I.st);
+    upload(I.dSkipStart, start, I.st);
+    upload(I.dSkipJ, part, I.st);
+    CU(cudaStreamSynchronize(I.st));
+    I.gvdwOn = true;
+    I.gvdwSlater = repulsion == 1;
+    I.rvdw = rvdw;
+    if (I.exec) {   // the graph gains the GVDW pass
         cudaGraphExecDestroy(I.exec);
         I.exec = nullptr;
     }
@@ -2008,6 +2111,8 @@ void Engine::paramGrad(double* dq, double* dradius, double* dalpha, double* dstr
     Impl& I = *impl;
     if (!I.haveResult)
         throw std::logic_error("pgm_b200: paramGrad needs a completed evaluation");
+    if (I.gvdwOn)
+        throw std::logic_error("pgm_b200: parameter gradients cover the electrostatics only (GVDW is set)");
     I.selectDevice();
     const Dev dv = I.makeDev(false, 0);
     const int blocks = (int) (((long long) I.n * 8 + 255) / 256);
@@ -2190,7 +2295,7 @@ int Engine::kernelLaunches() const {
         it = std::max(it, (int) I.lastResults[(size_t) k * NRES + 14]);
     const int fp = 4;
     const int perIt = fp + (I.nsys == 1 && I.fuseCgA ? 1 : 2);   // single system: A p in the gather
-    return 7 + (I.lastBuilt ? 5 : 0) + (I.s.polarizable ? 2 * fp + 2 + perIt * it : 0) + 7;
+    return 7 + (I.lastBuilt ? 5 : 0) + (I.s.polarizable ? 2 * fp + 2 + perIt * it : 0) + 7 + (I.gvdwOn ? 1 : 0);
 }
 
 void Engine::kernelTimes(int reps, double* ms) {
@@ -2287,7 +2392,7 @@ void Engine::computeBatch(const double* pos, const double* boxes, double* energi
             for (int c = 0; c < 5; c++)
                 energies[6 * k + c] = r[c];
         if (energies)
-            energies[6 * k + 5] = 0.0;
+            energies[6 * k + 5] = r[16];
         if (strain)
             for (int c = 0; c < 9; c++)
                 strain[9 * k + c] = r[5 + c];

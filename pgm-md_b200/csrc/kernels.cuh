@@ -1912,6 +1912,123 @@ __global__ void __launch_bounds__(256) k_pair_final(Dev dv) {
     }
 }
 
+// ------------------------------------------------------------------------------------------------ GVDW
+
+// G(y) = F(y)/y^6 and H(y) = G'(y)/y of the GVDW dispersion (core/gvdw_kernel.h:30-58): the series in y^2 below
+// y = 0.6 (coefficients dv.gvC, derived on the host), the closed form F = A^2 + g^2/2 above.
+template <typename R>
+__device__ __forceinline__ void gvdwG(R y, const double* C, R& G, R& H) {
+    const R c0 = R(8.0 / (9.0 * PI_D));
+    if (y < R(0.6)) {
+        const R y2 = y * y;
+        R g = R(0), h = R(0);
+#pragma unroll
+        for (int k = GVDW_TERMS - 1; k >= 0; k--)
+            g = g * y2 + (R) C[k];
+#pragma unroll
+        for (int k = GVDW_TERMS - 1; k >= 1; k--)
+            h = h * y2 + R(2 * k) * (R) C[k];
+        G = c0 * g;
+        H = c0 * h;
+        return;
+    }
+    const R isp = R(1.0 / SQRT_PI);
+    const R y2 = y * y, e = fexp(-y2);
+    const R A = ferf(y) - R(2) * isp * y * (R(1) + R(2) * y2 / R(3)) * e;
+    const R g = (R(4) / R(3)) * isp * y2 * y * e;
+    const R F = A * A + R(0.5) * g * g;
+    const R Ap = (R(8) / R(3)) * isp * y2 * y2 * e;
+    const R gp = R(4) * isp * y2 * (R(1) - R(2) * y2 / R(3)) * e;
+    const R Fp = R(2) * A * Ap + g * gp;
+    const R y6 = y2 * y2 * y2;
+    G = F / y6;
+    H = (Fp / y6 - R(6) * F / (y6 * y)) / y;
+}
+
+// The GVDW pass of a single-system engine after the final pair pass: per atom (a warp per slot, its
+// evaluation's list over the lanes) the pairs within rvdw that are not skipped and carry a parameter,
+// U = A exp(-B y^2) (Gaussian) or A exp(-B y) (Slater) - C6 b^6 G(y) with y = b r, b = 1/sqrt(2 (R_i^2 + R_j^2)),
+// A = a_i a_j, C6 = c_i c_j, B = (b_i + b_j)/2 (core/gvdw_kernel.h:64-78, the combination rule of
+// core/cuda/pgm_cuda.cu:398-413).  Pair arithmetic in R, sums in double; half the pair energy into fin[13], the
+// force -dU/dr x/r and half the strain dU/dx (x) x added to the pair force and strain (those in units of ke).
+template <typename R>
+__global__ void __launch_bounds__(256) k_gvdw(Dev dv) {
+    const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (slot >= dv.nAtoms)
+        return;
+    const int i = dv.slotAtom[slot];
+    const SysDev& S = dv.sys[0];
+    const double4 gi = dv.gv[i];
+    const double4 pwi = dv.posS[slot];
+    const double Ri = dv.radius[i];
+    const uint32_t* row = dv.list + (size_t) slot * dv.cap;
+    const int cnt = dv.listCount[slot];
+    const int sb = dv.skipStart[i], se = dv.skipStart[i + 1];
+    double acc[13];
+#pragma unroll
+    for (int k = 0; k < 13; k++)
+        acc[k] = 0.0;
+    if (gi.x != 0.0 || gi.y != 0.0)
+        for (int t = lane; t < cnt; t += 32) {
+            const uint32_t e = row[t];
+            const int js = entrySlot(e);
+            double sh[3];
+            entryShift(e, S.H, sh);
+            const double4 pwj = dv.posS[js];
+            const double x0 = pwi.x - pwj.x - sh[0], x1 = pwi.y - pwj.y - sh[1], x2 = pwi.z - pwj.z - sh[2];
+            const double r2 = x0 * x0 + x1 * x1 + x2 * x2;
+            if (!(r2 < dv.rvdw2))
+                continue;
+            const int j = dv.slotAtom[js];
+            const double4 gj = dv.gv[j];
+            const double Aij = gi.x * gj.x, C6 = gi.y * gj.y;
+            if (Aij == 0.0 && C6 == 0.0)
+                continue;
+            bool skip = false;
+            for (int k = sb; k < se && !skip; k++)
+                skip = dv.skipJ[k] == j;
+            if (skip)
+                continue;
+            const double Rj = dv.radius[j];
+            const R bij = R(1) / (R) sqrt(2.0 * (Ri * Ri + Rj * Rj));
+            const R r = (R) sqrt(r2), y = bij * r, b2 = bij * bij, b6 = b2 * b2 * b2, B = (R) (0.5 * (gi.z + gj.z));
+            R erep, drep;   // drep = (1/r) dU_rep/dr
+            if (dv.gvdwSlater) {
+                erep = (R) Aij * fexp(-B * y);
+                drep = r > R(0) ? -B * bij * erep / r : R(0);
+            } else {
+                erep = (R) Aij * fexp(-B * y * y);
+                drep = R(-2) * B * b2 * erep;
+            }
+            R G, H;
+            gvdwG<R>(y, dv.gvC, G, H);
+            const R U = erep - (R) C6 * b6 * G;
+            const double dEdR = -(double) (drep - (R) C6 * b6 * b2 * H);   // -(1/r) dU/dr
+            const double x[3] = {x0, x1, x2};
+            acc[0] += 0.5 * (double) U;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                acc[1 + k] += dEdR * x[k];
+#pragma unroll
+                for (int b = 0; b < 3; b++)
+                    acc[4 + 3 * k + b] -= 0.5 * dEdR * x[k] * x[b];
+            }
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < 13; k++)
+            acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if (lane == 0) {
+        const double ike = 1.0 / dv.ke;
+        dv.fin[(size_t) i * NFIN + 13] = acc[0];
+        for (int k = 0; k < 3; k++)
+            dv.Fpair[3 * i + k] += acc[1 + k] * ike;
+        for (int k = 0; k < 9; k++)
+            dv.spair[(size_t) i * 9 + k] += acc[4 + k] * ike;
+    }
+}
+
 // ------------------------------------------------------------------------------------------------ CG
 
 // b = E_perm (pair + reciprocal + self), norm = mean|alpha b| per system, initial guess x0
@@ -2244,6 +2361,7 @@ __global__ void __launch_bounds__(CHUNK) k_final_forces(Dev dv, int iterationsSo
         for (int k = 0; k < 9; k++)
             v[3 + k] = Sv[k];
         v[12] = dv.q[i];
+        v[13] = dv.gvdwOn ? dv.fin[(size_t) i * NFIN + 13] : 0.0;
     }
     double tot[14];
     __shared__ double sconv[NCONV], cgrp[CHUNK / 16][NCONV];
@@ -2285,6 +2403,7 @@ __global__ void __launch_bounds__(CHUNK) k_final_forces(Dev dv, int iterationsSo
         }
         res[14] = iterationsSolved ? dv.scal[s * NSCAL + SC_IT] : 0.0;
         res[15] = iterationsSolved ? dv.scal[s * NSCAL + SC_ERR] : 0.0;
+        res[16] = tot[13];   // GVDW [kJ/mol]
     }
 }
 

@@ -46,6 +46,9 @@ public:
     void setCovalent(int ncov, const int* atom, const int* partner, const double* strength);
     // the caller's pair candidates in place of the own pair search, until the next setAtoms
     void setCandidates(int nseg, const int* segI, const int* segShift, const int* segBegin, const int* candJ);
+    // the combination-rule GVDW van der Waals in the final pair pass, until the next setAtoms
+    void setGvdw(int repulsion, double rvdw, const double* sqrtA, const double* sqrtC6, const double* b, int nskip,
+                 const int* skipI, const int* skipJ);
     Terms compute(const double* pos, const double box[3][3], bool newStep, double* f, double* strain);
     Terms computeF(const float* pos, const double box[3][3], bool newStep, double* strain);
     void releasePositions() {}

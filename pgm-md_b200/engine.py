@@ -171,6 +171,17 @@ class Engine:
         _check(self._L.pgm_engine_set_candidates(self._h, len(seg_i), _i(seg_i), _i(seg_shift), _i(seg_begin),
                                                  _i(cand_j)))
 
+    def set_gvdw(self, repulsion, rvdw, sqrt_a, sqrt_c6, b, skip_i=(), skip_j=()):
+        """pgmcuda::Engine::setGvdw (core/cuda/pgm_cuda.h:57-65): the combination-rule GVDW van der Waals
+        (repulsion 0 Gaussian, 1 Slater) for the pairs within rvdw (<= cutoff) except the skipped ones; per atom
+        sqrt(A), sqrt(C6), b.  Its energy is Terms.gvdw; until the next set_atoms."""
+        sa, sc, bb = _f64(sqrt_a), _f64(sqrt_c6), _f64(b)
+        si, sj = _i32(skip_i), _i32(skip_j)
+        if not (len(sa) == len(sc) == len(bb) == self.n) or len(si) != len(sj):
+            raise ValueError("set_gvdw: per-atom arrays of n entries and skipped pairs of equal length")
+        _check(self._L.pgm_engine_set_gvdw(self._h, int(repulsion), float(rvdw), _d(sa), _d(sc), _d(bb), len(si),
+                                           _i(si), _i(sj)))
+
     def set_system(self, system):
         """set_atoms + set_covalent from a ``systems.System``."""
         self.set_atoms(system.q, system.radius, system.alpha)

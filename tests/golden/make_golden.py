@@ -10,6 +10,10 @@ the fixtures travel, the reference does not):
                     into oracle/_ref by oracle/Makefile) on the seeded synthetic systems: energy terms,
                     forces, strain derivative, induced and permanent dipoles, iterations, tol 1e-10,
                     predictor none, peek 0.
+  gvdw_box.npz      the GVDW known-answer box of the reference (tests/data/gvdw_box.txt, written by
+                    tests/gvdw_input.py: 512 waters, reduced triclinic box, radii, which atoms carry the van der
+                    Waals term, the prmtop's excluded pairs) with pmemd-pgm's energies of it at 1 nm for the two
+                    repulsion forms and their parameters (core/tests/test_gvdw.cpp:66-70).
   dmp8550_real.npz  the reference's real 8550-atom dimethylphenol liquid (amber/test/dmp: pGM parameters from
                     the POL_GAUSS_* sections of prmtop.gz, coordinates and box from the NetCDF restart restrt0)
                     with the benchmark's settings (cutoff 0.9 nm, beta 3.5 / nm, 48^3, order 6), and pgm_core's
@@ -102,6 +106,20 @@ def w512():
     print("w512_pgmjax.npz", {k: np.shape(v) for k, v in out.items()})
 
 
+def gvdw_box():
+    lines = open(REF / "tests/data/gvdw_box.txt").read().split("\n")
+    n = int(lines[0])
+    box = np.array([[float(v) for v in lines[1 + a].split()] for a in range(3)])
+    atoms = np.array([[float(v) for v in lines[4 + i].split()] for i in range(n)])
+    excl = np.array([[int(v) for v in ln.split()] for ln in lines[4 + n:] if ln.strip()], dtype=np.int32)
+    # pmemd-pgm VDWAALS of this box at 10 A (kcal/mol) with the global parameters of the two repulsion forms:
+    # A_rep [kcal/mol], C6 [kcal/mol A^6], B, 1 = Slater (core/tests/test_gvdw.cpp:66-70)
+    models = np.array([[87500.0, 594.825035, 4.52, 1, 784.7282], [422.0, 594.825035, 0.9453, 0, 868.3699]])
+    np.savez_compressed(OUT / "gvdw_box.npz", box=box, pos=atoms[:, :3], radius=atoms[:, 3],
+                        lj=atoms[:, 4].astype(np.uint8), excl=excl, rvdw=1.0, models=models)
+    print("gvdw_box.npz", n, "atoms", len(excl), "exclusions")
+
+
 def dmp8550_real():
     import gzip
     import tempfile
@@ -189,10 +207,12 @@ def ref_outputs():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["w512", "ref", "dmp"]
+    which = sys.argv[1:] or ["w512", "ref", "dmp", "gvdw"]
     if "w512" in which:
         w512()
     if "ref" in which:
         ref_outputs()
     if "dmp" in which:
         dmp8550_real()
+    if "gvdw" in which:
+        gvdw_box()
