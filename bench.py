@@ -162,8 +162,8 @@ def traffic_of(kernel):
 
 
 def algorithmic_bytes(kernel, S, precision, it):
-    """Algorithmic bytes per launch of the main kernels (the units and per-unit bytes are the ones DESIGN.md
-    states): s = real size, g = grid real size, P = directed pairs, p = order."""
+    """Algorithmic bytes per launch of the main kernels (the bytes each must move at least, per unit: atom,
+    directed pair, grid point): s = real size, g = grid real size, P = directed pairs, p = order."""
     s = 4 if precision else 8
     n, p = S.n, S.order
     P = S.meta.get("pairs", 0)
