@@ -85,6 +85,10 @@ int pgm_engine_set_covalent(pgm_engine* e, int ncov, const int* atom, const int*
  * the pairs beyond the cutoff are left out at every evaluation.  Single-system engines. */
 int pgm_engine_set_candidates(pgm_engine* e, int nseg, const int* seg_i, const int* seg_shift, const int* seg_begin,
                               const int* cand_j);
+/* Self-test of the failure path of the grid transforms' barriers (no counterpart in the reference): one block
+ * waits at a barrier that expects two; the wait gives up after its bounded number of polls, sets the error flag
+ * and returns.  *flag = 1 when it did (the expected outcome), *seconds the device time of the launch. */
+int pgm_engine_probe_barrier_timeout(pgm_engine* e, int* flag, double* seconds);
 /* pgmcuda::Engine::setGvdw (core/cuda/pgm_cuda.h:57-65): the combination-rule GVDW van der Waals
  * (core/gvdw_kernel.h) for the pairs within rvdw except the skipped ones: per atom sqrt_a = sqrt(A) [kJ/mol]^1/2,
  * sqrt_c6 = sqrt(C6) [kJ/mol nm^6]^1/2, b (zeros: no term), repulsion 0 Gaussian A exp(-B y^2), 1 Slater

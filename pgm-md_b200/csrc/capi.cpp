@@ -157,6 +157,15 @@ int pgm_engine_set_covalent(pgm_engine* e, int ncov, const int* atom, const int*
     });
 }
 
+int pgm_engine_probe_barrier_timeout(pgm_engine* e, int* flag, double* seconds) {
+    NEED(e);
+    return guarded([&] {
+        const int f = e->e->probeBarrierTimeout(seconds);
+        if (flag)
+            *flag = f;
+    });
+}
+
 int pgm_engine_set_gvdw(pgm_engine* e, int repulsion, double rvdw, const double* sqrt_a, const double* sqrt_c6,
                         const double* b, int nskip, const int* skip_i, const int* skip_j) {
     NEED(e);

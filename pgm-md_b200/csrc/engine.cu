@@ -1692,9 +1692,17 @@ struct Engine::Impl {
 
     // Host double positions, full evaluation, forces to the pinned buffer.
     Terms evalHost(const double* pos, const double* boxes, bool newStep, bool wantForces) {
-        checkPositions(pos, 3 * (size_t) n);
+        // one pass: the finiteness check with the copy into the pinned staging buffer
+        const size_t m = 3 * (size_t) n;
+        bool finite = true;
+        for (size_t k = 0; k < m; k++) {
+            const double v = pos[k];
+            finite &= std::isfinite(v);
+            hPos[k] = v;
+        }
+        if (!finite)
+            throw std::invalid_argument("pgm_b200: non-finite position");
         selectDevice();
-        std::memcpy(hPos, pos, 3 * (size_t) n * 8);
         for (int attempt = 0; attempt < 4; attempt++) {
             prepareControl(newStep, 0, nullptr, nullptr, 0, 0.0, nullptr);
             CU(cudaMemcpyAsync(dPosIn.p, hPos, 3 * (size_t) n * 8, cudaMemcpyHostToDevice, st));
@@ -1727,6 +1735,36 @@ void Engine::setAtoms(int n, const double* q, const double* radius, const double
                       int numGlobal) {
     impl->selectDevice();
     impl->setAtomsSingle(n, q, radius, alpha, globalIndex, numGlobal);
+}
+
+// Self-test of the grid transforms' bounded barrier: one block waits at a barrier that expects two; the wait
+// runs out, sets the error flag and returns.  Returns the flag (1: the wait gave up as designed) and the
+// device time of the launch.
+int Engine::probeBarrierTimeout(double* seconds) {
+    Impl& I = *impl;
+    I.selectDevice();
+    void* mem = nullptr;
+    CU(cudaMalloc(&mem, 64 * sizeof(int)));
+    int* words = (int*) mem;
+    CU(cudaMemsetAsync(words, 0, 64 * sizeof(int), I.st));
+    cudaEvent_t a, b;
+    CU(cudaEventCreate(&a));
+    CU(cudaEventCreate(&b));
+    CU(cudaEventRecord(a, I.st));
+    k_barrier_probe<<<1, 32, 0, I.st>>>((unsigned*) (words + 16), words);
+    CU(cudaGetLastError());
+    CU(cudaEventRecord(b, I.st));
+    int flags[16];
+    CU(cudaMemcpyAsync(flags, words, sizeof(flags), cudaMemcpyDeviceToHost, I.st));
+    CU(cudaStreamSynchronize(I.st));
+    float ms = 0.0f;
+    CU(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CU(cudaFree(mem));
+    if (seconds)
+        *seconds = ms * 1e-3;
+    return flags[11];
 }
 
 // The caller's pair candidates (core/cuda/pgm_cuda.h:68-73): segment sg holds the pairs (segI[sg], candJ[k]),

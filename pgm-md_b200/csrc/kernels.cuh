@@ -1364,6 +1364,10 @@ __device__ __forceinline__ bool fftgBarrier(unsigned* bar, unsigned nb, int* fla
     return ok != 0;
 }
 
+// Self-test of the bounded barrier wait: the launch's blocks wait at a barrier that expects one block more than
+// there are, so every wait runs out (FFTG_SPIN_LIMIT polls), sets flags[11] and returns.
+__global__ void k_barrier_probe(unsigned* bar, int* flags) { fftgBarrier(bar, gridDim.x + 1, flags); }
+
 // KC > 0: every grid of the launch is KC^3 (compile-time passes and index maps); 0: any grid.
 template <typename R, int KC>
 __global__ void __launch_bounds__(FftgThreads<R>::n) k_fft_grid(Dev dv, int gateDone) {

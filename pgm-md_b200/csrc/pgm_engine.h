@@ -46,6 +46,8 @@ public:
     void setCovalent(int ncov, const int* atom, const int* partner, const double* strength);
     // the caller's pair candidates in place of the own pair search, until the next setAtoms
     void setCandidates(int nseg, const int* segI, const int* segShift, const int* segBegin, const int* candJ);
+    // self-test of the grid transforms' bounded barrier wait (1: the wait gave up as designed)
+    int probeBarrierTimeout(double* seconds);
     // the combination-rule GVDW van der Waals in the final pair pass, until the next setAtoms
     void setGvdw(int repulsion, double rvdw, const double* sqrtA, const double* sqrtC6, const double* b, int nskip,
                  const int* skipI, const int* skipJ);

@@ -182,6 +182,14 @@ class Engine:
         _check(self._L.pgm_engine_set_gvdw(self._h, int(repulsion), float(rvdw), _d(sa), _d(sc), _d(bb), len(si),
                                            _i(si), _i(sj)))
 
+    def probe_barrier_timeout(self):
+        """Self-test of the grid transforms' bounded barrier: (gave_up, seconds); gave_up is True when the wait
+        ran out and reported it, as designed."""
+        flag = np.zeros(1, np.int32)
+        sec = np.zeros(1)
+        _check(self._L.pgm_engine_probe_barrier_timeout(self._h, _i(flag), _d(sec)))
+        return bool(flag[0]), float(sec[0])
+
     def set_system(self, system):
         """set_atoms + set_covalent from a ``systems.System``."""
         self.set_atoms(system.q, system.radius, system.alpha)
