@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 1024-system leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 98304-atom leg")
     ap.add_argument("--no-grad", action="store_true", help="skip the parameter-gradient leg")
+    ap.add_argument("--ref-large", action="store_true",
+                    help="reference arm: also one evaluation of the 98304-atom box on one core (about a minute)")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip the reference GPU engine timed on this GPU")
     return ap.parse_args()
@@ -293,10 +295,73 @@ def reference_arm(args):
             "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "reference",
                              "sample": f"{steps} steps x {cores} full evaluations of {WORKLOAD}"},
             "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["cpu_other_configs"] = cpu_other_configs(pkg, cores, ctx, args.ref_large)
     if not args.no_reference_gpu:
         line["reference_gpu"] = reference_gpu_leg(pkg, S, steps, max(args.warmup, 3))
     print(json.dumps(line))
     return 0
+
+
+BATCH_SAMPLE = 64
+
+
+def _ref_engine(pkg, S, tol):
+    from oracle import pgm_oracle as O
+    from oracle import ref as R
+    top = O.Topology(S.q, S.radius, S.alpha, S.cov_atom, S.cov_partner, S.cov_strength)
+    st = O.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=tol, max_iter=500, peek=0.65,
+                    predictor=0, ke=pkg.systems.KE_DEFAULT)
+    return R.RefEngine(top, st)
+
+
+def _batch_worker_init():
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, str(ROOT))
+    pkg, _ = system()
+    systems = pkg.systems.water_batch(nsys=1024, seed=1024, tol=TOL)[:BATCH_SAMPLE]
+    _REF["batch"] = [(S, _ref_engine(pkg, S, TOL)) for S in systems]
+
+
+def _batch_worker_eval(k):
+    S, e = _REF["batch"][k]
+    return e.compute(S.pos, S.box)
+
+
+def cpu_other_configs(pkg, cores, ctx, large):
+    """The reference pgm_core on the other configurations (bounded samples, FP64): the 216-water box on one
+    core; the first 64 boxes of the 1024-box water batch sequentially on one core and spread over all cores (one
+    process per core); with ``large`` one evaluation of the 98304-atom water box on one core (about a minute
+    and more: pgm_core's pair search tests all N^2 pairs)."""
+    out = {}
+    S = pkg.systems.water216()
+    e = _ref_engine(pkg, S, S.tol)
+    e.compute(S.pos, S.box)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        e.compute(S.pos, S.box)
+    out["water216"] = {"evals_per_s": 5 / (time.perf_counter() - t0), "cores": 1, "tol": S.tol}
+    systems = pkg.systems.water_batch(nsys=1024, seed=1024, tol=TOL)[:BATCH_SAMPLE]
+    engines = [_ref_engine(pkg, B, TOL) for B in systems]
+    t0 = time.perf_counter()
+    for B, eb in zip(systems, engines):
+        eb.compute(B.pos, B.box)
+    seq = time.perf_counter() - t0
+    with ctx.Pool(cores, initializer=_batch_worker_init) as pool:
+        pool.map(_batch_worker_eval, range(BATCH_SAMPLE))   # untimed: every worker's engines warm
+        t0 = time.perf_counter()
+        pool.map(_batch_worker_eval, range(BATCH_SAMPLE))
+        par = time.perf_counter() - t0
+    out["water_batch1024"] = {"sample": f"the first {BATCH_SAMPLE} of the 1024 boxes",
+                              "atoms": int(sum(B.n for B in systems)),
+                              "systems_per_s_1_core": BATCH_SAMPLE / seq,
+                              "systems_per_s_all_cores": BATCH_SAMPLE / par, "cores": cores}
+    if large:
+        S = pkg.systems.water98304(tol=TOL)
+        e = _ref_engine(pkg, S, TOL)
+        t0 = time.perf_counter()
+        e.compute(S.pos, S.box)
+        out["water98304"] = {"evals_per_s": 1.0 / (time.perf_counter() - t0), "cores": 1, "tol": TOL}
+    return out
 
 
 def reference_gpu_leg(pkg, S, steps, warmup):
