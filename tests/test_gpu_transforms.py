@@ -45,6 +45,25 @@ def test_transforms_single_system(precision, mode, name):
     assert a.iterations == b.iterations or precision == 1
 
 
+@pytest.mark.parametrize("K", [32, 40, 64])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_grid_transforms_compiled_sizes(precision, K):
+    # the grid kernel's compile-time sizes beside 48 (64^3 in FP64 takes 72 KB of shared memory per block)
+    S = PKG.systems.waters(64, 12.4, seed=21, grid=(K, K, K), cutoff=6.0, tol=1e-10)
+    out = []
+    for m in (0, 3):
+        eng = PKG.Engine(settings(S, precision))
+        eng.set_system(S)
+        eng.set_transforms(m)
+        assert eng.transforms() == m
+        out.append(eng.compute(S.pos, S.box))
+        eng.close()
+    a, b = out
+    lim_e, lim_f = (1e-12, 1e-12) if precision == 0 else (1e-6, 1e-5)
+    assert abs(a.energy - b.energy) <= lim_e * abs(a.energy)
+    assert rel_rms(b.forces, a.forces) <= lim_f
+
+
 @pytest.mark.parametrize("mode", [1, 2, 3])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_transforms_batch(precision, mode):
