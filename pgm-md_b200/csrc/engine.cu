@@ -1254,11 +1254,16 @@ struct Engine::Impl {
         k_cell_scan<<<1, 1024, 0, sm>>>(d);
         k_cell_scatter<<<tb, 256, 0, sm>>>(d);
         k_cell_sort<<<(totalCells + 7) / 8, 256, 0, sm>>>(d);
+        listKernel(sm, d);
+        CU(cudaGetLastError());
+    }
+
+    // The list's rows at a build (after the cell sort): the caller's candidates, or the cell search.
+    void listKernel(cudaStream_t sm, const Dev& d) {
         if (externalList)
             k_list_from_candidates<<<(n + 7) / 8, 256, 0, sm>>>(d);
         else
             k_build_list<<<totalCells, LIST_THREADS, 0, sm>>>(d);
-        CU(cudaGetLastError());
     }
 
     // The pair-list step of an evaluation: positions in (PME base and fraction), the stale test, the build when
@@ -2104,14 +2109,14 @@ void Engine::field(const double* pos, const double box[3][3], const double* qf, 
         k_cell_scatter<<<tb, 256, 0, I.st>>>(dv);
         k_cell_sort<<<(I.totalCells + 7) / 8, 256, 0, I.st>>>(dv);
         if (I.mixed()) {
-            k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(dv);
+            I.listKernel(I.st, dv);
             k_pair_compact<float><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
             k_splines<float><<<(3 * I.n + 255) / 256, 256, 0, I.st>>>(dv);
             k_influence<float><<<dim3(I.convBlocks, I.nsys), 256, 0, I.st>>>(dv);
             CU(cudaMemsetAsync(dv.grid, 0, I.gridTotal * I.realSize(), I.st));
             I.fieldPass<float, true>(I.st, I.side, dv, 0, dv.dtot, false);
         } else {
-            k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(dv);
+            I.listKernel(I.st, dv);
             k_pair_compact<double><<<(I.n + 7) / 8, 256, 0, I.st>>>(dv);
             k_splines<double><<<(3 * I.n + 255) / 256, 256, 0, I.st>>>(dv);
             k_influence<double><<<dim3(I.convBlocks, I.nsys), 256, 0, I.st>>>(dv);
@@ -2237,7 +2242,7 @@ Terms Engine::evaluateFixed(const double* pos, const double box[3][3], const dou
                 k_cell_scan<<<1, 1024, 0, I.st>>>(d);
                 k_cell_scatter<<<tb, 256, 0, I.st>>>(d);
                 k_cell_sort<<<(I.totalCells + 7) / 8, 256, 0, I.st>>>(d);
-                k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(d);
+                I.listKernel(I.st, d);
                 k_pair_compact<R><<<(I.n + 7) / 8, 256, 0, I.st>>>(d);
             }
             k_splines<R><<<(3 * I.n + 255) / 256, 256, 0, I.st>>>(d);
@@ -2360,7 +2365,7 @@ void Engine::kernelTimes(int reps, double* ms) {
     auto run = [&](auto tag) {
         typedef decltype(tag) R;
         ms[0] = timeIt([&] {
-            k_build_list<<<I.totalCells, LIST_THREADS, 0, I.st>>>(d);
+            I.listKernel(I.st, d);
             I.pairRecords<R>(I.st, d);
         });
         ms[1] = timeIt([&] { I.pairField<R, false>(I.st, d, 0); });

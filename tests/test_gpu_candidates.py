@@ -5,7 +5,8 @@ partners j, x = r_i + t.box - r_j, every pair once, the pairs beyond the cutoff 
 Candidates are the oracle's pairs within cutoff + 0.15 nm (the reference's minimum image, i < j), grouped into
 one segment per (i, shift).  With them the engine gives the energies, forces and pair set of its own list (FP64
 within 1e-12 relative: only the order of the pair sums differs; mixed within 1e-6 and 1e-5) over a moving
-trajectory, and the oracle's at tol 1e-10; a new set_atoms drops them; bad input is refused.
+trajectory, and the oracle's at tol 1e-10; the field entry point uses them too; a new set_atoms drops them; bad
+input is refused.
 """
 
 import numpy as np
@@ -76,6 +77,10 @@ def test_candidates_triclinic_and_reset():
     a, b = own.compute(S.pos, S.box), ext.compute(S.pos, S.box)
     assert abs(a.energy - b.energy) <= 1e-12 * abs(a.energy)
     assert rel_rms(b.forces, a.forces) <= 1e-11
+    # the field entry point builds its list from the candidates too
+    rng = np.random.default_rng(2)
+    q, d = rng.normal(0, 0.5, S.n), rng.normal(0, 0.01, (S.n, 3))
+    assert rel_rms(ext.field(S.pos, S.box, q, d), own.field(S.pos, S.box, q, d)) <= 1e-12
     # a new set_atoms drops the candidates: the own search again
     ext.set_system(S)
     c = ext.compute(S.pos, S.box)
