@@ -89,6 +89,10 @@ int pgm_engine_set_candidates(pgm_engine* e, int nseg, const int* seg_i, const i
  * waits at a barrier that expects two; the wait gives up after its bounded number of polls, sets the error flag
  * and returns.  *flag = 1 when it did (the expected outcome), *seconds the device time of the launch. */
 int pgm_engine_probe_barrier_timeout(pgm_engine* e, int* flag, double* seconds);
+/* The coefficients c[0..k-1] (k <= 32) of the GVDW dispersion's G(y)/G(0) = sum c_m y^(2m) that set_gvdw uses
+ * below y = 0.6, derived from the series of erf and exp (no counterpart in the reference, which tabulates them in
+ * core/gvdw_kernel.h:33-37).  Host only: needs no GPU. */
+int pgm_gvdw_series(double* c, int k);
 /* pgmcuda::Engine::setGvdw (core/cuda/pgm_cuda.h:57-65): the combination-rule GVDW van der Waals
  * (core/gvdw_kernel.h) for the pairs within rvdw except the skipped ones: per atom sqrt_a = sqrt(A) [kJ/mol]^1/2,
  * sqrt_c6 = sqrt(C6) [kJ/mol nm^6]^1/2, b (zeros: no term), repulsion 0 Gaussian A exp(-B y^2), 1 Slater

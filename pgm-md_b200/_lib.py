@@ -42,6 +42,7 @@ SIGNATURES = {
     "pgm_engine_set_candidates": (c_int, [c_void_p, c_int, P_I, P_I, P_I, P_I]),
     "pgm_engine_set_gvdw": (c_int, [c_void_p, c_int, c_double, P_D, P_D, P_D, c_int, P_I, P_I]),
     "pgm_engine_probe_barrier_timeout": (c_int, [c_void_p, P_I, P_D]),
+    "pgm_gvdw_series": (c_int, [P_D, c_int]),
     "pgm_engine_compute": (c_int, [c_void_p, P_D, P_D, c_int, P_D, P_D, ctypes.POINTER(PgmTerms)]),
     "pgm_engine_compute_f": (c_int, [c_void_p, P_F, P_D, c_int, P_D, ctypes.POINTER(PgmTerms)]),
     "pgm_engine_forces": (P_D, [c_void_p]),

@@ -157,6 +157,14 @@ int pgm_engine_set_covalent(pgm_engine* e, int ncov, const int* atom, const int*
     });
 }
 
+int pgm_gvdw_series(double* c, int k) {
+    return guarded([&] {
+        if (!c || k < 1 || k > 32)
+            throw std::invalid_argument("pgm_b200: gvdw_series needs 1 <= k <= 32 and an output array");
+        pgmb200::gvdwSeries(c, k);
+    });
+}
+
 int pgm_engine_probe_barrier_timeout(pgm_engine* e, int* flag, double* seconds) {
     NEED(e);
     return guarded([&] {

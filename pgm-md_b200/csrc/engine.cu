@@ -1840,6 +1840,33 @@ void Engine::setCandidates(int nseg, const int* segI, const int* segShift, const
     }
 }
 
+// The series of the GVDW G(y) / G(0) in y^2, c[0..K-1]: with A(y) = (2/sqrt(pi)) sum a_n y^(2n+1) from the series of
+// erf and exp (a_0 = a_1 = 0), G pi/4 = y^4 (sum_{n>=2} a_n y^(2n-4))^2 + (2/9) e^(-2 y^2).
+void gvdwSeries(double* c, int K) {
+    std::vector<double> a(K + 3), coef(K);
+    double fact = 1.0;   // n!
+    for (int n2 = 0; n2 < K + 3; n2++) {
+        if (n2 > 0)
+            fact *= n2;
+        const double sg = (n2 % 2) ? -1.0 : 1.0;
+        double t = sg / (fact * (2 * n2 + 1)) - sg / fact;
+        if (n2 >= 1)
+            t -= (2.0 / 3.0) * (-sg) / (fact / n2);
+        a[n2] = t;
+    }
+    fact = 1.0;
+    for (int k = 0; k < K; k++) {
+        if (k > 0)
+            fact *= k;
+        coef[k] = (2.0 / 9.0) * std::pow(-2.0, k) / fact;
+    }
+    for (int m1 = 0; m1 < K; m1++)
+        for (int m2 = 0; m1 + m2 + 2 < K; m2++)
+            coef[m1 + m2 + 2] += a[m1 + 2] * a[m2 + 2];
+    for (int k = 0; k < K; k++)
+        c[k] = coef[k] / coef[0];
+}
+
 // The combination-rule GVDW (core/cuda/pgm_cuda.h:57-65): per atom sqrt(A), sqrt(C6), b (zeros: none),
 // repulsion 0 Gaussian, 1 Slater; the pairs within rvdw except the skipped ones (once each), added in the final
 // pass (energy Terms::gvdw, forces and strain added to the evaluation's).  rvdw may not exceed the cutoff (the
@@ -1882,33 +1909,7 @@ void Engine::setGvdw(int repulsion, double rvdw, const double* sqrtA, const doub
     }
     for (int i = 0; i < n; i++)
         std::sort(part.begin() + start[i], part.begin() + start[i + 1]);
-    // the series of G(y) / G(0) in y^2: A(y) = (2/sqrt(pi)) sum a_n y^(2n+1) from the series of erf and exp
-    // (a_0 = a_1 = 0), G pi/4 = y^4 (sum_{n>=2} a_n y^(2n-4))^2 + (2/9) e^(-2 y^2)
-    {
-        const int K = GVDW_TERMS;
-        std::vector<double> a(K + 3), coef(K);
-        double fact = 1.0;   // n!
-        for (int n2 = 0; n2 < K + 3; n2++) {
-            if (n2 > 0)
-                fact *= n2;
-            const double sg = (n2 % 2) ? -1.0 : 1.0;
-            double t = sg / (fact * (2 * n2 + 1)) - sg / fact;
-            if (n2 >= 1)
-                t -= (2.0 / 3.0) * (-sg) / (fact / n2);
-            a[n2] = t;
-        }
-        fact = 1.0;
-        for (int k = 0; k < K; k++) {
-            if (k > 0)
-                fact *= k;
-            coef[k] = (2.0 / 9.0) * std::pow(-2.0, k) / fact;
-        }
-        for (int m1 = 0; m1 < K; m1++)
-            for (int m2 = 0; m1 + m2 + 2 < K; m2++)
-                coef[m1 + m2 + 2] += a[m1 + 2] * a[m2 + 2];
-        for (int k = 0; k < K; k++)
-            I.gvC[k] = coef[k] / coef[0];
-    }
+    gvdwSeries(I.gvC, GVDW_TERMS);
     I.selectDevice();
     CU(cudaStreamSynchronize(I.st));
     upload(I.dGv, gv, I.st);

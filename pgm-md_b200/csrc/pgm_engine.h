@@ -34,6 +34,9 @@ struct Terms {
     double total() const { return direct + reciprocal + self + background + polarization + gvdw; }
 };
 
+// Coefficients c[0..k-1] of the GVDW dispersion's G(y) / G(0) as a series in y^2 (derived from erf and exp).
+void gvdwSeries(double* c, int k);
+
 class Engine {
 public:
     explicit Engine(const Settings& settings);

@@ -71,3 +71,18 @@ def test_gvdw_box_forces_and_strain_finite_differences():
         ep = GV.gvdw_energy(pos @ (np.eye(3) + eps).T, box @ (np.eye(3) + eps).T, *args)[0]
         em = GV.gvdw_energy(pos @ (np.eye(3) - eps).T, box @ (np.eye(3) - eps).T, *args)[0]
         assert abs((ep - em) / (2 * h) - S[3 * a + bb]) <= 1e-5 * np.abs(S).max()
+
+
+def test_engine_series_matches_checker():
+    """The engine's host derivation of the G(y) series (pgm_gvdw_series, double arithmetic) against the checker's
+    exact rationals, and the reference's published table to its printed digits (core/gvdw_kernel.h:33-37 gives
+    c_1 = -2, c_2 = 58/25, c_3 = -188/105)."""
+    import ctypes
+    from pgm_md_b200 import _lib
+    c = np.zeros(GV.SERIES_TERMS)
+    assert _lib.load().pgm_gvdw_series(c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(c)) == 0
+    ref = GV.series_coefficients()
+    assert np.all(np.abs(c - ref) <= 1e-14 * np.abs(ref))
+    assert c[0] == 1.0 and abs(c[1] + 2.0) < 1e-15 and abs(c[2] - 58 / 25) < 1e-15 and abs(c[3] + 188 / 105) < 1e-15
+    bad = np.zeros(1)
+    assert _lib.load().pgm_gvdw_series(bad.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0) != 0
