@@ -211,7 +211,12 @@ def roofline_table(S, kt, it, precision):
     return {"kernel": dom, "bound": "hbm", "achieved": per[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
             "frac": per[dom]["frac"], "peak_source": peak_kind, "traffic": traffic_of(dom),
             "bytes_per_launch": per[dom]["bytes_per_launch"], "ms_per_launch": kt[dom],
-            "fft_chain_share": per["fft_chain"]["share"], "per_kernel": per}
+            "fft_chain_share": per["fft_chain"]["share"], "per_kernel": per,
+            "note": "each kernel relaunched alone, back to back on the engine's stream (no L2 flush between "
+                    "launches, as inside an evaluation): where its data fits in the 126 MB L2 (the 8550-atom "
+                    "workload's 61 MB of pair records) it is served from L2, and frac is its algorithmic "
+                    "bytes per second against the HBM copy figure; traffic is the DRAM bytes of one cold "
+                    "launch (ncu), which equal the algorithmic bytes"}
 
 
 def md_positions(S, phase, count):
