@@ -1,0 +1,54 @@
+"""The bench line's roofline arithmetic, without a GPU: algorithmic bytes per launch follow the per-unit figures
+the bench states (a mixed pair-field launch moves 24 B per directed pair plus its per-atom terms), achieved =
+bytes / launch time, frac = achieved / the peak, and the dominant kernel is the engine's own kernel with the
+largest share of an evaluation (the cuFFT chain listed beside it, never chosen)."""
+
+import importlib.util
+
+import numpy as np
+import pytest
+
+from conftest import PKG, ROOT
+
+
+@pytest.fixture(scope="module")
+def bench():
+    spec = importlib.util.spec_from_file_location("pgm_b200_bench", ROOT / "bench.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_algorithmic_bytes_per_unit(bench):
+    S = PKG.systems.water216()
+    S.meta["pairs"] = 1000
+    n, p = S.n, S.order
+    assert bench.algorithmic_bytes("pair_field", S, 1, 9) == 1000 * 24 + n * (4 * 4 + 24)
+    assert bench.algorithmic_bytes("pair_field", S, 0, 9) == 1000 * (4 + 16) + n * (32 + 32 + 24)
+    assert bench.algorithmic_bytes("spread", S, 1, 9) == n * (7 * 4 + p ** 3 * 4)
+    G = int(np.prod(S.grid))
+    Gc = S.grid[0] * S.grid[1] * (S.grid[2] // 2 + 1)
+    assert bench.algorithmic_bytes("fft_chain", S, 1, 9) == 2 * (G * 4 + Gc * 8) + Gc * 20
+    assert bench.algorithmic_bytes("no_such_kernel", S, 1, 9) is None
+
+
+def test_roofline_table_arithmetic(bench):
+    S = PKG.systems.water216()
+    S.meta["pairs"] = 200000
+    it = 9
+    kt = {"pair_list": 0.05, "pair_field": 0.010, "spread": 0.008, "gather": 0.009, "pair_final": 0.02,
+          "fft_chain": 0.5, "cg_update": 0.004}
+    roof = bench.roofline_table(S, kt, it, 1)
+    peak, _ = bench.peaks()
+    for k, ms in kt.items():
+        row = roof["per_kernel"][k]
+        assert row["launches_per_eval"] == bench.launches_per_eval(k, it)
+        b = bench.algorithmic_bytes(k, S, 1, it)
+        assert row["bytes_per_launch"] == b
+        assert row["achieved_gbs"] == pytest.approx(b / (ms * 1e-3) / 1e9)
+        assert row["frac"] == pytest.approx(row["achieved_gbs"] / peak)
+    shares = {k: ms * bench.launches_per_eval(k, it) for k, ms in kt.items() if k != "fft_chain"}
+    assert roof["kernel"] == max(shares, key=shares.get) != "fft_chain"
+    assert roof["frac"] == pytest.approx(roof["achieved"] / roof["peak"])
+    assert roof["bound"] == "hbm" and roof["unit"] == "GB/s" and "note" in roof
+    assert sum(r["share"] for r in roof["per_kernel"].values()) == pytest.approx(1.0)
