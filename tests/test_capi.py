@@ -48,3 +48,29 @@ def test_null_engine_rejected():
     L = _lib.load()
     assert L.pgm_engine_set_atoms(None, 1, None, None, None, None, 1) == -1
     assert b"null" in L.pgm_last_error()
+
+
+def test_header_is_plain_c_and_links(tmp_path):
+    """include/pgm_b200.h compiles as strict C99 (a cgo / C caller's view), and a C program links the library and
+    calls its host-only entry points with the header's struct layout (the Python binding's as well)."""
+    import shutil
+    import subprocess
+    from pgm_md_b200 import _lib
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "caller.c"
+    src.write_text(
+        '#include "pgm_b200.h"\n#include <stdio.h>\n'
+        "int main(void) {\n"
+        "    pgm_settings s;\n    pgm_settings_default(&s);\n    double c[15];\n"
+        "    const int rc = pgm_gvdw_series(c, 15);\n"
+        '    printf("%zu %.17g %d %d %.17g\\n", sizeof(pgm_settings), s.cutoff, s.order, rc, c[1]);\n'
+        "    return rc;\n}\n")
+    lib_dir = _lib.LIB_PATH.parent
+    exe = tmp_path / "caller"
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", str(HEADER.parent),
+                    str(src), "-L", str(lib_dir), "-lpgm_b200", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert int(out[0]) == ctypes.sizeof(_lib.PgmSettings)
+    assert float(out[1]) == 0.9 and int(out[2]) == 6 and int(out[3]) == 0 and float(out[4]) == -2.0
