@@ -212,20 +212,21 @@ int pgm_engine_compute_batch(pgm_engine* e, const double* pos, const double* box
                              double* strain, int* iterations);
 
 /* The directed pair list of one periodic system without allocating anything (no counterpart in the
- * reference).  For callers that cannot allocate device memory: code running while its stream is captured into
- * a CUDA graph (cudaMalloc is not allowed there), and MD engines or allocators that own all of the device memory
- * and pass fixed buffers.  Same list as the engine's (the reference's minimum image and r < cutoff test,
+ * reference).  For callers that cannot allocate device memory: MD engines whose memory pool owns all of the
+ * device memory and passes fixed buffers, hosts that reserve their device memory up front, and loops that
+ * cannot afford cudaMalloc's implicit synchronisation of the device.  Same list as the engine's (the reference's minimum image and r < cutoff test,
  * core/pgm_core.cpp:64-87), computed by the engine's own kernels; their scratch lives in one static device
  * array of the library (about 4 MB, held by every GPU that loads the library until exit).
  *   n          atoms, 1..16384 (larger: PGM_ERR_CAPACITY); pos_dev device double n*3; box double[9] (host)
  *   outputs    device int arrays: slot_atom_dev[n] (row s of the list belongs to atom slot_atom_dev[s]),
  *              counts_dev[n] (neighbours in row s), neighbors_dev[n*cap] (row s: atom indices j, both
  *              directions, in a deterministic order); rows longer than cap are cut and the call returns
- *              PGM_ERR_CAPACITY with *max_count (may be NULL) the longest row.
- *   stream     cudaStream_t; the call waits for its own work before returning.
- * The first call on a device looks up the scratch array's device address (make it before any stream capture
- * on that device).  Calls share the scratch: calls that overlap on the GPU (other threads, other streams)
- * race and must be serialised by the caller. */
+ *              PGM_ERR_CAPACITY.  *max_count (may be NULL) receives the longest row on every call.
+ *   stream     cudaStream_t; the call copies its small parameter blocks from host memory to the scratch and
+ *              waits for its own work on this stream before returning.
+ * The first call on a device looks up the scratch array's device address (under a lock).  Calls share the
+ * scratch: calls that overlap on the GPU (other threads, other streams) race and must be serialised by the
+ * caller. */
 int pgm_pair_list_noalloc(int n, const double* pos_dev, const double* box, double cutoff, int cap, int* slot_atom_dev,
                           int* counts_dev, int* neighbors_dev, void* stream, int* max_count);
 

@@ -7,11 +7,13 @@
 #include "pgm_engine.h"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <tuple>
@@ -58,34 +60,53 @@ struct Buf {
     template <class T> T* as() const { return (T*) p; }
 };
 
-// |sum_k M_p(k+1) exp(2 pi i m k/K)|^2 with zeros replaced by the mean of their neighbours: the B-spline
-// moduli of the smooth-PME influence function (the formula of core/pgm_math.h:98-126).
+// The B-spline moduli b(m) = |sum_k M_p(k + 1) exp(2 pi i m k / K)|^2, m < K, of the smooth-PME influence
+// function, with the reference's convention that a modulus below 1e-7 (an interpolation zero, odd p at the
+// Nyquist index) takes the mean of its two neighbours (core/pgm_math.h:98-126 defines the quantity).
+//   * M_p at the integer knots comes from the closed form M_p(x) = 1/(p-1)! sum_{j<x} (-1)^j C(p, j) (x - j)^(p-1),
+//     summed exactly in 128-bit integers (p <= 12 keeps every term below 2^63) and divided once, so every
+//     knot value is correctly rounded;
+//   * M_p(k + 1) vanishes for k >= p - 1, so the transform runs over the support only, and each phase m k is
+//     reduced modulo K before it becomes an angle, which keeps the angles exact for large m k.
 std::vector<double> bsplineModuli(int K, int p) {
-    std::vector<double> M(p + 1, 0.0), tmp(p + 1, 0.0);
-    M[0] = 1.0;
-    for (int k = 2; k <= p; k++) {
-        for (int j = 0; j < k; j++) {
-            const double cur = (j < k - 1 ? M[j] : 0.0), prev = (j > 0 ? M[j - 1] : 0.0);
-            tmp[j] = (j * cur + (k - j) * prev) / (k - 1);
+    if (p < 2 || p > MAXP)
+        throw std::invalid_argument("pgm_b200: spline order outside 2.." + std::to_string(MAXP));
+    auto binom = [](int nn, int kk) {
+        __int128 c = 1;
+        for (int t = 1; t <= kk; t++)
+            c = c * (nn - kk + t) / t;
+        return c;
+    };
+    __int128 factorial = 1;
+    for (int t = 2; t < p; t++)
+        factorial *= t;
+    std::vector<double> knot(p, 0.0);   // knot[x] = M_p(x), x = 1 .. p - 1
+    for (int x = 1; x < p; x++) {
+        __int128 acc = 0;
+        for (int j = 0; j < x; j++) {
+            __int128 pw = 1;
+            for (int t = 0; t < p - 1; t++)
+                pw *= (x - j);
+            acc += ((j & 1) ? -1 : 1) * binom(p, j) * pw;
         }
-        for (int j = 0; j < k; j++)
-            M[j] = tmp[j];
+        knot[x] = (double) ((long double) acc / (long double) factorial);
     }
-    std::vector<double> data(K, 0.0), mod(K), out(K);
-    for (int k = 0; k < p - 1 && k < K; k++)
-        data[k] = M[k + 1];
+    std::vector<double> modulus(K);
     for (int m = 0; m < K; m++) {
-        double sc = 0, ss = 0;
-        for (int k = 0; k < K; k++) {
-            const double arg = 2 * PI_D * m * k / K;
-            sc += data[k] * std::cos(arg);
-            ss += data[k] * std::sin(arg);
+        double re = 0.0, im = 0.0;
+        for (int k = 0; k + 1 < p && k < K; k++) {   // (a grid smaller than the support is not aliased)
+            const long long phase = ((long long) m * k) % K;
+            const double ang = 2.0 * PI_D * (double) phase / (double) K;
+            re += knot[k + 1] * std::cos(ang);
+            im += knot[k + 1] * std::sin(ang);
         }
-        mod[m] = sc * sc + ss * ss;
+        modulus[m] = re * re + im * im;
     }
+    std::vector<double> fixed(modulus);
     for (int m = 0; m < K; m++)
-        out[m] = mod[m] < 1e-7 ? 0.5 * (mod[(m - 1 + K) % K] + mod[(m + 1) % K]) : mod[m];
-    return out;
+        if (modulus[m] < 1e-7)
+            fixed[m] = 0.5 * (modulus[m == 0 ? K - 1 : m - 1] + modulus[m + 1 == K ? 0 : m + 1]);
+    return fixed;
 }
 
 // H^-1 by cofactors and |det H| (core/pgm_core.cpp:94-111).
@@ -1282,6 +1303,29 @@ struct Engine::Impl {
         CU(cudaGetLastError());
     }
 
+    // Ends the work captured so far on st with a conditional node (IF or WHILE on `cond`): the node follows
+    // everything the stream's capture depends on now, and the stream's later captured work follows the node.
+    // Returns the node's body graph, filled by a capture of its own once the main capture has ended.
+    static cudaGraph_t appendConditional(cudaStream_t st, cudaGraphConditionalHandle cond,
+                                         cudaGraphConditionalNodeType kind) {
+        cudaStreamCaptureStatus state = cudaStreamCaptureStatusNone;
+        cudaGraph_t target = nullptr;
+        const cudaGraphNode_t* frontier = nullptr;
+        size_t frontierSize = 0;
+        CU(cudaStreamGetCaptureInfo(st, &state, nullptr, &target, &frontier, &frontierSize));
+        if (state != cudaStreamCaptureStatusActive || !target)
+            throw std::runtime_error("pgm_b200: a conditional node outside an active capture");
+        cudaGraphNodeParams params = {};
+        params.type = cudaGraphNodeTypeConditional;
+        params.conditional.handle = cond;
+        params.conditional.type = kind;
+        params.conditional.size = 1;
+        cudaGraphNode_t added = nullptr;
+        CU(cudaGraphAddNode(&added, target, frontier, frontierSize, &params));
+        CU(cudaStreamUpdateCaptureDependencies(st, &added, 1, cudaStreamSetCaptureDependencies));
+        return params.conditional.phGraph_out[0];
+    }
+
     // The stale test and the build when stale (a conditional node of the graph, its body captured after the main
     // capture; without graphs a host decision).
     void enqueueStaleBuild(cudaStream_t sm, const Dev& d) {
@@ -1289,20 +1333,7 @@ struct Engine::Impl {
         k_displace<<<tb, 256, 0, sm>>>(d);
         CU(cudaGetLastError());
         if (capturing) {
-            cudaStreamCaptureStatus status;
-            const cudaGraphNode_t* deps = nullptr;
-            size_t numDeps = 0;
-            cudaGraph_t g;
-            CU(cudaStreamGetCaptureInfo(sm, &status, nullptr, &g, &deps, &numDeps));
-            cudaGraphNodeParams cp = {};
-            cp.type = cudaGraphNodeTypeConditional;
-            cp.conditional.handle = d.listCond;
-            cp.conditional.type = cudaGraphCondTypeIf;
-            cp.conditional.size = 1;
-            cudaGraphNode_t node;
-            CU(cudaGraphAddNode(&node, g, deps, numDeps, &cp));
-            listBody = cp.conditional.phGraph_out[0];
-            CU(cudaStreamUpdateCaptureDependencies(sm, &node, 1, cudaStreamSetCaptureDependencies));
+            listBody = appendConditional(sm, d.listCond, cudaGraphCondTypeIf);
         } else {
             CU(cudaMemcpyAsync(hFlags, d.flags, 16 * sizeof(int), cudaMemcpyDeviceToHost, sm));
             CU(cudaStreamSynchronize(sm));
@@ -1406,22 +1437,8 @@ struct Engine::Impl {
         listBody = nullptr;
         try {
             enqueuePre<R>(st, side, d);
-            if (s.polarizable) {
-                cudaStreamCaptureStatus status;
-                const cudaGraphNode_t* deps = nullptr;
-                size_t numDeps = 0;
-                cudaGraph_t capturing;
-                CU(cudaStreamGetCaptureInfo(st, &status, nullptr, &capturing, &deps, &numDeps));
-                cudaGraphNodeParams cp = {};
-                cp.type = cudaGraphNodeTypeConditional;
-                cp.conditional.handle = handle;
-                cp.conditional.type = cudaGraphCondTypeWhile;
-                cp.conditional.size = 1;
-                cudaGraphNode_t node;
-                CU(cudaGraphAddNode(&node, capturing, deps, numDeps, &cp));
-                body = cp.conditional.phGraph_out[0];
-                CU(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
-            }
+            if (s.polarizable)   // the CG loop
+                body = appendConditional(st, handle, cudaGraphCondTypeWhile);
             enqueuePost<R>(st, side, d);
         } catch (...) {
             capturing = false;
@@ -1785,44 +1802,46 @@ void Engine::setCandidates(int nseg, const int* segI, const int* segShift, const
         throw std::invalid_argument("pgm_b200: setCandidates: bad segment arrays");
     I.selectDevice();
     const int n = I.n;
-    std::vector<int> start(n + 1, 0);
     const int total = nseg > 0 ? segBegin[nseg] : 0;
     if (nseg > 0 && (segBegin[0] != 0 || total < 0 || (total > 0 && !candJ)))
         throw std::invalid_argument("pgm_b200: setCandidates: segBegin must start at 0 and candJ hold its total");
+    // every candidate as two directed entries (owner, partner, shift of the partner's image seen from the
+    // owner), then grouped by owner with a stable sort, so each row keeps the caller's order
+    struct Directed {
+        int owner, partner, shift;
+    };
+    auto packShift = [](const int* t, int sign) {
+        return (sign * t[0] + 128) | ((sign * t[1] + 128) << 8) | ((sign * t[2] + 128) << 16);
+    };
+    std::vector<Directed> entries;
+    entries.reserve(2 * (size_t) std::max(total, 0));
     for (int sg = 0; sg < nseg; sg++) {
         const int i = segI[sg];
+        const int* t = segShift + 3 * sg;
         if (i < 0 || i >= n || segBegin[sg + 1] < segBegin[sg])
             throw std::invalid_argument("pgm_b200: setCandidates: atom index or segment bounds out of range");
-        for (int a = 0; a < 3; a++)
-            if (segShift[3 * sg + a] < -127 || segShift[3 * sg + a] > 127)
-                throw std::invalid_argument("pgm_b200: setCandidates: box shift out of range");
+        if (std::abs(t[0]) > 127 || std::abs(t[1]) > 127 || std::abs(t[2]) > 127)
+            throw std::invalid_argument("pgm_b200: setCandidates: box shift out of range");
         for (int k = segBegin[sg]; k < segBegin[sg + 1]; k++) {
-            const int j = candJ[k];
-            if (j < 0 || j >= n)
+            if (candJ[k] < 0 || candJ[k] >= n)
                 throw std::invalid_argument("pgm_b200: setCandidates: partner index out of range");
-            start[i + 1]++;
-            start[j + 1]++;
+            entries.push_back({i, candJ[k], packShift(t, 1)});
+            entries.push_back({candJ[k], i, packShift(t, -1)});
         }
     }
-    for (int i = 0; i < n; i++)
-        start[i + 1] += start[i];
-    std::vector<int> fill(start.begin(), start.end() - 1), jj(std::max(1, start[n])), tt(std::max(1, start[n]));
-    auto pack = [](int a, int b, int c) { return (a + 128) | ((b + 128) << 8) | ((c + 128) << 16); };
+    std::stable_sort(entries.begin(), entries.end(),
+                     [](const Directed& a, const Directed& b) { return a.owner < b.owner; });
+    std::vector<int> start(n + 1, 0), jj(std::max<size_t>(1, entries.size())), tt(jj.size());
+    for (size_t k = 0; k < entries.size(); k++) {
+        start[entries[k].owner + 1] = (int) k + 1;   // one past the owner's last entry
+        jj[k] = entries[k].partner;
+        tt[k] = entries[k].shift;
+    }
     int longest = 0;
-    for (int sg = 0; sg < nseg; sg++) {
-        const int i = segI[sg], *t = segShift + 3 * sg;
-        for (int k = segBegin[sg]; k < segBegin[sg + 1]; k++) {
-            const int j = candJ[k];
-            int q = fill[i]++;
-            jj[q] = j;
-            tt[q] = pack(t[0], t[1], t[2]);
-            q = fill[j]++;
-            jj[q] = i;
-            tt[q] = pack(-t[0], -t[1], -t[2]);
-        }
-    }
-    for (int i = 0; i < n; i++)
+    for (int i = 0; i < n; i++) {   // owners without entries continue from their predecessor
+        start[i + 1] = std::max(start[i + 1], start[i]);
         longest = std::max(longest, start[i + 1] - start[i]);
+    }
     CU(cudaStreamSynchronize(I.st));
     upload(I.dCandStart, start, I.st);
     upload(I.dCandJ, jj, I.st);
@@ -1893,22 +1912,22 @@ void Engine::setGvdw(int repulsion, double rvdw, const double* sqrtA, const doub
         gv[4 * i + 2] = b[i];
         gv[4 * i + 3] = 0.0;
     }
-    std::vector<int> start(n + 1, 0);
+    // the skipped pairs in both directions, ordered by (atom, partner); row a is the run of atom a
+    std::vector<std::pair<int, int>> skipped;
+    skipped.reserve(2 * (size_t) nskip);
     for (int k = 0; k < nskip; k++) {
         if (skipI[k] < 0 || skipI[k] >= n || skipJ[k] < 0 || skipJ[k] >= n)
             throw std::invalid_argument("pgm_b200: GVDW skipped pair index out of range");
-        start[skipI[k] + 1]++;
-        start[skipJ[k] + 1]++;
+        skipped.emplace_back(skipI[k], skipJ[k]);
+        skipped.emplace_back(skipJ[k], skipI[k]);
     }
-    for (int i = 0; i < n; i++)
-        start[i + 1] += start[i];
-    std::vector<int> fill(start.begin(), start.end() - 1), part(std::max(1, start[n]));
-    for (int k = 0; k < nskip; k++) {
-        part[fill[skipI[k]]++] = skipJ[k];
-        part[fill[skipJ[k]]++] = skipI[k];
-    }
-    for (int i = 0; i < n; i++)
-        std::sort(part.begin() + start[i], part.begin() + start[i + 1]);
+    std::sort(skipped.begin(), skipped.end());
+    std::vector<int> start(n + 1), part(std::max<size_t>(1, skipped.size()));
+    for (int a = 0; a <= n; a++)
+        start[a] = (int) (std::lower_bound(skipped.begin(), skipped.end(), std::make_pair(a, INT_MIN)) -
+                          skipped.begin());
+    for (size_t k = 0; k < skipped.size(); k++)
+        part[k] = skipped[k].second;
     gvdwSeries(I.gvC, GVDW_TERMS);
     I.selectDevice();
     CU(cudaStreamSynchronize(I.st));
@@ -2451,12 +2470,12 @@ void Engine::computeBatch(const double* pos, const double* boxes, double* energi
 
 // ---------------------------------------------------------------------------------------------- no allocation
 //
-// A pair-list entry point for callers that cannot allocate device memory: code that runs while a caller's
-// CUDA stream is being captured into a graph (cudaMalloc is not allowed there), MD engines and allocators that
-// own every byte of the GPU and hand out fixed buffers, and hosts that reserved the device memory up front.
-// It runs the engine's own cell-list and pair-list kernels, with their scratch (cell counts and offsets, the
-// cell-sorted copies of the atoms) in one statically sized device array instead of engine-owned
-// allocations.  Every GPU that loads the library holds that array (about 4 MB) until the process exits.
+// A pair-list entry point for callers that cannot allocate device memory: MD engines whose memory pool owns
+// every byte of the GPU and hands out fixed buffers, hosts that reserve their device memory up front and must
+// not grow it, and loops that cannot afford cudaMalloc's implicit synchronisation of the whole device.  It runs
+// the engine's own cell-list and pair-list kernels, with their scratch (cell counts and offsets, the
+// cell-sorted copies of the atoms) in one statically sized device array instead of engine-owned allocations.
+// Every GPU that loads the library holds that array (about 4 MB) until the process exits.
 namespace pgmb200 {
 namespace {
 
@@ -2482,13 +2501,28 @@ __global__ void k_entries_to_atoms(const int* slotAtom, const int* counts, int* 
     }
 }
 
-// Device address of the scratch on the current device: looked up on the first call on that device.
+// The longest row before any clamping: the largest count (rows beyond cap already raised flags[0] to their
+// length in the build, so the maximum over both is the longest row either way), into flags[12].
+__global__ void k_longest_row(const int* counts, int n, int* flags) {
+    int m = 0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x)
+        m = max(m, counts[s]);
+    for (int o = 16; o > 0; o >>= 1)
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0)
+        atomicMax(&flags[12], max(m, flags[0]));
+}
+
+// Device address of the scratch on the current device: looked up on the first call on that device, under a
+// lock, so that first calls from several host threads do not race on the table.
 unsigned char* noallocScratch() {
+    static std::mutex lock;
     static unsigned char* addr[64] = {nullptr};
     int dev = 0;
     CU(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64)
         throw std::runtime_error("pgm_b200: device index beyond 63");
+    std::lock_guard<std::mutex> guard(lock);
     if (!addr[dev]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
@@ -2608,12 +2642,13 @@ int pairListNoAlloc(int n, const double* posDev, const double* box, double cutof
     k_cell_sort<<<(S.cellCount + 7) / 8, 256, 0, st>>>(d);
     k_build_list<<<S.cellCount, LIST_THREADS, 0, st>>>(d);
     k_entries_to_atoms<<<n, 128, 0, st>>>(slotAtomOut, countsOut, neighborsOut, cap, n);
+    k_longest_row<<<std::min((n + 255) / 256, 64), 256, 0, st>>>(countsOut, n, flags);
     CU(cudaGetLastError());
     int hflags[16];
     CU(cudaMemcpyAsync(hflags, flags, sizeof(hflags), cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
     if (maxCount)
-        *maxCount = hflags[0];
+        *maxCount = hflags[12];
     return hflags[0] > cap ? 1 : 0;
 }
 

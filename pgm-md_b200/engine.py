@@ -423,9 +423,10 @@ class Engine:
 def pair_list_noalloc(n, pos_dev_ptr, box, cutoff, cap, slot_atom_ptr, counts_ptr, neighbors_ptr, stream_ptr=0):
     """The directed pair list of one periodic system into caller-owned device buffers, allocating nothing
     (pgm_pair_list_noalloc of include/pgm_b200.h): for callers that cannot allocate device memory, such as
-    code running inside a stream capture or under an allocator that owns the whole GPU.  Buffers are raw
-    device pointers: positions double n*3; slot_atom int n, counts int n, neighbors int n*cap.  Returns the
-    longest row; raises PgmError (status -4) when n exceeds 16384 or a row exceeds cap."""
+    MD engines whose memory pool owns the whole GPU, or hosts that reserve their device memory up front.
+    Buffers are raw device pointers: positions double n*3; slot_atom int n, counts int n, neighbors int n*cap.
+    Returns the longest row; raises PgmError (status -4, with .max_count the longest row) when n exceeds 16384
+    or a row exceeds cap.  The call waits for its own work on the stream before it returns."""
     L = _lib.load()
     box = _f64(box)
     mx = ctypes.c_int(0)

@@ -22,7 +22,7 @@ the fixtures travel, the reference does not):
                     them); coordinates, forces and dipoles as float32 (the coordinates are the inputs of both
                     the reference run and the tests, so their rounding is part of the case).
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle && PGM_REFERENCE=<reference tree> python tests/golden/make_golden.py [--ref <reference tree>]
 """
 
 from __future__ import annotations
@@ -35,7 +35,17 @@ from pathlib import Path
 import numpy as np
 
 ROOT = Path(__file__).resolve().parents[2]
-REF = Path("/root/reference")
+def _reference_tree() -> Path:
+    """The reference tree: --ref <path>, else $PGM_REFERENCE (no default: the fixtures are made where it lies)."""
+    import os
+    if "--ref" in sys.argv:
+        return Path(sys.argv[sys.argv.index("--ref") + 1])
+    if os.environ.get("PGM_REFERENCE"):
+        return Path(os.environ["PGM_REFERENCE"])
+    raise SystemExit("make_golden.py: give the reference tree with --ref <path> or PGM_REFERENCE")
+
+
+REF = _reference_tree() if __name__ == "__main__" else None
 OUT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
