@@ -240,6 +240,16 @@ def water_batch(nsys=1024, seed=1024, nmin=8, nmax=512, density=0.0334, tol=1e-5
     return out
 
 
+def water64_boxes(nsys=256, seed=5000, density=0.0334, tol=1e-8):
+    """The differentiation workload's boxes: ``nsys`` boxes of 64 waters built as water216 is (4^3 jittered
+    lattice, random orientations, the same parameters) at 0.0334 molecules/A^3 (L = 12.4 A), grid the smallest
+    2-3-5 size >= L / 1 A (15^3), cutoff L/2, beta 0.35/A; box k has seed ``seed + k``."""
+    L = (64 / density) ** (1.0 / 3.0)
+    K = fft_size(L / 1.0)
+    return [waters(64, L, seed=seed + k, grid=(K, K, K), cutoff=min(9.0, L / 2.0), tol=tol, lattice=4,
+                   name=f"water64[{k}]") for k in range(nsys)]
+
+
 def perturbed(sys_: System, rel=0.05, seed=0):
     """The same system with every parameter scaled by (1 + N(0, rel)) per atom type / dipole type."""
     rng = np.random.default_rng(seed)

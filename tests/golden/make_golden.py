@@ -14,6 +14,11 @@ the fixtures travel, the reference does not):
                     tests/gvdw_input.py: 512 waters, reduced triclinic box, radii, which atoms carry the van der
                     Waals term, the prmtop's excluded pairs) with pmemd-pgm's energies of it at 1 nm for the two
                     repulsion forms and their parameters (core/tests/test_gvdw.cpp:66-70).
+  ref_water98304.npz           pgm_core on the 98304-atom water box (tol 1e-10; forces and dipoles float32)
+  ref_water_batch_sample.npz   pgm_core on a stratified sample of 32 of the 1024 batch boxes (tol 1e-10)
+  grad_water64x16.npz,
+  grad_dimethylphenol8550.npz  central differences of pgm_core's energy and force-matching loss per parameter
+                               type (GOLDEN_GRAD_TOL=1e-12 python tests/golden/make_golden.py grad)
   dmp8550_real.npz  the reference's real 8550-atom dimethylphenol liquid (amber/test/dmp: pGM parameters from
                     the POL_GAUSS_* sections of prmtop.gz, coordinates and box from the NetCDF restart restrt0)
                     with the benchmark's settings (cutoff 0.9 nm, beta 3.5 / nm, 48^3, order 6), and pgm_core's
@@ -28,6 +33,7 @@ the fixtures travel, the reference does not):
 from __future__ import annotations
 
 import importlib.util
+import os
 import re
 import sys
 from pathlib import Path
@@ -216,8 +222,176 @@ def ref_outputs():
         print(f"ref_{name}.npz", S.n, "atoms", e, eng.iterations(), "iterations", len(i), "pairs")
 
 
+TERM_NAMES = ("direct", "reciprocal", "self", "background", "polarization")
+
+
+def _ref_eval(S, tol, want=("forces", "mu")):
+    """One pgm_core evaluation (the reference itself, oracle/_ref) at tol, predictor none, peek 0."""
+    from oracle import pgm_oracle as O
+    from oracle import ref as R
+    systems = load_systems()
+    top = O.Topology(S.q, S.radius, S.alpha, S.cov_atom, S.cov_partner, S.cov_strength)
+    st = O.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=tol, max_iter=1000, peek=0.0,
+                    predictor=0, ke=systems.KE_DEFAULT)
+    eng = R.RefEngine(top, st)
+    e = eng.compute(S.pos, S.box)
+    t = eng.terms()
+    out = dict(energy=e, terms=np.array([t[k] for k in TERM_NAMES]), strain=eng.strain(),
+               iterations=eng.iterations())
+    if "forces" in want:
+        out["forces"] = eng.forces.copy()
+    if "mu" in want:
+        out["mu"] = eng.induced()
+    return out
+
+
+def water98304_ref():
+    """The 98304-atom water box (32768 waters, 104^3) through pgm_core at tol 1e-10: terms, strain, iterations,
+    forces and induced dipoles (float32), and a digest of the generator's positions."""
+    systems = load_systems()
+    S = systems.water98304()
+    r = _ref_eval(S, 1e-10)
+    np.savez_compressed(OUT / "ref_water98304.npz", pos_digest=np.array([S.pos.sum(), (S.pos ** 2).sum()]),
+                        energy=r["energy"], terms=r["terms"], strain=r["strain"], iterations=r["iterations"],
+                        forces=r["forces"].astype(np.float32), mu=r["mu"].astype(np.float32), tol=1e-10)
+    print("ref_water98304.npz", S.n, "atoms", r["energy"], r["iterations"], "iterations")
+
+
+def batch_sample_indices(systems_list, per_grid=3):
+    """A stratified sample of the 1024-box batch: every box of the largest molecule count, and per distinct grid
+    shape its smallest, its largest and its median box (at least one of each shape)."""
+    counts = np.array([len(S.q) for S in systems_list])
+    grids = np.array([S.grid[0] for S in systems_list])
+    pick = set(np.flatnonzero(counts == counts.max()).tolist())
+    for K in sorted(set(grids.tolist())):
+        idx = np.flatnonzero(grids == K)
+        order = idx[np.argsort(counts[idx], kind="stable")]
+        for k in {0, len(order) // 2, len(order) - 1} if per_grid >= 3 else {0}:
+            pick.add(int(order[k]))
+    return np.array(sorted(pick))
+
+
+def batch_sample_ref():
+    """pgm_core at tol 1e-10 on a stratified sample of the 1024 water boxes (water_batch(), seed 1024):
+    per-system terms, strain, iterations, forces (float32) and induced dipoles (float32), concatenated in the
+    sample's order."""
+    systems = load_systems()
+    boxes = systems.water_batch()
+    sample = batch_sample_indices(boxes)
+    rows = [_ref_eval(boxes[k], 1e-10) for k in sample]
+    np.savez_compressed(OUT / "ref_water_batch_sample.npz", sample=sample,
+                        natoms=np.array([len(boxes[k].q) for k in sample]),
+                        grid=np.array([boxes[k].grid[0] for k in sample]),
+                        energy=np.array([r["energy"] for r in rows]), terms=np.stack([r["terms"] for r in rows]),
+                        strain=np.stack([r["strain"] for r in rows]),
+                        iterations=np.array([r["iterations"] for r in rows]),
+                        forces=np.concatenate([r["forces"] for r in rows]).astype(np.float32),
+                        mu=np.concatenate([r["mu"] for r in rows]).astype(np.float32), tol=1e-10)
+    print("ref_water_batch_sample.npz", len(sample), "boxes, grids", sorted(set(boxes[k].grid[0] for k in sample)))
+
+
+def _with_params(S, name, values):
+    from dataclasses import replace
+    return replace(S, **{name: values})
+
+
+def _as_fields(S):
+    return {k: getattr(S, k) for k in S.__dataclass_fields__}
+
+
+def _fd_job(args):
+    """(+h, -h) energies and forces of pgm_core with one per-type parameter moved (a worker of the FD pool; the
+    system travels as its fields)."""
+    fields, name, t, h, tol = args
+    S = load_systems().System(**fields)
+    out = []
+    for sgn in (1.0, -1.0):
+        vals = getattr(S, name).copy()
+        idx = (S.cov_types if name == "cov_strength" else S.types) == t
+        vals[idx] += sgn * h
+        r = _ref_eval(_with_params(S, name, vals), tol, want=("forces",))
+        out.append((r["energy"], r["forces"]))
+    return out
+
+
+PARAM_NAMES = ("q", "cov_strength", "alpha", "radius")
+
+
+def type_values(S, name):
+    ty = S.cov_types if name == "cov_strength" else S.types
+    v = np.zeros(int(ty.max()) + 1)
+    v[ty] = getattr(S, name)
+    return v
+
+
+def gradient_fixture(S, F_target, tol, pool):
+    """Central differences (h = 1e-5 relative to the type's value) of pgm_core's energy and of the force-matching
+    loss L = sum |F - F_target|^2 per parameter type, plus the energy and L at the unperturbed parameters."""
+    jobs, keys = [], []
+    for name in PARAM_NAMES:
+        vals = type_values(S, name)
+        for t in range(len(vals)):
+            h = 1e-5 * abs(vals[t])
+            jobs.append((_as_fields(S), name, t, h, tol))
+            keys.append((name, t, h))
+    res = pool.map(_fd_job, jobs)
+    out = {}
+    for (name, t, h), ((ep, fp), (em, fm)) in zip(keys, res):
+        lp = float(np.sum((fp - F_target) ** 2))
+        lm = float(np.sum((fm - F_target) ** 2))
+        out.setdefault("dE_" + name, []).append((ep - em) / (2 * h))
+        out.setdefault("dL_" + name, []).append((lp - lm) / (2 * h))
+    r0 = _ref_eval(S, tol, want=("forces",))
+    out = {k: np.array(v) for k, v in out.items()}
+    out["energy"] = r0["energy"]
+    out["loss"] = float(np.sum((r0["forces"] - F_target) ** 2))
+    return out
+
+
+def gradients_ref():
+    """Gradient goldens of the differentiation workload (FP64 pgm_core, central differences with h = 1e-5
+    relative, at tol $GOLDEN_GRAD_TOL; the committed files use 1e-12, where the differences carry no CG noise,
+    while the tests run the engine at the workload's 1e-8): (a) 16 of the 256 boxes of 64 waters, (b) the
+    8550-atom dimethylphenol liquid.  The
+    force-matching target F_target is pgm_core's forces with every per-type parameter scaled by
+    (1 + N(0, 0.05)) (systems.perturbed, seed 1 + box index), stored with the fixture."""
+    import multiprocessing as mp
+    systems = load_systems()
+    tol = float(os.environ.get("GOLDEN_GRAD_TOL", "1e-8"))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(int(os.environ.get("GOLDEN_PROCS", "8"))) as pool:
+        boxes = systems.water64_boxes()
+        sel = np.arange(16)
+        fx = {}
+        for k in sel:
+            S = boxes[k]
+            St = systems.perturbed(S, rel=0.05, seed=1 + int(k))
+            Ft = _ref_eval(St, tol, want=("forces",))["forces"]
+            g = gradient_fixture(S, Ft, tol, pool)
+            fx[f"b{k}_Ft"] = Ft
+            for key, v in g.items():
+                fx[f"b{k}_{key}"] = v
+            print("water64 box", k, "E", g["energy"], "L", g["loss"])
+        np.savez_compressed(OUT / "grad_water64x16.npz", boxes=sel, tol=tol, **fx)
+        S = systems.dimethylphenol8550(tol=tol)
+        St = systems.perturbed(S, rel=0.05, seed=8550)
+        Ft = _ref_eval(St, tol, want=("forces",))["forces"]
+        g = gradient_fixture(S, Ft, tol, pool)
+        np.savez_compressed(OUT / "grad_dimethylphenol8550.npz", tol=tol, Ft=Ft,
+                            **{k: v for k, v in g.items()})
+        print("dimethylphenol8550 E", g["energy"], "L", g["loss"])
+
+
 if __name__ == "__main__":
     which = sys.argv[1:] or ["w512", "ref", "dmp", "gvdw"]
+    which = [w for w in which if not w.startswith("--") and w != (sys.argv[sys.argv.index("--ref") + 1]
+                                                                  if "--ref" in sys.argv else None)]
+    if "water98304" in which:
+        water98304_ref()
+    if "batch" in which:
+        batch_sample_ref()
+    if "grad" in which:
+        gradients_ref()
     if "w512" in which:
         w512()
     if "ref" in which:

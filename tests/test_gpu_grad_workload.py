@@ -1,0 +1,117 @@
+"""The differentiation workload at its own sizes: per-type parameter gradients of the total energy and of the
+force-matching loss L = sum |F - F_target|^2 on (a) 16 of the 256 boxes of 64 waters, in one batched launch,
+and (b) the 8550-atom dimethylphenol liquid, with the engine at the workload's tol 1e-8.
+
+The goldens (tests/golden/grad_*.npz, from tests/golden/make_golden.py) are central differences of the
+reference pgm_core itself (h = 1e-5 relative to each type's value) with F_target from pgm_core at every
+per-type parameter scaled by (1 + N(0, 0.05)); they are taken at tol 1e-12 so that the differences carry no CG
+noise.  Bar: 1e-5 relative, per parameter kind as a vector norm and per element against the larger of the
+element and 1e-3 of the kind's largest element (the energy differences of a 2.7e5 kJ/mol system resolve small
+gradients only to about 1e-4 of their size)."""
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, PKG
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ("q", "cov_strength", "alpha", "radius")
+
+
+def per_type(values, index, ntypes):
+    out = np.zeros(ntypes)
+    np.add.at(out, index, values)
+    return out
+
+
+def check(got, fd, what, lim=1e-5):
+    got = np.asarray(got, np.float64)
+    fd = np.asarray(fd, np.float64)
+    assert np.linalg.norm(got - fd) <= lim * np.linalg.norm(fd), (what, got, fd)
+    floor = 1e-3 * np.abs(fd).max()
+    assert (np.abs(got - fd) <= lim * np.maximum(np.abs(fd), floor) + 1e-300).all(), (what, got, fd)
+
+
+def engine(S, precision, tol=1e-8):
+    e = PKG.Engine(PKG.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=6, tol=tol, max_iter=1000, peek=0.0,
+                                predictor=0, ke=PKG.systems.KE_DEFAULT, precision=precision))
+    return e
+
+
+@pytest.fixture(scope="module")
+def water64():
+    d = np.load(GOLDEN / "grad_water64x16.npz")
+    boxes = PKG.systems.water64_boxes(nsys=int(d["boxes"].max()) + 1)
+    return [boxes[int(k)] for k in d["boxes"]], d
+
+
+@pytest.mark.parametrize("precision", [PKG.FP64, PKG.MIXED])
+def test_water64_batch_energy_gradients(water64, precision):
+    boxes, d = water64
+    eng = engine(boxes[0], precision)
+    eng.set_systems(boxes)
+    out = eng.compute_batch(np.concatenate([s.pos for s in boxes]), np.stack([s.box for s in boxes]))
+    g = eng.param_grad()
+    eng.close()
+    off, coff = 0, 0
+    for k, S in zip(d["boxes"], boxes):
+        assert abs(out["energies"][list(d["boxes"]).index(k), :5].sum() - float(d[f"b{k}_energy"])) <= \
+            1e-6 * abs(float(d[f"b{k}_energy"]))
+        for name in NAMES:
+            if name == "cov_strength":
+                part, ty = g[name][coff:coff + len(S.cov_atom)], S.cov_types
+            else:
+                part, ty = g[name][off:off + S.n], S.types
+            fd = d[f"b{k}_dE_{name}"]
+            check(per_type(part, ty, len(fd)), fd, (int(k), name))
+        off += S.n
+        coff += len(S.cov_atom)
+
+
+def test_water64_force_matching_gradients(water64):
+    grad_mod = __import__("pgm_md_b200.autograd", fromlist=["autograd"])
+    boxes, d = water64
+    for k, S in zip(d["boxes"], boxes):
+        eng = engine(S, PKG.FP64)
+        eng.set_system(S)
+        L, g, _ = grad_mod.force_matching_atom_grads(eng, S, d[f"b{k}_Ft"], tol=1e-8)
+        eng.close()
+        assert abs(L - float(d[f"b{k}_loss"])) <= 1e-6 * float(d[f"b{k}_loss"])
+        for name in NAMES:
+            ty = S.cov_types if name == "cov_strength" else S.types
+            fd = d[f"b{k}_dL_{name}"]
+            check(per_type(g[name], ty, len(fd)), fd, (int(k), name))
+
+
+@pytest.fixture(scope="module")
+def dmp():
+    d = np.load(GOLDEN / "grad_dimethylphenol8550.npz")
+    return PKG.systems.dimethylphenol8550(tol=1e-8), d
+
+
+@pytest.mark.parametrize("precision", [PKG.FP64, PKG.MIXED])
+def test_dimethylphenol8550_energy_gradients(dmp, precision):
+    S, d = dmp
+    eng = engine(S, precision)
+    eng.set_system(S)
+    r = eng.compute(S.pos, S.box)
+    g = eng.param_grad()
+    eng.close()
+    assert abs(r.energy - float(d["energy"])) <= 1e-6 * abs(float(d["energy"]))
+    for name in NAMES:
+        ty = S.cov_types if name == "cov_strength" else S.types
+        check(per_type(g[name], ty, len(d["dE_" + name])), d["dE_" + name], name)
+
+
+def test_dimethylphenol8550_force_matching_gradients(dmp):
+    grad_mod = __import__("pgm_md_b200.autograd", fromlist=["autograd"])
+    S, d = dmp
+    eng = engine(S, PKG.FP64)
+    eng.set_system(S)
+    L, g, _ = grad_mod.force_matching_atom_grads(eng, S, d["Ft"], tol=1e-8)
+    eng.close()
+    assert abs(L - float(d["loss"])) <= 1e-6 * float(d["loss"])
+    for name in NAMES:
+        ty = S.cov_types if name == "cov_strength" else S.types
+        check(per_type(g[name], ty, len(d["dL_" + name])), d["dL_" + name], name)
