@@ -164,39 +164,48 @@ def traffic_of(kernel):
 
 
 def algorithmic_bytes(kernel, S, precision, it):
-    """Algorithmic bytes per launch of the main kernels (the bytes each must move at least, per unit: atom,
-    directed pair, grid point): s = real size, g = grid real size, P = directed pairs, p = order."""
+    """Algorithmic bytes per launch of the main kernels, the minimum each must move (per unit: atom, directed
+    pair, grid point): s = real size, g = grid real size (= s), P = directed pairs within the cutoff,
+    p = order, G = K1 K2 K3, G_c = K1 K2 (K3/2 + 1):
+      spread      N (7 s + p^3 g)          q, d, base, fraction in; p^3 grid updates
+      gather      N (7 s + 3 s + p^3 g)    the same in, p^3 grid reads, the field out
+      pair field  P 4 + N 10 s             a list index per pair, own position, charge and dipole, field out
+      FFT chain   2 (G g + 2 G_c g) + 4 G_c g   r2c and c2r, the convolution (read F and G, write F)
+      CG update   3 N 8 10                 ten FP64 vector streams of 3N
+      pair list   N 24 + P 4               positions in, list entries out
+      final pass  P 4 + N (10 s + 128)     a list index per pair, the sources, 16 doubles out per atom"""
     s = 4 if precision else 8
+    g = s
     n, p = S.n, S.order
     P = S.meta.get("pairs", 0)
     K1, K2, K3 = S.grid
     G = K1 * K2 * K3
     Gc = K1 * K2 * (K3 // 2 + 1)
-    if kernel == "spread":           # q, d, base, fraction in; p^3 grid updates
-        return n * (7 * s + p ** 3 * s)
-    if kernel == "gather":           # splines in, p^3 grid reads, 3 field values out
-        return n * (7 * s + 3 * 8 + p ** 3 * s)
-    if kernel == "pair_field":       # mixed: per directed pair a 24 B record (x, G1 | G2, slot of j); FP64: 4 B entry
-        # + (G1, G2); per atom: (d, q) in R (gathered, each once), position (FP64), field out (24 B)
-        if precision:
-            return P * 24 + n * (4 * s + 24)
-        return P * (4 + 2 * s) + n * (32 + 4 * s + 24)
-    if kernel == "fft_chain":        # r2c + convolution (read F, G, write F) + c2r
-        return 2 * (G * s + Gc * 2 * s) + Gc * (2 * s + s + 2 * s)
-    if kernel == "pair_list":        # build + compaction (skin 0): slot-order positions, wraps and radii read, the
-        # list written and read back, the entries and pair records of the evaluation written
+    return {"spread": n * (7 * s + p ** 3 * g), "gather": n * (7 * s + 3 * s + p ** 3 * g),
+            "pair_field": P * 4 + n * 10 * s, "fft_chain": 2 * (G * g + 2 * Gc * g) + 4 * Gc * g,
+            "cg_update": 3 * n * 8 * 10, "pair_list": n * 24 + P * 4,
+            "pair_final": P * 4 + n * (10 * s + 128)}.get(kernel)
+
+
+def design_bytes(kernel, S, precision):
+    """The bytes the engine's own data layout moves per launch, where it differs from the algorithmic figure:
+    the pair passes stream a record per directed pair (mixed: x, G1 | G2, slot of j, 24 B; FP64: the 4 B entry
+    and (G1, G2)) instead of recomputing the radial kernels."""
+    s = 4 if precision else 8
+    n, P = S.n, S.meta.get("pairs", 0)
+    if kernel == "pair_field":
+        return P * 24 + n * (4 * s + 24) if precision else P * (4 + 2 * s) + n * (32 + 4 * s + 24)
+    if kernel == "pair_list":
         rec = 24 if precision else 2 * s
         return n * (32 + 32 + 16 + 8) + P * (4 + 4 + 4 + rec)
-    if kernel == "pair_final":
-        return P * 4 + n * (32 + 4 * s + 8 * 16)
-    if kernel == "cg_update":
-        return n * 3 * 8 * 6
-    return None
+    return algorithmic_bytes(kernel, S, precision, 0)
 
 
-def roofline_table(S, kt, it, precision):
-    """Per-kernel algorithmic bandwidth against the measured HBM copy bandwidth; the dominant kernel is the
-    engine's own kernel with the largest share of an evaluation (the cuFFT chain is listed beside it)."""
+def roofline_table(S, kt, it, precision, kt_cold=None):
+    """Per-kernel algorithmic bandwidth against the measured HBM copy bandwidth.  Each kernel is relaunched
+    alone on the engine's stream: warm (back to back, as inside an evaluation: inputs that fit the 126 MB L2
+    stay there) and cold (L2 overwritten before each launch).  The dominant kernel is the engine's own kernel
+    with the largest share of an evaluation (the FFT chain, cuFFT's or the grid kernel, is listed beside it)."""
     peak, peak_kind = peaks()
     share = {k: v * launches_per_eval(k, it) for k, v in kt.items()}
     total = sum(share.values())
@@ -204,19 +213,29 @@ def roofline_table(S, kt, it, precision):
     for k, ms in kt.items():
         alg = algorithmic_bytes(k, S, precision, it)
         ach = alg / (ms * 1e-3) / 1e9 if alg else None
-        per[k] = {"ms_per_launch": ms, "launches_per_eval": launches_per_eval(k, it), "share": share[k] / total,
-                  "bytes_per_launch": alg, "achieved_gbs": ach, "frac": ach / peak if ach else None}
+        row = {"ms_per_launch": ms, "launches_per_eval": launches_per_eval(k, it), "share": share[k] / total,
+               "bytes_per_launch": alg, "achieved_gbs": ach, "frac": ach / peak if ach else None,
+               "design_bytes": design_bytes(k, S, precision)}
+        if kt_cold:
+            mc = kt_cold[k]
+            row.update({"ms_per_launch_cold": mc, "achieved_gbs_cold": alg / (mc * 1e-3) / 1e9,
+                        "frac_cold": alg / (mc * 1e-3) / 1e9 / peak})
+        per[k] = row
     own = {k: v for k, v in share.items() if k != "fft_chain"}
     dom = max(own, key=own.get)
-    return {"kernel": dom, "bound": "hbm", "achieved": per[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
-            "frac": per[dom]["frac"], "peak_source": peak_kind, "traffic": traffic_of(dom),
-            "bytes_per_launch": per[dom]["bytes_per_launch"], "ms_per_launch": kt[dom],
-            "fft_chain_share": per["fft_chain"]["share"], "per_kernel": per,
-            "note": "each kernel relaunched alone, back to back on the engine's stream (no L2 flush between "
-                    "launches, as inside an evaluation): where its data fits in the 126 MB L2 (the 8550-atom "
-                    "workload's 61 MB of pair records) it is served from L2, and frac is its algorithmic "
-                    "bytes per second against the HBM copy figure; traffic is the DRAM bytes of one cold "
-                    "launch (ncu), which equal the algorithmic bytes"}
+    out = {"kernel": dom, "bound": "hbm", "achieved": per[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
+           "frac": per[dom]["frac"], "peak_source": peak_kind, "traffic": traffic_of(dom),
+           "bytes_per_launch": per[dom]["bytes_per_launch"], "design_bytes": per[dom]["design_bytes"],
+           "ms_per_launch": kt[dom], "fft_chain_share": per["fft_chain"]["share"], "per_kernel": per,
+           "bytes_convention": "algorithmic bytes per launch (pair field P*4 + N*10s, spread N(7s + p^3 g), "
+                               "gather N(10s + p^3 g), ...); design_bytes: what the engine's layout moves",
+           "note": "frac: warm relaunches (back to back, inputs that fit the 126 MB L2 stay there, as inside an "
+                   "evaluation); frac_cold: L2 overwritten before each launch; traffic: DRAM bytes of one cold "
+                   "launch from the committed ncu summary"}
+    if kt_cold:
+        out["frac_cold"] = per[dom]["frac_cold"]
+        out["ms_per_launch_cold"] = kt_cold[dom]
+    return out
 
 
 def md_positions(S, phase, count):
@@ -295,10 +314,12 @@ def reference_arm(args):
     line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus, "steps": steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * total / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-            "config": config(S, {"implementation": "reference pgm_core (core/pgm_core.cpp) FP64, one process per core",
-                                 "step": f"{cores} evaluations in parallel, one per process"}),
+            "config": config(S, {"parallelism": "1 GPU"}),
+            "reference_impl": {"implementation": "reference pgm_core (core/pgm_core.cpp) FP64, one process per core",
+                               "step": f"{cores} evaluations in parallel, one per process"},
             "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "reference",
-                             "sample": f"{steps} steps x {cores} full evaluations of {WORKLOAD}"},
+                             "sample": f"{steps} steps x {cores} full evaluations of {WORKLOAD}",
+                             "cpu": cpu_model()},
             "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     line["cpu_other_configs"] = cpu_other_configs(pkg, cores, ctx, args.ref_large)
     if not args.no_reference_gpu:
@@ -613,23 +634,31 @@ def main():
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = world * e2e_steps / float(t.item())
-    # roofline of the dominant kernel (relaunched alone, CUDA events on the engine's stream)
+    # roofline of the dominant kernel (relaunched alone, CUDA events on the engine's stream): warm, and cold with
+    # the L2 overwritten before every launch
     mixed.compute(S.pos, S.box)
     it = mixed.iterations()
     kt = mixed.kernel_times(reps=20)
-    roof = roofline_table(S, kt, it, 1)
+    kt_cold = mixed.kernel_times(reps=10, flush_ptr=flush.data_ptr(), flush_bytes=flush.numel() * 4)
+    roof = roofline_table(S, kt, it, 1, kt_cold)
     fp64.compute(S.pos, S.box)
     kt64 = fp64.kernel_times(reps=10)
+    kt64_cold = fp64.kernel_times(reps=5, flush_ptr=flush.data_ptr(), flush_bytes=flush.numel() * 4)
+    roof64 = roofline_table(S, kt64, fp64.iterations(), 0, kt64_cold)
     md = md_leg(pkg, S, make, lanes, dev)
     line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
             "config": config(S, {"parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                                  "pair_lanes": lanes, "transforms": TRANSFORMS[mixed.transforms()],
-                                 "cg_iterations": int(np.median(its_mixed))}),
+                                 "cg_iterations": int(np.median(its_mixed)),
+                                 "fp64_evals_per_s": fp64_value, "mixed_over_fp64": value / fp64_value}),
             "fp64": {"value": fp64_value, "unit": "evals/s", "steps": fsteps, "pair_lanes": lanes64,
                      "transforms": TRANSFORMS[fp64.transforms()],
-                     "cg_iterations": int(np.median(its_fp64)), "kernel_ms": kt64},
+                     "cg_iterations": int(np.median(its_fp64)), "kernel_ms": kt64,
+                     "roofline_per_kernel": roof64["per_kernel"],
+                     "autotune_ms": getattr(fp64, "autotune_report", None)},
+            "autotune_ms": getattr(mixed, "autotune_report", None),
             "mixed_over_fp64": value / fp64_value,
             "kept_list": {"value": kept_value, "unit": "evals/s", "steps": fsteps, "list_builds": kept_builds,
                           "note": "mixed, Verlet list kept (skin 0.15 nm, positions unchanged): the reference "
@@ -701,7 +730,12 @@ def large_leg(pkg, local, world, dist):
                               "ns_per_day_2fs": v / world * 86400 * 2e-6, "cg_iterations": res["r"].iterations}
         if tol == 1e-5:
             kt = eng.kernel_times(reps=5)
+            flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+            kt_cold = eng.kernel_times(reps=5, flush_ptr=flush.data_ptr(), flush_bytes=flush.numel() * 4)
+            del flush
+            S.meta["pairs"] = eng.num_candidates()
             out["kernel_ms"] = kt
+            out["roofline_per_kernel"] = roofline_table(S, kt, res["r"].iterations, 1, kt_cold)["per_kernel"]
         eng.close()
     return out
 
@@ -742,7 +776,8 @@ def batch_leg(pkg, local, rank, world, dist):
     kt = eng.kernel_times(reps=3)
     npairs = eng.num_candidates()
     peak, peak_kind = peaks()
-    pf_bytes = npairs * 24 + eng.n * 40
+    pf_bytes = npairs * 4 + eng.n * 40          # the algorithmic bytes: a list index per pair, 10 reals per atom
+    pf_design = npairs * 24 + eng.n * 40        # the engine's 24 B pair records
     pf_gbs = pf_bytes / (kt["pair_field"] * 1e-3) / 1e9
     energies = sh.gather_energies(parts[rank], res["r"]["energies"], len(systems))
     out = {"workload": "water_batch1024", "systems": len(systems), "atoms": int(sum(s.n for s in systems)),
@@ -752,7 +787,9 @@ def batch_leg(pkg, local, rank, world, dist):
            "ms_per_batch_by_transforms": {TRANSFORMS[m]: 1e3 * v for m, v in per_mode.items()},
            "directed_pairs": npairs, "kernel_ms": kt,
            "pair_field_roofline": {"bound": "hbm", "bytes_per_launch": pf_bytes, "achieved": pf_gbs, "peak": peak,
-                                   "unit": "GB/s", "frac": pf_gbs / peak, "peak_source": peak_kind},
+                                   "unit": "GB/s", "frac": pf_gbs / peak, "peak_source": peak_kind,
+                                   "design_bytes": pf_design,
+                                   "design_frac": pf_design / (kt["pair_field"] * 1e-3) / 1e9 / peak},
            "energies_finite": bool(np.isfinite(energies).all())}
     eng.close()
     if rank == 0:
@@ -836,27 +873,44 @@ def _oracle_reference(pkg, S, tol):
     top = O.Topology(S.q, S.radius, S.alpha, S.cov_atom, S.cov_partner, S.cov_strength)
     st = O.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=tol, max_iter=1000, peek=0.0,
                     predictor=0, ke=pkg.systems.KE_DEFAULT)
+    names = ("direct", "reciprocal", "self", "background", "polarization")
     if R.available():
         e = R.RefEngine(top, st)
         E = e.compute(S.pos, S.box)
-        return E, e.forces, "reference pgm_core (oracle/_ref), tol 1e-10"
+        t = e.terms()
+        return dict(energy=E, forces=e.forces, terms=[t[k] for k in names], mu=e.induced(), strain=e.strain(),
+                    kind="reference pgm_core (oracle/_ref), tol 1e-10")
     e = O.Engine(top, st)
     E = e.compute(S.pos, S.box)
-    return E, e.forces, "numpy oracle, tol 1e-10"
+    return dict(energy=E, forces=e.forces, terms=[e.terms[k] for k in names], mu=e.mu, strain=e.strain,
+                kind="numpy oracle, tol 1e-10")
 
 
 def accuracy(pkg, S, mixed, fp64, make_refined=None):
-    """Errors of the GPU paths (at the benchmark tolerance) against the FP64 oracle at tol 1e-10; the mixed
-    path with FP64 refinement also timed (host call, direct launches)."""
-    E0, F0, kind = _oracle_reference(pkg, S, 1e-10)
-    out = {"oracle": kind}
+    """Errors of the GPU paths (at the benchmark tolerance) against the FP64 oracle at tol 1e-10: the total
+    energy, every energy term (relative to the term, and to the total), the forces (relative RMS), the strain
+    derivative and the induced dipoles (relative RMS and largest component error relative to the largest
+    dipole); the mixed path with FP64 refinement also timed (host call, direct launches)."""
+    ref = _oracle_reference(pkg, S, 1e-10)
+    E0, F0, mu0 = ref["energy"], ref["forces"], ref["mu"]
+    out = {"oracle": ref["kind"]}
     engines = [("mixed", mixed), ("fp64", fp64)]
     if make_refined is not None:
         engines.append(("mixed_fp64_refined", make_refined()))
+    names = ("direct", "reciprocal", "self", "background", "polarization")
     for name, eng in engines:
         r = eng.compute(S.pos, S.box)
+        mu = eng.induced_dipoles()
+        td = r.terms.as_dict()
         out[name] = {"force_rel_rms": float(np.linalg.norm(r.forces - F0) / np.linalg.norm(F0)),
-                     "energy_rel": float(abs(r.energy - E0) / abs(E0)), "iterations": r.iterations}
+                     "energy_rel": float(abs(r.energy - E0) / abs(E0)), "iterations": r.iterations,
+                     "term_rel": {k: float(abs(td[k] - ref["terms"][j]) / max(abs(ref["terms"][j]), 1e-300))
+                                  for j, k in enumerate(names)},
+                     "term_err_over_total": {k: float(abs(td[k] - ref["terms"][j]) / abs(E0))
+                                             for j, k in enumerate(names)},
+                     "strain_rel_max": float(np.abs(r.strain - ref["strain"]).max() / np.abs(ref["strain"]).max()),
+                     "dipole_rel_rms": float(np.linalg.norm(mu - mu0) / np.linalg.norm(mu0)),
+                     "dipole_max_err_rel": float(np.abs(mu - mu0).max() / np.abs(mu0).max())}
         if name == "mixed_fp64_refined":
             dt = _timed(lambda: eng.compute(S.pos, S.box), 5, 1)
             out[name]["evals_per_s_host_call"] = 1.0 / dt
@@ -882,7 +936,20 @@ def cpu_baseline(pkg, S):
         e.compute(S.pos, S.box)
     dt = time.perf_counter() - t0
     return {"value": n / dt, "unit": "evals/s", "cores": 1, "kind": "reference",
-            "sample": f"{n} full evaluations of {WORKLOAD} (pgm_core, single-threaded)"}
+            "sample": f"{n} full evaluations of {WORKLOAD} (pgm_core, single-threaded)", "cpu": cpu_model()}
+
+
+def cpu_model():
+    """The host CPU's model name and logical core count (from /proc/cpuinfo)."""
+    name, count = None, 0
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                count += 1
+                name = name or ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return {"model": name, "logical_cores": count or os.cpu_count()}
 
 
 if __name__ == "__main__":

@@ -15,6 +15,7 @@
 #ifndef PGM_B200_H_
 #define PGM_B200_H_
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -185,6 +186,12 @@ int pgm_engine_solve(pgm_engine* e, const double* rhs, double* x, double tol, in
  * pair lanes: lanes per atom of the pair passes (4, 8, 16 or 32; the autotuner's knob). */
 int pgm_engine_kernel_launches(pgm_engine* e);
 int pgm_engine_kernel_times(pgm_engine* e, int reps, double* ms);
+/* The same kernels timed cold: before each of the reps launches the caller's device buffer flush_dev
+ * (flush_bytes, larger than the 126 MB L2) is overwritten, and only the launch lies between the events. */
+int pgm_engine_kernel_times_cold(pgm_engine* e, int reps, void* flush_dev, size_t flush_bytes, double* ms);
+/* Median device time [ms] of reps whole new-step evaluations at the last evaluation's positions and boxes
+ * (already on the device), the predictor history saved and restored: the autotuner's measure. */
+int pgm_engine_time_evaluations(pgm_engine* e, int reps, double* ms);
 int pgm_engine_set_pair_lanes(pgm_engine* e, int lanes);
 int pgm_engine_pair_lanes(pgm_engine* e);
 /* Field-pass transforms (the autotuner's second knob; no counterpart in the reference, which calls cuFFT):

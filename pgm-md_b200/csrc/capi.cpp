@@ -376,6 +376,24 @@ int pgm_engine_kernel_times(pgm_engine* e, int reps, double* ms) {
     });
 }
 
+int pgm_engine_kernel_times_cold(pgm_engine* e, int reps, void* flush_dev, size_t flush_bytes, double* ms) {
+    NEED(e);
+    return guarded([&] {
+        if (reps <= 0 || !ms || !flush_dev || flush_bytes == 0)
+            throw std::invalid_argument("pgm_b200: kernel_times_cold arguments");
+        e->e->kernelTimes(reps, ms, flush_dev, flush_bytes);
+    });
+}
+
+int pgm_engine_time_evaluations(pgm_engine* e, int reps, double* ms) {
+    NEED(e);
+    return guarded([&] {
+        if (reps <= 0 || !ms)
+            throw std::invalid_argument("pgm_b200: time_evaluations arguments");
+        *ms = e->e->timeEvaluations(reps);
+    });
+}
+
 int pgm_engine_set_pair_lanes(pgm_engine* e, int lanes) {
     NEED(e);
     return guarded([&] { e->e->setPairLanes(lanes); });

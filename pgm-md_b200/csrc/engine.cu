@@ -1391,7 +1391,7 @@ struct Engine::Impl {
     }
 
     template <typename R> void enqueuePost(cudaStream_t sm, cudaStream_t sd, const Dev& d) {
-        const int tb = (n + 255) / 256, wblocks = (n + 7) / 8;
+        const int tb = (n + 255) / 256;
         CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
         k_final_prep<<<tb, 256, 0, sm>>>(d, s.polarizable ? 1 : 0);
         launchSpread<R>(sm, d, 0, d.dtot);
@@ -2361,7 +2361,7 @@ int Engine::kernelLaunches() const {
     return 7 + (I.lastBuilt ? 5 : 0) + (I.s.polarizable ? 2 * fp + 2 + perIt * it : 0) + 7 + (I.gvdwOn ? 1 : 0);
 }
 
-void Engine::kernelTimes(int reps, double* ms) {
+void Engine::kernelTimes(int reps, double* ms, void* flush, size_t flushBytes) {
     Impl& I = *impl;
     if (!I.haveResult)
         throw std::logic_error("pgm_b200: kernelTimes needs a completed evaluation");
@@ -2370,17 +2370,33 @@ void Engine::kernelTimes(int reps, double* ms) {
     cudaEvent_t a, b;
     CU(cudaEventCreate(&a));
     CU(cudaEventCreate(&b));
-    const int wb = (I.n + 7) / 8;
+    // warm: reps launches back to back between two events (as inside an evaluation, the inputs stay in L2 where
+    // they fit); cold: before every launch the caller's buffer (larger than L2) is overwritten, and only the
+    // launch itself lies between the events
     auto timeIt = [&](auto&& fn) {
         fn();
-        CU(cudaEventRecord(a, I.st));
-        for (int r = 0; r < reps; r++)
+        if (!flush) {
+            CU(cudaEventRecord(a, I.st));
+            for (int r = 0; r < reps; r++)
+                fn();
+            CU(cudaEventRecord(b, I.st));
+            CU(cudaEventSynchronize(b));
+            float t = 0;
+            CU(cudaEventElapsedTime(&t, a, b));
+            return (double) t / reps;
+        }
+        double total = 0.0;
+        for (int r = 0; r < reps; r++) {
+            CU(cudaMemsetAsync(flush, r & 0xff, flushBytes, I.st));
+            CU(cudaEventRecord(a, I.st));
             fn();
-        CU(cudaEventRecord(b, I.st));
-        CU(cudaEventSynchronize(b));
-        float t = 0;
-        CU(cudaEventElapsedTime(&t, a, b));
-        return (double) t / reps;
+            CU(cudaEventRecord(b, I.st));
+            CU(cudaEventSynchronize(b));
+            float t = 0;
+            CU(cudaEventElapsedTime(&t, a, b));
+            total += t;
+        }
+        return total / reps;
     };
     auto run = [&](auto tag) {
         typedef decltype(tag) R;
@@ -2413,6 +2429,49 @@ void Engine::kernelTimes(int reps, double* ms) {
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     I.haveResult = true;
+}
+
+// Median device time [ms] of reps whole evaluations at the last evaluation's positions and boxes (already on
+// the device), new step each (the benchmark's step: list, permanent field, the solve from the engine's initial
+// guess, final pass), CUDA events around each launch on the engine's stream.  The predictor history is saved
+// and restored, so the caller's trajectory state is unchanged.
+double Engine::timeEvaluations(int reps) {
+    Impl& I = *impl;
+    if (!I.haveResult || I.launched)
+        throw std::logic_error("pgm_b200: timeEvaluations needs a completed evaluation and no call in flight");
+    if (reps <= 0)
+        throw std::invalid_argument("pgm_b200: timeEvaluations needs reps > 0");
+    I.selectDevice();
+    const bool keepHistory = I.numGlobal > 0 && I.dHist.p;
+    std::vector<unsigned char> hist(keepHistory ? (size_t) historySize() : 0);
+    if (keepHistory)
+        getHistory(hist.data());
+    const std::vector<double> boxes = I.launchBoxes;
+    const std::vector<double> results = I.lastResults;
+    cudaEvent_t a, b;
+    CU(cudaEventCreate(&a));
+    CU(cudaEventCreate(&b));
+    std::vector<double> t;
+    for (int r = 0; r < reps; r++) {
+        for (int attempt = 0; attempt < 4; attempt++) {
+            I.prepareControl(true, 0, nullptr, nullptr, 0, 0.0, nullptr);
+            CU(cudaEventRecord(a, I.st));
+            I.launch(boxes.data());
+            CU(cudaEventRecord(b, I.st));
+            if (I.finish())
+                break;
+        }
+        float ms = 0;
+        CU(cudaEventElapsedTime(&ms, a, b));
+        t.push_back(ms);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (keepHistory)
+        setHistory(hist.data());
+    I.lastResults = results;
+    std::sort(t.begin(), t.end());
+    return t[t.size() / 2];
 }
 
 void Engine::setPairLanes(int lanes) {

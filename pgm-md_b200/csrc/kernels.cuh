@@ -806,6 +806,7 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
         // points spread over the lanes (p = 6: 6 + 1 iterations instead of 2 x 6 with 4 lanes busy in the second)
         constexpr int PP = P > 0 ? P : 1;
         constexpr int NPAIR = PP * PP, FULL = NPAIR / 32, LEFT = NPAIR % 32, LROUNDS = (LEFT * PP + 31) / 32;
+        constexpr int LEFTD = LEFT > 0 ? LEFT : 1;   // (a divisor for the leftover rounds, which run only when LEFT > 0)
         const size_t plane = (size_t) K1 * K2;
 #pragma unroll
         for (int rd = 0; rd < FULL; rd++) {
@@ -825,7 +826,7 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
         for (int lr = 0; lr < LROUNDS; lr++) {
             const int k = lane + 32 * lr;
             if (k < LEFT * PP) {
-                const int pr = 32 * FULL + k % LEFT, j1 = k / LEFT;
+                const int pr = 32 * FULL + k % LEFTD, j1 = k / LEFTD;
                 const int j2 = pr / PP, j3 = pr % PP;
                 const R t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
                 const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
@@ -1559,6 +1560,7 @@ __device__ __forceinline__ void gatherSlot(const Dev& dv, const SysDev& S, int s
         // full rounds: lane -> column (j2, j3), loop over j1; the leftover columns' points over the lanes
         constexpr int PP = P > 0 ? P : 1;
         constexpr int NPAIR = PP * PP, FULL = NPAIR / 32, LEFT = NPAIR % 32, LROUNDS = (LEFT * PP + 31) / 32;
+        constexpr int LEFTD = LEFT > 0 ? LEFT : 1;   // (a divisor for the leftover rounds, which run only when LEFT > 0)
         const size_t plane = (size_t) K1 * K2;
 #pragma unroll
         for (int rd = 0; rd < FULL; rd++) {
@@ -1594,7 +1596,7 @@ __device__ __forceinline__ void gatherSlot(const Dev& dv, const SysDev& S, int s
         for (int lr = 0; lr < LROUNDS; lr++) {
             const int k = lane + 32 * lr;
             if (k < LEFT * PP) {
-                const int pr = 32 * FULL + k % LEFT, j1 = k / LEFT;
+                const int pr = 32 * FULL + k % LEFTD, j1 = k / LEFTD;
                 const int j2 = pr / PP, j3 = pr % PP;
                 const R ph = grid[(size_t) wrapIndex(b0 - j1, K0) * plane + (size_t) wrapIndex(b1 - j2, K1) * K2 +
                                   wrapIndex(b2 - j3, K2)];

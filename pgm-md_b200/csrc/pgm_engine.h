@@ -90,9 +90,12 @@ public:
     int solve(const double* rhs, double* x, double tol);
 
     // measurement: own kernels per evaluation; average durations [ms] of the main kernels relaunched
-    // alone (0 pair list, 1 pair field pass, 2 spread, 3 gather, 4 final pair pass, 5 FFT chain, 6 CG update)
+    // alone (0 pair list, 1 pair field pass, 2 spread, 3 gather, 4 final pair pass, 5 FFT chain, 6 CG update),
+    // warm (back to back) or, with a flush buffer larger than L2, cold (the buffer overwritten before each launch)
     int kernelLaunches() const;
-    void kernelTimes(int reps, double* ms);
+    void kernelTimes(int reps, double* ms, void* flush = nullptr, size_t flushBytes = 0);
+    // median device time [ms] of reps whole new-step evaluations at the last evaluation's positions
+    double timeEvaluations(int reps);
     void setPairLanes(int lanes);
     // field-pass transforms: 0 cuFFT 3D plans + influence product kernel, 1 one cluster kernel per launch,
     // 2 cuFFT 2D plans over the x-planes + one x-line kernel with the influence product, 3 one cooperative kernel

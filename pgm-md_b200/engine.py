@@ -337,12 +337,24 @@ class Engine:
 
     KERNELS = ("pair_list", "pair_field", "spread", "gather", "pair_final", "fft_chain", "cg_update")
 
-    def kernel_times(self, reps=20):
+    def kernel_times(self, reps=20, flush_ptr=None, flush_bytes=0):
         """Average device durations [ms] of the main kernels relaunched alone (CUDA events on the engine's
-        stream) after an evaluation."""
+        stream) after an evaluation: warm (back to back), or cold when a device buffer larger than L2 is given
+        (flush_ptr, flush_bytes; overwritten before every launch, only the launch timed)."""
         ms = np.zeros(7)
-        _check(self._L.pgm_engine_kernel_times(self._h, int(reps), _d(ms)))
+        if flush_ptr is None:
+            _check(self._L.pgm_engine_kernel_times(self._h, int(reps), _d(ms)))
+        else:
+            _check(self._L.pgm_engine_kernel_times_cold(self._h, int(reps), ctypes.c_void_p(flush_ptr),
+                                                        int(flush_bytes), _d(ms)))
         return dict(zip(self.KERNELS, ms.tolist()))
+
+    def time_evaluations(self, reps=20):
+        """Median device time [ms] of ``reps`` whole new-step evaluations at the last evaluation's positions
+        (already on the device); the predictor history is left as it was."""
+        ms = ctypes.c_double(0)
+        _check(self._L.pgm_engine_time_evaluations(self._h, int(reps), ctypes.byref(ms)))
+        return ms.value
 
     def set_pair_lanes(self, lanes):
         _check(self._L.pgm_engine_set_pair_lanes(self._h, int(lanes)))
@@ -359,34 +371,31 @@ class Engine:
     def transforms(self):
         return int(self._L.pgm_engine_transforms(self._h))
 
-    def autotune(self, pos, box, reps=10, candidates=(4, 8, 16, 32)):
-        """Picks the lanes per atom of the pair passes and the kind of field-pass transforms by timing each
-        candidate on this system (batched engines: pass the batch's positions and boxes).  Returns the lanes."""
+    def autotune(self, pos, box, reps=20, candidates=(4, 8, 16, 32)):
+        """Picks the lanes per atom of the pair passes and the kind of field-pass transforms by timing whole
+        evaluations of this system (batched engines: pass the batch's positions and boxes): every pair of
+        (lanes, transforms) the grids allow, each the median of ``reps`` new-step evaluations on the device
+        (inputs resident, no host copies).  Keeps the fastest; every candidate's time is in
+        ``self.autotune_report`` [ms].  Returns the lanes."""
         batched = getattr(self, "nsys", 1) > 1
-        run = (lambda: self.compute_batch(pos, box)) if batched else (lambda: self.compute(pos, box, new_step=False))
-        best, best_t = None, None
-        for lanes in candidates:
-            self.set_pair_lanes(lanes)
-            run()
-            kt = self.kernel_times(reps)
-            t = kt["pair_field"] + kt["pair_final"] / max(1, self.iterations() + 2)
-            if best_t is None or t < best_t:
-                best, best_t = lanes, t
-        self.set_pair_lanes(best)
-        ft = {}
-        for mode in (0, 1, 2, 3):   # whole evaluations (the transforms run beside the pair passes), fastest call
+        if batched:
+            self.compute_batch(pos, box)
+        else:
+            self.compute(pos, box)
+        report = {}
+        for mode in (0, 1, 2, 3):
             self.set_transforms(mode)
             if self.transforms() != mode:
                 continue
-            run()
-            ts = []
-            for _ in range(max(5, 2 * reps)):
-                t0 = time.perf_counter()
-                run()
-                ts.append(time.perf_counter() - t0)
-            ft[mode] = float(np.min(ts))
-        self.set_transforms(min(ft, key=ft.get))
-        return best
+            for lanes in candidates:
+                self.set_pair_lanes(lanes)
+                self.time_evaluations(2)   # (captures the graph of this choice)
+                report[(lanes, mode)] = self.time_evaluations(reps)
+        lanes, mode = min(report, key=report.get)
+        self.set_pair_lanes(lanes)
+        self.set_transforms(mode)
+        self.autotune_report = {f"lanes{k[0]}_transforms{k[1]}": v for k, v in report.items()}
+        return lanes
 
     # ---------------------------------------------------------------- batched
     def set_systems(self, systems):

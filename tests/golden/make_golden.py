@@ -325,13 +325,16 @@ def type_values(S, name):
 
 
 def gradient_fixture(S, F_target, tol, pool):
-    """Central differences (h = 1e-5 relative to the type's value) of pgm_core's energy and of the force-matching
-    loss L = sum |F - F_target|^2 per parameter type, plus the energy and L at the unperturbed parameters."""
+    """Central differences of pgm_core's energy and of the force-matching loss L = sum |F - F_target|^2 per
+    parameter type, plus the energy and L at the unperturbed parameters.  The step is 1e-5 relative to the
+    type's value, or to the RMS of its kind's values where that is larger: a value near zero (a bond dipole of
+    1e-6 e nm) would otherwise give a step whose energy change drowns in the rounding of the energy."""
     jobs, keys = [], []
     for name in PARAM_NAMES:
         vals = type_values(S, name)
+        scale = float(np.sqrt(np.mean(vals ** 2)))
         for t in range(len(vals)):
-            h = 1e-5 * abs(vals[t])
+            h = 1e-5 * max(abs(vals[t]), scale)
             jobs.append((_as_fields(S), name, t, h, tol))
             keys.append((name, t, h))
     res = pool.map(_fd_job, jobs)

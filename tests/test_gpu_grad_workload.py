@@ -3,7 +3,8 @@ force-matching loss L = sum |F - F_target|^2 on (a) 16 of the 256 boxes of 64 wa
 and (b) the 8550-atom dimethylphenol liquid, with the engine at the workload's tol 1e-8.
 
 The goldens (tests/golden/grad_*.npz, from tests/golden/make_golden.py) are central differences of the
-reference pgm_core itself (h = 1e-5 relative to each type's value) with F_target from pgm_core at every
+reference pgm_core itself (h = 1e-5 relative to each type's value, or to its kind's RMS value where that is
+larger) with F_target from pgm_core at every
 per-type parameter scaled by (1 + N(0, 0.05)); they are taken at tol 1e-12 so that the differences carry no CG
 noise.  Bar: 1e-5 relative, per parameter kind as a vector norm and per element against the larger of the
 element and 1e-3 of the kind's largest element (the energy differences of a 2.7e5 kJ/mol system resolve small
