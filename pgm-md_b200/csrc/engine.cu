@@ -2461,6 +2461,7 @@ double Engine::timeEvaluations(int reps) {
             if (I.finish())
                 break;
         }
+        CU(cudaEventSynchronize(b));
         float ms = 0;
         CU(cudaEventElapsedTime(&ms, a, b));
         t.push_back(ms);
