@@ -36,7 +36,8 @@ METRIC = "pGM E+F evals/s, 8550-atom PME, mixed vs FP64 GPU at force relRMS≤1e
 WORKLOAD = "dimethylphenol8550"
 TOL = 1e-5
 TRANSFORMS = {0: "cuFFT + influence product", 1: "cluster kernel", 2: "cuFFT 2D + x-line kernel",
-              3: "grid kernel (block per x-plane)"}
+              3: "grid kernel (block per x-plane)",
+              4: "grid kernel + persistent CG kernel (whole solve in one cooperative launch)"}
 
 
 def parse():
@@ -760,7 +761,7 @@ def batch_leg(pkg, local, rank, world, dist):
     chosen = eng.transforms()
     res = {}
     per_mode = {}
-    for mode in (0, 1, 2, 3):   # every kind of transforms timed (every rank the same steps); the autotuned one reported
+    for mode in (0, 1, 2, 3, 4):   # every kind of transforms timed (every rank the same steps); the autotuned one reported
         eng.set_transforms(mode)
         if eng.transforms() != mode:
             continue

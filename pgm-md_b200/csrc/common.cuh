@@ -173,7 +173,16 @@ struct Dev {
     double* hist;             // 4 * 3 * numGlobal
     const int* globalIndex;
     int numGlobal;
+    // the persistent CG kernel (mixed, one system): plane bins and spline records of the atoms, per-slot PME
+    // weights (q, e0, e1, e2) of the current source, per-(j1, slot) gather sums, block shares, barrier words
+    void* pmeRec;
+    int* pmeBinStart;
+    float4* srcW;
+    float4* gpart;
+    double* pcgPartial;
+    unsigned* pcgBar;
     // graph
+    int loopCond;                          // 1: the CG loop is a conditional while node (k_cg_init sets it)
     cudaGraphConditionalHandle cond;       // CG while loop
     cudaGraphConditionalHandle listCond;   // pair-list build if stale
     int useCond;

@@ -4,6 +4,7 @@
 // initial guess, the CG loop as a conditional while node (its body: spread || pair pass, FFT chain, gather,
 // two CG kernels), and the final pass.  Kernels are in kernels.cuh; the C ABI is in capi.cu.
 #include "kernels.cuh"
+#include "persistent.cuh"
 #include "pgm_engine.h"
 
 #include <algorithm>
@@ -174,13 +175,18 @@ struct Engine::Impl {
     // field-pass transforms: TF_CUFFT cuFFT 3D plans + influence product; TF_CLUSTER one cluster kernel;
     // TF_SPLIT cuFFT 2D plans over the x-planes + one kernel for the x-lines with the influence product;
     // TF_GRID one cooperative kernel, a block per x-plane
-    enum { TF_CUFFT = 0, TF_CLUSTER = 1, TF_SPLIT = 2, TF_GRID = 3 };
+    // TF_PCG the grid kernel for the field passes outside the CG loop, and the whole CG loop as one persistent
+    //   cooperative kernel (mixed precision, one system)
+    enum { TF_CUFFT = 0, TF_CLUSTER = 1, TF_SPLIT = 2, TF_GRID = 3, TF_PCG = 4 };
     int tfMode = TF_CUFFT;     // in use
     int tfWant = TF_CUFFT;     // the caller's choice (setTransforms)
     bool fuseCgA = true;       // single system: A p and alph in the CG gather's epilogue (else a separate kernel)
     bool clusterOk = false;    // the systems' grids and the GPU allow the cluster kernel
     bool splitOk = false;      // the systems' x extents allow the x-line kernel
     bool gridOk = false;       // the systems' grids and the GPU allow the grid-transform kernel
+    bool pcgOk = false;        // the persistent CG kernel applies (mixed, one system, grid kernel, order 6)
+    int pcgBlocks = 0;         // its blocks (one per SM)
+    size_t pcgSmem = 0;
     int fftcBuf = 0, fftcC = 16, fftgBuf = 0, maxK0 = 0;
     int fftgKc = 0;            // the grid transforms' compile-time size (every grid fftgKc^3), or 0
     size_t fftgSmem = 0;
@@ -191,7 +197,7 @@ struct Engine::Impl {
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
         dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dPairA, dPairB, dPairC, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
-        dScal, dPartial, dGPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
+        dScal, dPartial, dGPartial, dPmeRec, dPmeBins, dSrcW, dGPart, dPcgPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dTwiddle, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
         dGradQ, dGradR, dSList, dSListCount, dPosBuild, dAtomSlot, dCandStart, dCandJ, dCandT, dGv, dSkipStart, dSkipJ;
@@ -267,7 +273,8 @@ struct Engine::Impl {
         plans64.clear();
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
                       &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dPairA, &dPairB, &dPairC, &dFlags, &dDS,
-                      &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dGPartial, &dSysCounter, &dEpair,
+                      &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dGPartial, &dPmeRec, &dPmeBins, &dSrcW, &dGPart,
+                      &dPcgPartial, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dTwiddle, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
                       &dCovByAtomOff, &dCovByAtom, &dCovByPartnerOff, &dCovByPartner, &dChunkSys, &dChunkBegin,
@@ -679,6 +686,7 @@ struct Engine::Impl {
         maxLineBlocks = 0;
         for (int k = 0; k < nsys; k++)
             maxLineBlocks = std::max(maxLineBlocks, (sysK[k][1] * (sysK[k][2] / 2 + 1) + XL_LINES - 1) / XL_LINES);
+        preparePersistent();
         selectTransforms();
         // chunks
         chunkSys.clear();
@@ -725,7 +733,7 @@ struct Engine::Impl {
         dSListCount.ensure(n * sizeof(int));
         dAtomSlot.ensure(n * sizeof(int));
         dPosBuild.ensure(3 * (size_t) n * 8);
-        dFlags.ensure((16 + 2 * (size_t) nsys) * sizeof(int));
+        dFlags.ensure(flagBytes());
         dDS.ensure(n * 4 * R);
         for (Buf* b : {&dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dEpair, &dErec, &dFpair, &dFrec, &dEtot,
                        &dForces})
@@ -1015,6 +1023,12 @@ struct Engine::Impl {
         d.fftcC = fftcC;
         d.fftgBuf = fftgBuf;
         d.fftgBar = (unsigned*) (dFlags.as<int>() + 16);
+        d.pcgBar = (unsigned*) (dFlags.as<int>() + 16 + 2 * nsys);
+        d.pmeRec = dPmeRec.p;
+        d.pmeBinStart = dPmeBins.as<int>();
+        d.srcW = dSrcW.as<float4>();
+        d.gpart = dGPart.as<float4>();
+        d.pcgPartial = dPcgPartial.as<double>();
         d.moduli = dModuli.as<double>();
         d.ncov = (int) covAtom.size();
         d.covAtom = dCovAtom.as<int>();
@@ -1032,6 +1046,7 @@ struct Engine::Impl {
         d.numGlobal = numGlobal;
         d.cond = h;
         d.useCond = forGraph ? 1 : 0;
+        d.loopCond = (forGraph && h != 0) ? 1 : 0;
         return d;
     }
 
@@ -1124,6 +1139,74 @@ struct Engine::Impl {
 
     // The transform pair with the influence product of a field pass: one cluster kernel (all systems), or
     // cuFFT plans and the product kernel.  The FP64 shadow of a mixed engine takes the cuFFT path.
+    // The persistent CG kernel's conditions and launch shape: mixed precision, one polarizable system, order 6,
+    // the grid kernel possible, K0 plane blocks plus at least PCG_MIN_PAIR_BLOCKS pair blocks resident at once
+    // (one per SM), and its shared memory.
+    void preparePersistent() {
+        pcgOk = false;
+        if (!mixed() || nsys != 1 || !gridOk || s.order != 6 || !s.polarizable)
+            return;
+        int sms = 0, coop = 0, optin = 0;
+        CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, devId));
+        CU(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, devId));
+        CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, devId));
+        const int* K = sysK[0].data();
+        pcgSmem = (3 * (size_t) FFT_MAXK + 2 * (size_t) fftgBuf) * 8 + (size_t) K[1] * K[2] * 8;
+        if (!coop || pcgSmem > (size_t) optin || K[0] + PCG_MIN_PAIR_BLOCKS > sms)
+            return;
+        void (*kfn)(Dev) = persistentKernel(pairGS);
+        CU(cudaFuncSetAttribute((const void*) kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) pcgSmem));
+        int perSm = 0;
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kfn, PCG_THREADS, pcgSmem));
+        if (perSm < 1)
+            return;
+        pcgBlocks = sms;
+        pcgOk = true;
+        dPmeRec.ensure((size_t) n * sizeof(PmeRec<6>));
+        dPmeBins.ensure((FFT_MAXK + 1) * sizeof(int));
+        dSrcW.ensure((size_t) n * sizeof(float4));
+        dGPart.ensure((size_t) 6 * n * sizeof(float4));
+        dPcgPartial.ensure((size_t) 2 * pcgBlocks * 4 * 8);
+    }
+
+    // The persistent kernel for the pair lanes (8, 16 or 32; 4 runs as 8) and the grid's compile-time size.
+    void (*persistentKernel(int lanes))(Dev) {
+        const int kc = fftgKc;
+        auto pick = [&](auto gsTag) -> void (*)(Dev) {
+            constexpr int GS = decltype(gsTag)::value;
+            switch (kc) {
+            case 32: return k_cg_persistent<6, GS, 32>;
+            case 48: return k_cg_persistent<6, GS, 48>;
+            case 64: return k_cg_persistent<6, GS, 64>;
+            default: return k_cg_persistent<6, GS, 0>;
+            }
+        };
+        if (lanes >= 32)
+            return pick(std::integral_constant<int, 32>());
+        if (lanes >= 16)
+            return pick(std::integral_constant<int, 16>());
+        return pick(std::integral_constant<int, 8>());
+    }
+
+    // The whole CG loop: one cooperative launch of the persistent kernel (one block per SM).
+    void launchPersistent(cudaStream_t sm, const Dev& d) {
+        void (*kfn)(Dev) = persistentKernel(pairGS);
+        CU(cudaFuncSetAttribute((const void*) kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) pcgSmem));
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.gridDim = dim3(pcgBlocks);
+        cfg.blockDim = dim3(PCG_THREADS);
+        cfg.dynamicSmemBytes = pcgSmem;
+        cfg.stream = sm;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        CU(cudaLaunchKernelEx(&cfg, kfn, d));
+    }
+
+    bool persistentMode() const { return tfMode == TF_PCG; }
+
     // The transform mode in use: the caller's choice where the systems' grids allow it, else cuFFT.
     void selectTransforms() {
         int m = TF_CUFFT;
@@ -1133,6 +1216,8 @@ struct Engine::Impl {
             m = TF_SPLIT;
         if (tfWant == TF_GRID && gridOk)
             m = TF_GRID;
+        if (tfWant == TF_PCG && pcgOk)
+            m = TF_PCG;
         if (m != tfMode && exec) {
             cudaGraphExecDestroy(exec);
             exec = nullptr;
@@ -1177,7 +1262,7 @@ struct Engine::Impl {
             splitChain<R>(sm, d, gate);
             return;
         }
-        if (tfMode == TF_GRID) {   // cooperative: the blocks of a system meet at two barriers
+        if (tfMode == TF_GRID || tfMode == TF_PCG) {   // cooperative: the blocks of a system meet at two barriers
             cudaLaunchConfig_t cfg = {};
             cudaLaunchAttribute at[1];
             at[0].id = cudaLaunchAttributeCooperative;
@@ -1354,6 +1439,8 @@ struct Engine::Impl {
             pairRecords<R>(sd, d);
             CU(cudaEventRecord(evJoin, sd));
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
+            if (persistentMode())
+                k_pme_bins<6><<<1, 1024, 0, sm>>>(d);
             k_perm<<<tb, 256, 0, sm>>>(d);
             k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
@@ -1426,7 +1513,8 @@ struct Engine::Impl {
         cudaGraph_t graph;
         CU(cudaGraphCreate(&graph, 0));
         cudaGraphConditionalHandle handle = 0, listHandle = 0;
-        if (s.polarizable)
+        const bool loopNode = s.polarizable && !persistentMode();   // (the persistent kernel loops by itself)
+        if (loopNode)
             CU(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
         if (verletList())   // (a handle without its conditional node makes the instantiation fail)
             CU(cudaGraphConditionalHandleCreate(&listHandle, graph, 0, cudaGraphCondAssignDefault));
@@ -1437,8 +1525,10 @@ struct Engine::Impl {
         listBody = nullptr;
         try {
             enqueuePre<R>(st, side, d);
-            if (s.polarizable)   // the CG loop
+            if (loopNode)   // the CG loop
                 body = appendConditional(st, handle, cudaGraphCondTypeWhile);
+            else if (s.polarizable)
+                launchPersistent(st, d);
             enqueuePost<R>(st, side, d);
         } catch (...) {
             capturing = false;
@@ -1483,7 +1573,9 @@ struct Engine::Impl {
     template <typename R> void runDirect() {
         const Dev d = makeDev(false, 0);
         enqueuePre<R>(st, side, d);
-        if (s.polarizable) {
+        if (s.polarizable && persistentMode()) {
+            launchPersistent(st, d);
+        } else if (s.polarizable) {
             static const bool trace = std::getenv("PGM_B200_TRACE") != nullptr;
             for (int it = 0; it <= s.maxIter + 1; it++) {
                 CU(cudaMemcpyAsync(hFlags, d.flags, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1648,7 +1740,8 @@ struct Engine::Impl {
     }
 
     // The flags and the grid transforms' barrier words (cleared together at the start of every call).
-    size_t flagBytes() const { return (16 + 2 * (size_t) nsys) * sizeof(int); }
+    // (16 flags, 2 barrier words per system for the grid transforms, 2 for the persistent CG kernel)
+    size_t flagBytes() const { return (16 + 2 * (size_t) nsys + 2) * sizeof(int); }
 
     // After the flags came back: a grid-transform barrier that gave up leaves the evaluation's results
     // undefined (the barrier words are reset at the next evaluation's start).
@@ -2358,6 +2451,8 @@ int Engine::kernelLaunches() const {
         it = std::max(it, (int) I.lastResults[(size_t) k * NRES + 14]);
     const int fp = 4;
     const int perIt = fp + (I.nsys == 1 && I.fuseCgA ? 1 : 2);   // single system: A p in the gather
+    if (I.persistentMode() && I.s.polarizable)   // the bins and one persistent launch for the whole loop
+        return 7 + (I.lastBuilt ? 5 : 0) + 2 * fp + 2 + 2 + 7 + (I.gvdwOn ? 1 : 0);
     return 7 + (I.lastBuilt ? 5 : 0) + (I.s.polarizable ? 2 * fp + 2 + perIt * it : 0) + 7 + (I.gvdwOn ? 1 : 0);
 }
 
@@ -2488,9 +2583,10 @@ void Engine::setPairLanes(int lanes) {
 int Engine::pairLanes() const { return impl->pairGS; }
 
 void Engine::setTransforms(int mode) {
-    if (mode < 0 || mode > 3)
+    if (mode < 0 || mode > 4)
         throw std::invalid_argument("pgm_b200: transforms must be 0 (cuFFT), 1 (cluster kernel), 2 (2D cuFFT + "
-                                    "x-line kernel) or 3 (grid kernel)");
+                                    "x-line kernel), 3 (grid kernel) or 4 (grid kernel and the persistent CG "
+                                    "kernel)");
     impl->tfWant = mode;
     impl->selectTransforms();
 }

@@ -2116,7 +2116,7 @@ __global__ void __launch_bounds__(CHUNK) k_cg_init(Dev dv) {
             dv.flags[5] = dv.nSys - ndone;
             dv.flags[4] = 0;
             dv.flags[3] = 0;
-            if (dv.useCond)
+            if (dv.useCond && dv.loopCond)
                 cudaGraphSetConditional(dv.cond, (ndone < dv.nSys) ? 1u : 0u);
         }
     }

@@ -365,7 +365,8 @@ class Engine:
     def set_transforms(self, mode):
         """Field-pass transforms: 0 cuFFT 3D plans + influence product, 1 one cluster kernel per pass, 2 cuFFT 2D
         plans over the x-planes + one x-line kernel with the influence product, 3 one cooperative kernel with a
-        block per x-plane."""
+        block per x-plane, 4 that kernel for the field passes around the CG loop and the whole CG loop as one
+        persistent cooperative kernel (mixed precision, one system, order 6); transforms() tells which runs."""
         _check(self._L.pgm_engine_set_transforms(self._h, int(mode)))
 
     def transforms(self):
@@ -383,7 +384,7 @@ class Engine:
         else:
             self.compute(pos, box)
         report = {}
-        for mode in (0, 1, 2, 3):
+        for mode in (0, 1, 2, 3, 4):
             self.set_transforms(mode)
             if self.transforms() != mode:
                 continue

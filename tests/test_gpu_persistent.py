@@ -1,0 +1,78 @@
+"""The persistent CG kernel (transforms mode 4: the whole mixed-precision CG loop of one system as one
+cooperative launch, PME planes spread, transformed and gathered in shared memory, the direct-space pass on the
+other SMs) against the reference pgm_core's outputs and against the engine's own graph loop (mode 3), on the
+committed goldens: the 216-water box (20^3 grid), the triclinic test box (48^3) and the real 8550-atom
+dimethylphenol liquid (48^3).  Bars as for every mixed path: energy 1e-6, forces 1e-5 relative RMS at tol 1e-10
+against the oracle; the same CG iteration count as the graph loop."""
+
+import numpy as np
+import pytest
+
+from conftest import PKG, load_dmp_real, load_golden_system
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_engine(S, mode, tol=1e-10, lanes=16):
+    e = PKG.Engine(PKG.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=6, tol=tol, max_iter=500, peek=0.0,
+                                predictor=0, ke=PKG.systems.KE_DEFAULT, precision=PKG.MIXED, skin=0.0))
+    e.set_system(S)
+    e.set_pair_lanes(lanes)
+    e.set_transforms(mode)
+    return e
+
+
+def golden(name):
+    if name == "dmp8550_real":
+        return load_dmp_real()
+    return load_golden_system(name)
+
+
+@pytest.mark.parametrize("name", ["water216", "tiny_triclinic", "dmp8550_real"])
+@pytest.mark.parametrize("lanes", [8, 32])
+def test_persistent_cg_against_reference(name, lanes):
+    S, d = golden(name)
+    eng = mixed_engine(S, 4, lanes=lanes)
+    assert eng.transforms() == 4
+    r = eng.compute(S.pos, S.box)
+    mu = eng.induced_dipoles()
+    ref_graph = mixed_engine(S, 3, lanes=lanes)
+    g = ref_graph.compute(S.pos, S.box)
+    e_ref = float(d["energy"])
+    assert abs(r.energy - e_ref) <= 1e-6 * abs(e_ref), (r.energy, e_ref)
+    F = np.asarray(d["forces"], np.float64)
+    assert np.linalg.norm(r.forces - F) <= 1e-5 * np.linalg.norm(F)
+    assert np.linalg.norm(mu - d["mu"]) <= 1e-5 * np.linalg.norm(d["mu"])
+    assert r.iterations == g.iterations
+    assert abs(r.energy - g.energy) <= 1e-6 * abs(e_ref)
+    assert np.linalg.norm(r.forces - g.forces) <= 1e-5 * np.linalg.norm(F)
+    # the launch count: the whole loop is one launch whatever the iterations
+    assert eng.kernel_launches() < ref_graph.kernel_launches()
+    eng.close()
+    ref_graph.close()
+
+
+def test_persistent_cg_repeated_calls_and_tolerance():
+    """The benchmark's tolerance (1e-5) on the 8550-atom liquid, three calls in a row: the same iterations and
+    energies within the mixed path's run-to-run spread (the field passes around the loop use float atomics)."""
+    S, d = golden("dmp8550_real")
+    eng = mixed_engine(S, 4, tol=1e-5)
+    rs = [eng.compute(S.pos, S.box) for _ in range(3)]
+    e_ref = float(d["energy"])
+    F = np.asarray(d["forces"], np.float64)
+    for r in rs:
+        assert r.iterations == rs[0].iterations
+        assert abs(r.energy - e_ref) <= 1e-6 * abs(e_ref)
+        assert np.linalg.norm(r.forces - F) <= 1e-5 * np.linalg.norm(F)
+    eng.close()
+
+
+def test_persistent_cg_not_applicable_falls_back():
+    """Batched engines and FP64 engines do not take mode 4; transforms() reports what runs."""
+    S, _ = golden("water216")
+    e = PKG.Engine(PKG.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=6, tol=1e-8, max_iter=500, peek=0.0,
+                                predictor=0, ke=PKG.systems.KE_DEFAULT, precision=PKG.FP64))
+    e.set_system(S)
+    e.set_transforms(4)
+    assert e.transforms() != 4
+    e.close()
