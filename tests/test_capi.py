@@ -74,3 +74,41 @@ def test_header_is_plain_c_and_links(tmp_path):
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
     assert int(out[0]) == ctypes.sizeof(_lib.PgmSettings)
     assert float(out[1]) == 0.9 and int(out[2]) == 6 and int(out[3]) == 0 and float(out[4]) == -2.0
+
+
+def build_core_engine_check(out_dir):
+    """Compiles tests/cpp/core_engine_check.cpp (a pgmcore-style C++ caller of the engine through
+    pgm-md_b200/csrc/pgm_core_b200.h) against the library; returns the executable."""
+    import shutil
+    import subprocess
+    from pgm_md_b200 import _lib
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no C++ compiler")
+    lib_dir = _lib.LIB_PATH.parent
+    exe = Path(out_dir) / "core_engine_check"
+    subprocess.run([gxx, "-std=c++17", "-O2", "-Wall", "-Werror", "-I", str(ROOT / "pgm-md_b200" / "csrc"),
+                    str(ROOT / "tests" / "cpp" / "core_engine_check.cpp"), "-L", str(lib_dir), "-lpgm_b200",
+                    f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
+    return exe
+
+
+def test_core_shaped_cpp_surface_builds_and_links(tmp_path):
+    """The pgmcore::Engine-shaped C++ class compiles as a caller sees it and links the library (it runs on
+    the GPU in tests/test_gpu_core_api.py)."""
+    assert build_core_engine_check(tmp_path).exists()
+
+
+def test_openmm_kernel_recipe_needs_an_openmm_sdk():
+    """The OpenMM CUDA-platform kernel (pgm-md_b200/openmm) builds only against an OpenMM SDK: without
+    OPENMM_DIR its recipe stops with a message and status 2."""
+    import os
+    import subprocess
+    env = {k: v for k, v in os.environ.items() if k != "OPENMM_DIR"}
+    r = subprocess.run(["make", "-s", "-C", str(ROOT / "pgm-md_b200" / "openmm")], capture_output=True, text=True,
+                       env=env)
+    assert r.returncode == 2 and "OPENMM_DIR" in r.stdout
+    src = (ROOT / "pgm-md_b200" / "openmm" / "PgmB200OpenMMKernel.cpp").read_text()
+    for call in ("pgm_engine_launch_device", "pgm_engine_finish_device", "setForcesValid", "registerKernelFactories",
+                 "getLongForceBuffer", "getAtomIndex"):
+        assert call in src, call
