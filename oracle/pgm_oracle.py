@@ -668,6 +668,8 @@ class Engine:
         self.E_total = E
         self.phi_rec_atoms = pot
         self.d = d
+        self.E_rec = Erec
+        self.f2_rec = f2v
         # covalent chain rule: core/pgm_core.cpp:511-529
         if len(self.top.cov_atom):
             v, L = self._cov_vectors()
@@ -728,6 +730,182 @@ class Engine:
             u = v / L[:, None]
             dc = -np.sum(self.E_total[self.top.cov_atom] * u, axis=1)
         return dict(q=s.ke * dq, radius=s.ke * dR, alpha=s.ke * dal, cov_strength=s.ke * dc)
+
+
+    # ---------------------------------------------------------------- force-matching adjoint (extension)
+    def _pme_tangent(self, dip, quad_d=None, quad_w=None):
+        """PME potential and field at every atom of the sources: dipoles dip and, when given, the quadrupoles
+        quad_d (x) quad_w (the derivative of a dipole d moved along w: sum_ab ed_a ew_b d2 theta / dw_a dw_b).
+        Returns (potential, field)."""
+        K1, K2, K3 = self.s.grid
+        p = self.s.order
+        e = self.frac_dipoles(dip)
+        ed = self.frac_dipoles(quad_d) if quad_d is not None else None
+        ew = self.frac_dipoles(quad_w) if quad_w is not None else None
+        Q = np.zeros(K1 * K2 * K3)
+        th, dth, d2 = self.theta, self.dtheta, self.d2theta
+        for j1 in range(p):
+            g1 = self._grid_index(0, j1)
+            for j2 in range(p):
+                g2 = self._grid_index(1, j2)
+                for j3 in range(p):
+                    g3 = self._grid_index(2, j3)
+                    t = (th[0, :, j1], th[1, :, j2], th[2, :, j3])
+                    u = (dth[0, :, j1], dth[1, :, j2], dth[2, :, j3])
+                    v = (d2[0, :, j1], d2[1, :, j2], d2[2, :, j3])
+                    w = e[:, 0] * u[0] * t[1] * t[2] + e[:, 1] * t[0] * u[1] * t[2] + e[:, 2] * t[0] * t[1] * u[2]
+                    if ed is not None:
+                        for a in range(3):
+                            for b in range(3):
+                                fac = []
+                                for c in range(3):
+                                    if c == a and c == b:
+                                        fac.append(v[c])
+                                    elif c == a or c == b:
+                                        fac.append(u[c])
+                                    else:
+                                        fac.append(t[c])
+                                w = w + ed[:, a] * ew[:, b] * fac[0] * fac[1] * fac[2]
+                    Q += np.bincount((g1 * K2 + g2) * K3 + g3, weights=w, minlength=K1 * K2 * K3)
+        F = np.fft.rfftn(Q.reshape(K1, K2, K3))
+        phi = (np.fft.irfftn(F * self.influence, s=(K1, K2, K3), axes=(0, 1, 2)) * (K1 * K2 * K3)).reshape(-1)
+        f, _, pot = self._interp(phi, want_pot=True)
+        E = np.zeros((self.n, 3))
+        for k in range(3):
+            E[:, k] -= (self.s.grid[0] * self.recip[k][0] * f[:, 0] + self.s.grid[1] * self.recip[k][1] * f[:, 1]
+                        + self.s.grid[2] * self.recip[k][2] * f[:, 2])
+        return pot, E
+
+    def _pair_tangent(self, dr, dd):
+        """Directional derivatives of the direct-space potential, field and radius gradient at every atom along
+        the displacement dr of the positions and the change dd of the dipoles (charges fixed):
+          D phi_i = sum_j -q_j G1 (x.dx) + dd_j.x G1 + d_j.dx G1 - (d_j.x) G2 (x.dx)
+          D E_i   = sum_j q_j dx G1 - q_j x G2 (x.dx) - dd_j G1 + d_j G2 (x.dx) + (dd_j.x + d_j.dx) x G2
+                          + (d_j.x) dx G2 - (d_j.x) x G3 (x.dx)
+          D gR_i  = sum_j D U_a (-2 R_i a^3), U_a the pair energy with dG_n/da = H_n, D H_n = -2 a^2 (x.dx) H_n,
+        with x = r_i - r_j, dx = dr_i - dr_j (dG_n = -G_{n+1} x.dx from dG_n/dr = -r G_{n+1})."""
+        n = self.n
+        q, d, R = self.top.q, self.d, self.top.radius
+        Dphi = np.zeros(n)
+        DE = np.zeros((n, 3))
+        DgR = np.zeros(n)
+        if len(self.pi) == 0:
+            return Dphi, DE, DgR
+        i, j, x, G, r, a = self.pi, self.pj, self.px, self.pG, self.pr, self.pa
+        dx = dr[i] - dr[j]
+        xd = np.sum(x * dx, axis=1)
+        qi, qj, di, dj, ddi, ddj = q[i], q[j], d[i], d[j], dd[i], dd[j]
+        djx, dix = np.sum(dj * x, axis=1), np.sum(di * x, axis=1)
+        ddjx, ddix = np.sum(ddj * x, axis=1), np.sum(ddi * x, axis=1)
+        djdx, didx = np.sum(dj * dx, axis=1), np.sum(di * dx, axis=1)
+        Dphi += np.bincount(i, weights=-qj * G[1] * xd + ddjx * G[1] + djdx * G[1] - djx * G[2] * xd, minlength=n)
+        Dphi += np.bincount(j, weights=-qi * G[1] * xd - ddix * G[1] - didx * G[1] + dix * G[2] * xd, minlength=n)
+        for k in range(3):
+            ei = (qj * dx[:, k] * G[1] - qj * x[:, k] * G[2] * xd - ddj[:, k] * G[1] + dj[:, k] * G[2] * xd
+                  + (ddjx + djdx) * x[:, k] * G[2] + djx * dx[:, k] * G[2] - djx * x[:, k] * G[3] * xd)
+            ej = (-qi * dx[:, k] * G[1] + qi * x[:, k] * G[2] * xd - ddi[:, k] * G[1] + di[:, k] * G[2] * xd
+                  + (ddix + didx) * x[:, k] * G[2] + dix * dx[:, k] * G[2] - dix * x[:, k] * G[3] * xd)
+            DE[:, k] += np.bincount(i, weights=ei, minlength=n) + np.bincount(j, weights=ej, minlength=n)
+        H0 = (2.0 / SQRT_PI) * np.exp(-(a * r) ** 2)
+        H1 = H0 * 2 * a * a
+        H2 = H1 * 2 * a * a
+        c = -2.0 * a * a * xd
+        Ddjx, Ddix = ddjx + djdx, ddix + didx
+        Ddidj = np.sum(ddi * dj + di * ddj, axis=1)
+        didj = np.sum(di * dj, axis=1)
+        DU = (qi * qj * c * H0 + (qi * Ddjx - qj * Ddix) * H1 + (qi * djx - qj * dix) * c * H1 + Ddidj * H1
+              + didj * c * H1 - (Ddix * djx + dix * Ddjx) * H2 - dix * djx * c * H2)
+        DgR += np.bincount(i, weights=DU * (-2.0 * R[i] * a ** 3), minlength=n)
+        DgR += np.bincount(j, weights=DU * (-2.0 * R[j] * a ** 3), minlength=n)
+        return Dphi, DE, DgR
+
+    def _solve_rhs(self, rhs):
+        """(alpha^-1 - T) x = rhs by Jacobi PCG from x = alpha rhs to tol 1e-14 (rows with alpha = 0: 0)."""
+        al = self.top.alpha
+        zero = np.zeros(self.n)
+        pol = (al > 0)[:, None]
+        safe = np.where(al > 0, al, 1.0)[:, None]
+
+        def applyA(v):
+            return np.where(pol, v / safe - self.field(zero, v), 0.0)
+
+        b = np.where(pol, rhs, 0.0)
+        x = al[:, None] * b
+        r = b - applyA(x)
+        z = al[:, None] * r
+        pdir = z.copy()
+        rz = float(np.sum(r * z))
+        nb = float(np.sum(np.abs(al[:, None] * b))) + 1e-300
+        for _ in range(1000):
+            if float(np.sum(np.abs(al[:, None] * r))) <= 1e-14 * nb:
+                break
+            Ap = applyA(pdir)
+            alph = rz / max(float(np.sum(pdir * Ap)), 1e-300)
+            x = x + alph * pdir
+            rn = r - alph * Ap
+            zn = al[:, None] * rn
+            beta = float(np.sum(zn * (rn - r))) / max(rz, 1e-300)
+            pdir = zn + beta * pdir
+            r, z = rn, zn
+            rz = float(np.sum(r * z))
+        return x
+
+    def force_matching_gradients(self, F_target):
+        """dL/d(parameter) of L = sum |F - F_target|^2 at the solved dipoles of the last ``compute`` (peek 0), by
+        one adjoint solve (no reference counterpart).  With w = 2 (F - F_target), g = dE/dtheta at fixed mu and
+        E_tot the total field at fixed mu,
+            dL/dtheta = -D_w g + D_u g,   (alpha^-1 - T) u = -D_w E_tot,
+        D_w the derivative along the displacement w of the positions (mu fixed; the covalent dipoles follow
+        their bonds), D_u the derivative along u of the induced dipoles; every derivative analytic:
+          D_w phi_i   = [direct part] + phi_tangent(r_i) - E_rec(r_i) . w_i
+          D_w E_tot_i = [direct part] + E_tangent(r_i) - Hess phi_rec(r_i) w_i + cs D_w p_i
+        where the tangent sources are the dipoles q_j w_j + D_w p_j and the quadrupoles d_j (x) w_j.
+        Returns (L, dict of per-atom / per-dipole gradients)."""
+        s = self.s
+        n = self.n
+        q, d, al = self.top.q, self.d, self.top.alpha
+        F = self.forces
+        w = 2.0 * (F - np.asarray(F_target, np.float64))
+        L = float(np.sum((F - F_target) ** 2))
+        cs = 4.0 * s.beta ** 3 / (3.0 * SQRT_PI)
+        ncov = len(self.top.cov_atom)
+        Dp = np.zeros((n, 3))
+        if ncov:
+            v, Lc = self._cov_vectors()
+            u_c = v / Lc[:, None]
+            ia, ja, c = self.top.cov_atom, self.top.cov_partner, self.top.cov_strength
+            dv = w[ja] - w[ia]
+            Du_c = (dv - np.sum(u_c * dv, axis=1)[:, None] * u_c) / Lc[:, None]
+            for k in range(3):
+                Dp[:, k] = np.bincount(ia, weights=c * Du_c[:, k], minlength=n)
+        # along w (positions moved, mu fixed)
+        Dphi, DE, DgR = self._pair_tangent(w, Dp)
+        pot_t, E_t = self._pme_tangent(q[:, None] * w + Dp, d, w)
+        H = np.zeros((n, 3, 3))
+        f2 = self.f2_rec
+        f2m = np.empty((n, 3, 3))
+        f2m[:, 0, 0], f2m[:, 1, 1], f2m[:, 2, 2] = f2[:, 0], f2[:, 1], f2[:, 2]
+        f2m[:, 0, 1] = f2m[:, 1, 0] = f2[:, 3]
+        f2m[:, 0, 2] = f2m[:, 2, 0] = f2[:, 4]
+        f2m[:, 1, 2] = f2m[:, 2, 1] = f2[:, 5]
+        Kr = np.array([[s.grid[a] * self.recip[k][a] for a in range(3)] for k in range(3)])   # [k][a]
+        H = np.einsum("ka,nab,lb->nkl", Kr, f2m, Kr)
+        Dw_phi = Dphi + pot_t - np.sum(self.E_rec * w, axis=1)
+        Dw_E = DE + E_t - np.einsum("nkl,nl->nk", H, w) + cs * Dp
+        gw = dict(q=s.ke * Dw_phi, radius=s.ke * DgR, alpha=np.zeros(n), cov_strength=np.zeros(ncov))
+        if ncov:
+            gw["cov_strength"] = -s.ke * (np.sum(Dw_E[ia] * u_c, axis=1) + np.sum(self.E_total[ia] * Du_c, axis=1))
+        # the adjoint solve, then along u (dipoles changed, positions fixed)
+        u = self._solve_rhs(-Dw_E)
+        zero3 = np.zeros((n, 3))
+        Dphi_u, DE_u, DgR_u = self._pair_tangent(zero3, u)
+        pot_u, E_u = self._pme_tangent(u)
+        gu = dict(q=s.ke * (Dphi_u + pot_u), radius=s.ke * DgR_u,
+                  alpha=np.where(al > 0, -s.ke * np.sum(self.mu * u, axis=1) / np.where(al > 0, al, 1.0) ** 2, 0.0),
+                  cov_strength=np.zeros(ncov))
+        if ncov:
+            gu["cov_strength"] = -s.ke * np.sum((DE_u + E_u + cs * u)[ia] * u_c, axis=1)
+        return L, {k: -gw[k] + gu[k] for k in gw}
 
 
 def evaluate(pos, box, top: Topology, s: Settings):

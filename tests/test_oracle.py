@@ -159,3 +159,25 @@ def test_pair_set_cells_equals_all_pairs():
     i, j, _ = O.pair_set(S.pos, S.box, 0.6)
     ci, cj = O.pair_set_cells(S.pos, S.box, 0.6)
     assert np.array_equal(i, ci) and np.array_equal(j, cj)
+
+
+def test_oracle_force_matching_adjoint_against_reference_differences():
+    """The oracle's analytic force-matching gradient (one adjoint solve, tangent pair and PME passes) against
+    central differences of the reference pgm_core's loss: per type, on two of the 64-water boxes of the
+    differentiation workload (tests/golden/grad_water64x16.npz), to 1e-6 relative."""
+    import numpy as np
+    from oracle import pgm_oracle as O
+    d = np.load(GOLDEN / "grad_water64x16.npz")
+    boxes = PKG.systems.water64_boxes(nsys=2)
+    for k in (0, 1):
+        S = boxes[k]
+        e = O.Engine(oracle_topology(S), oracle_settings(S, tol=1e-12))
+        e.compute(S.pos, S.box)
+        L, g = e.force_matching_gradients(d[f"b{k}_Ft"])
+        assert abs(L - float(d[f"b{k}_loss"])) <= 1e-8 * L
+        for name in ("q", "cov_strength", "alpha", "radius"):
+            ty = S.cov_types if name == "cov_strength" else S.types
+            fd = d[f"b{k}_dL_{name}"]
+            got = np.zeros(len(fd))
+            np.add.at(got, ty, g[name])
+            assert np.linalg.norm(got - fd) <= 1e-6 * np.linalg.norm(fd), (k, name, got, fd)
