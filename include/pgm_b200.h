@@ -178,6 +178,16 @@ int pgm_engine_param_grad(pgm_engine* e, double* dq, double* dradius, double* da
 int pgm_engine_evaluate_fixed(pgm_engine* e, const double* pos, const double* box, const double* mu, int keep_list,
                               double* forces, double* field, pgm_terms* terms);
 int pgm_engine_solve(pgm_engine* e, const double* rhs, double* x, double tol, int* iterations);
+/* Gradient of the force-matching loss L = sum |F - F_target|^2 of the last evaluation (run it with peek 0, so
+ * that the energy is stationary in the induced dipoles) with respect to every per-atom charge (dq), Gaussian
+ * radius (dradius), polarizability (dalpha) and per-dipole covalent strength (dstrength), each may be NULL,
+ * by ONE adjoint solve (alpha^-1 - T) u = -D_w E_tot to tol and analytic tangent passes (w = 2 (F - F_target);
+ * no iterations unrolled, damping terms recomputed per pair).  f_target: n*3 host forces (batched engines:
+ * every system's, concatenated; the gradient covers every system at once).  *loss = L, *iterations = the
+ * adjoint's CG iterations (either may be NULL).  No counterpart in the reference, which lists parameter
+ * derivatives as not implemented (docs/openmm.md:265). */
+int pgm_engine_force_matching_grad(pgm_engine* e, const double* f_target, double tol, double* dq, double* dradius,
+                                   double* dalpha, double* dstrength, double* loss, int* iterations);
 
 /* Measurement (no counterpart in the reference): the number of this library's kernels the last evaluation
  * ran (cuFFT transforms not counted); average device durations [ms] over reps launches of the main kernels

@@ -50,38 +50,23 @@ class PGMEnergy(torch.autograd.Function):
         return grad_out * gq, grad_out * gc, grad_out * ga, grad_out * gR, None, None
 
 
-def force_matching_atom_grads(engine, system, F_target, tol=1e-10, probe=1e-5):
+def force_matching_atom_grads(engine, system, F_target, tol=1e-10):
     """dL/d(per-atom q, radius, alpha; per-dipole strength) of L = sum |F - F_target|^2 by one adjoint solve.
 
-    With w = 2 (F - F_target), E the energy at fixed induced dipoles mu, g_theta = dE/dtheta at fixed mu and
-    E_tot the total field at fixed mu:
-        dL/dtheta = -D_w g_theta + D_u g_theta,   u = -(alpha^-1 - T)^-1 D_w E_tot,
-    where D_w is the derivative along the displacement w of the positions (mu fixed) and D_u the derivative
-    along u of the dipoles (positions fixed).  D_w comes from central differences of the analytic g_theta and
-    E_tot (step `probe` nm for the largest displacement, the pair list of the solution kept, so the function
-    is smooth); D_u from central differences in mu, exact here because g_theta is at most quadratic in mu.
-    The engine must run with peek = 0 (the energy is then stationary in mu).  Returns (L, grads, F)."""
-    res = engine.compute(system.pos, system.box, new_step=True)
-    F = res.forces
-    mu = engine.induced_dipoles()
-    w = 2.0 * (F - F_target)
-    L = float(np.sum((F - F_target) ** 2))
-    h = probe / max(np.abs(w).max(), 1e-300)
-
-    def probe_at(pos, m):
-        r = engine.evaluate_fixed(pos, system.box, m, keep_list=True)
-        return engine.param_grad(), r.extra["field"]
-
-    gp, Ep = probe_at(system.pos + h * w, mu)
-    gm, Em = probe_at(system.pos - h * w, mu)
-    Dw_g = {k: (gp[k] - gm[k]) / (2 * h) for k in gp}
-    Dw_E = (Ep - Em) / (2 * h)
-    engine.evaluate_fixed(system.pos, system.box, mu, keep_list=True)   # the solution's geometry again
-    u, _ = engine.solve(-Dw_E, tol=tol)
-    hu = 1e-3 * max(np.abs(mu).max(), 1e-30) / max(np.abs(u).max(), 1e-300)
-    gup, _ = probe_at(system.pos, mu + hu * u)
-    gum, _ = probe_at(system.pos, mu - hu * u)
-    grads = {k: -Dw_g[k] + (gup[k] - gum[k]) / (2 * hu) for k in Dw_g}
+    With w = 2 (F - F_target), g_theta = dE/dtheta at fixed induced dipoles mu and E_tot the total field at fixed
+    mu:  dL/dtheta = -D_w g_theta + D_u g_theta,  (alpha^-1 - T) u = -D_w E_tot,  D_w the derivative along the
+    displacement w of the positions (mu fixed), D_u along u of the dipoles.  The engine forms every derivative
+    analytically on the GPU (tangent pair and PME passes, the radial kernels recomputed per pair) and solves for
+    u with its own CG kernels (pgm_engine_force_matching_grad); no iterations are unrolled.  Run the engine with
+    peek = 0 (the energy is then stationary in mu).  Works for batched engines (system = a list of systems, the
+    target forces concatenated).  Returns (L, grads, F)."""
+    if isinstance(system, (list, tuple)):
+        pos = np.concatenate([s.pos for s in system])
+        boxes = np.stack([s.box for s in system])
+        F = engine.compute_batch(pos, boxes)["forces"]
+    else:
+        F = engine.compute(system.pos, system.box, new_step=True).forces
+    L, grads, _ = engine.force_matching_grad(np.asarray(F_target, np.float64), tol=tol)
     return L, grads, F
 
 

@@ -365,6 +365,18 @@ int pgm_engine_solve(pgm_engine* e, const double* rhs, double* x, double tol, in
     });
 }
 
+int pgm_engine_force_matching_grad(pgm_engine* e, const double* f_target, double tol, double* dq, double* dradius,
+                                   double* dalpha, double* dstrength, double* loss, int* iterations) {
+    NEED(e);
+    return guarded([&] {
+        if (!f_target || !(tol > 0))
+            throw std::invalid_argument("pgm_b200: force_matching_grad needs f_target and tol > 0");
+        const double L = e->e->forceMatchingGrad(f_target, tol, dq, dradius, dalpha, dstrength, iterations);
+        if (loss)
+            *loss = L;
+    });
+}
+
 int pgm_engine_kernel_launches(pgm_engine* e) { return (e && e->e) ? e->e->kernelLaunches() : -1; }
 
 int pgm_engine_kernel_times(pgm_engine* e, int reps, double* ms) {

@@ -134,6 +134,7 @@ struct Dev {
     double* Etot;             // 3n
     double* fin;              // n * NFIN per-atom final sums
     double* potRec;           // n
+    double* hrec;             // 6n second-derivative sums of the final reciprocal potential (00 11 22 01 02 12)
     double* forces;           // 3n output (double)
     double* results;          // nSys * NRES
     double* convPartial;      // sum over systems of convBlocks * NCONV

@@ -5,6 +5,7 @@
 // two CG kernels), and the final pass.  Kernels are in kernels.cuh; the C ABI is in capi.cu.
 #include "kernels.cuh"
 #include "persistent.cuh"
+#include "adjoint.cuh"
 #include "pgm_engine.h"
 
 #include <algorithm>
@@ -197,7 +198,7 @@ struct Engine::Impl {
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
         dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dPairA, dPairB, dPairC, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
-        dScal, dPartial, dGPartial, dPmeRec, dPmeBins, dSrcW, dGPart, dPcgPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
+        dScal, dPartial, dGPartial, dHrec, dFm, dPmeRec, dPmeBins, dSrcW, dGPart, dPcgPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dTwiddle, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
         dGradQ, dGradR, dSList, dSListCount, dPosBuild, dAtomSlot, dCandStart, dCandJ, dCandT, dGv, dSkipStart, dSkipJ;
@@ -273,7 +274,7 @@ struct Engine::Impl {
         plans64.clear();
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
                       &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dPairA, &dPairB, &dPairC, &dFlags, &dDS,
-                      &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dGPartial, &dPmeRec, &dPmeBins, &dSrcW, &dGPart,
+                      &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dGPartial, &dHrec, &dFm, &dPmeRec, &dPmeBins, &dSrcW, &dGPart,
                       &dPcgPartial, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dTwiddle, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
@@ -741,6 +742,7 @@ struct Engine::Impl {
         dSpair.ensure(9 * (size_t) n * 8);
         dFin.ensure((size_t) n * NFIN * 8);
         dPot.ensure(n * 8);
+        dHrec.ensure(6 * (size_t) n * 8);
         dGradQ.ensure(n * 8);
         dGradR.ensure(n * 8);
         dScal.ensure(nsys * NSCAL * 8);
@@ -1011,6 +1013,7 @@ struct Engine::Impl {
         d.Etot = dEtot.as<double>();
         d.fin = dFin.as<double>();
         d.potRec = dPot.as<double>();
+        d.hrec = dHrec.as<double>();
         d.forces = dForces.as<double>();
         d.results = dResults.as<double>();
         d.convPartial = dConvPartial.as<double>();
@@ -1206,6 +1209,11 @@ struct Engine::Impl {
     }
 
     bool persistentMode() const { return tfMode == TF_PCG; }
+
+    int solveDevice(double tol);
+    template <typename R>
+    void tangentPass(const Dev& d, const FmBufs& B, const double* dr, const double* dd, const double* dip,
+                     const double* quadD, int withQ);
 
     // The transform mode in use: the caller's choice where the systems' grids allow it, else cuFFT.
     void selectTransforms() {
@@ -2393,6 +2401,169 @@ Terms Engine::evaluateFixed(const double* pos, const double box[3][3], const dou
         return I.termsOf(0);
     }
     throw std::runtime_error("pgm_b200: pair list did not fit after growing it");
+}
+
+// (alpha^-1 - T) x = b for the right-hand side already in b, on the geometry of the last evaluation, every
+// system of the engine at once (rows of non-polarizable atoms: 0); the solution in x.  Returns the largest
+// iteration count.
+int Engine::Impl::solveDevice(double tol) {
+    prepareControl(true, 0, nullptr, nullptr, 0, 0.0, nullptr);
+    hCtl->histSlot = -1;
+    hCtl->customRhs = 1;
+    hCtl->guess = 1;
+    pendingSlot = -1;
+    CU(cudaMemcpyAsync(dCtl.p, hCtl, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+    Dev d = makeDev(false, 0);
+    d.tol = tol;
+    auto run = [&](auto tag) {
+        typedef decltype(tag) R;
+        CU(cudaMemsetAsync(d.flags, 0, flagBytes(), st));
+        k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, st>>>(d);
+        CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), st));
+        fieldPass<R, false>(st, side, d, 1, d.x, false);
+        k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, st>>>(d);
+        CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), st));
+        for (int it = 0; it <= s.maxIter + 1; it++) {
+            CU(cudaMemcpyAsync(hFlags, d.flags, 16 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            CU(cudaStreamSynchronize(st));
+            barrierCheck();
+            if (hFlags[2] >= nsys)
+                break;
+            enqueueIteration<R>(st, side, d);
+        }
+    };
+    if (mixed())
+        run(float());
+    else
+        run(double());
+    std::vector<double> sc((size_t) nsys * NSCAL);
+    CU(cudaMemcpyAsync(sc.data(), dScal.p, sc.size() * 8, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    hCtl->customRhs = 0;
+    int most = 0;
+    for (int k = 0; k < nsys; k++)
+        most = std::max(most, (int) sc[(size_t) k * NSCAL + SC_IT]);
+    return most;
+}
+
+// One tangent pass: the direct-space derivatives (k_pair_tangent) beside the PME tangent (spread of the tangent
+// sources, transforms with the influence product, potential and field gathered), into the pass buffers.
+template <typename R>
+void Engine::Impl::tangentPass(const Dev& d, const FmBufs& B, const double* dr, const double* dd, const double* dip,
+                               const double* quadD, int withQ) {
+    const int blocks = (int) (((long long) n * 8 + 255) / 256), wb = (n + 7) / 8;
+    k_pair_tangent<8><<<blocks, 256, 0, st>>>(d, dr, dd, B.pphi, B.pE, B.pR);
+    CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), st));
+    k_spread_tangent<R><<<wb, 256, 0, st>>>(d, dip, quadD, B.w, withQ);
+    CU(cudaGetLastError());
+    fftChain<R>(st, d, false, false);
+    k_gather_tangent<R><<<wb, 256, 0, st>>>(d, B.tphi, B.tE);
+    CU(cudaGetLastError());
+}
+
+// The force-matching gradient of the last evaluation (see adjoint.cuh): w = 2 (F - F_target) from the
+// evaluation's forces, the pass along w, the adjoint solve (alpha^-1 - T) u = -D_w E_tot, the pass along u;
+// per-atom dq, dR, dalpha and per-dipole dc = -(w-pass) + (u-pass).  Works on batched engines (every system at
+// once).  Returns the loss L = sum |F - F_target|^2 and the adjoint's iterations.
+double Engine::forceMatchingGrad(const double* fTarget, double tol, double* dq, double* dradius, double* dalpha,
+                                 double* dstrength, int* iterations) {
+    Impl& I = *impl;
+    if (!I.haveResult)
+        throw std::logic_error("pgm_b200: forceMatchingGrad needs a completed evaluation");
+    if (I.gvdwOn)
+        throw std::logic_error("pgm_b200: parameter gradients cover the electrostatics only (GVDW is set)");
+    if (I.s.peek != 0.0)
+        throw std::logic_error("pgm_b200: the force-matching adjoint needs peek = 0 (a stationary energy in mu)");
+    if (!fTarget || !(tol > 0))
+        throw std::invalid_argument("pgm_b200: forceMatchingGrad needs the target forces and tol > 0");
+    I.selectDevice();
+    const size_t n = I.n, ncov = I.covAtom.size();
+    // buffers: w, dp, pphi, pE, pR, tphi, tE, gq, gR, ga, gc, Ed
+    const size_t words = 3 * n + 3 * n + n + 3 * n + n + n + 3 * n + n + n + n + std::max<size_t>(ncov, 1) + 3 * n;
+    I.dFm.ensure(words * 8);
+    double* base = I.dFm.as<double>();
+    FmBufs B;
+    size_t off = 0;
+    auto take = [&](size_t m) {
+        double* p = base + off;
+        off += m;
+        return p;
+    };
+    B.w = take(3 * n);
+    B.dp = take(3 * n);
+    B.pphi = take(n);
+    B.pE = take(3 * n);
+    B.pR = take(n);
+    B.tphi = take(n);
+    B.tE = take(3 * n);
+    B.gq = take(n);
+    B.gR = take(n);
+    B.ga = take(n);
+    B.gc = take(std::max<size_t>(ncov, 1));
+    B.Ed = take(3 * n);
+    // w = 2 (F - F_target) and the loss, on the host (the forces of the last evaluation)
+    std::vector<double> F(3 * n), w(3 * n);
+    CU(cudaMemcpyAsync(F.data(), I.dForces.p, 3 * n * 8, cudaMemcpyDeviceToHost, I.st));
+    CU(cudaStreamSynchronize(I.st));
+    double loss = 0.0;
+    for (size_t k = 0; k < 3 * n; k++) {
+        const double r = F[k] - fTarget[k];
+        loss += r * r;
+        w[k] = 2.0 * r;
+    }
+    CU(cudaMemcpyAsync(B.w, w.data(), 3 * n * 8, cudaMemcpyHostToDevice, I.st));
+    const Dev d = I.makeDev(false, 0);
+    const int tb = (int) ((n + 255) / 256);
+    std::vector<double> gqW(n), gRW(n), gcW(ncov), gqU(n), gRU(n), gaU(n), gcU(ncov);
+    auto fetch = [&](std::vector<double>& q_, std::vector<double>& R_, std::vector<double>* a_,
+                     std::vector<double>& c_) {
+        CU(cudaMemcpyAsync(q_.data(), B.gq, n * 8, cudaMemcpyDeviceToHost, I.st));
+        CU(cudaMemcpyAsync(R_.data(), B.gR, n * 8, cudaMemcpyDeviceToHost, I.st));
+        if (a_)
+            CU(cudaMemcpyAsync(a_->data(), B.ga, n * 8, cudaMemcpyDeviceToHost, I.st));
+        if (ncov)
+            CU(cudaMemcpyAsync(c_.data(), B.gc, ncov * 8, cudaMemcpyDeviceToHost, I.st));
+        CU(cudaStreamSynchronize(I.st));
+    };
+    // the pass along w (the final pass's fields and Hessian sums are still in place)
+    k_fm_dp<<<tb, 256, 0, I.st>>>(d, B.w, B.dp);
+    if (I.mixed())
+        I.tangentPass<float>(d, B, B.w, B.dp, B.dp, d.dtot, 1);
+    else
+        I.tangentPass<double>(d, B, B.w, B.dp, B.dp, d.dtot, 1);
+    k_fm_assemble_w<<<tb, 256, 0, I.st>>>(d, B);
+    if (ncov)
+        k_fm_cov<<<(int) ((ncov + 255) / 256), 256, 0, I.st>>>(d, B, 1);
+    k_fm_rhs<<<(int) ((3 * n + 255) / 256), 256, 0, I.st>>>(d, B.Ed);
+    CU(cudaGetLastError());
+    fetch(gqW, gRW, nullptr, gcW);
+    // the adjoint solve: u in x
+    const int its = I.solveDevice(tol);
+    if (iterations)
+        *iterations = its;
+    // the pass along u
+    const double* u = I.dX.as<double>();
+    if (I.mixed())
+        I.tangentPass<float>(d, B, nullptr, u, u, nullptr, 0);
+    else
+        I.tangentPass<double>(d, B, nullptr, u, u, nullptr, 0);
+    k_fm_assemble_u<<<tb, 256, 0, I.st>>>(d, B, u);
+    if (ncov)
+        k_fm_cov<<<(int) ((ncov + 255) / 256), 256, 0, I.st>>>(d, B, 0);
+    CU(cudaGetLastError());
+    fetch(gqU, gRU, &gaU, gcU);
+    for (size_t i = 0; i < n; i++) {
+        if (dq)
+            dq[i] = -gqW[i] + gqU[i];
+        if (dradius)
+            dradius[i] = -gRW[i] + gRU[i];
+        if (dalpha)
+            dalpha[i] = gaU[i];
+    }
+    if (dstrength)
+        for (size_t m = 0; m < ncov; m++)
+            dstrength[m] = -gcW[m] + gcU[m];
+    return loss;
 }
 
 int Engine::solve(const double* rhs, double* x, double tol) {

@@ -1681,6 +1681,8 @@ __device__ __forceinline__ void gatherSlot(const Dev& dv, const SysDev& S, int s
     }
     if (FINAL && lane == 0)
         dv.potRec[i] = F2[6];
+    if (FINAL && lane < 6 && dv.hrec)   // (the potential's Hessian at the atom, for the force-matching adjoint)
+        dv.hrec[6 * (size_t) i + lane] = F2[lane];
 }
 
 // A warp per slot, reads from the grid (L2).  CGA (the CG iterations of a single-system engine): each atom's

@@ -88,6 +88,11 @@ public:
     // (alpha^-1 - T) x = rhs on the geometry of the last evaluation (rows of non-polarizable atoms: 0);
     // returns the CG iterations.
     int solve(const double* rhs, double* x, double tol);
+    // Gradient of the force-matching loss L = sum |F - F_target|^2 of the last evaluation (peek 0) with
+    // respect to the per-atom charges, radii, polarizabilities and the per-dipole strengths, by one adjoint
+    // solve to tol with analytic tangent passes; batched engines: every system at once.  Returns L.
+    double forceMatchingGrad(const double* fTarget, double tol, double* dq, double* dradius, double* dalpha,
+                             double* dstrength, int* iterations);
 
     // measurement: own kernels per evaluation; average durations [ms] of the main kernels relaunched
     // alone (0 pair list, 1 pair field pass, 2 spread, 3 gather, 4 final pair pass, 5 FFT chain, 6 CG update),

@@ -311,6 +311,20 @@ class Engine:
         _check(self._L.pgm_engine_param_grad(self._h, _d(dq), _d(dR), _d(da), _d(dc)))
         return dict(q=dq, radius=dR, alpha=da, cov_strength=dc[: self.ncov])
 
+    def force_matching_grad(self, F_target, tol=1e-10):
+        """Gradient of the force-matching loss L = sum |F - F_target|^2 of the last evaluation (peek 0) with
+        respect to the per-atom q, radius, alpha and the per-dipole strengths: one adjoint solve to ``tol`` and
+        analytic tangent passes on the GPU (pgm_engine_force_matching_grad).  Batched engines: F_target holds
+        every system's target forces, concatenated.  Returns (L, gradients dict, adjoint CG iterations)."""
+        ft = _f64(F_target, (self.n, 3))
+        dq, dR, da = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+        dc = np.zeros(max(self.ncov, 1))
+        L = ctypes.c_double(0)
+        it = ctypes.c_int(0)
+        _check(self._L.pgm_engine_force_matching_grad(self._h, _d(ft), float(tol), _d(dq), _d(dR), _d(da), _d(dc),
+                                                       ctypes.byref(L), ctypes.byref(it)))
+        return L.value, dict(q=dq, radius=dR, alpha=da, cov_strength=dc[: self.ncov]), it.value
+
     def evaluate_fixed(self, pos, box, mu, keep_list=False):
         """Energy, forces and total field [e/nm^2] at given induced dipoles, no solve (adjoint probes); with
         keep_list the previous evaluation's pair list and box are reused.  param_grad() then gives dE/dtheta at

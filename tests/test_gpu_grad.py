@@ -78,10 +78,11 @@ def test_evaluate_fixed_and_solve():
     assert np.abs(x - mu).max() <= 1e-8 * np.abs(mu).max()
 
 
-def test_force_matching_gradient_vs_finite_differences():
+@pytest.mark.parametrize("precision", [0, 1])
+def test_force_matching_gradient_vs_finite_differences(precision):
     """dL/d(per-type parameter) of L = sum |F - F_target|^2 (F_target from parameters perturbed by
     N(0, 0.05)) by one adjoint solve, against central differences of L on the FP64 oracle (h = 1e-5 relative),
-    to 1e-5 relative."""
+    to 1e-5 relative; and per atom against the oracle's analytic adjoint (FP64 1e-7, mixed 1e-5)."""
     import torch
     grad_mod = __import__("pgm_md_b200.autograd", fromlist=["autograd"])
     S = PKG.systems.waters(8, 6.3, seed=12, grid=(8, 8, 8), cutoff=3.1, tol=1e-12, lattice=2)
@@ -89,9 +90,18 @@ def test_force_matching_gradient_vs_finite_differences():
     ora_t = O.Engine(oracle_topology(Sp), oracle_settings(Sp, tol=1e-12))
     ora_t.compute(Sp.pos, Sp.box)
     Ft = ora_t.forces
-    eng = engine_for(S, PKG.FP64)
+    eng = engine_for(S, precision)
     params = grad_mod.type_parameters(S)
     L = grad_mod.force_matching_loss(eng, S, Ft, *params)
+    ora = O.Engine(oracle_topology(S), oracle_settings(S, tol=1e-12))
+    ora.compute(S.pos, S.box)
+    Lo, go = ora.force_matching_gradients(Ft)
+    eng.compute(S.pos, S.box)
+    Lg, gg, _ = eng.force_matching_grad(Ft, tol=1e-12)
+    lim = 1e-7 if precision == 0 else 1e-5
+    assert abs(Lg - Lo) <= lim * Lo
+    for k in ("q", "radius", "alpha", "cov_strength"):
+        assert np.linalg.norm(gg[k] - go[k]) <= lim * np.linalg.norm(go[k]), k
     L.backward()
     s = oracle_settings(S, tol=1e-12)
 
