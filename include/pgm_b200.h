@@ -203,6 +203,12 @@ int pgm_engine_kernel_times_cold(pgm_engine* e, int reps, void* flush_dev, size_
  * (already on the device), the predictor history saved and restored: the autotuner's measure. */
 int pgm_engine_time_evaluations(pgm_engine* e, int reps, double* ms);
 int pgm_engine_set_pair_lanes(pgm_engine* e, int lanes);
+/* PME spread and gather of the field passes (the autotuner's third knob; no counterpart in the reference):
+ * 0 a warp per atom with p^3 global atomics / loads; 1 plane-owner tiles -- a block per (x-plane, 16-row chunk)
+ * accumulates or reads its tile in shared memory for the atoms whose stencil reaches it (mixed precision, one
+ * system, order 6; elsewhere 0 runs).  pgm_engine_pme_kernels tells which runs. */
+int pgm_engine_set_pme_kernels(pgm_engine* e, int kind);
+int pgm_engine_pme_kernels(pgm_engine* e);
 int pgm_engine_pair_lanes(pgm_engine* e);
 /* Field-pass transforms (the autotuner's second knob; no counterpart in the reference, which calls cuFFT):
  * 0 cuFFT R2C / C2R 3D plans with an influence-product kernel; 1 one kernel per pass in which a thread-block

@@ -76,6 +76,8 @@ SIGNATURES = {
     "pgm_engine_kernel_times_cold": (c_int, [c_void_p, c_int, c_void_p, ctypes.c_size_t, P_D]),
     "pgm_engine_time_evaluations": (c_int, [c_void_p, c_int, P_D]),
     "pgm_engine_set_pair_lanes": (c_int, [c_void_p, c_int]),
+    "pgm_engine_set_pme_kernels": (c_int, [c_void_p, c_int]),
+    "pgm_engine_pme_kernels": (c_int, [c_void_p]),
     "pgm_engine_pair_lanes": (c_int, [c_void_p]),
     "pgm_engine_set_transforms": (c_int, [c_void_p, c_int]),
     "pgm_engine_transforms": (c_int, [c_void_p]),

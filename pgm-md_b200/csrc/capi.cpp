@@ -406,6 +406,13 @@ int pgm_engine_time_evaluations(pgm_engine* e, int reps, double* ms) {
     });
 }
 
+int pgm_engine_set_pme_kernels(pgm_engine* e, int kind) {
+    NEED(e);
+    return guarded([&] { e->e->setPmeKernels(kind); });
+}
+
+int pgm_engine_pme_kernels(pgm_engine* e) { return (e && e->e) ? e->e->pmeKernels() : -1; }
+
 int pgm_engine_set_pair_lanes(pgm_engine* e, int lanes) {
     NEED(e);
     return guarded([&] { e->e->setPairLanes(lanes); });

@@ -6,6 +6,7 @@
 #include "kernels.cuh"
 #include "persistent.cuh"
 #include "adjoint.cuh"
+#include "planes.cuh"
 #include "pgm_engine.h"
 
 #include <algorithm>
@@ -186,6 +187,10 @@ struct Engine::Impl {
     bool splitOk = false;      // the systems' x extents allow the x-line kernel
     bool gridOk = false;       // the systems' grids and the GPU allow the grid-transform kernel
     bool pcgOk = false;        // the persistent CG kernel applies (mixed, one system, grid kernel, order 6)
+    bool planesOk = false;     // the plane-owner spread and gather apply (mixed, one system, order 6)
+    int pmeWant = 0;           // the caller's choice of spread / gather kernels: 0 a warp per atom, 1 plane tiles
+    int planeNyc = 1;          // row chunks per x-plane of the plane-owner kernels
+    size_t planeSmem = 0;
     int pcgBlocks = 0;         // its blocks (one per SM)
     size_t pcgSmem = 0;
     int fftcBuf = 0, fftcC = 16, fftgBuf = 0, maxK0 = 0;
@@ -198,7 +203,7 @@ struct Engine::Impl {
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
         dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dPairA, dPairB, dPairC, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
-        dScal, dPartial, dGPartial, dHrec, dFm, dPmeRec, dPmeBins, dSrcW, dGPart, dPcgPartial, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
+        dScal, dPartial, dGPartial, dHrec, dFm, dPmeRec, dPmeBins, dSrcW, dGPart, dPcgPartial, dBinCount, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dTwiddle, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
         dGradQ, dGradR, dSList, dSListCount, dPosBuild, dAtomSlot, dCandStart, dCandJ, dCandT, dGv, dSkipStart, dSkipJ;
@@ -275,7 +280,7 @@ struct Engine::Impl {
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
                       &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dPairA, &dPairB, &dPairC, &dFlags, &dDS,
                       &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dGPartial, &dHrec, &dFm, &dPmeRec, &dPmeBins, &dSrcW, &dGPart,
-                      &dPcgPartial, &dSysCounter, &dEpair,
+                      &dPcgPartial, &dBinCount, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dTwiddle, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
                       &dCovByAtomOff, &dCovByAtom, &dCovByPartnerOff, &dCovByPartner, &dChunkSys, &dChunkBegin,
@@ -688,6 +693,7 @@ struct Engine::Impl {
         for (int k = 0; k < nsys; k++)
             maxLineBlocks = std::max(maxLineBlocks, (sysK[k][1] * (sysK[k][2] / 2 + 1) + XL_LINES - 1) / XL_LINES);
         preparePersistent();
+        preparePlanes();
         selectTransforms();
         // chunks
         chunkSys.clear();
@@ -1172,6 +1178,42 @@ struct Engine::Impl {
         dPcgPartial.ensure((size_t) 2 * pcgBlocks * 4 * 8);
     }
 
+    // The plane-owner spread and gather: mixed precision, one system, order 6; tiles of PL_YCH rows (+ 5 halo
+    // rows) of an x-plane in shared memory.
+    void preparePlanes() {
+        planesOk = false;
+        if (!mixed() || nsys != 1 || s.order != 6)
+            return;
+        const int* K = sysK[0].data();
+        planeNyc = (K[1] + PL_YCH - 1) / PL_YCH;
+        planeSmem = (size_t) (PL_YCH + 5) * K[2] * sizeof(float);
+        int optin = 0;
+        CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, devId));
+        if (planeSmem > (size_t) optin)
+            return;
+        for (const void* f : {(const void*) k_spread_planes<6>, (const void*) k_gather_planes<6>})
+            CU(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) planeSmem));
+        const size_t nbins = (size_t) K[0] * planeNyc;
+        dPmeRec.ensure((size_t) n * sizeof(PmeRec<6>));
+        dPmeBins.ensure((std::max<size_t>(nbins, FFT_MAXK) + 1) * sizeof(int));
+        dBinCount.ensure(nbins * sizeof(int));
+        dSrcW.ensure((size_t) n * sizeof(float4));
+        dGPart.ensure((size_t) 6 * n * sizeof(float4));
+        planesOk = true;
+    }
+
+    bool planesMode() const { return planesOk && pmeWant == 1 && tfMode != TF_PCG; }
+
+    // The plane bins and records of the evaluation (after k_splines).
+    void enqueuePlaneBins(cudaStream_t sm, const Dev& d) {
+        const int nbins = sysK[0][0] * planeNyc, tb = (n + 255) / 256;
+        CU(cudaMemsetAsync(dBinCount.p, 0, nbins * sizeof(int), sm));
+        k_plane_bin_count<<<tb, 256, 0, sm>>>(d, planeNyc, dBinCount.as<int>());
+        k_plane_bin_scan<<<1, 1024, 0, sm>>>(d, nbins, dBinCount.as<int>());
+        k_plane_bin_fill<6><<<tb, 256, 0, sm>>>(d, planeNyc, dBinCount.as<int>());
+        CU(cudaGetLastError());
+    }
+
     // The persistent kernel for the pair lanes (8, 16 or 32; 4 runs as 8) and the grid's compile-time size.
     void (*persistentKernel(int lanes))(Dev) {
         const int kc = fftgKc;
@@ -1300,6 +1342,12 @@ struct Engine::Impl {
     }
 
     template <typename R> void launchSpread(cudaStream_t sm, const Dev& d, int mode, double* vec) {
+        if (std::is_same<R, float>::value && planesMode()) {   // sources per slot, then plane tiles
+            k_plane_sources<<<(n + 255) / 256, 256, 0, sm>>>(d, mode, vec);
+            k_spread_planes<6><<<dim3(sysK[0][0], planeNyc), PL_THREADS, planeSmem, sm>>>(d, planeNyc);
+            CU(cudaGetLastError());
+            return;
+        }
         const int wb = (n + 7) / 8;
         switch (s.order) {
         case 4: k_spread<R, 4><<<wb, 256, 0, sm>>>(d, mode, vec); break;
@@ -1313,6 +1361,12 @@ struct Engine::Impl {
 
     // CGA: the CG iteration's gather of a single-system engine, with A p and alph in its epilogue.
     template <typename R, bool FINAL, bool CGA = false> void launchGather(cudaStream_t sm, const Dev& d, int gate) {
+        if (std::is_same<R, float>::value && !FINAL && !CGA && planesMode()) {   // plane tiles, then E_rec per atom
+            k_gather_planes<6><<<dim3(sysK[0][0], planeNyc), PL_THREADS, planeSmem, sm>>>(d, planeNyc);
+            k_gather_planes_finish<6><<<(n + 255) / 256, 256, 0, sm>>>(d);
+            CU(cudaGetLastError());
+            return;
+        }
         const int wb = (n + 7) / 8;
         switch (s.order) {
         case 4: k_gather<R, FINAL, 4, CGA><<<wb, 256, 0, sm>>>(d, gate); break;
@@ -1449,6 +1503,8 @@ struct Engine::Impl {
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
             if (persistentMode())
                 k_pme_bins<6><<<1, 1024, 0, sm>>>(d);
+            else if (std::is_same<R, float>::value && planesMode())
+                enqueuePlaneBins(sm, d);
             k_perm<<<tb, 256, 0, sm>>>(d);
             k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
@@ -1468,6 +1524,8 @@ struct Engine::Impl {
         } else {
             pairRecords<R>(sm, d);
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
+            if (std::is_same<R, float>::value && planesMode())
+                enqueuePlaneBins(sm, d);
             k_perm<<<tb, 256, 0, sm>>>(d);
             k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
             CU(cudaGetLastError());
@@ -1475,7 +1533,7 @@ struct Engine::Impl {
     }
 
     template <typename R> void enqueueIteration(cudaStream_t sm, cudaStream_t sd, const Dev& d) {
-        if (nsys == 1 && fuseCgA) {   // A p and alph in the gather's epilogue
+        if (nsys == 1 && fuseCgA && !(std::is_same<R, float>::value && planesMode())) {   // A p, alph in the gather
             fieldPass<R, false, true>(sm, sd, d, 2, d.p, true);
         } else {
             fieldPass<R, false>(sm, sd, d, 2, d.p, true);
@@ -2367,6 +2425,8 @@ Terms Engine::evaluateFixed(const double* pos, const double box[3][3], const dou
                 k_pair_compact<R><<<(I.n + 7) / 8, 256, 0, I.st>>>(d);
             }
             k_splines<R><<<(3 * I.n + 255) / 256, 256, 0, I.st>>>(d);
+            if (std::is_same<R, float>::value && I.planesMode())
+                I.enqueuePlaneBins(I.st, d);
             k_perm<<<tb, 256, 0, I.st>>>(d);
             k_influence<R><<<dim3(I.convBlocks, I.nsys), 256, 0, I.st>>>(d);
             CU(cudaGetLastError());
@@ -2740,6 +2800,21 @@ double Engine::timeEvaluations(int reps) {
     std::sort(t.begin(), t.end());
     return t[t.size() / 2];
 }
+
+// The PME spread / gather kernels of the field passes: 0 a warp per atom (every engine), 1 plane-owner tiles in
+// shared memory (mixed precision, one system, order 6; else 0 runs).
+void Engine::setPmeKernels(int kind) {
+    if (kind != 0 && kind != 1)
+        throw std::invalid_argument("pgm_b200: PME kernels must be 0 (a warp per atom) or 1 (plane tiles)");
+    Impl& I = *impl;
+    if (kind != I.pmeWant && I.exec) {
+        cudaGraphExecDestroy(I.exec);
+        I.exec = nullptr;
+    }
+    I.pmeWant = kind;
+}
+
+int Engine::pmeKernels() const { return impl->planesMode() ? 1 : 0; }
 
 void Engine::setPairLanes(int lanes) {
     if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)

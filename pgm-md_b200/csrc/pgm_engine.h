@@ -106,6 +106,10 @@ public:
     // 2 cuFFT 2D plans over the x-planes + one x-line kernel with the influence product, 3 one cooperative kernel
     // with a block per x-plane (1, 2 and 3 where the grids allow them; transforms() tells which runs)
     void setTransforms(int mode);
+    // PME spread / gather of the field passes: 0 a warp per atom, 1 plane-owner tiles in shared memory (mixed
+    // precision, one system, order 6; pmeKernels() tells which runs)
+    void setPmeKernels(int kind);
+    int pmeKernels() const;
     int transforms() const;
     int pairLanes() const;
 

@@ -370,6 +370,14 @@ class Engine:
         _check(self._L.pgm_engine_time_evaluations(self._h, int(reps), ctypes.byref(ms)))
         return ms.value
 
+    def set_pme_kernels(self, kind):
+        """PME spread / gather of the field passes: 0 a warp per atom, 1 plane-owner tiles in shared memory
+        (mixed precision, one system, order 6); pme_kernels() tells which runs."""
+        _check(self._L.pgm_engine_set_pme_kernels(self._h, int(kind)))
+
+    def pme_kernels(self):
+        return int(self._L.pgm_engine_pme_kernels(self._h))
+
     def set_pair_lanes(self, lanes):
         _check(self._L.pgm_engine_set_pair_lanes(self._h, int(lanes)))
 
@@ -402,14 +410,19 @@ class Engine:
             self.set_transforms(mode)
             if self.transforms() != mode:
                 continue
-            for lanes in candidates:
-                self.set_pair_lanes(lanes)
-                self.time_evaluations(2)   # (captures the graph of this choice)
-                report[(lanes, mode)] = self.time_evaluations(reps)
-        lanes, mode = min(report, key=report.get)
+            for pme in (0, 1):
+                self.set_pme_kernels(pme)
+                if self.pme_kernels() != pme:
+                    continue
+                for lanes in candidates:
+                    self.set_pair_lanes(lanes)
+                    self.time_evaluations(2)   # (captures the graph of this choice)
+                    report[(lanes, mode, pme)] = self.time_evaluations(reps)
+        lanes, mode, pme = min(report, key=report.get)
         self.set_pair_lanes(lanes)
         self.set_transforms(mode)
-        self.autotune_report = {f"lanes{k[0]}_transforms{k[1]}": v for k, v in report.items()}
+        self.set_pme_kernels(pme)
+        self.autotune_report = {f"lanes{k[0]}_transforms{k[1]}_pme{k[2]}": v for k, v in report.items()}
         return lanes
 
     # ---------------------------------------------------------------- batched

@@ -25,10 +25,11 @@ def rel_rms(a, b):
     return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
 
 
-def single_engine(S, precision, tol):
+def single_engine(S, precision, tol, pme=0):
     e = PKG.Engine(PKG.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=6, tol=tol, max_iter=500, peek=0.0,
                                 predictor=0, ke=PKG.systems.KE_DEFAULT, precision=precision))
     e.set_system(S)
+    e.set_pme_kernels(pme)
     return e
 
 
@@ -40,10 +41,12 @@ def water98304():
     return S, d
 
 
-@pytest.mark.parametrize("precision,tol", [(PKG.FP64, 1e-10), (PKG.MIXED, 1e-5), (PKG.MIXED, 1e-4)])
-def test_water98304_against_reference(water98304, precision, tol):
+@pytest.mark.parametrize("precision,tol,pme", [(PKG.FP64, 1e-10, 0), (PKG.MIXED, 1e-5, 0), (PKG.MIXED, 1e-4, 0),
+                                               (PKG.MIXED, 1e-5, 1)])
+def test_water98304_against_reference(water98304, precision, tol, pme):
     S, d = water98304
-    eng = single_engine(S, precision, tol)
+    eng = single_engine(S, precision, tol, pme)
+    assert eng.pme_kernels() == pme
     r = eng.compute(S.pos, S.box)
     mu = eng.induced_dipoles()
     eng.close()

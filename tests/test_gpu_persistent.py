@@ -13,12 +13,13 @@ from conftest import PKG, load_dmp_real, load_golden_system
 pytestmark = pytest.mark.gpu
 
 
-def mixed_engine(S, mode, tol=1e-10, lanes=16):
+def mixed_engine(S, mode, tol=1e-10, lanes=16, pme=0):
     e = PKG.Engine(PKG.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=6, tol=tol, max_iter=500, peek=0.0,
                                 predictor=0, ke=PKG.systems.KE_DEFAULT, precision=PKG.MIXED, skin=0.0))
     e.set_system(S)
     e.set_pair_lanes(lanes)
     e.set_transforms(mode)
+    e.set_pme_kernels(pme)
     return e
 
 
@@ -76,3 +77,34 @@ def test_persistent_cg_not_applicable_falls_back():
     e.set_transforms(4)
     assert e.transforms() != 4
     e.close()
+
+
+@pytest.mark.parametrize("name", ["water216", "tiny_triclinic", "dmp8550_real"])
+@pytest.mark.parametrize("mode", [0, 3])
+def test_plane_owner_spread_gather_against_reference(name, mode):
+    """The plane-owner spread and gather (PME kernels 1: tiles of 16 rows of an x-plane in shared memory) with
+    cuFFT (mode 0) and with the grid kernel (mode 3), against the reference's outputs and against the warp-per-atom
+    kernels (the same CG iterations)."""
+    S, d = golden(name)
+    eng = mixed_engine(S, mode, pme=1)
+    assert eng.pme_kernels() == 1
+    r = eng.compute(S.pos, S.box)
+    base = mixed_engine(S, mode, pme=0)
+    g = base.compute(S.pos, S.box)
+    e_ref = float(d["energy"])
+    F = np.asarray(d["forces"], np.float64)
+    assert abs(r.energy - e_ref) <= 1e-6 * abs(e_ref), (r.energy, e_ref)
+    assert np.linalg.norm(r.forces - F) <= 1e-5 * np.linalg.norm(F)
+    assert r.iterations == g.iterations
+    kt = eng.kernel_times(reps=3)
+    assert kt["spread"] > 0 and kt["gather"] > 0
+    eng.close()
+    base.close()
+
+
+def test_plane_owner_with_the_persistent_kernel_is_exclusive():
+    """Mode 4 runs its own in-loop PME; asking for plane tiles as well leaves mode 4 in charge."""
+    S, _ = golden("tiny_triclinic")
+    eng = mixed_engine(S, 4, pme=1)
+    assert eng.transforms() == 4 and eng.pme_kernels() == 0
+    eng.close()
