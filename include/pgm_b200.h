@@ -123,7 +123,9 @@ int pgm_engine_release_positions(pgm_engine* e);
  * positions from the device array posq4 (float4, w ignored, caller order); forces added atomically to the
  * device 64-bit fixed-point buffer force_fixed (x of atom i at i, y at i + stride, z at i + 2 stride,
  * scale fixed_scale); stream: the caller's cudaStream_t (its work so far comes first).  finish_device sets
- * *valid = 1 (the list is rebuilt every evaluation, so an evaluation is never stale). */
+ * *valid = 0 when the evaluation must be repeated (the pair list outgrew its rows and was grown, or a pair
+ * within the cutoff changed its image since the list's build and the list is rebuilt), as the reference's
+ * finishDevice returns false (core/cuda/pgm_cuda.h:107); else 1. */
 int pgm_engine_launch_device(pgm_engine* e, const void* posq4, const double* box, int new_step,
                              long long* force_fixed, int stride, double fixed_scale, void* stream);
 int pgm_engine_finish_device(pgm_engine* e, pgm_terms* terms, int* valid);
