@@ -772,6 +772,7 @@ def batch_leg(pkg, local, rank, world, dist):
         per_mode[mode] = float(t.item())
     eng.set_transforms(chosen)
     res["r"] = eng.compute_batch(pos, boxes)
+    active = eng.active_systems()
     dt = per_mode[chosen]
     # main kernels relaunched alone; the field pair pass streams P x 24-byte pair records (mixed) from HBM here
     kt = eng.kernel_times(reps=3)
@@ -784,6 +785,7 @@ def batch_leg(pkg, local, rank, world, dist):
     out = {"workload": "water_batch1024", "systems": len(systems), "atoms": int(sum(s.n for s in systems)),
            "systems_per_s": len(systems) / dt, "ms_per_batch": 1e3 * dt,
            "max_cg_iterations": int(res["r"]["iterations"].max()), "partition": "atom-balanced, one launch per rank",
+           "active_systems_per_iteration": active,
            "pair_lanes": lanes, "transforms": TRANSFORMS[chosen],
            "ms_per_batch_by_transforms": {TRANSFORMS[m]: 1e3 * v for m, v in per_mode.items()},
            "directed_pairs": npairs, "kernel_ms": kt,

@@ -197,6 +197,10 @@ int pgm_engine_force_matching_grad(pgm_engine* e, const double* f_target, double
  * [2] PME spread, [3] PME gather, [4] final pair pass, [5] FFT chain (r2c, convolution, c2r), [6] CG kernel.
  * pair lanes: lanes per atom of the pair passes (4, 8, 16 or 32; the autotuner's knob). */
 int pgm_engine_kernel_launches(pgm_engine* e);
+/* Batched engines: the number of systems still iterating before each CG iteration of the last evaluation
+ * (counts[k], k = 0 .. its iterations; converged systems retire from the loop); returns how many values were
+ * written (at most cap), or a negative status. */
+int pgm_engine_active_systems(pgm_engine* e, int* counts, int cap);
 int pgm_engine_kernel_times(pgm_engine* e, int reps, double* ms);
 /* The same kernels timed cold: before each of the reps launches the caller's device buffer flush_dev
  * (flush_bytes, larger than the 126 MB L2) is overwritten, and only the launch lies between the events. */

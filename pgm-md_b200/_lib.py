@@ -72,6 +72,7 @@ SIGNATURES = {
     "pgm_engine_solve": (c_int, [c_void_p, P_D, P_D, c_double, P_I]),
     "pgm_engine_force_matching_grad": (c_int, [c_void_p, P_D, c_double, P_D, P_D, P_D, P_D, P_D, P_I]),
     "pgm_engine_kernel_launches": (c_int, [c_void_p]),
+    "pgm_engine_active_systems": (c_int, [c_void_p, P_I, c_int]),
     "pgm_engine_kernel_times": (c_int, [c_void_p, c_int, P_D]),
     "pgm_engine_kernel_times_cold": (c_int, [c_void_p, c_int, c_void_p, ctypes.c_size_t, P_D]),
     "pgm_engine_time_evaluations": (c_int, [c_void_p, c_int, P_D]),

@@ -377,6 +377,17 @@ int pgm_engine_force_matching_grad(pgm_engine* e, const double* f_target, double
     });
 }
 
+int pgm_engine_active_systems(pgm_engine* e, int* counts, int cap) {
+    if (!e || !e->e || !counts || cap < 0)
+        return -1;
+    try {
+        return e->e->activeSystems(counts, cap);
+    } catch (const std::exception& ex) {
+        g_lastError = ex.what();
+        return PGM_ERR_CUDA;
+    }
+}
+
 int pgm_engine_kernel_launches(pgm_engine* e) { return (e && e->e) ? e->e->kernelLaunches() : -1; }
 
 int pgm_engine_kernel_times(pgm_engine* e, int reps, double* ms) {

@@ -125,6 +125,8 @@ struct Dev {
     double* partial;          // nChunks * 16
     double* gpartial;         // per gather block: p . A p partials (the CG gather of a single-system engine)
     int* sysCounter;          // nSys
+    int* activeHist;          // batched CG: systems still iterating before iteration k (k = 0 .. iterations);
+                              // flags[13] counts the loop's iterations
     // fields / forces
     double* Epair;            // 3n
     double* Erec;             // 3n

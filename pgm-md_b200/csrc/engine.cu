@@ -203,7 +203,7 @@ struct Engine::Impl {
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
         dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dPairA, dPairB, dPairC, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
-        dScal, dPartial, dGPartial, dHrec, dFm, dPmeRec, dPmeBins, dSrcW, dGPart, dPcgPartial, dBinCount, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
+        dScal, dPartial, dGPartial, dHrec, dFm, dPmeRec, dPmeBins, dSrcW, dGPart, dPcgPartial, dBinCount, dActive, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dTwiddle, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
         dGradQ, dGradR, dSList, dSListCount, dPosBuild, dAtomSlot, dCandStart, dCandJ, dCandT, dGv, dSkipStart, dSkipJ;
@@ -280,7 +280,7 @@ struct Engine::Impl {
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
                       &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dPairA, &dPairB, &dPairC, &dFlags, &dDS,
                       &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dGPartial, &dHrec, &dFm, &dPmeRec, &dPmeBins, &dSrcW, &dGPart,
-                      &dPcgPartial, &dBinCount, &dSysCounter, &dEpair,
+                      &dPcgPartial, &dBinCount, &dActive, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dTwiddle, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
                       &dCovByAtomOff, &dCovByAtom, &dCovByPartnerOff, &dCovByPartner, &dChunkSys, &dChunkBegin,
@@ -755,6 +755,7 @@ struct Engine::Impl {
         dPartial.ensure(chunkSys.size() * 16 * 8);
         dGPartial.ensure(((size_t) n + 7) / 8 * 8);
         dSysCounter.ensure(nsys * sizeof(int));
+        dActive.ensure(((size_t) s.maxIter + 2) * sizeof(int));
         CU(cudaMemset(dSysCounter.p, 0, nsys * sizeof(int)));
         dResults.ensure(nsys * NRES * 8);
         dConvPartial.ensure((size_t) nsys * convBlocks * NCONV * 8);
@@ -1011,6 +1012,7 @@ struct Engine::Impl {
         d.partial = dPartial.as<double>();
         d.gpartial = dGPartial.as<double>();
         d.sysCounter = dSysCounter.as<int>();
+        d.activeHist = dActive.as<int>();
         d.Epair = dEpair.as<double>();
         d.Erec = dErec.as<double>();
         d.Fpair = dFpair.as<double>();
@@ -2667,6 +2669,21 @@ int Engine::solve(const double* rhs, double* x, double tol) {
     CU(cudaStreamSynchronize(I.st));
     I.hCtl->customRhs = 0;
     return (int) sc[SC_IT];
+}
+
+// Systems still iterating before each CG iteration of the last batched evaluation (k = 0 .. its iterations),
+// at most cap values; returns how many were written.
+int Engine::activeSystems(int* counts, int cap) const {
+    const Impl& I = *impl;
+    if (!I.haveResult || I.nsys < 2 || !I.s.polarizable)
+        return 0;
+    int it = 0;
+    for (int k = 0; k < I.nsys; k++)
+        it = std::max(it, (int) I.lastResults[(size_t) k * NRES + 14]);
+    const int m = std::min(cap, std::min(it + 1, I.s.maxIter + 2));
+    if (m > 0)
+        CU(cudaMemcpy(counts, I.dActive.p, m * sizeof(int), cudaMemcpyDeviceToHost));
+    return m;
 }
 
 int Engine::kernelLaunches() const {

@@ -2118,6 +2118,8 @@ __global__ void __launch_bounds__(CHUNK) k_cg_init(Dev dv) {
             dv.flags[5] = dv.nSys - ndone;
             dv.flags[4] = 0;
             dv.flags[3] = 0;
+            if (dv.activeHist && dv.maxIter >= 0)
+                dv.activeHist[0] = dv.nSys - ndone;
             if (dv.useCond && dv.loopCond)
                 cudaGraphSetConditional(dv.cond, (ndone < dv.nSys) ? 1u : 0u);
         }
@@ -2255,6 +2257,9 @@ __global__ void __launch_bounds__(CHUNK) k_cg_upd(Dev dv) {
             const int ndone = atomicAdd(&dv.flags[2], 0);
             dv.flags[5] = dv.nSys - ndone;   // systems active in the next iteration
             dv.flags[4] = 0;
+            const int loopIt = ++dv.flags[13];
+            if (dv.activeHist && loopIt <= dv.maxIter + 1)
+                dv.activeHist[loopIt] = dv.nSys - ndone;
             if (dv.useCond)
                 cudaGraphSetConditional(dv.cond, (ndone < dv.nSys) ? 1u : 0u);
         }

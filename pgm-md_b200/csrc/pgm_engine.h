@@ -98,6 +98,8 @@ public:
     // alone (0 pair list, 1 pair field pass, 2 spread, 3 gather, 4 final pair pass, 5 FFT chain, 6 CG update),
     // warm (back to back) or, with a flush buffer larger than L2, cold (the buffer overwritten before each launch)
     int kernelLaunches() const;
+    // batched CG: systems still iterating before each iteration of the last evaluation; returns the count
+    int activeSystems(int* counts, int cap) const;
     void kernelTimes(int reps, double* ms, void* flush = nullptr, size_t flushBytes = 0);
     // median device time [ms] of reps whole new-step evaluations at the last evaluation's positions
     double timeEvaluations(int reps);

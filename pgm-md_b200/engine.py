@@ -351,6 +351,14 @@ class Engine:
 
     KERNELS = ("pair_list", "pair_field", "spread", "gather", "pair_final", "fft_chain", "cg_update")
 
+    def active_systems(self):
+        """Batched engines: systems still iterating before each CG iteration of the last evaluation."""
+        counts = np.zeros(1024, np.int32)
+        m = int(self._L.pgm_engine_active_systems(self._h, _i(counts), len(counts)))
+        if m < 0:
+            raise PgmError(m, self._L.pgm_last_error().decode())
+        return counts[:m].tolist()
+
     def kernel_times(self, reps=20, flush_ptr=None, flush_bytes=0):
         """Average device durations [ms] of the main kernels relaunched alone (CUDA events on the engine's
         stream) after an evaluation: warm (back to back), or cold when a device buffer larger than L2 is given

@@ -89,3 +89,18 @@ def test_batch_param_gradients():
             assert np.linalg.norm(g[k][part] - ref) <= 1e-7 * np.linalg.norm(ref), (k, S.n)
         off += S.n
         coff += len(S.cov_atom)
+
+
+def test_batch_retires_converged_systems():
+    """The batched CG retires converged systems: the count of systems still iterating before each iteration
+    (pgm_engine_active_systems) equals the number of systems whose own iteration count exceeds it, and falls to
+    zero at the last iteration."""
+    systems = PKG.systems.water_batch(nsys=10, seed=9, nmin=8, nmax=120, tol=1e-9)
+    eng = batch_engine(systems, PKG.FP64, tol=1e-9)
+    out = eng.compute_batch(np.concatenate([s.pos for s in systems]), np.stack([s.box for s in systems]))
+    counts = eng.active_systems()
+    its = np.asarray(out["iterations"])
+    assert len(counts) == its.max() + 1
+    assert counts == [int(np.sum(its > k)) for k in range(its.max() + 1)]
+    assert counts[-1] == 0 and all(a >= b for a, b in zip(counts, counts[1:]))
+    eng.close()
