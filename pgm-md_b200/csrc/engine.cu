@@ -692,8 +692,8 @@ struct Engine::Impl {
         maxLineBlocks = 0;
         for (int k = 0; k < nsys; k++)
             maxLineBlocks = std::max(maxLineBlocks, (sysK[k][1] * (sysK[k][2] / 2 + 1) + XL_LINES - 1) / XL_LINES);
-        preparePersistent();
         preparePlanes();
+        preparePersistent();
         selectTransforms();
         // chunks
         chunkSys.clear();
@@ -1155,8 +1155,8 @@ struct Engine::Impl {
     // (one per SM), and its shared memory.
     void preparePersistent() {
         pcgOk = false;
-        if (!mixed() || nsys != 1 || !gridOk || s.order != 6 || !s.polarizable)
-            return;
+        if (!mixed() || nsys != 1 || !gridOk || !planesOk || s.order != 6 || !s.polarizable)
+            return;   // (it takes the plane-owner kernels' bins)
         int sms = 0, coop = 0, optin = 0;
         CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, devId));
         CU(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, devId));
@@ -1165,7 +1165,7 @@ struct Engine::Impl {
         pcgSmem = (3 * (size_t) FFT_MAXK + 2 * (size_t) fftgBuf) * 8 + (size_t) K[1] * K[2] * 8;
         if (!coop || pcgSmem > (size_t) optin || K[0] + PCG_MIN_PAIR_BLOCKS > sms)
             return;
-        void (*kfn)(Dev) = persistentKernel(pairGS);
+        void (*kfn)(Dev, int) = persistentKernel(pairGS);
         CU(cudaFuncSetAttribute((const void*) kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) pcgSmem));
         int perSm = 0;
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kfn, PCG_THREADS, pcgSmem));
@@ -1204,7 +1204,7 @@ struct Engine::Impl {
         planesOk = true;
     }
 
-    bool planesMode() const { return planesOk && pmeWant == 1 && tfMode != TF_PCG; }
+    bool planesMode() const { return planesOk && pmeWant == 1; }
 
     // The plane bins and records of the evaluation (after k_splines).
     void enqueuePlaneBins(cudaStream_t sm, const Dev& d) {
@@ -1217,9 +1217,9 @@ struct Engine::Impl {
     }
 
     // The persistent kernel for the pair lanes (8, 16 or 32; 4 runs as 8) and the grid's compile-time size.
-    void (*persistentKernel(int lanes))(Dev) {
+    void (*persistentKernel(int lanes))(Dev, int) {
         const int kc = fftgKc;
-        auto pick = [&](auto gsTag) -> void (*)(Dev) {
+        auto pick = [&](auto gsTag) -> void (*)(Dev, int) {
             constexpr int GS = decltype(gsTag)::value;
             switch (kc) {
             case 32: return k_cg_persistent<6, GS, 32>;
@@ -1237,7 +1237,7 @@ struct Engine::Impl {
 
     // The whole CG loop: one cooperative launch of the persistent kernel (one block per SM).
     void launchPersistent(cudaStream_t sm, const Dev& d) {
-        void (*kfn)(Dev) = persistentKernel(pairGS);
+        void (*kfn)(Dev, int) = persistentKernel(pairGS);
         CU(cudaFuncSetAttribute((const void*) kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) pcgSmem));
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute at[1];
@@ -1249,7 +1249,7 @@ struct Engine::Impl {
         cfg.stream = sm;
         cfg.attrs = at;
         cfg.numAttrs = 1;
-        CU(cudaLaunchKernelEx(&cfg, kfn, d));
+        CU(cudaLaunchKernelEx(&cfg, kfn, d, planeNyc));
     }
 
     bool persistentMode() const { return tfMode == TF_PCG; }
@@ -1503,9 +1503,7 @@ struct Engine::Impl {
             pairRecords<R>(sd, d);
             CU(cudaEventRecord(evJoin, sd));
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
-            if (persistentMode())
-                k_pme_bins<6><<<1, 1024, 0, sm>>>(d);
-            else if (std::is_same<R, float>::value && planesMode())
+            if (std::is_same<R, float>::value && (planesMode() || persistentMode()))
                 enqueuePlaneBins(sm, d);
             k_perm<<<tb, 256, 0, sm>>>(d);
             k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);

@@ -38,62 +38,19 @@ template <int P> struct PmeRec {
     float c[6 * P];
 };
 
-// Plane bins of a single system's atoms: slots ordered by b0 mod K0 (the x-plane of their j1 = 0 stencil
-// point), so that the block of plane x finds the atoms that reach it, b0 = x .. x + P - 1 (mod K0), in P
-// consecutive bins; and each binned atom's spline record (from k_splines' coefficients).  One block, once per
-// evaluation.  The order inside a bin follows the atomics; nothing downstream depends on it (the spread's
-// fixed-point sums commute exactly and every gather result has a slot of its own).
-template <int P>
-__global__ void __launch_bounds__(1024) k_pme_bins(Dev dv) {
-    __shared__ int fill[FFT_MAXK];
-    const SysDev& S = dv.sys[0];
-    const int K0 = S.K[0], n = dv.nAtoms;
-    for (int b = threadIdx.x; b < K0; b += blockDim.x)
-        fill[b] = 0;
-    __syncthreads();
-    for (int slot = threadIdx.x; slot < n; slot += blockDim.x)
-        atomicAdd(&fill[wrapIndex(dv.baseS[slot].x, K0)], 1);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int b = 0; b < K0; b++) {
-            const int c = fill[b];
-            fill[b] = acc;
-            dv.pmeBinStart[b] = acc;
-            acc += c;
-        }
-        dv.pmeBinStart[K0] = acc;
-    }
-    __syncthreads();
-    PmeRec<P>* rec = (PmeRec<P>*) dv.pmeRec;
-    const float* spl = (const float*) dv.spl;
-    for (int slot = threadIdx.x; slot < n; slot += blockDim.x) {
-        const int4 b = dv.baseS[slot];
-        const int b0 = wrapIndex(b.x, K0);
-        PmeRec<P>& r = rec[atomicAdd(&fill[b0], 1)];
-        r.idx = make_int4(slot, b.y, b.z, b0);
-        const float* sp = spl + (size_t) slot * 9 * MAXP;
-#pragma unroll
-        for (int dim = 0; dim < 3; dim++)
-#pragma unroll
-            for (int kind = 0; kind < 2; kind++)
-#pragma unroll
-                for (int j = 0; j < P; j++)
-                    r.c[dim * 2 * P + kind * P + j] = sp[(kind * 3 + dim) * MAXP + j];
-    }
-}
-
-// The atoms that reach plane x: bin (x + j1) mod K0 for j1 < P; t-th of them -> (j1, record index).
+// The atoms that reach plane x: those of b0 = (x + j1) mod K0 for j1 < P, bins b0 nyc .. b0 nyc + nyc - 1 (the
+// plane-owner kernels' bins by x-plane and row chunk, contiguous per x-plane; nyc = 1: bins by x-plane only);
+// t-th of them -> (j1, record index).
 template <int P>
 struct PlaneAtoms {
     int start[P], cum[P + 1];
-    __device__ __forceinline__ void init(const int* binStart, int x, int K0) {
+    __device__ __forceinline__ void init(const int* binStart, int x, int K0, int nyc) {
         cum[0] = 0;
 #pragma unroll
         for (int j = 0; j < P; j++) {
-            const int b = wrapIndex(x + j, K0);
+            const int b = wrapIndex(x + j, K0) * nyc;
             start[j] = binStart[b];
-            cum[j + 1] = cum[j] + binStart[b + 1] - binStart[b];
+            cum[j + 1] = cum[j] + binStart[b + nyc] - binStart[b];
         }
     }
     __device__ __forceinline__ int total() const { return cum[P]; }
@@ -174,7 +131,7 @@ __device__ __forceinline__ void pcgTotals(const double* part, int nb, unsigned m
 
 // KC > 0: the grid is KC^3 (compile-time line transforms); 0: any grid the plane blocks handle.
 template <int P, int GS, int KC>
-__global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv) {
+__global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int nyc) {
     typedef cufftComplex C;
     const SysDev& S = dv.sys[0];
     double* sc = dv.scal;
@@ -207,7 +164,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv) {
             W1[m] = tw[S.twOff[1] + m];
         for (int m = tid; m < K2; m += nT)
             W2[m] = tw[S.twOff[2] + m];
-        pa.init(dv.pmeBinStart, x, K0);
+        pa.init(dv.pmeBinStart, x, K0, nyc);
     }
     C* const spec = (C*) dv.spec + S.specOff;
     C* const myPlane = spec + (size_t) x * nline;

@@ -102,9 +102,16 @@ def test_plane_owner_spread_gather_against_reference(name, mode):
     base.close()
 
 
-def test_plane_owner_with_the_persistent_kernel_is_exclusive():
-    """Mode 4 runs its own in-loop PME; asking for plane tiles as well leaves mode 4 in charge."""
-    S, _ = golden("tiny_triclinic")
+@pytest.mark.parametrize("name", ["tiny_triclinic", "dmp8550_real"])
+def test_persistent_kernel_with_plane_owner_passes(name):
+    """Mode 4 with the plane-owner spread and gather for the passes around its loop (the two share the plane
+    bins), against the reference's outputs."""
+    S, d = golden(name)
     eng = mixed_engine(S, 4, pme=1)
-    assert eng.transforms() == 4 and eng.pme_kernels() == 0
+    assert eng.transforms() == 4 and eng.pme_kernels() == 1
+    r = eng.compute(S.pos, S.box)
+    e_ref = float(d["energy"])
+    F = np.asarray(d["forces"], np.float64)
+    assert abs(r.energy - e_ref) <= 1e-6 * abs(e_ref)
+    assert np.linalg.norm(r.forces - F) <= 1e-5 * np.linalg.norm(F)
     eng.close()
