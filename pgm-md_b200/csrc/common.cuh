@@ -127,6 +127,13 @@ struct Dev {
     int* sysCounter;          // nSys
     int* activeHist;          // batched CG: systems still iterating before iteration k (k = 0 .. iterations);
                               // flags[13] counts the loop's iterations
+    // batched CG: the systems still iterating, compacted after every iteration -- actSys[k] their indices in
+    // order, actOff[k] the first virtual slot of the k-th (actOff[actCount[0]] = active slots), actCount[0] how
+    // many; the iteration's per-slot kernels map virtual slots onto them, so converged systems cost nothing
+    int* actSys;
+    int* actOff;
+    int* actCount;
+    int useActive;            // 1: the per-slot CG kernels take virtual slots (batched engines)
     // fields / forces
     double* Epair;            // 3n
     double* Erec;             // 3n

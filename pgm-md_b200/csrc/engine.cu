@@ -203,7 +203,7 @@ struct Engine::Impl {
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
         dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dPairA, dPairB, dPairC, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
-        dScal, dPartial, dGPartial, dHrec, dFm, dPmeRec, dPmeBins, dSrcW, dGPart, dPcgPartial, dBinCount, dActive, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
+        dScal, dPartial, dGPartial, dHrec, dFm, dPmeRec, dPmeBins, dSrcW, dGPart, dPcgPartial, dBinCount, dActive, dActSys, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dTwiddle, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
         dGradQ, dGradR, dSList, dSListCount, dPosBuild, dAtomSlot, dCandStart, dCandJ, dCandT, dGv, dSkipStart, dSkipJ;
@@ -280,7 +280,7 @@ struct Engine::Impl {
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
                       &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dPairA, &dPairB, &dPairC, &dFlags, &dDS,
                       &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dGPartial, &dHrec, &dFm, &dPmeRec, &dPmeBins, &dSrcW, &dGPart,
-                      &dPcgPartial, &dBinCount, &dActive, &dSysCounter, &dEpair,
+                      &dPcgPartial, &dBinCount, &dActive, &dActSys, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
                       &dConvOff, &dGrid, &dSpec, &dInfl, &dTwiddle, &dModuli, &dCovAtom, &dCovPartner, &dCovStrength,
                       &dCovByAtomOff, &dCovByAtom, &dCovByPartnerOff, &dCovByPartner, &dChunkSys, &dChunkBegin,
@@ -756,6 +756,7 @@ struct Engine::Impl {
         dGPartial.ensure(((size_t) n + 7) / 8 * 8);
         dSysCounter.ensure(nsys * sizeof(int));
         dActive.ensure(((size_t) s.maxIter + 2) * sizeof(int));
+        dActSys.ensure((2 * (size_t) nsys + 2) * sizeof(int));   // actSys, actOff, actCount
         CU(cudaMemset(dSysCounter.p, 0, nsys * sizeof(int)));
         dResults.ensure(nsys * NRES * 8);
         dConvPartial.ensure((size_t) nsys * convBlocks * NCONV * 8);
@@ -1013,6 +1014,10 @@ struct Engine::Impl {
         d.gpartial = dGPartial.as<double>();
         d.sysCounter = dSysCounter.as<int>();
         d.activeHist = dActive.as<int>();
+        d.actSys = dActSys.as<int>();
+        d.actOff = d.actSys + nsys;
+        d.actCount = d.actOff + nsys + 1;
+        d.useActive = nsys > 1 ? 1 : 0;
         d.Epair = dEpair.as<double>();
         d.Erec = dErec.as<double>();
         d.Fpair = dFpair.as<double>();

@@ -17,6 +17,87 @@ __device__ __forceinline__ int wrapIndex(int g, int K) {
     return g;
 }
 
+// Block-wide compaction of the systems still iterating (scal[DONE] == 0) into actSys / actOff / actCount, in
+// system order; every thread of one block calls it (a system's slots are the contiguous run of its cells).
+__device__ __forceinline__ void compactActive(const Dev& dv) {
+    __shared__ int wtot[32];
+    __shared__ int carry;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (threadIdx.x == 0)
+        carry = 0;
+    __syncthreads();
+    __shared__ int slotCarry;
+    if (threadIdx.x == 0)
+        slotCarry = 0;
+    __syncthreads();
+    for (int base = 0; base < dv.nSys; base += blockDim.x) {
+        const int s = base + threadIdx.x;
+        const bool act = s < dv.nSys && dv.scal[s * NSCAL + SC_DONE] == 0.0;
+        const int cnt = act ? dv.sys[s].atomEnd - dv.sys[s].atomBegin : 0;
+        // two exclusive scans (systems and slots) in one pass of warp scans
+        int a = act ? 1 : 0, c = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int ya = __shfl_up_sync(0xffffffffu, a, o), yc = __shfl_up_sync(0xffffffffu, c, o);
+            if (lane >= o) {
+                a += ya;
+                c += yc;
+            }
+        }
+        __shared__ int wa[32], wc[32];
+        if (lane == 31) {
+            wa[wid] = a;
+            wc[wid] = c;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int ra = 0, rc = 0;
+            for (int w = 0; w < nw; w++) {
+                const int ta = wa[w], tc = wc[w];
+                wa[w] = ra;
+                wc[w] = rc;
+                ra += ta;
+                rc += tc;
+            }
+            wtot[0] = ra;
+            wtot[1] = rc;
+        }
+        __syncthreads();
+        if (act) {
+            const int k = carry + wa[wid] + a - 1;
+            dv.actSys[k] = s;
+            dv.actOff[k] = slotCarry + wc[wid] + c - cnt;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            carry += wtot[0];
+            slotCarry += wtot[1];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        dv.actOff[carry] = slotCarry;
+        dv.actCount[0] = carry;
+    }
+}
+
+// The slot of virtual slot v of the compacted active systems, or -1 beyond them.
+__device__ __forceinline__ int activeSlot(const Dev& dv, int v) {
+    const int na = dv.actCount[0];
+    if (na <= 0 || v >= dv.actOff[na])
+        return -1;
+    int lo = 0, hi = na - 1;   // the last k with actOff[k] <= v
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (dv.actOff[mid] <= v)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const SysDev& S = dv.sys[dv.actSys[lo]];
+    return dv.cellStart[S.cellOff] + (v - dv.actOff[lo]);
+}
+
 // ------------------------------------------------------------------------------------------------ prep
 
 // Per atom, what & 1: the positions copied in from the caller's device array, the PME base index and fraction
@@ -738,8 +819,10 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
     constexpr int PM = P > 0 ? P : MAXP;
     __shared__ R sth[8][3][PM], sdth[8][3][PM];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int slot = blockIdx.x * 8 + wib;
-    if (slot >= dv.nAtoms)
+    int slot = blockIdx.x * 8 + wib;
+    if (mode == 2 && dv.useActive)   // the CG direction of a batch: the active systems' slots only
+        slot = activeSlot(dv, slot);
+    if (slot < 0 || slot >= dv.nAtoms)
         return;
     const int i = dv.slotAtom[slot];
     const int s = dv.atomSys[i];
@@ -1693,9 +1776,11 @@ __global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
     constexpr int PM = P > 0 ? P : MAXP;
     __shared__ R sth[8][3][PM], sdth[8][3][PM], sd2[8][3][FINAL ? PM : 1];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int slot = blockIdx.x * 8 + wib;
+    int slot = blockIdx.x * 8 + wib;
     if constexpr (!CGA) {
-        if (slot >= dv.nAtoms)
+        if (gateDone && dv.useActive)   // a batch's CG iteration: the active systems' slots only
+            slot = activeSlot(dv, slot);
+        if (slot < 0 || slot >= dv.nAtoms)
             return;
         const int i = dv.slotAtom[slot];
         const int s = dv.atomSys[i];
@@ -1762,8 +1847,11 @@ template <typename R, bool WITHQ, int GS>
 __global__ void __launch_bounds__(256) k_pair_field(Dev dv, int gateDone) {
     typedef typename V4T<R>::T R4;
     typedef typename V2T<R>::T R2;
-    const int g = (blockIdx.x * blockDim.x + threadIdx.x) / GS, lane = threadIdx.x % GS;
-    if (g >= dv.nAtoms)
+    int g = (blockIdx.x * blockDim.x + threadIdx.x) / GS;
+    const int lane = threadIdx.x % GS;
+    if (gateDone && dv.useActive)   // a batch's CG iteration: the active systems' slots only
+        g = activeSlot(dv, g);
+    if (g < 0 || g >= dv.nAtoms)
         return;
     const int slot = g;
     const int i = dv.slotAtom[slot];
@@ -2101,6 +2189,9 @@ __global__ void __launch_bounds__(CHUNK) k_cg_init(Dev dv) {
         }
     }
     double tot[2];
+    __shared__ int decides;
+    if (threadIdx.x == 0)
+        decides = 0;
     if (chunkFinish<2>(dv, chunk, s, v, 2u, tot) && threadIdx.x == 0) {
         double* sc = dv.scal + s * NSCAL;
         sc[SC_RZ] = tot[0];
@@ -2122,7 +2213,13 @@ __global__ void __launch_bounds__(CHUNK) k_cg_init(Dev dv) {
                 dv.activeHist[0] = dv.nSys - ndone;
             if (dv.useCond && dv.loopCond)
                 cudaGraphSetConditional(dv.cond, (ndone < dv.nSys) ? 1u : 0u);
+            decides = 1;
         }
+    }
+    __syncthreads();
+    if (decides && dv.useActive) {   // (every system's DONE is final: each system's last chunk came first)
+        __threadfence();
+        compactActive(dv);
     }
 }
 
@@ -2233,6 +2330,9 @@ __global__ void __launch_bounds__(CHUNK) k_cg_upd(Dev dv) {
         }
     }
     double tot[3];
+    __shared__ int decides;
+    if (threadIdx.x == 0)
+        decides = 0;
     if (chunkFinish<3>(dv, chunk, s, v, 4u, tot) && threadIdx.x == 0) {
         sc[SC_BETA] = tot[0] / fmax(sc[SC_RZ], 1e-300);
         sc[SC_RZ] = tot[1];
@@ -2246,23 +2346,29 @@ __global__ void __launch_bounds__(CHUNK) k_cg_upd(Dev dv) {
         if (dv.nSys == 1) {   // the only system decides alone
             if (dv.useCond)
                 cudaGraphSetConditional(dv.cond, more ? 1u : 0u);
-            return;
+        } else {
+            __threadfence();
+            // the last active system of this iteration to finish decides whether the loop goes on (the count of
+            // active systems is read before this system's arrival, so before the last arrival resets it)
+            const int expected = atomicAdd(&dv.flags[5], 0);
+            const int active = atomicAdd(&dv.flags[4], 1) + 1;
+            if (active == expected) {
+                const int ndone = atomicAdd(&dv.flags[2], 0);
+                dv.flags[5] = dv.nSys - ndone;   // systems active in the next iteration
+                dv.flags[4] = 0;
+                const int loopIt = ++dv.flags[13];
+                if (dv.activeHist && loopIt <= dv.maxIter + 1)
+                    dv.activeHist[loopIt] = dv.nSys - ndone;
+                if (dv.useCond)
+                    cudaGraphSetConditional(dv.cond, (ndone < dv.nSys) ? 1u : 0u);
+                decides = 1;
+            }
         }
+    }
+    __syncthreads();
+    if (decides && dv.useActive) {   // the next iteration's virtual slots
         __threadfence();
-        // the last active system of this iteration to finish decides whether the loop goes on (the count of
-        // active systems is read before this system's arrival, so before the last arrival resets it)
-        const int expected = atomicAdd(&dv.flags[5], 0);
-        const int active = atomicAdd(&dv.flags[4], 1) + 1;
-        if (active == expected) {
-            const int ndone = atomicAdd(&dv.flags[2], 0);
-            dv.flags[5] = dv.nSys - ndone;   // systems active in the next iteration
-            dv.flags[4] = 0;
-            const int loopIt = ++dv.flags[13];
-            if (dv.activeHist && loopIt <= dv.maxIter + 1)
-                dv.activeHist[loopIt] = dv.nSys - ndone;
-            if (dv.useCond)
-                cudaGraphSetConditional(dv.cond, (ndone < dv.nSys) ? 1u : 0u);
-        }
+        compactActive(dv);
     }
 }
 
