@@ -54,6 +54,10 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="with --profile")
     ap.add_argument("--profile-workload", default=WORKLOAD, choices=[WORKLOAD, "water98304", "water_batch1024"],
                     help="with --profile: the system evaluated")
+    ap.add_argument("--profile-transforms", type=int, default=-1,
+                    help="with --profile: the field-pass transforms (0..4; -1: the engine's default)")
+    ap.add_argument("--profile-pme", type=int, default=0, help="with --profile: PME kernels (0 warp per atom, 1 tiles)")
+    ap.add_argument("--profile-lanes", type=int, default=16, help="with --profile: pair lanes")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 1024-system leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 98304-atom leg")
     ap.add_argument("--no-grad", action="store_true", help="skip the parameter-gradient leg")
@@ -539,6 +543,10 @@ def main():
         if args.profile_workload == "water98304":
             S = pkg.systems.water98304(tol=TOL)
         eng = make(pkg.MIXED if args.precision == "mixed" else pkg.FP64)
+        eng.set_pair_lanes(args.profile_lanes)
+        if args.profile_transforms >= 0:
+            eng.set_transforms(args.profile_transforms)
+        eng.set_pme_kernels(args.profile_pme)
         pos_p = torch.from_numpy(S.pos).to(dev).contiguous()
         f_p = torch.zeros((S.n, 3), dtype=torch.float64, device=dev)
         for _ in range(args.warmup + args.steps):
@@ -547,7 +555,8 @@ def main():
             eng.finish_device()
         torch.cuda.synchronize()
         print(json.dumps({"profile": args.precision, "evaluations": args.warmup + args.steps,
-                          "iterations": eng.iterations(), "launches_per_eval": eng.kernel_launches()}))
+                          "iterations": eng.iterations(), "launches_per_eval": eng.kernel_launches(),
+                          "transforms": eng.transforms(), "pme_kernels": eng.pme_kernels()}))
         eng.close()
         return 0
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
