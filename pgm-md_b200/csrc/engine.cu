@@ -1170,7 +1170,7 @@ struct Engine::Impl {
         pcgSmem = (3 * (size_t) FFT_MAXK + 2 * (size_t) fftgBuf) * 8 + (size_t) K[1] * K[2] * 8;
         if (!coop || pcgSmem > (size_t) optin || K[0] + PCG_MIN_PAIR_BLOCKS > sms)
             return;
-        void (*kfn)(Dev, int) = persistentKernel(pairGS);
+        PcgKernel kfn = persistentKernel(pairGS);
         CU(cudaFuncSetAttribute((const void*) kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) pcgSmem));
         int perSm = 0;
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kfn, PCG_THREADS, pcgSmem));
@@ -1222,16 +1222,17 @@ struct Engine::Impl {
     }
 
     // The persistent kernel for the pair lanes (8, 16 or 32; 4 runs as 8) and the grid's compile-time size.
-    void (*persistentKernel(int lanes))(Dev, int) {
+    // pass 0: the CG loop; 1 / 2: one field pass of dipoles (and charges).
+    typedef void (*PcgKernel)(Dev, int, const double*);
+    PcgKernel persistentKernel(int lanes, int pass = 0) {
         const int kc = fftgKc;
-        auto pick = [&](auto gsTag) -> void (*)(Dev, int) {
+        auto pick = [&](auto gsTag) -> PcgKernel {
             constexpr int GS = decltype(gsTag)::value;
-            switch (kc) {
-            case 32: return k_cg_persistent<6, GS, 32>;
-            case 48: return k_cg_persistent<6, GS, 48>;
-            case 64: return k_cg_persistent<6, GS, 64>;
-            default: return k_cg_persistent<6, GS, 0>;
-            }
+            if (kc == 48)
+                return pass == 0 ? k_cg_persistent<6, GS, 48, 0> : pass == 1 ? k_cg_persistent<6, GS, 48, 1>
+                                                                             : k_cg_persistent<6, GS, 48, 2>;
+            return pass == 0 ? k_cg_persistent<6, GS, 0, 0> : pass == 1 ? k_cg_persistent<6, GS, 0, 1>
+                                                                        : k_cg_persistent<6, GS, 0, 2>;
         };
         if (lanes >= 32)
             return pick(std::integral_constant<int, 32>());
@@ -1240,9 +1241,10 @@ struct Engine::Impl {
         return pick(std::integral_constant<int, 8>());
     }
 
-    // The whole CG loop: one cooperative launch of the persistent kernel (one block per SM).
-    void launchPersistent(cudaStream_t sm, const Dev& d) {
-        void (*kfn)(Dev, int) = persistentKernel(pairGS);
+    // The whole CG loop (pass 0), or one field pass of the dipoles vec (1) and the charges (2): one cooperative
+    // launch of the persistent kernel (one block per SM).
+    void launchPersistent(cudaStream_t sm, const Dev& d, int pass = 0, const double* vec = nullptr) {
+        PcgKernel kfn = persistentKernel(pairGS, pass);
         CU(cudaFuncSetAttribute((const void*) kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) pcgSmem));
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute at[1];
@@ -1254,7 +1256,7 @@ struct Engine::Impl {
         cfg.stream = sm;
         cfg.attrs = at;
         cfg.numAttrs = 1;
-        CU(cudaLaunchKernelEx(&cfg, kfn, d, planeNyc));
+        CU(cudaLaunchKernelEx(&cfg, kfn, d, planeNyc, vec));
     }
 
     bool persistentMode() const { return tfMode == TF_PCG; }
@@ -1512,6 +1514,17 @@ struct Engine::Impl {
                 enqueuePlaneBins(sm, d);
             k_perm<<<tb, 256, 0, sm>>>(d);
             k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
+            if (std::is_same<R, float>::value && persistentMode()) {
+                // the two passes before the loop as one cooperative launch each (the persistent kernel's
+                // machinery: PME planes in shared memory beside the direct-space pass)
+                CU(cudaStreamWaitEvent(sm, evJoin, 0));
+                launchPersistent(sm, d, 2, d.perm);
+                k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+                launchPersistent(sm, d, 1, d.x);
+                k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+                CU(cudaGetLastError());
+                return;
+            }
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
             launchSpread<R>(sm, d, 0, d.perm);
             transformPair<R>(sm, d, false);

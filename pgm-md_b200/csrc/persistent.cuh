@@ -66,7 +66,7 @@ struct PlaneAtoms {
 // Direct-space field of the direction p (mixed pair records) at slots g0, g0 + gstride, ...: GS lanes per slot,
 // E_i = sum_j -p_j G1 + (p_j . x) x G2 (core/pgm_core.cpp:274-284), products in float, sums across lanes in
 // double, written to Epair (caller order).
-template <int GS>
+template <int GS, bool WITHQ>
 __device__ __forceinline__ void pcgPairField(const Dev& dv, int g0, int gstride) {
     const int lane = threadIdx.x % GS;
     const unsigned gm = groupMask<GS>();
@@ -81,7 +81,9 @@ __device__ __forceinline__ void pcgPairField(const Dev& dv, int g0, int gstride)
             const float4 xg = arow[t];
             const float2 gb = brow[t];
             const float4 dj = __ldcg(dS + realAsSlot(gb.y));   // (written by other blocks in this launch)
-            const float c = (dj.x * xg.x + dj.y * xg.y + dj.z * xg.z) * gb.x;
+            float c = (dj.x * xg.x + dj.y * xg.y + dj.z * xg.z) * gb.x;
+            if (WITHQ)
+                c += dj.w * xg.w;
             a0 += c * xg.x - dj.x * xg.w;
             a1 += c * xg.y - dj.y * xg.w;
             a2 += c * xg.z - dj.z * xg.w;
@@ -130,12 +132,14 @@ __device__ __forceinline__ void pcgTotals(const double* part, int nb, unsigned m
 }
 
 // KC > 0: the grid is KC^3 (compile-time line transforms); 0: any grid the plane blocks handle.
-template <int P, int GS, int KC>
-__global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int nyc) {
+// PASS 0: the CG loop.  PASS 1 / 2: ONE field pass of the same machinery -- the field at every atom of the dipoles
+// vec (2: and the charges), E_pair and E_rec written per atom -- for the passes around the loop.
+template <int P, int GS, int KC, int PASS>
+__global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int nyc, const double* vec) {
     typedef cufftComplex C;
     const SysDev& S = dv.sys[0];
     double* sc = dv.scal;
-    if (sc[SC_DONE] != 0.0)
+    if (PASS == 0 && sc[SC_DONE] != 0.0)
         return;   // converged at the initial guess (every block alike)
     const int n = dv.nAtoms, nb = gridDim.x, tid = threadIdx.x, nT = blockDim.x;
     const int K0 = KC > 0 ? KC : S.K[0], K1 = KC > 0 ? KC : S.K[1], K2 = KC > 0 ? KC : S.K[2];
@@ -178,17 +182,22 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int ny
     double rz = sc[SC_RZ], beta = sc[SC_BETA], it = sc[SC_IT];
     const double norm = sc[SC_NORM];
     for (;;) {
-        // ---- S: direction p = z + beta p; float copy for the pair pass; PME weights
+        // ---- S: direction p = z + beta p (or the pass's sources); float copy for the pair pass; PME weights
         for (int s = s0 + tid; s < s1; s += nT) {
             const int i = dv.slotAtom[s];
             double d[3];
 #pragma unroll
             for (int k = 0; k < 3; k++) {
-                d[k] = dv.z[3 * i + k] + beta * dv.p[3 * i + k];
-                dv.p[3 * i + k] = d[k];
+                if (PASS == 0) {
+                    d[k] = dv.z[3 * i + k] + beta * dv.p[3 * i + k];
+                    dv.p[3 * i + k] = d[k];
+                } else {
+                    d[k] = vec[3 * i + k];
+                }
             }
-            ((float4*) dv.dS)[s] = make_float4((float) d[0], (float) d[1], (float) d[2], 0.f);
-            srcW[s] = make_float4(0.f, (float) (S.K[0] * (d[0] * S.recip[0] + d[1] * S.recip[3] + d[2] * S.recip[6])),
+            const float qf = PASS == 2 ? (float) dv.q[i] : 0.f;
+            ((float4*) dv.dS)[s] = make_float4((float) d[0], (float) d[1], (float) d[2], qf);
+            srcW[s] = make_float4(qf, (float) (S.K[0] * (d[0] * S.recip[0] + d[1] * S.recip[3] + d[2] * S.recip[6])),
                                   (float) (S.K[1] * (d[0] * S.recip[1] + d[1] * S.recip[4] + d[2] * S.recip[7])),
                                   (float) (S.K[2] * (d[0] * S.recip[2] + d[1] * S.recip[5] + d[2] * S.recip[8])));
         }
@@ -349,10 +358,28 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int ny
             }
         } else {
             const int groups = nT / GS;
-            pcgPairField<GS>(dv, (x - K0) * groups + tid / GS, (nb - K0) * groups);
+            pcgPairField<GS, PASS == 2>(dv, (x - K0) * groups + tid / GS, (nb - K0) * groups);
         }
         if (!fftgBarrier(gbar, (unsigned) nb, dv.flags))
             return;
+        if (PASS != 0) {   // one field pass: E_rec per atom from the plane shares, then done
+            for (int s = s0 + tid; s < s1; s += nT) {
+                const int i = dv.slotAtom[s];
+                double f[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                for (int j1 = 0; j1 < P; j1++) {
+                    const float4 g = __ldcg(gpart + (size_t) j1 * n + s);
+                    f[0] += g.x;
+                    f[1] += g.y;
+                    f[2] += g.z;
+                }
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+                    dv.Erec[3 * i + k] = -(S.K[0] * S.recip[3 * k] * f[0] + S.K[1] * S.recip[3 * k + 1] * f[1] +
+                                           S.K[2] * S.recip[3 * k + 2] * f[2]);
+            }
+            return;
+        }
         // ---- A: rows of A p, the block's share of p . A p
         {
             double v[1] = {0.0};
