@@ -31,6 +31,10 @@ constexpr int PCG_MIN_PAIR_BLOCKS = 16;      // blocks left for the pair pass be
 constexpr float PCG_FIX = 4294967296.0f;     // 2^32: the fixed-point scale of the shared-memory spread
 constexpr float PCG_UNFIX = 2.3283064365386963e-10f;   // 2^-32
 
+// Row stride (8-byte words) of the shared fixed-point plane: at least K2 and 6 mod 16, so that the 16 points a
+// half-warp adds (rows j2, j2 + 1, j2 + 2 of six consecutive columns) fall on distinct banks.
+__host__ __device__ inline int pcgPlaneStride(int K2) { return K2 + ((6 - K2 % 16) + 16) % 16; }
+
 // The spline record of one atom of the plane bins (order P): its slot, b1, b2 and b0 mod K0, and theta and
 // dtheta of the three dimensions, c[dim 2P + kind P + j].
 template <int P> struct PmeRec {
@@ -142,8 +146,10 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int ny
     if (PASS == 0 && sc[SC_DONE] != 0.0)
         return;   // converged at the initial guess (every block alike)
     const int n = dv.nAtoms, nb = gridDim.x, tid = threadIdx.x, nT = blockDim.x;
+    const int warp = tid >> 5, lane = tid & 31, nwarps = nT >> 5;
     const int K0 = KC > 0 ? KC : S.K[0], K1 = KC > 0 ? KC : S.K[1], K2 = KC > 0 ? KC : S.K[2];
     const int K2h = K2 / 2 + 1, NP = (K1 + 1) / 2, ly = K1 + 1, lx = K0 + 1;
+    const int K2s = pcgPlaneStride(K2);
     const int x = blockIdx.x;
     const bool planeBlock = x < K0;
     const int nline = K1 * K2h, lpb = (nline + K0 - 1) / K0, l0 = x * lpb;
@@ -205,30 +211,24 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int ny
             return;
         // ---- F: the plane blocks' reciprocal part, the other blocks' direct part
         if (planeBlock) {
-            for (int e = tid; e < K1 * K2; e += nT)
+            for (int e = tid; e < K1 * K2s; e += nT)
                 plane[e] = 0ull;
             __syncthreads();
-            for (int t = tid; t < pa.total(); t += nT) {
+            // a warp per atom, its lanes over the p^2 points (j2, j3) of this plane: the row stride K2s = 6 mod 16
+            // puts the 16 points of each half-warp on distinct 8-byte banks
+            for (int t = warp; t < pa.total(); t += nwarps) {
                 int j1;
                 const PmeRec<P>& r = rec[pa.locate(t, j1)];
                 const int4 id = r.idx;
                 const float4 w = __ldcg(srcW + id.x);
                 const float t1 = r.c[j1], u1 = r.c[P + j1];
                 const float qe = w.x * t1 + w.y * u1, e1t = w.z * t1, e2t = w.w * t1;
-                int col[P];
-#pragma unroll
-                for (int j3 = 0; j3 < P; j3++)
-                    col[j3] = wrapIndex(id.z - j3, K2);
-#pragma unroll
-                for (int j2 = 0; j2 < P; j2++) {
+                for (int k = lane; k < P * P; k += 32) {
+                    const int j2 = k / P, j3 = k - j2 * P;
                     const float t2 = r.c[2 * P + j2], u2 = r.c[3 * P + j2];
-                    const float A2 = t2 * qe + e1t * u2, B2 = e2t * t2;
-                    unsigned long long* row = plane + wrapIndex(id.y - j2, K1) * K2;
-#pragma unroll
-                    for (int j3 = 0; j3 < P; j3++) {
-                        const float v = A2 * r.c[4 * P + j3] + B2 * r.c[5 * P + j3];
-                        atomicAdd(row + col[j3], (unsigned long long) __float2ll_rn(v * PCG_FIX));
-                    }
+                    const float v = (t2 * qe + e1t * u2) * r.c[4 * P + j3] + e2t * t2 * r.c[5 * P + j3];
+                    atomicAdd(plane + wrapIndex(id.y - j2, K1) * K2s + wrapIndex(id.z - j3, K2),
+                              (unsigned long long) __float2ll_rn(v * PCG_FIX));
                 }
             }
             __syncthreads();
@@ -236,8 +236,8 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int ny
             for (int e = tid; e < NP * K2; e += nT) {
                 const int pr = qd(e, K2, iK2), z = e - pr * K2;
                 C v;
-                v.x = __ll2float_rn((long long) plane[2 * pr * K2 + z]) * PCG_UNFIX;
-                v.y = (2 * pr + 1 < K1) ? __ll2float_rn((long long) plane[(2 * pr + 1) * K2 + z]) * PCG_UNFIX : 0.f;
+                v.x = __ll2float_rn((long long) plane[2 * pr * K2s + z]) * PCG_UNFIX;
+                v.y = (2 * pr + 1 < K1) ? __ll2float_rn((long long) plane[(2 * pr + 1) * K2s + z]) * PCG_UNFIX : 0.f;
                 b0[e] = v;
             }
             __syncthreads();
@@ -328,33 +328,28 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int ny
             const C* Zt = fftLinesK<float, 1, KC>(O2, Gy, NP, K2, K2, W2);
             // gather at the same atoms: this plane's part of f_a = sum (d theta_a) theta theta phi
             const float* phi = (const float*) Zt;   // row y at [(y / 2) K2 + z] component y & 1
-            for (int t = tid; t < pa.total(); t += nT) {
+            for (int t = warp; t < pa.total(); t += nwarps) {   // a warp per atom, the lanes over its points
                 int j1;
                 const PmeRec<P>& r = rec[pa.locate(t, j1)];
                 const int4 id = r.idx;
-                int col[P];
-#pragma unroll
-                for (int j3 = 0; j3 < P; j3++)
-                    col[j3] = wrapIndex(id.z - j3, K2);
                 float A = 0.f, B = 0.f, Cc = 0.f;
-#pragma unroll
-                for (int j2 = 0; j2 < P; j2++) {
+                for (int k = lane; k < P * P; k += 32) {
+                    const int j2 = k / P, j3 = k - j2 * P;
                     const int yy = wrapIndex(id.y - j2, K1);
-                    const float* row = phi + 2 * ((yy >> 1) * K2) + (yy & 1);
-                    float st = 0.f, su = 0.f;
-#pragma unroll
-                    for (int j3 = 0; j3 < P; j3++) {
-                        const float ph = row[2 * col[j3]];
-                        st += r.c[4 * P + j3] * ph;
-                        su += r.c[5 * P + j3] * ph;
-                    }
-                    const float t2 = r.c[2 * P + j2], u2 = r.c[3 * P + j2];
-                    A += t2 * st;
-                    B += u2 * st;
-                    Cc += t2 * su;
+                    const float ph = phi[2 * ((yy >> 1) * K2 + wrapIndex(id.z - j3, K2)) + (yy & 1)];
+                    const float t2 = r.c[2 * P + j2], u2 = r.c[3 * P + j2], t3 = r.c[4 * P + j3];
+                    A += t2 * t3 * ph;
+                    B += u2 * t3 * ph;
+                    Cc += t2 * r.c[5 * P + j3] * ph;
                 }
-                const float t1 = r.c[j1], u1 = r.c[P + j1];
-                gpart[(size_t) j1 * n + id.x] = make_float4(u1 * A, t1 * B, t1 * Cc, 0.f);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    A += __shfl_xor_sync(0xffffffffu, A, o);
+                    B += __shfl_xor_sync(0xffffffffu, B, o);
+                    Cc += __shfl_xor_sync(0xffffffffu, Cc, o);
+                }
+                if (lane == 0)
+                    gpart[(size_t) j1 * n + id.x] = make_float4(r.c[P + j1] * A, r.c[j1] * B, r.c[j1] * Cc, 0.f);
             }
         } else {
             const int groups = nT / GS;
