@@ -30,6 +30,8 @@ constexpr int PCG_THREADS = 512;
 constexpr int PCG_MIN_PAIR_BLOCKS = 16;      // blocks left for the pair pass beside the plane blocks
 constexpr float PCG_FIX = 4294967296.0f;     // 2^32: the fixed-point scale of the shared-memory spread
 constexpr float PCG_UNFIX = 2.3283064365386963e-10f;   // 2^-32
+constexpr int PCG_BATCH = 256;               // atoms staged at a time by a plane block
+constexpr int PCG_STAGE = 32;                // words staged per atom (order 6: 4 x 6 coefficients + 6)
 
 // Row stride (8-byte words) of the shared fixed-point plane: at least K2 and 6 mod 16, so that the 16 points a
 // half-warp adds (rows j2, j2 + 1, j2 + 2 of six consecutive columns) fall on distinct banks.
@@ -140,6 +142,7 @@ __device__ __forceinline__ void pcgTotals(const double* part, int nb, unsigned m
 // vec (2: and the charges), E_pair and E_rec written per atom -- for the passes around the loop.
 template <int P, int GS, int KC, int PASS>
 __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int nyc, const double* vec) {
+    static_assert(4 * P + 6 <= PCG_STAGE && PCG_BATCH <= PCG_THREADS, "staging layout");
     typedef cufftComplex C;
     const SysDev& S = dv.sys[0];
     double* sc = dv.scal;
@@ -165,6 +168,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int ny
     C* const b0 = W2 + FFT_MAXK;
     C* const b1 = b0 + dv.fftgBuf;
     unsigned long long* const plane = (unsigned long long*) (b1 + dv.fftgBuf);
+    float* const stage = (float*) (plane + K1 * K2s);   // PCG_BATCH x PCG_STAGE words
     const C* tw = (const C*) dv.twiddle;
     PlaneAtoms<P> pa;
     if (planeBlock) {
@@ -214,24 +218,43 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int ny
             for (int e = tid; e < K1 * K2s; e += nT)
                 plane[e] = 0ull;
             __syncthreads();
-            // a warp per atom, its lanes over the p^2 points (j2, j3) of this plane: the row stride K2s = 6 mod 16
-            // puts the 16 points of each half-warp on distinct 8-byte banks
-            for (int t = warp; t < pa.total(); t += nwarps) {
-                int j1;
-                const PmeRec<P>& r = rec[pa.locate(t, j1)];
-                const int4 id = r.idx;
-                const float4 w = __ldcg(srcW + id.x);
-                const float t1 = r.c[j1], u1 = r.c[P + j1];
-                const float qe = w.x * t1 + w.y * u1, e1t = w.z * t1, e2t = w.w * t1;
-                for (int k = lane; k < P * P; k += 32) {
-                    const int j2 = k / P, j3 = k - j2 * P;
-                    const float t2 = r.c[2 * P + j2], u2 = r.c[3 * P + j2];
-                    const float v = (t2 * qe + e1t * u2) * r.c[4 * P + j3] + e2t * t2 * r.c[5 * P + j3];
-                    atomicAdd(plane + wrapIndex(id.y - j2, K1) * K2s + wrapIndex(id.z - j3, K2),
-                              (unsigned long long) __float2ll_rn(v * PCG_FIX));
+            // batches of PCG_BATCH atoms: every thread stages one atom's coefficients of this plane in shared
+            // memory (its loads all in flight at once), then a warp per atom adds its p^2 points, the lanes over
+            // (j2, j3); the row stride K2s = 6 mod 16 puts the 16 points of each half-warp on distinct banks
+            for (int t0 = 0; t0 < pa.total(); t0 += PCG_BATCH) {
+                const int nbat = min(PCG_BATCH, pa.total() - t0);
+                if (tid < nbat) {
+                    int j1;
+                    const PmeRec<P>& r = rec[pa.locate(t0 + tid, j1)];
+                    const int4 id = r.idx;
+                    const float4 w = __ldcg(srcW + id.x);
+                    const float t1 = r.c[j1], u1 = r.c[P + j1];
+                    const float qe = w.x * t1 + w.y * u1, e1t = w.z * t1, e2t = w.w * t1;
+                    float* st = stage + tid * PCG_STAGE;
+#pragma unroll
+                    for (int j = 0; j < P; j++) {
+                        const float t2 = r.c[2 * P + j], u2 = r.c[3 * P + j];
+                        st[j] = t2 * qe + e1t * u2;          // A(j2)
+                        st[P + j] = e2t * t2;                // B(j2)
+                        st[2 * P + j] = r.c[4 * P + j];      // theta_3
+                        st[3 * P + j] = r.c[5 * P + j];      // dtheta_3
+                    }
+                    ((int*) st)[4 * P] = id.y;
+                    ((int*) st)[4 * P + 1] = id.z;
                 }
+                __syncthreads();
+                for (int a = warp; a < nbat; a += nwarps) {
+                    const float* st = stage + a * PCG_STAGE;
+                    const int b1 = ((const int*) st)[4 * P], b2 = ((const int*) st)[4 * P + 1];
+                    for (int k = lane; k < P * P; k += 32) {
+                        const int j2 = k / P, j3 = k - j2 * P;
+                        const float v = st[j2] * st[2 * P + j3] + st[P + j2] * st[3 * P + j3];
+                        atomicAdd(plane + wrapIndex(b1 - j2, K1) * K2s + wrapIndex(b2 - j3, K2),
+                                  (unsigned long long) __float2ll_rn(v * PCG_FIX));
+                    }
+                }
+                __syncthreads();
             }
-            __syncthreads();
             // plane x: rows 2p, 2p + 1 as one complex row [pair][z]; z; separation into y-lines [kz][y]; y
             for (int e = tid; e < NP * K2; e += nT) {
                 const int pr = qd(e, K2, iK2), z = e - pr * K2;
@@ -328,28 +351,55 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int ny
             const C* Zt = fftLinesK<float, 1, KC>(O2, Gy, NP, K2, K2, W2);
             // gather at the same atoms: this plane's part of f_a = sum (d theta_a) theta theta phi
             const float* phi = (const float*) Zt;   // row y at [(y / 2) K2 + z] component y & 1
-            for (int t = warp; t < pa.total(); t += nwarps) {   // a warp per atom, the lanes over its points
-                int j1;
-                const PmeRec<P>& r = rec[pa.locate(t, j1)];
-                const int4 id = r.idx;
-                float A = 0.f, B = 0.f, Cc = 0.f;
-                for (int k = lane; k < P * P; k += 32) {
-                    const int j2 = k / P, j3 = k - j2 * P;
-                    const int yy = wrapIndex(id.y - j2, K1);
-                    const float ph = phi[2 * ((yy >> 1) * K2 + wrapIndex(id.z - j3, K2)) + (yy & 1)];
-                    const float t2 = r.c[2 * P + j2], u2 = r.c[3 * P + j2], t3 = r.c[4 * P + j3];
-                    A += t2 * t3 * ph;
-                    B += u2 * t3 * ph;
-                    Cc += t2 * r.c[5 * P + j3] * ph;
-                }
+            // the same batches: stage the coefficients, then a warp per atom sums its points, the lanes over them
+            for (int t0 = 0; t0 < pa.total(); t0 += PCG_BATCH) {
+                const int nbat = min(PCG_BATCH, pa.total() - t0);
+                if (tid < nbat) {
+                    int j1;
+                    const PmeRec<P>& r = rec[pa.locate(t0 + tid, j1)];
+                    const int4 id = r.idx;
+                    float* st = stage + tid * PCG_STAGE;
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    A += __shfl_xor_sync(0xffffffffu, A, o);
-                    B += __shfl_xor_sync(0xffffffffu, B, o);
-                    Cc += __shfl_xor_sync(0xffffffffu, Cc, o);
+                    for (int j = 0; j < P; j++) {
+                        st[j] = r.c[2 * P + j];              // theta_2
+                        st[P + j] = r.c[3 * P + j];          // dtheta_2
+                        st[2 * P + j] = r.c[4 * P + j];      // theta_3
+                        st[3 * P + j] = r.c[5 * P + j];      // dtheta_3
+                    }
+                    ((int*) st)[4 * P] = id.y;
+                    ((int*) st)[4 * P + 1] = id.z;
+                    ((int*) st)[4 * P + 2] = id.x;
+                    st[4 * P + 3] = r.c[j1];                 // theta_1 (this plane)
+                    st[4 * P + 4] = r.c[P + j1];             // dtheta_1
+                    ((int*) st)[4 * P + 5] = j1;
                 }
-                if (lane == 0)
-                    gpart[(size_t) j1 * n + id.x] = make_float4(r.c[P + j1] * A, r.c[j1] * B, r.c[j1] * Cc, 0.f);
+                __syncthreads();
+                for (int a = warp; a < nbat; a += nwarps) {
+                    const float* st = stage + a * PCG_STAGE;
+                    const int b1 = ((const int*) st)[4 * P], b2 = ((const int*) st)[4 * P + 1];
+                    float A = 0.f, B = 0.f, Cc = 0.f;
+                    for (int k = lane; k < P * P; k += 32) {
+                        const int j2 = k / P, j3 = k - j2 * P;
+                        const int yy = wrapIndex(b1 - j2, K1);
+                        const float ph = phi[2 * ((yy >> 1) * K2 + wrapIndex(b2 - j3, K2)) + (yy & 1)];
+                        const float t3 = st[2 * P + j3];
+                        A += st[j2] * t3 * ph;
+                        B += st[P + j2] * t3 * ph;
+                        Cc += st[j2] * st[3 * P + j3] * ph;
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        A += __shfl_xor_sync(0xffffffffu, A, o);
+                        B += __shfl_xor_sync(0xffffffffu, B, o);
+                        Cc += __shfl_xor_sync(0xffffffffu, Cc, o);
+                    }
+                    if (lane == 0) {
+                        const float t1 = st[4 * P + 3], u1 = st[4 * P + 4];
+                        gpart[(size_t) ((const int*) st)[4 * P + 5] * n + ((const int*) st)[4 * P + 2]] =
+                            make_float4(u1 * A, t1 * B, t1 * Cc, 0.f);
+                    }
+                }
+                __syncthreads();
             }
         } else {
             const int groups = nT / GS;
