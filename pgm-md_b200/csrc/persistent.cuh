@@ -31,7 +31,8 @@ constexpr int PCG_MIN_PAIR_BLOCKS = 16;      // blocks left for the pair pass be
 constexpr float PCG_FIX = 4294967296.0f;     // 2^32: the fixed-point scale of the shared-memory spread
 constexpr float PCG_UNFIX = 2.3283064365386963e-10f;   // 2^-32
 constexpr int PCG_BATCH = 256;               // atoms staged at a time by a plane block
-constexpr int PCG_STAGE = 32;                // words staged per atom (order 6: 4 x 6 coefficients + 6)
+constexpr int PCG_STAGE = 33;                // words staged per atom (order 6: 4 x 6 coefficients + 6), odd: the
+                                             // threads of a warp stage on distinct banks
 
 // Row stride (8-byte words) of the shared fixed-point plane: at least K2 and 6 mod 16, so that the 16 points a
 // half-warp adds (rows j2, j2 + 1, j2 + 2 of six consecutive columns) fall on distinct banks.
