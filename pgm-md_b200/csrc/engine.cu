@@ -1167,8 +1167,7 @@ struct Engine::Impl {
         CU(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, devId));
         CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, devId));
         const int* K = sysK[0].data();
-        pcgSmem = (3 * (size_t) FFT_MAXK + 2 * (size_t) fftgBuf) * 8 + (size_t) K[1] * pcgPlaneStride(K[2]) * 8 +
-                  (size_t) PCG_BATCH * PCG_STAGE * 4;
+        pcgSmem = (3 * (size_t) FFT_MAXK + 2 * (size_t) fftgBuf) * 8 + (size_t) K[1] * K[2] * 8;
         if (!coop || pcgSmem > (size_t) optin || K[0] + PCG_MIN_PAIR_BLOCKS > sms)
             return;
         PcgKernel kfn = persistentKernel(pairGS);

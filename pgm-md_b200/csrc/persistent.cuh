@@ -30,13 +30,6 @@ constexpr int PCG_THREADS = 512;
 constexpr int PCG_MIN_PAIR_BLOCKS = 16;      // blocks left for the pair pass beside the plane blocks
 constexpr float PCG_FIX = 4294967296.0f;     // 2^32: the fixed-point scale of the shared-memory spread
 constexpr float PCG_UNFIX = 2.3283064365386963e-10f;   // 2^-32
-constexpr int PCG_BATCH = 256;               // atoms staged at a time by a plane block
-constexpr int PCG_STAGE = 33;                // words staged per atom (order 6: 4 x 6 coefficients + 6), odd: the
-                                             // threads of a warp stage on distinct banks
-
-// Row stride (8-byte words) of the shared fixed-point plane: at least K2 and 6 mod 16, so that the 16 points a
-// half-warp adds (rows j2, j2 + 1, j2 + 2 of six consecutive columns) fall on distinct banks.
-__host__ __device__ inline int pcgPlaneStride(int K2) { return K2 + ((6 - K2 % 16) + 16) % 16; }
 
 // The spline record of one atom of the plane bins (order P): its slot, b1, b2 and b0 mod K0, and theta and
 // dtheta of the three dimensions, c[dim 2P + kind P + j].
@@ -143,17 +136,14 @@ __device__ __forceinline__ void pcgTotals(const double* part, int nb, unsigned m
 // vec (2: and the charges), E_pair and E_rec written per atom -- for the passes around the loop.
 template <int P, int GS, int KC, int PASS>
 __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int nyc, const double* vec) {
-    static_assert(4 * P + 6 <= PCG_STAGE && PCG_BATCH <= PCG_THREADS, "staging layout");
     typedef cufftComplex C;
     const SysDev& S = dv.sys[0];
     double* sc = dv.scal;
     if (PASS == 0 && sc[SC_DONE] != 0.0)
         return;   // converged at the initial guess (every block alike)
     const int n = dv.nAtoms, nb = gridDim.x, tid = threadIdx.x, nT = blockDim.x;
-    const int warp = tid >> 5, lane = tid & 31, nwarps = nT >> 5;
     const int K0 = KC > 0 ? KC : S.K[0], K1 = KC > 0 ? KC : S.K[1], K2 = KC > 0 ? KC : S.K[2];
     const int K2h = K2 / 2 + 1, NP = (K1 + 1) / 2, ly = K1 + 1, lx = K0 + 1;
-    const int K2s = pcgPlaneStride(K2);
     const int x = blockIdx.x;
     const bool planeBlock = x < K0;
     const int nline = K1 * K2h, lpb = (nline + K0 - 1) / K0, l0 = x * lpb;
@@ -169,7 +159,6 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int ny
     C* const b0 = W2 + FFT_MAXK;
     C* const b1 = b0 + dv.fftgBuf;
     unsigned long long* const plane = (unsigned long long*) (b1 + dv.fftgBuf);
-    float* const stage = (float*) (plane + K1 * K2s);   // PCG_BATCH x PCG_STAGE words
     const C* tw = (const C*) dv.twiddle;
     PlaneAtoms<P> pa;
     if (planeBlock) {
@@ -216,52 +205,39 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int ny
             return;
         // ---- F: the plane blocks' reciprocal part, the other blocks' direct part
         if (planeBlock) {
-            for (int e = tid; e < K1 * K2s; e += nT)
+            for (int e = tid; e < K1 * K2; e += nT)
                 plane[e] = 0ull;
             __syncthreads();
-            // batches of PCG_BATCH atoms: every thread stages one atom's coefficients of this plane in shared
-            // memory (its loads all in flight at once), then a warp per atom adds its p^2 points, the lanes over
-            // (j2, j3); the row stride K2s = 6 mod 16 puts the 16 points of each half-warp on distinct banks
-            for (int t0 = 0; t0 < pa.total(); t0 += PCG_BATCH) {
-                const int nbat = min(PCG_BATCH, pa.total() - t0);
-                if (tid < nbat) {
-                    int j1;
-                    const PmeRec<P>& r = rec[pa.locate(t0 + tid, j1)];
-                    const int4 id = r.idx;
-                    const float4 w = __ldcg(srcW + id.x);
-                    const float t1 = r.c[j1], u1 = r.c[P + j1];
-                    const float qe = w.x * t1 + w.y * u1, e1t = w.z * t1, e2t = w.w * t1;
-                    float* st = stage + tid * PCG_STAGE;
+            for (int t = tid; t < pa.total(); t += nT) {
+                int j1;
+                const PmeRec<P>& r = rec[pa.locate(t, j1)];
+                const int4 id = r.idx;
+                const float4 w = __ldcg(srcW + id.x);
+                const float t1 = r.c[j1], u1 = r.c[P + j1];
+                const float qe = w.x * t1 + w.y * u1, e1t = w.z * t1, e2t = w.w * t1;
+                int col[P];
 #pragma unroll
-                    for (int j = 0; j < P; j++) {
-                        const float t2 = r.c[2 * P + j], u2 = r.c[3 * P + j];
-                        st[j] = t2 * qe + e1t * u2;          // A(j2)
-                        st[P + j] = e2t * t2;                // B(j2)
-                        st[2 * P + j] = r.c[4 * P + j];      // theta_3
-                        st[3 * P + j] = r.c[5 * P + j];      // dtheta_3
-                    }
-                    ((int*) st)[4 * P] = id.y;
-                    ((int*) st)[4 * P + 1] = id.z;
-                }
-                __syncthreads();
-                for (int a = warp; a < nbat; a += nwarps) {
-                    const float* st = stage + a * PCG_STAGE;
-                    const int b1 = ((const int*) st)[4 * P], b2 = ((const int*) st)[4 * P + 1];
-                    for (int k = lane; k < P * P; k += 32) {
-                        const int j2 = k / P, j3 = k - j2 * P;
-                        const float v = st[j2] * st[2 * P + j3] + st[P + j2] * st[3 * P + j3];
-                        atomicAdd(plane + wrapIndex(b1 - j2, K1) * K2s + wrapIndex(b2 - j3, K2),
-                                  (unsigned long long) __float2ll_rn(v * PCG_FIX));
+                for (int j3 = 0; j3 < P; j3++)
+                    col[j3] = wrapIndex(id.z - j3, K2);
+#pragma unroll
+                for (int j2 = 0; j2 < P; j2++) {
+                    const float t2 = r.c[2 * P + j2], u2 = r.c[3 * P + j2];
+                    const float A2 = t2 * qe + e1t * u2, B2 = e2t * t2;
+                    unsigned long long* row = plane + wrapIndex(id.y - j2, K1) * K2;
+#pragma unroll
+                    for (int j3 = 0; j3 < P; j3++) {
+                        const float v = A2 * r.c[4 * P + j3] + B2 * r.c[5 * P + j3];
+                        atomicAdd(row + col[j3], (unsigned long long) __float2ll_rn(v * PCG_FIX));
                     }
                 }
-                __syncthreads();
             }
+            __syncthreads();
             // plane x: rows 2p, 2p + 1 as one complex row [pair][z]; z; separation into y-lines [kz][y]; y
             for (int e = tid; e < NP * K2; e += nT) {
                 const int pr = qd(e, K2, iK2), z = e - pr * K2;
                 C v;
-                v.x = __ll2float_rn((long long) plane[2 * pr * K2s + z]) * PCG_UNFIX;
-                v.y = (2 * pr + 1 < K1) ? __ll2float_rn((long long) plane[(2 * pr + 1) * K2s + z]) * PCG_UNFIX : 0.f;
+                v.x = __ll2float_rn((long long) plane[2 * pr * K2 + z]) * PCG_UNFIX;
+                v.y = (2 * pr + 1 < K1) ? __ll2float_rn((long long) plane[(2 * pr + 1) * K2 + z]) * PCG_UNFIX : 0.f;
                 b0[e] = v;
             }
             __syncthreads();
@@ -352,55 +328,33 @@ __global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int ny
             const C* Zt = fftLinesK<float, 1, KC>(O2, Gy, NP, K2, K2, W2);
             // gather at the same atoms: this plane's part of f_a = sum (d theta_a) theta theta phi
             const float* phi = (const float*) Zt;   // row y at [(y / 2) K2 + z] component y & 1
-            // the same batches: stage the coefficients, then a warp per atom sums its points, the lanes over them
-            for (int t0 = 0; t0 < pa.total(); t0 += PCG_BATCH) {
-                const int nbat = min(PCG_BATCH, pa.total() - t0);
-                if (tid < nbat) {
-                    int j1;
-                    const PmeRec<P>& r = rec[pa.locate(t0 + tid, j1)];
-                    const int4 id = r.idx;
-                    float* st = stage + tid * PCG_STAGE;
+            for (int t = tid; t < pa.total(); t += nT) {
+                int j1;
+                const PmeRec<P>& r = rec[pa.locate(t, j1)];
+                const int4 id = r.idx;
+                int col[P];
 #pragma unroll
-                    for (int j = 0; j < P; j++) {
-                        st[j] = r.c[2 * P + j];              // theta_2
-                        st[P + j] = r.c[3 * P + j];          // dtheta_2
-                        st[2 * P + j] = r.c[4 * P + j];      // theta_3
-                        st[3 * P + j] = r.c[5 * P + j];      // dtheta_3
-                    }
-                    ((int*) st)[4 * P] = id.y;
-                    ((int*) st)[4 * P + 1] = id.z;
-                    ((int*) st)[4 * P + 2] = id.x;
-                    st[4 * P + 3] = r.c[j1];                 // theta_1 (this plane)
-                    st[4 * P + 4] = r.c[P + j1];             // dtheta_1
-                    ((int*) st)[4 * P + 5] = j1;
-                }
-                __syncthreads();
-                for (int a = warp; a < nbat; a += nwarps) {
-                    const float* st = stage + a * PCG_STAGE;
-                    const int b1 = ((const int*) st)[4 * P], b2 = ((const int*) st)[4 * P + 1];
-                    float A = 0.f, B = 0.f, Cc = 0.f;
-                    for (int k = lane; k < P * P; k += 32) {
-                        const int j2 = k / P, j3 = k - j2 * P;
-                        const int yy = wrapIndex(b1 - j2, K1);
-                        const float ph = phi[2 * ((yy >> 1) * K2 + wrapIndex(b2 - j3, K2)) + (yy & 1)];
-                        const float t3 = st[2 * P + j3];
-                        A += st[j2] * t3 * ph;
-                        B += st[P + j2] * t3 * ph;
-                        Cc += st[j2] * st[3 * P + j3] * ph;
-                    }
+                for (int j3 = 0; j3 < P; j3++)
+                    col[j3] = wrapIndex(id.z - j3, K2);
+                float A = 0.f, B = 0.f, Cc = 0.f;
 #pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) {
-                        A += __shfl_xor_sync(0xffffffffu, A, o);
-                        B += __shfl_xor_sync(0xffffffffu, B, o);
-                        Cc += __shfl_xor_sync(0xffffffffu, Cc, o);
+                for (int j2 = 0; j2 < P; j2++) {
+                    const int yy = wrapIndex(id.y - j2, K1);
+                    const float* row = phi + 2 * ((yy >> 1) * K2) + (yy & 1);
+                    float st = 0.f, su = 0.f;
+#pragma unroll
+                    for (int j3 = 0; j3 < P; j3++) {
+                        const float ph = row[2 * col[j3]];
+                        st += r.c[4 * P + j3] * ph;
+                        su += r.c[5 * P + j3] * ph;
                     }
-                    if (lane == 0) {
-                        const float t1 = st[4 * P + 3], u1 = st[4 * P + 4];
-                        gpart[(size_t) ((const int*) st)[4 * P + 5] * n + ((const int*) st)[4 * P + 2]] =
-                            make_float4(u1 * A, t1 * B, t1 * Cc, 0.f);
-                    }
+                    const float t2 = r.c[2 * P + j2], u2 = r.c[3 * P + j2];
+                    A += t2 * st;
+                    B += u2 * st;
+                    Cc += t2 * su;
                 }
-                __syncthreads();
+                const float t1 = r.c[j1], u1 = r.c[P + j1];
+                gpart[(size_t) j1 * n + id.x] = make_float4(u1 * A, t1 * B, t1 * Cc, 0.f);
             }
         } else {
             const int groups = nT / GS;
