@@ -1176,7 +1176,7 @@ struct Engine::Impl {
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kfn, PCG_THREADS, pcgSmem));
         if (perSm < 1)
             return;
-        pcgBlocks = sms;
+        pcgBlocks = sms * std::min(perSm, PCG_BLOCKS_PER_SM);   // (the plane blocks, 0 .. K0-1, one per SM)
         pcgOk = true;
         dPmeRec.ensure((size_t) n * sizeof(PmeRec<6>));
         dPmeBins.ensure((FFT_MAXK + 1) * sizeof(int));

@@ -28,6 +28,7 @@ namespace pgmb200 {
 
 constexpr int PCG_THREADS = 512;
 constexpr int PCG_MIN_PAIR_BLOCKS = 16;      // blocks left for the pair pass beside the plane blocks
+constexpr int PCG_BLOCKS_PER_SM = 2;         // resident blocks per SM (64 registers per thread): 32 warps per SM
 constexpr float PCG_FIX = 4294967296.0f;     // 2^32: the fixed-point scale of the shared-memory spread
 constexpr float PCG_UNFIX = 2.3283064365386963e-10f;   // 2^-32
 
@@ -135,7 +136,7 @@ __device__ __forceinline__ void pcgTotals(const double* part, int nb, unsigned m
 // PASS 0: the CG loop.  PASS 1 / 2: ONE field pass of the same machinery -- the field at every atom of the dipoles
 // vec (2: and the charges), E_pair and E_rec written per atom -- for the passes around the loop.
 template <int P, int GS, int KC, int PASS>
-__global__ void __launch_bounds__(PCG_THREADS, 1) k_cg_persistent(Dev dv, int nyc, const double* vec) {
+__global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persistent(Dev dv, int nyc, const double* vec) {
     typedef cufftComplex C;
     const SysDev& S = dv.sys[0];
     double* sc = dv.scal;
