@@ -28,7 +28,7 @@ namespace pgmb200 {
 
 constexpr int PCG_THREADS = 512;
 constexpr int PCG_MIN_PAIR_BLOCKS = 16;      // blocks left for the pair pass beside the plane blocks
-constexpr int PCG_BLOCKS_PER_SM = 2;         // resident blocks per SM (64 registers per thread): 32 warps per SM
+constexpr int PCG_BLOCKS_PER_SM = 1;         // resident blocks per SM (two, at 64 registers, measured slower)
 constexpr float PCG_FIX = 4294967296.0f;     // 2^32: the fixed-point scale of the shared-memory spread
 constexpr float PCG_UNFIX = 2.3283064365386963e-10f;   // 2^-32
 
