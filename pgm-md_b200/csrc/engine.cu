@@ -1201,6 +1201,12 @@ struct Engine::Impl {
         for (const void* f : {(const void*) k_spread_planes<6>, (const void*) k_gather_planes<6>})
             CU(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) planeSmem));
         const size_t nbins = (size_t) K[0] * planeNyc;
+        if (nbins > (size_t) PL_MAX_SMEM_BINS)
+            return;   // (the binning kernels keep a block's histogram of every bin in shared memory)
+        CU(cudaFuncSetAttribute((const void*) k_plane_bin_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int) (nbins * sizeof(int))));
+        CU(cudaFuncSetAttribute((const void*) k_plane_bin_fill<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int) (2 * nbins * sizeof(int))));
         dPmeRec.ensure((size_t) n * sizeof(PmeRec<6>));
         dPmeBins.ensure((std::max<size_t>(nbins, FFT_MAXK) + 1) * sizeof(int));
         dBinCount.ensure(nbins * sizeof(int));
@@ -1213,11 +1219,11 @@ struct Engine::Impl {
 
     // The plane bins and records of the evaluation (after k_splines).
     void enqueuePlaneBins(cudaStream_t sm, const Dev& d) {
-        const int nbins = sysK[0][0] * planeNyc, tb = (n + 255) / 256;
+        const int nbins = sysK[0][0] * planeNyc, bb = (n + PL_BIN_SLOTS - 1) / PL_BIN_SLOTS;
         CU(cudaMemsetAsync(dBinCount.p, 0, nbins * sizeof(int), sm));
-        k_plane_bin_count<<<tb, 256, 0, sm>>>(d, planeNyc, dBinCount.as<int>());
+        k_plane_bin_count<<<bb, 256, nbins * sizeof(int), sm>>>(d, planeNyc, dBinCount.as<int>());
         k_plane_bin_scan<<<1, 1024, 0, sm>>>(d, nbins, dBinCount.as<int>());
-        k_plane_bin_fill<6><<<tb, 256, 0, sm>>>(d, planeNyc, dBinCount.as<int>());
+        k_plane_bin_fill<6><<<bb, 256, 2 * nbins * sizeof(int), sm>>>(d, planeNyc, dBinCount.as<int>());
         CU(cudaGetLastError());
     }
 

@@ -214,6 +214,10 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
                 const PmeRec<P>& r = rec[pa.locate(t, j1)];
                 const int4 id = r.idx;
                 const float4 w = __ldcg(srcW + id.x);
+                float c[4 * P];   // (in registers before the atomics, which would otherwise force reloads)
+#pragma unroll
+                for (int k = 0; k < 4 * P; k++)
+                    c[k] = r.c[2 * P + k];
                 const float t1 = r.c[j1], u1 = r.c[P + j1];
                 const float qe = w.x * t1 + w.y * u1, e1t = w.z * t1, e2t = w.w * t1;
                 int col[P];
@@ -222,12 +226,11 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
                     col[j3] = wrapIndex(id.z - j3, K2);
 #pragma unroll
                 for (int j2 = 0; j2 < P; j2++) {
-                    const float t2 = r.c[2 * P + j2], u2 = r.c[3 * P + j2];
-                    const float A2 = t2 * qe + e1t * u2, B2 = e2t * t2;
+                    const float A2 = c[j2] * qe + e1t * c[P + j2], B2 = e2t * c[j2];
                     unsigned long long* row = plane + wrapIndex(id.y - j2, K1) * K2;
 #pragma unroll
                     for (int j3 = 0; j3 < P; j3++) {
-                        const float v = A2 * r.c[4 * P + j3] + B2 * r.c[5 * P + j3];
+                        const float v = A2 * c[2 * P + j3] + B2 * c[3 * P + j3];
                         atomicAdd(row + col[j3], (unsigned long long) __float2ll_rn(v * PCG_FIX));
                     }
                 }

@@ -21,11 +21,24 @@ __device__ __forceinline__ int planeBin(const int4& b, const SysDev& S, int nyc)
     return wrapIndex(b.x, S.K[0]) * nyc + wrapIndex(b.y, S.K[1]) / PL_YCH;
 }
 
-// Bin counts (cleared before), then their exclusive scan, then the records in bin order.
-__global__ void k_plane_bin_count(Dev dv, int nyc, int* count) {
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot < dv.nAtoms)
-        atomicAdd(&count[planeBin(dv.baseS[slot], dv.sys[0], nyc)], 1);
+// Bin counts (cleared before; a block-local histogram in shared memory, then one global add per nonzero bin of
+// the block), then their exclusive scan, then the records in bin order.
+constexpr int PL_BIN_SLOTS = 2048;   // slots per binning block
+constexpr int PL_MAX_SMEM_BINS = 8192;
+
+__global__ void __launch_bounds__(256) k_plane_bin_count(Dev dv, int nyc, int* count) {
+    extern __shared__ int hist[];
+    const int nbins = dv.sys[0].K[0] * nyc;
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+        hist[b] = 0;
+    __syncthreads();
+    const int s0 = blockIdx.x * PL_BIN_SLOTS, s1 = min(dv.nAtoms, s0 + PL_BIN_SLOTS);
+    for (int slot = s0 + threadIdx.x; slot < s1; slot += blockDim.x)
+        atomicAdd(&hist[planeBin(dv.baseS[slot], dv.sys[0], nyc)], 1);
+    __syncthreads();
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+        if (hist[b])
+            atomicAdd(&count[b], hist[b]);
 }
 
 __global__ void __launch_bounds__(1024) k_plane_bin_scan(Dev dv, int nbins, int* count) {
@@ -74,23 +87,52 @@ __global__ void __launch_bounds__(1024) k_plane_bin_scan(Dev dv, int nbins, int*
         dv.pmeBinStart[nbins] = carry;
 }
 
+// The records in bin order: each block ranks its slots per bin in shared memory, claims a run of each bin's
+// records with one global add per nonzero bin, and writes its records there; a warp writes a record's 40 words
+// with its lanes (coalesced), the spline words read once per slot.
 template <int P>
-__global__ void k_plane_bin_fill(Dev dv, int nyc, int* fill) {
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= dv.nAtoms)
-        return;
+__global__ void __launch_bounds__(256) k_plane_bin_fill(Dev dv, int nyc, int* fill) {
+    extern __shared__ int hist[];   // nbins counts, then the block's base per bin
     const SysDev& S = dv.sys[0];
-    const int4 b = dv.baseS[slot];
-    PmeRec<P>& r = ((PmeRec<P>*) dv.pmeRec)[atomicAdd(&fill[planeBin(b, S, nyc)], 1)];
-    r.idx = make_int4(slot, wrapIndex(b.y, S.K[1]), b.z, wrapIndex(b.x, S.K[0]));
-    const float* sp = (const float*) dv.spl + (size_t) slot * 9 * MAXP;
+    const int nbins = S.K[0] * nyc;
+    int* base = hist + nbins;
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+        hist[b] = 0;
+    __syncthreads();
+    const int s0 = blockIdx.x * PL_BIN_SLOTS, s1 = min(dv.nAtoms, s0 + PL_BIN_SLOTS);
+    constexpr int PER = PL_BIN_SLOTS / 256;
+    int rank[PER];
 #pragma unroll
-    for (int dim = 0; dim < 3; dim++)
+    for (int k = 0; k < PER; k++) {
+        const int slot = s0 + threadIdx.x + k * 256;
+        rank[k] = slot < s1 ? atomicAdd(&hist[planeBin(dv.baseS[slot], S, nyc)], 1) : 0;
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x)
+        base[b] = hist[b] ? atomicAdd(&fill[b], hist[b]) : 0;
+    __syncthreads();
+    // where each of the block's slots goes, staged so that a warp can then write whole records
+    __shared__ int dest[PL_BIN_SLOTS];
 #pragma unroll
-        for (int kind = 0; kind < 2; kind++)
-#pragma unroll
-            for (int j = 0; j < P; j++)
-                r.c[dim * 2 * P + kind * P + j] = sp[(kind * 3 + dim) * MAXP + j];
+    for (int k = 0; k < PER; k++) {
+        const int slot = s0 + threadIdx.x + k * 256;
+        if (slot < s1)
+            dest[slot - s0] = base[planeBin(dv.baseS[slot], S, nyc)] + rank[k];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int slot = s0 + warp; slot < s1; slot += 8) {
+        PmeRec<P>& r = ((PmeRec<P>*) dv.pmeRec)[dest[slot - s0]];
+        const float* sp = (const float*) dv.spl + (size_t) slot * 9 * MAXP;
+        if (lane == 0) {
+            const int4 b = dv.baseS[slot];
+            r.idx = make_int4(slot, wrapIndex(b.y, S.K[1]), b.z, wrapIndex(b.x, S.K[0]));
+        }
+        for (int w = lane; w < 6 * P; w += 32) {   // word w = dim 2P + kind P + j
+            const int dim = w / (2 * P), kind = (w / P) % 2, j = w % P;
+            r.c[w] = sp[(kind * 3 + dim) * MAXP + j];
+        }
+    }
 }
 
 // The sources of a field pass per slot: mode 0 charges and vec, 1 vec only, 2 the CG direction p = z + beta p
@@ -158,6 +200,12 @@ __global__ void __launch_bounds__(PL_THREADS) k_spread_planes(Dev dv, int nyc) {
         const PmeRec<P>& r = rec[planeLocate<P>(start, cum, t, j1)];
         const int4 id = r.idx;
         const float4 w = dv.srcW[id.x];
+        // the record's coefficients in registers first (the shared atomics below would otherwise make the
+        // compiler reload them after every update)
+        float c[4 * P];
+#pragma unroll
+        for (int k = 0; k < 4 * P; k++)
+            c[k] = r.c[2 * P + k];
         const float t1 = r.c[j1], u1 = r.c[P + j1];
         const float qe = w.x * t1 + w.y * u1, e1t = w.z * t1, e2t = w.w * t1;
         int col[P];
@@ -166,12 +214,11 @@ __global__ void __launch_bounds__(PL_THREADS) k_spread_planes(Dev dv, int nyc) {
             col[j3] = wrapIndex(id.z - j3, K2);
 #pragma unroll
         for (int j2 = 0; j2 < P; j2++) {
-            const float t2 = r.c[2 * P + j2], u2 = r.c[3 * P + j2];
-            const float A2 = t2 * qe + e1t * u2, B2 = e2t * t2;
+            const float A2 = c[j2] * qe + e1t * c[P + j2], B2 = e2t * c[j2];
             float* row = tile + (id.y - j2 - y0 + P - 1) * K2;
 #pragma unroll
             for (int j3 = 0; j3 < P; j3++)
-                atomicAdd(row + col[j3], A2 * r.c[4 * P + j3] + B2 * r.c[5 * P + j3]);
+                atomicAdd(row + col[j3], A2 * c[2 * P + j3] + B2 * c[3 * P + j3]);
         }
     }
     __syncthreads();
