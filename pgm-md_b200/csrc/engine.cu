@@ -7,6 +7,7 @@
 #include "persistent.cuh"
 #include "adjoint.cuh"
 #include "planes.cuh"
+#include "lines.cuh"
 #include "pgm_engine.h"
 
 #include <algorithm>
@@ -188,7 +189,8 @@ struct Engine::Impl {
     bool gridOk = false;       // the systems' grids and the GPU allow the grid-transform kernel
     bool pcgOk = false;        // the persistent CG kernel applies (mixed, one system, grid kernel, order 6)
     bool planesOk = false;     // the plane-owner spread and gather apply (mixed, one system, order 6)
-    int pmeWant = 0;           // the caller's choice of spread / gather kernels: 0 a warp per atom, 1 plane tiles
+    int pmeWant = 0;           // the caller's choice of spread / gather kernels: 0 a warp per atom, 1 plane tiles,
+                               // 2 float4 lines
     int planeNyc = 1;          // row chunks per x-plane of the plane-owner kernels
     size_t planeSmem = 0;
     int pcgBlocks = 0;         // its blocks (one per SM)
@@ -1216,6 +1218,10 @@ struct Engine::Impl {
     }
 
     bool planesMode() const { return planesOk && pmeWant == 1; }
+    // the float4 line spread and gather: mixed precision, orders 4, 5, 6 and 8, any number of systems
+    bool linesMode() const {
+        return pmeWant == 2 && mixed() && (s.order == 4 || s.order == 5 || s.order == 6 || s.order == 8);
+    }
 
     // The plane bins and records of the evaluation (after k_splines).
     void enqueuePlaneBins(cudaStream_t sm, const Dev& d) {
@@ -1223,7 +1229,8 @@ struct Engine::Impl {
         CU(cudaMemsetAsync(dBinCount.p, 0, nbins * sizeof(int), sm));
         k_plane_bin_count<<<bb, 256, nbins * sizeof(int), sm>>>(d, planeNyc, dBinCount.as<int>());
         k_plane_bin_scan<<<1, 1024, 0, sm>>>(d, nbins, dBinCount.as<int>());
-        k_plane_bin_fill<6><<<bb, 256, 2 * nbins * sizeof(int), sm>>>(d, planeNyc, dBinCount.as<int>());
+        k_plane_bin_fill<6><<<(n + PL_FILL_SLOTS - 1) / PL_FILL_SLOTS, PL_FILL_SLOTS, 2 * nbins * sizeof(int), sm>>>(
+            d, planeNyc, dBinCount.as<int>());
         CU(cudaGetLastError());
     }
 
@@ -1363,6 +1370,16 @@ struct Engine::Impl {
             CU(cudaGetLastError());
             return;
         }
+        if (std::is_same<R, float>::value && linesMode()) {
+            switch (s.order) {
+            case 4: k_spread_lines<4><<<lineBlocks<4>(n), 256, 0, sm>>>(d, mode, vec); break;
+            case 5: k_spread_lines<5><<<lineBlocks<5>(n), 256, 0, sm>>>(d, mode, vec); break;
+            case 6: k_spread_lines<6><<<lineBlocks<6>(n), 256, 0, sm>>>(d, mode, vec); break;
+            default: k_spread_lines<8><<<lineBlocks<8>(n), 256, 0, sm>>>(d, mode, vec);
+            }
+            CU(cudaGetLastError());
+            return;
+        }
         const int wb = (n + 7) / 8;
         switch (s.order) {
         case 4: k_spread<R, 4><<<wb, 256, 0, sm>>>(d, mode, vec); break;
@@ -1379,6 +1396,16 @@ struct Engine::Impl {
         if (std::is_same<R, float>::value && !FINAL && !CGA && planesMode()) {   // plane tiles, then E_rec per atom
             k_gather_planes<6><<<dim3(sysK[0][0], planeNyc), PL_THREADS, planeSmem, sm>>>(d, planeNyc);
             k_gather_planes_finish<6><<<(n + 255) / 256, 256, 0, sm>>>(d);
+            CU(cudaGetLastError());
+            return;
+        }
+        if (std::is_same<R, float>::value && !FINAL && linesMode()) {
+            switch (s.order) {
+            case 4: k_gather_lines<4, CGA><<<lineBlocks<4>(n), 256, 0, sm>>>(d, gate); break;
+            case 5: k_gather_lines<5, CGA><<<lineBlocks<5>(n), 256, 0, sm>>>(d, gate); break;
+            case 6: k_gather_lines<6, CGA><<<lineBlocks<6>(n), 256, 0, sm>>>(d, gate); break;
+            default: k_gather_lines<8, CGA><<<lineBlocks<8>(n), 256, 0, sm>>>(d, gate);
+            }
             CU(cudaGetLastError());
             return;
         }
@@ -2841,10 +2868,11 @@ double Engine::timeEvaluations(int reps) {
 }
 
 // The PME spread / gather kernels of the field passes: 0 a warp per atom (every engine), 1 plane-owner tiles in
-// shared memory (mixed precision, one system, order 6; else 0 runs).
+// shared memory (mixed precision, one system, order 6), 2 float4 lines (mixed precision, orders 4, 5, 6, 8);
+// where the choice does not apply, 0 runs.
 void Engine::setPmeKernels(int kind) {
-    if (kind != 0 && kind != 1)
-        throw std::invalid_argument("pgm_b200: PME kernels must be 0 (a warp per atom) or 1 (plane tiles)");
+    if (kind < 0 || kind > 2)
+        throw std::invalid_argument("pgm_b200: PME kernels must be 0 (a warp per atom), 1 (plane tiles) or 2 (lines)");
     Impl& I = *impl;
     if (kind != I.pmeWant && I.exec) {
         cudaGraphExecDestroy(I.exec);
@@ -2853,7 +2881,7 @@ void Engine::setPmeKernels(int kind) {
     I.pmeWant = kind;
 }
 
-int Engine::pmeKernels() const { return impl->planesMode() ? 1 : 0; }
+int Engine::pmeKernels() const { return impl->planesMode() ? 1 : impl->linesMode() ? 2 : 0; }
 
 void Engine::setPairLanes(int lanes) {
     if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)

@@ -87,51 +87,48 @@ __global__ void __launch_bounds__(1024) k_plane_bin_scan(Dev dv, int nbins, int*
         dv.pmeBinStart[nbins] = carry;
 }
 
-// The records in bin order: each block ranks its slots per bin in shared memory, claims a run of each bin's
-// records with one global add per nonzero bin, and writes its records there; a warp writes a record's 40 words
-// with its lanes (coalesced), the spline words read once per slot.
+// The records in bin order: a block of 256 slots ranks them per bin in shared memory and claims a run of each
+// bin's records with one global add per nonzero bin; then the block writes its records word by word, consecutive
+// threads on consecutive words of a record (coalesced), reading the spline words from the slot's record.
+constexpr int PL_FILL_SLOTS = 256;
+
 template <int P>
-__global__ void __launch_bounds__(256) k_plane_bin_fill(Dev dv, int nyc, int* fill) {
+__global__ void __launch_bounds__(PL_FILL_SLOTS) k_plane_bin_fill(Dev dv, int nyc, int* fill) {
     extern __shared__ int hist[];   // nbins counts, then the block's base per bin
+    __shared__ int dest[PL_FILL_SLOTS];
     const SysDev& S = dv.sys[0];
     const int nbins = S.K[0] * nyc;
     int* base = hist + nbins;
     for (int b = threadIdx.x; b < nbins; b += blockDim.x)
         hist[b] = 0;
     __syncthreads();
-    const int s0 = blockIdx.x * PL_BIN_SLOTS, s1 = min(dv.nAtoms, s0 + PL_BIN_SLOTS);
-    constexpr int PER = PL_BIN_SLOTS / 256;
-    int rank[PER];
-#pragma unroll
-    for (int k = 0; k < PER; k++) {
-        const int slot = s0 + threadIdx.x + k * 256;
-        rank[k] = slot < s1 ? atomicAdd(&hist[planeBin(dv.baseS[slot], S, nyc)], 1) : 0;
+    const int s0 = blockIdx.x * PL_FILL_SLOTS, slot = s0 + threadIdx.x;
+    const bool on = slot < dv.nAtoms;
+    int bin = 0, rank = 0;
+    if (on) {
+        bin = planeBin(dv.baseS[slot], S, nyc);
+        rank = atomicAdd(&hist[bin], 1);
     }
     __syncthreads();
     for (int b = threadIdx.x; b < nbins; b += blockDim.x)
         base[b] = hist[b] ? atomicAdd(&fill[b], hist[b]) : 0;
     __syncthreads();
-    // where each of the block's slots goes, staged so that a warp can then write whole records
-    __shared__ int dest[PL_BIN_SLOTS];
-#pragma unroll
-    for (int k = 0; k < PER; k++) {
-        const int slot = s0 + threadIdx.x + k * 256;
-        if (slot < s1)
-            dest[slot - s0] = base[planeBin(dv.baseS[slot], S, nyc)] + rank[k];
-    }
+    dest[threadIdx.x] = on ? base[bin] + rank : 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int slot = s0 + warp; slot < s1; slot += 8) {
-        PmeRec<P>& r = ((PmeRec<P>*) dv.pmeRec)[dest[slot - s0]];
-        const float* sp = (const float*) dv.spl + (size_t) slot * 9 * MAXP;
-        if (lane == 0) {
-            const int4 b = dv.baseS[slot];
-            r.idx = make_int4(slot, wrapIndex(b.y, S.K[1]), b.z, wrapIndex(b.x, S.K[0]));
+    constexpr int W = 4 + 6 * P;   // words per record: idx, then c[w], w = dim 2P + kind P + j
+    static_assert(sizeof(PmeRec<P>) == W * 4, "record words");
+    const int nrec = min(PL_FILL_SLOTS, dv.nAtoms - s0);
+    for (int t = threadIdx.x; t < nrec * W; t += blockDim.x) {
+        const int r = t / W, w = t - r * W, sl = s0 + r;
+        int v;
+        if (w < 4) {
+            const int4 b = dv.baseS[sl];
+            v = w == 0 ? sl : w == 1 ? wrapIndex(b.y, S.K[1]) : w == 2 ? b.z : wrapIndex(b.x, S.K[0]);
+        } else {
+            const int c = w - 4, dim = c / (2 * P), kind = (c / P) % 2, j = c % P;
+            v = __float_as_int(((const float*) dv.spl)[(size_t) sl * 9 * MAXP + (kind * 3 + dim) * MAXP + j]);
         }
-        for (int w = lane; w < 6 * P; w += 32) {   // word w = dim 2P + kind P + j
-            const int dim = w / (2 * P), kind = (w / P) % 2, j = w % P;
-            r.c[w] = sp[(kind * 3 + dim) * MAXP + j];
-        }
+        ((int*) dv.pmeRec)[(size_t) dest[r] * W + w] = v;
     }
 }
 
