@@ -56,7 +56,7 @@ def parse():
                     help="with --profile: the system evaluated")
     ap.add_argument("--profile-transforms", type=int, default=-1,
                     help="with --profile: the field-pass transforms (0..4; -1: the engine's default)")
-    ap.add_argument("--profile-pme", type=int, default=0, help="with --profile: PME kernels (0 warp per atom, 1 tiles, 2 float4 lines)")
+    ap.add_argument("--profile-pme", type=int, default=0, help="with --profile: PME kernels (0 warp per atom, 1 plane tiles, 2 float4 lines, 3 cell tiles)")
     ap.add_argument("--profile-lanes", type=int, default=16, help="with --profile: pair lanes")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 1024-system leg")
     ap.add_argument("--no-large", action="store_true", help="skip the 98304-atom leg")

@@ -213,8 +213,10 @@ int pgm_engine_set_pair_lanes(pgm_engine* e, int lanes);
  * 0 a warp per atom with p^3 global atomics / loads; 1 plane-owner tiles -- a block per (x-plane, 16-row chunk)
  * accumulates or reads its tile in shared memory for the atoms whose stencil reaches it (mixed precision, one
  * system, order 6); 2 float4 lines -- a thread per (atom, x-plane of its stencil) adds or loads each z line of
- * the stencil as aligned float4 words (mixed precision, orders 4, 5, 6, 8, batches too).  Where the choice does
- * not apply, 0 runs; pgm_engine_pme_kernels tells which runs. */
+ * the stencil as aligned float4 words (mixed precision, orders 4, 5, 6, 8, batches too); 3 cell-group tiles -- a
+ * block per group of the pair search's cells accumulates or reads its atoms' grid window in shared memory (mixed
+ * precision, one system, orders 4, 5, 6, 8).  Where the choice does not apply, 0 runs; pgm_engine_pme_kernels
+ * tells which runs. */
 int pgm_engine_set_pme_kernels(pgm_engine* e, int kind);
 int pgm_engine_pme_kernels(pgm_engine* e);
 int pgm_engine_pair_lanes(pgm_engine* e);

@@ -18,7 +18,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libpgm_b200.so"
 SOURCES = [CSRC / "engine.cu", CSRC / "capi.cpp"]
-HEADERS = [CSRC / "common.cuh", CSRC / "kernels.cuh", CSRC / "pgm_engine.h", ROOT / "include" / "pgm_b200.h"]
+HEADERS = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "pgm_b200.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

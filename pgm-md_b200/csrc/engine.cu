@@ -8,6 +8,7 @@
 #include "adjoint.cuh"
 #include "planes.cuh"
 #include "lines.cuh"
+#include "tiles.cuh"
 #include "pgm_engine.h"
 
 #include <algorithm>
@@ -245,6 +246,7 @@ struct Engine::Impl {
     std::vector<double> launchBoxes;   // nsys * 9, the boxes of the evaluation in flight
     cudaGraph_t listBody = nullptr;    // body of the build's conditional node while capturing
     int graphCells = -1;               // cell count the graph was captured with
+    int graphTiles[2] = {-1, -1};      // tile groups and capacity the graph was captured with
     bool capturing = false;
 
     // last evaluation
@@ -1223,6 +1225,85 @@ struct Engine::Impl {
         return pmeWant == 2 && mixed() && (s.order == 4 || s.order == 5 || s.order == 6 || s.order == 8);
     }
 
+    // The cell-group tiles of one system: G cells a side per group (the largest of 4, 3, 2, 1 that leaves at
+    // least 100 groups and a tile within 96 KB, else the largest whose tile fits; PGM_B200_TILE_G overrides), the
+    // tile capacity in floats (the
+    // window of G cells' base indices + 1 for rounding + p - 1 halo + the list skin's drift both ways), and the
+    // group count.  groups = 0: no tiling applies.
+    void tileGeometry(int& G, int& cap, int& groups) const {
+        G = cap = groups = 0;
+        if (nsys != 1 || totalCells == 0)
+            return;
+        const SysDev& S = sysHost[0];
+        int win[5][3];
+        for (int g = 1; g <= TL_MAX_G; g++)
+            for (int a = 0; a < 3; a++) {
+                const double col = std::sqrt(S.recip[a] * S.recip[a] + S.recip[3 + a] * S.recip[3 + a] +
+                                             S.recip[6 + a] * S.recip[6 + a]);
+                const int drift = 1 + (int) std::ceil(s.skin * S.K[a] * col);
+                win[g][a] = (S.K[a] * g + S.cellN[a] - 1) / S.cellN[a] + 1 + (s.order - 1) + 2 * drift;
+            }
+        auto groupsOf = [&](int g) {
+            return ((S.cellN[0] + g - 1) / g) * ((S.cellN[1] + g - 1) / g) * ((S.cellN[2] + g - 1) / g);
+        };
+        auto capOf = [&](int g) { return (long long) win[g][0] * win[g][1] * win[g][2]; };
+        int pick = 0;
+        if (const char* e = std::getenv("PGM_B200_TILE_G"))
+            pick = std::max(1, std::min(TL_MAX_G, std::atoi(e)));
+        for (int g = TL_MAX_G; g >= 1 && !pick; g--)
+            if (groupsOf(g) >= 100 && capOf(g) * 4 <= 96 * 1024)
+                pick = g;
+        for (int g = TL_MAX_G; g >= 1 && !pick; g--)   // (small systems: the fewest groups that fit)
+            if (capOf(g) * 4 <= 96 * 1024)
+                pick = g;
+        if (!pick || capOf(pick) * 4 > 200 * 1024 || (size_t) groupsOf(pick) > ((size_t) n + 7) / 8)
+            return;   // (the tile beyond shared memory, or more groups than the block partials hold)
+        G = pick;
+        cap = (int) capOf(pick);
+        groups = groupsOf(pick);
+    }
+
+    // the cell-group tile spread and gather: mixed precision, one system, orders 4, 5, 6 and 8
+    bool tilesMode() const {
+        if (pmeWant != 3 || !mixed() || nsys != 1 ||
+            !(s.order == 4 || s.order == 5 || s.order == 6 || s.order == 8))
+            return false;
+        if (totalCells == 0)
+            return true;   // (no box yet: the geometry is settled at the first evaluation)
+        int G, cap, groups;
+        tileGeometry(G, cap, groups);
+        return groups > 0;
+    }
+
+    template <int P> void launchTiles(cudaStream_t sm, const Dev& d, bool spread, int mode, double* vec, int gate,
+                                      bool cga) {
+        int G, cap, groups;
+        tileGeometry(G, cap, groups);
+        const size_t smem = (size_t) cap * sizeof(float);
+        static std::once_flag once[4];
+        std::call_once(once[P == 4 ? 0 : P == 5 ? 1 : P == 6 ? 2 : 3], [] {
+            for (const void* f : {(const void*) k_spread_tiles<P>, (const void*) k_gather_tiles<P, false>,
+                                  (const void*) k_gather_tiles<P, true>})
+                CU(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        });
+        if (spread)
+            k_spread_tiles<P><<<groups, TL_THREADS, smem, sm>>>(d, mode, vec, G, cap);
+        else if (cga)
+            k_gather_tiles<P, true><<<groups, TL_THREADS, smem, sm>>>(d, gate, G, cap);
+        else
+            k_gather_tiles<P, false><<<groups, TL_THREADS, smem, sm>>>(d, gate, G, cap);
+        CU(cudaGetLastError());
+    }
+
+    void launchTilesOrder(cudaStream_t sm, const Dev& d, bool spread, int mode, double* vec, int gate, bool cga) {
+        switch (s.order) {
+        case 4: launchTiles<4>(sm, d, spread, mode, vec, gate, cga); break;
+        case 5: launchTiles<5>(sm, d, spread, mode, vec, gate, cga); break;
+        case 6: launchTiles<6>(sm, d, spread, mode, vec, gate, cga); break;
+        default: launchTiles<8>(sm, d, spread, mode, vec, gate, cga);
+        }
+    }
+
     // The plane bins and records of the evaluation (after k_splines).
     void enqueuePlaneBins(cudaStream_t sm, const Dev& d) {
         const int nbins = sysK[0][0] * planeNyc, bb = (n + PL_BIN_SLOTS - 1) / PL_BIN_SLOTS;
@@ -1370,6 +1451,10 @@ struct Engine::Impl {
             CU(cudaGetLastError());
             return;
         }
+        if (std::is_same<R, float>::value && tilesMode()) {
+            launchTilesOrder(sm, d, true, mode, vec, 0, false);
+            return;
+        }
         if (std::is_same<R, float>::value && linesMode()) {
             switch (s.order) {
             case 4: k_spread_lines<4><<<lineBlocks<4>(n), 256, 0, sm>>>(d, mode, vec); break;
@@ -1397,6 +1482,10 @@ struct Engine::Impl {
             k_gather_planes<6><<<dim3(sysK[0][0], planeNyc), PL_THREADS, planeSmem, sm>>>(d, planeNyc);
             k_gather_planes_finish<6><<<(n + 255) / 256, 256, 0, sm>>>(d);
             CU(cudaGetLastError());
+            return;
+        }
+        if (std::is_same<R, float>::value && !FINAL && tilesMode()) {
+            launchTilesOrder(sm, d, false, 0, nullptr, gate, CGA);
             return;
         }
         if (std::is_same<R, float>::value && !FINAL && linesMode()) {
@@ -1684,6 +1773,12 @@ struct Engine::Impl {
         }
         CU(cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority));
         graphCells = totalCells;
+        {
+            int G, cap, groups;
+            tileGeometry(G, cap, groups);
+            graphTiles[0] = groups;
+            graphTiles[1] = cap;
+        }
         CU(cudaGraphDestroy(graph));
     }
 
@@ -1814,7 +1909,10 @@ struct Engine::Impl {
             throw std::logic_error("pgm_b200: compute before setAtoms");
         const bool grew = setBoxes(boxes);
         // the graph's launch shapes hold the cell count (another box can change it without growing the storage)
-        if ((grew || totalCells != graphCells) && exec) {
+        // and the tile kernels' groups
+        int tG, tCap, tGroups;
+        tileGeometry(tG, tCap, tGroups);
+        if ((grew || totalCells != graphCells || tGroups != graphTiles[0] || tCap != graphTiles[1]) && exec) {
             cudaGraphExecDestroy(exec);
             exec = nullptr;
         }
@@ -2868,11 +2966,13 @@ double Engine::timeEvaluations(int reps) {
 }
 
 // The PME spread / gather kernels of the field passes: 0 a warp per atom (every engine), 1 plane-owner tiles in
-// shared memory (mixed precision, one system, order 6), 2 float4 lines (mixed precision, orders 4, 5, 6, 8);
-// where the choice does not apply, 0 runs.
+// shared memory (mixed precision, one system, order 6), 2 float4 lines (mixed precision, orders 4, 5, 6, 8),
+// 3 cell-group tiles in shared memory (mixed precision, one system, orders 4, 5, 6, 8); where the choice does not
+// apply, 0 runs.
 void Engine::setPmeKernels(int kind) {
-    if (kind < 0 || kind > 2)
-        throw std::invalid_argument("pgm_b200: PME kernels must be 0 (a warp per atom), 1 (plane tiles) or 2 (lines)");
+    if (kind < 0 || kind > 3)
+        throw std::invalid_argument(
+            "pgm_b200: PME kernels must be 0 (a warp per atom), 1 (plane tiles), 2 (lines) or 3 (cell tiles)");
     Impl& I = *impl;
     if (kind != I.pmeWant && I.exec) {
         cudaGraphExecDestroy(I.exec);
@@ -2881,7 +2981,9 @@ void Engine::setPmeKernels(int kind) {
     I.pmeWant = kind;
 }
 
-int Engine::pmeKernels() const { return impl->planesMode() ? 1 : impl->linesMode() ? 2 : 0; }
+int Engine::pmeKernels() const {
+    return impl->planesMode() ? 1 : impl->linesMode() ? 2 : impl->tilesMode() ? 3 : 0;
+}
 
 void Engine::setPairLanes(int lanes) {
     if (lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)

@@ -109,8 +109,8 @@ public:
     // with a block per x-plane (1, 2 and 3 where the grids allow them; transforms() tells which runs)
     void setTransforms(int mode);
     // PME spread / gather of the field passes: 0 a warp per atom, 1 plane-owner tiles in shared memory (mixed
-    // precision, one system, order 6), 2 float4 lines (mixed precision, orders 4, 5, 6, 8); pmeKernels() tells
-    // which runs
+    // precision, one system, order 6), 2 float4 lines (mixed precision, orders 4, 5, 6, 8), 3 cell-group tiles
+    // (mixed precision, one system, orders 4, 5, 6, 8); pmeKernels() tells which runs
     void setPmeKernels(int kind);
     int pmeKernels() const;
     int transforms() const;

@@ -381,7 +381,8 @@ class Engine:
     def set_pme_kernels(self, kind):
         """PME spread / gather of the field passes: 0 a warp per atom, 1 plane-owner tiles in shared memory
         (mixed precision, one system, order 6), 2 float4 lines (mixed precision, orders 4, 5, 6, 8, batches
-        too); pme_kernels() tells which runs."""
+        too), 3 cell-group tiles in shared memory (mixed precision, one system, orders 4, 5, 6, 8);
+        pme_kernels() tells which runs."""
         _check(self._L.pgm_engine_set_pme_kernels(self._h, int(kind)))
 
     def pme_kernels(self):
@@ -419,7 +420,7 @@ class Engine:
             self.set_transforms(mode)
             if self.transforms() != mode:
                 continue
-            for pme in (0, 1, 2):
+            for pme in (0, 1, 2, 3):
                 self.set_pme_kernels(pme)
                 if self.pme_kernels() != pme:
                     continue

@@ -42,7 +42,8 @@ def water98304():
 
 
 @pytest.mark.parametrize("precision,tol,pme", [(PKG.FP64, 1e-10, 0), (PKG.MIXED, 1e-5, 0), (PKG.MIXED, 1e-4, 0),
-                                               (PKG.MIXED, 1e-5, 1), (PKG.MIXED, 1e-5, 2)])
+                                               (PKG.MIXED, 1e-5, 1), (PKG.MIXED, 1e-5, 2),
+                                               (PKG.MIXED, 1e-5, 3)])
 def test_water98304_against_reference(water98304, precision, tol, pme):
     S, d = water98304
     eng = single_engine(S, precision, tol, pme)
