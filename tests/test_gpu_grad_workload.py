@@ -37,10 +37,12 @@ def check(got, fd, what, lim=1e-5, elem=(1e-5, 1e-3)):
 
 
 # Mixed precision's force-matching gradient: the 1e-5 bar holds for each parameter kind as a vector; single
-# elements may reach 3e-5 of the larger of themselves and 1 % of their kind's largest, because w = 2 (F - F_target)
+# elements may reach 1e-4 of the larger of themselves and 1 % of their kind's largest, because w = 2 (F - F_target)
 # is a difference of forces about 20 times smaller than the forces (F_target from parameters perturbed by 5 %), so
-# the mixed path's force error (3e-7 relative RMS) enters dL/dtheta about 20 times enlarged.
-FM_ELEM = {PKG.FP64: (1e-5, 1e-3), PKG.MIXED: (3e-5, 1e-2)}
+# the mixed path's force error (3e-7 relative RMS) enters dL/dtheta about 20 times enlarged.  (Measured on a B200:
+# the largest element error of the 64-water batch moves between 3e-5 and 5e-5 from run to run with the float
+# atomics' order; the FP64 path holds every element to 1e-5.)
+FM_ELEM = {PKG.FP64: (1e-5, 1e-3), PKG.MIXED: (1e-4, 1e-2)}
 
 
 def engine(S, precision, tol=1e-8):

@@ -90,7 +90,7 @@ def test_line_kernels_not_applicable():
     assert e.pme_kernels() == 0
     e.close()
     with pytest.raises(Exception):
-        mixed_engine(S, 0, 3)
+        mixed_engine(S, 0, 4)
 
 
 def test_line_kernels_batch_sample():
