@@ -111,6 +111,7 @@ struct Dev {
                               // followed by the grid transforms' barriers (2 per system)
     // dipoles
     void* dS;                 // slot-order R4 (dipole xyz, charge w) for the pair passes
+    void* dS2;                // the second source set of a dual pair pass (the predicted guess's dipoles)
     double* perm;             // 3n
     double* mu;               // 3n
     double* dtot;             // 3n
@@ -136,6 +137,7 @@ struct Dev {
     int useActive;            // 1: the per-slot CG kernels take virtual slots (batched engines)
     // fields / forces
     double* Epair;            // 3n
+    double* Epair2;           // 3n: the dual pair pass's field of dS2
     double* Erec;             // 3n
     double* Fpair;            // 3n
     double* spair;            // 9n pair strain

@@ -206,6 +206,7 @@ struct Engine::Impl {
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
         dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dPairA, dPairB, dPairC, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
+        dDS2, dEpair2, dErec2, dGrid2,
         dScal, dPartial, dGPartial, dHrec, dFm, dPmeRec, dPmeBins, dSrcW, dGPart, dPcgPartial, dBinCount, dActive, dActSys, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dTwiddle, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
@@ -247,6 +248,7 @@ struct Engine::Impl {
     cudaGraph_t listBody = nullptr;    // body of the build's conditional node while capturing
     int graphCells = -1;               // cell count the graph was captured with
     int graphTiles[2] = {-1, -1};      // tile groups and capacity the graph was captured with
+    bool graphDual = false;            // the graph's first pass is the dual one (a predicted guess)
     bool capturing = false;
 
     // last evaluation
@@ -283,6 +285,7 @@ struct Engine::Impl {
         plans64.clear();
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
                       &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dPairA, &dPairB, &dPairC, &dFlags, &dDS,
+                      &dDS2, &dEpair2, &dErec2, &dGrid2,
                       &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dGPartial, &dHrec, &dFm, &dPmeRec, &dPmeBins, &dSrcW, &dGPart,
                       &dPcgPartial, &dBinCount, &dActive, &dActSys, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
@@ -746,6 +749,9 @@ struct Engine::Impl {
         dPosBuild.ensure(3 * (size_t) n * 8);
         dFlags.ensure(flagBytes());
         dDS.ensure(n * 4 * R);
+        dDS2.ensure(n * 4 * R);
+        dEpair2.ensure(3 * n * 8);
+        dErec2.ensure(3 * n * 8);
         for (Buf* b : {&dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dEpair, &dErec, &dFpair, &dFrec, &dEtot,
                        &dForces})
             b->ensure(3 * n * 8);
@@ -769,6 +775,7 @@ struct Engine::Impl {
             convOff[k] = k * convBlocks;
         upload(dConvOff, convOff, st);
         dGrid.ensure(gridTotal * R);
+        dGrid2.ensure(gridTotal * R);
         dSpec.ensure(specTotal * 2 * R);
         dInfl.ensure(specTotal * R);
         if (refining()) {
@@ -1004,6 +1011,7 @@ struct Engine::Impl {
         d.pairC = dPairC.p;
         d.flags = dFlags.as<int>();
         d.dS = dDS.p;
+        d.dS2 = dDS2.p;
         d.perm = dPerm.as<double>();
         d.mu = dMu.as<double>();
         d.dtot = dDtot.as<double>();
@@ -1023,6 +1031,7 @@ struct Engine::Impl {
         d.actCount = d.actOff + nsys + 1;
         d.useActive = nsys > 1 ? 1 : 0;
         d.Epair = dEpair.as<double>();
+        d.Epair2 = dEpair2.as<double>();
         d.Erec = dErec.as<double>();
         d.Fpair = dFpair.as<double>();
         d.spair = dSpair.as<double>();
@@ -1509,17 +1518,29 @@ struct Engine::Impl {
         CU(cudaGetLastError());
     }
 
-    template <typename R, bool WITHQ> void pairField(cudaStream_t sm, const Dev& d, int gate) {
+    template <typename R, bool WITHQ, bool DUAL = false> void pairField(cudaStream_t sm, const Dev& d, int gate) {
         const long long threads = (long long) n * pairGS;
         const int blocks = (int) ((threads + 255) / 256);
         const int sh = pairSmem;
         switch (pairGS) {
-        case 4: k_pair_field<R, WITHQ, 4><<<blocks, 256, sh, sm>>>(d, gate); break;
-        case 16: k_pair_field<R, WITHQ, 16><<<blocks, 256, sh, sm>>>(d, gate); break;
-        case 8: k_pair_field<R, WITHQ, 8><<<blocks, 256, sh, sm>>>(d, gate); break;
-        default: k_pair_field<R, WITHQ, 32><<<blocks, 256, sh, sm>>>(d, gate);
+        case 4: k_pair_field<R, WITHQ, 4, DUAL><<<blocks, 256, sh, sm>>>(d, gate); break;
+        case 16: k_pair_field<R, WITHQ, 16, DUAL><<<blocks, 256, sh, sm>>>(d, gate); break;
+        case 8: k_pair_field<R, WITHQ, 8, DUAL><<<blocks, 256, sh, sm>>>(d, gate); break;
+        default: k_pair_field<R, WITHQ, 32, DUAL><<<blocks, 256, sh, sm>>>(d, gate);
         }
         CU(cudaGetLastError());
+    }
+
+    // A predicted step (guess from history, not from E_perm): the permanent field and T x0 from one pair sweep
+    // over the records and two PME passes, the second on its own grid (the transforms in sequence: they share
+    // the spectrum buffer and the grid kernel's barrier words).  The engine's own passes otherwise.
+    // (PGM_B200_DUAL=0 keeps the two passes apart, for comparison)
+    bool dualFirstPass() const {
+        const char* e = std::getenv("PGM_B200_DUAL");
+        if (e && e[0] == '0')
+            return false;
+        return s.polarizable && hCtl && hCtl->guess >= 1 && !hCtl->customRhs && !persistentMode() && !refining() &&
+               !planesMode() && !tilesMode();
     }
 
     // field of (q?, vec) at every atom into Epair / Erec: spread on sm, then the pair pass on sm beside the
@@ -1645,6 +1666,33 @@ struct Engine::Impl {
                 launchPersistent(sm, d, 1, d.x);
                 k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
                 CU(cudaGetLastError());
+                return;
+            }
+            if (dualFirstPass()) {
+                // x0 first; (q, perm) into the grid and dS, x0 into the second grid and dS2; the two transforms
+                // on the main stream while the records finish on the side stream; one pair sweep for both fields
+                Dev d2 = d;   // the second source set: its grid, its float copy, its reciprocal field
+                d2.grid = dGrid2.p;
+                d2.dS = dDS2.p;
+                d2.Erec = dErec2.as<double>();
+                k_cg_guess<<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
+                CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
+                CU(cudaMemsetAsync(d2.grid, 0, gridTotal * realSize(), sm));
+                launchSpread<R>(sm, d, 0, d.perm);
+                launchSpread<R>(sm, d2, 1, d.x);
+                transformPair<R>(sm, d, false);
+                transformPair<R>(sm, d2, false);
+                CU(cudaStreamWaitEvent(sm, evJoin, 0));
+                pairField<R, true, true>(sm, d, 0);
+                launchGather<R, false>(sm, d, 0);
+                launchGather<R, false>(sm, d2, 0);
+                k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+                Dev d3 = d;   // T x0: the second set's pair and reciprocal fields
+                d3.Epair = dEpair2.as<double>();
+                d3.Erec = dErec2.as<double>();
+                k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d3);
+                CU(cudaGetLastError());
+                CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
                 return;
             }
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
@@ -1773,6 +1821,7 @@ struct Engine::Impl {
         }
         CU(cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority));
         graphCells = totalCells;
+        graphDual = dualFirstPass();
         {
             int G, cap, groups;
             tileGeometry(G, cap, groups);
@@ -1912,7 +1961,8 @@ struct Engine::Impl {
         // and the tile kernels' groups
         int tG, tCap, tGroups;
         tileGeometry(tG, tCap, tGroups);
-        if ((grew || totalCells != graphCells || tGroups != graphTiles[0] || tCap != graphTiles[1]) && exec) {
+        if ((grew || totalCells != graphCells || tGroups != graphTiles[0] || tCap != graphTiles[1] ||
+             dualFirstPass() != graphDual) && exec) {
             cudaGraphExecDestroy(exec);
             exec = nullptr;
         }

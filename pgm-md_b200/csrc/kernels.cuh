@@ -1843,7 +1843,9 @@ __global__ void __launch_bounds__(256) k_gather(Dev dv, int gateDone) {
 // + (d_j . x) x G2 (core/pgm_core.cpp:274-284), products in precision R, sums in double.  GS lanes per atom.
 // Mixed: the pair records (x, G1, G2, slot of j) stream from the evaluation's list and only (d_j, q_j) is
 // gathered; FP64: x from the gathered slot-order positions, (G1, G2) streamed.
-template <typename R, bool WITHQ, int GS>
+// DUAL: one sweep over the records for two source sets, (q, d) from dS (with WITHQ) into Epair and the dipoles
+// of dS2 into Epair2, each summed exactly as a pass of its own would sum it.
+template <typename R, bool WITHQ, int GS, bool DUAL = false>
 __global__ void __launch_bounds__(256) k_pair_field(Dev dv, int gateDone) {
     typedef typename V4T<R>::T R4;
     typedef typename V2T<R>::T R2;
@@ -1861,14 +1863,17 @@ __global__ void __launch_bounds__(256) k_pair_field(Dev dv, int gateDone) {
     const R4* arow = (const R4*) dv.pairA + (size_t) slot * dv.cap;
     const R2* brow = (const R2*) dv.pairB + (size_t) slot * dv.cap;
     const R4* dS = (const R4*) dv.dS;
+    const R4* dS2 = (const R4*) dv.dS2;
     const int cnt = dv.listCount[slot];
     R a0 = 0, a1 = 0, a2 = 0;   // per-lane sums in R (about cnt / GS terms each), across lanes in double
+    R b0 = 0, b1 = 0, b2 = 0;   // (DUAL: the second set's)
     if constexpr (PairRec<R>::storeX) {
 #pragma unroll 4
         for (int t = lane; t < cnt; t += GS) {
             const R4 xg = arow[t];
             const R2 gb = brow[t];
-            const R4 dj = dS[realAsSlot(gb.y)];
+            const int js = realAsSlot(gb.y);
+            const R4 dj = dS[js];
             const R djx = dj.x * xg.x + dj.y * xg.y + dj.z * xg.z;
             R c = djx * gb.x;
             if (WITHQ)
@@ -1876,6 +1881,13 @@ __global__ void __launch_bounds__(256) k_pair_field(Dev dv, int gateDone) {
             a0 += c * xg.x - dj.x * xg.w;
             a1 += c * xg.y - dj.y * xg.w;
             a2 += c * xg.z - dj.z * xg.w;
+            if (DUAL) {
+                const R4 ej = dS2[js];
+                const R c2 = (ej.x * xg.x + ej.y * xg.y + ej.z * xg.z) * gb.x;
+                b0 += c2 * xg.x - ej.x * xg.w;
+                b1 += c2 * xg.y - ej.y * xg.w;
+                b2 += c2 * xg.z - ej.z * xg.w;
+            }
         }
     } else {
         const SysDev& S = dv.sys[s];
@@ -1898,20 +1910,38 @@ __global__ void __launch_bounds__(256) k_pair_field(Dev dv, int gateDone) {
             a0 += c * x0 - dj.x * G.x;
             a1 += c * x1 - dj.y * G.x;
             a2 += c * x2 - dj.z * G.x;
+            if (DUAL) {
+                const R4 ej = dS2[js];
+                const R c2 = (ej.x * x0 + ej.y * x1 + ej.z * x2) * G.y;
+                b0 += c2 * x0 - ej.x * G.x;
+                b1 += c2 * x1 - ej.y * G.x;
+                b2 += c2 * x2 - ej.z * G.x;
+            }
         }
     }
     double E0 = a0, E1 = a1, E2 = a2;
+    double H0 = b0, H1 = b1, H2 = b2;
     const unsigned gm = groupMask<GS>();
 #pragma unroll
     for (int o = GS / 2; o > 0; o >>= 1) {
         E0 += __shfl_xor_sync(gm, E0, o, GS);
         E1 += __shfl_xor_sync(gm, E1, o, GS);
         E2 += __shfl_xor_sync(gm, E2, o, GS);
+        if (DUAL) {
+            H0 += __shfl_xor_sync(gm, H0, o, GS);
+            H1 += __shfl_xor_sync(gm, H1, o, GS);
+            H2 += __shfl_xor_sync(gm, H2, o, GS);
+        }
     }
     if (lane == 0) {
         dv.Epair[3 * i] = E0;
         dv.Epair[3 * i + 1] = E1;
         dv.Epair[3 * i + 2] = E2;
+        if (DUAL) {
+            dv.Epair2[3 * i] = H0;
+            dv.Epair2[3 * i + 1] = H1;
+            dv.Epair2[3 * i + 2] = H2;
+        }
     }
 }
 
@@ -2127,6 +2157,32 @@ __global__ void __launch_bounds__(256) k_gvdw(Dev dv) {
 
 // ------------------------------------------------------------------------------------------------ CG
 
+// The initial guess x0 of component g = 3 gi + k when it does not depend on b (guess 1: zero; 2: history slot;
+// 3: mu3 from history; 4: mu4 from history) (core/pgm_core.cpp:309-329).
+__device__ __forceinline__ double historyGuess(const Dev& dv, int guess, size_t g, size_t hs) {
+    const int h0 = dv.ctl->h[0], h1 = dv.ctl->h[1], h2 = dv.ctl->h[2], h3 = dv.ctl->h[3];
+    switch (guess) {
+    case 1: return 0.0;
+    case 2: return dv.hist[h0 * hs + g];
+    case 3: return 3 * dv.hist[h0 * hs + g] - 3 * dv.hist[h1 * hs + g] + dv.hist[h2 * hs + g];
+    default:
+        return 4 * dv.hist[h0 * hs + g] - 6 * dv.hist[h1 * hs + g] + 4 * dv.hist[h2 * hs + g] - dv.hist[h3 * hs + g];
+    }
+}
+
+// x0 of a predicted step before the permanent field (guess >= 1), so that one pair sweep forms E_perm and T x0
+// together; k_cg_b then writes the same x0 again.
+__global__ void k_cg_guess(Dev dv) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * dv.nAtoms)
+        return;
+    const int i = t / 3, k = t % 3;
+    const int guess = dv.ctl->guess;
+    const int gi = dv.globalIndex ? dv.globalIndex[i] : i;
+    const double x0 = guess >= 1 ? historyGuess(dv, guess, (size_t) 3 * gi + k, (size_t) 3 * dv.numGlobal) : 0.0;
+    dv.x[t] = (guess >= 2 && !(dv.alpha[i] > 0)) ? 0.0 : x0;
+}
+
 // b = E_perm (pair + reciprocal + self), norm = mean|alpha b| per system, initial guess x0
 // (guess 0: alpha b; 1: zero; 2: history slot; 3: mu3 from history; 4: mu4 from history)
 // (core/pgm_core.cpp:297-329).
@@ -2141,22 +2197,13 @@ __global__ void __launch_bounds__(CHUNK) k_cg_b(Dev dv) {
         const double al = dv.alpha[i];
         const int gi = dv.globalIndex ? dv.globalIndex[i] : i;
         const size_t hs = (size_t) 3 * dv.numGlobal;
-        const int guess = dv.ctl->guess, h0 = dv.ctl->h[0], h1 = dv.ctl->h[1], h2 = dv.ctl->h[2], h3 = dv.ctl->h[3];
+        const int guess = dv.ctl->guess;
         const bool custom = dv.ctl->customRhs != 0;
         for (int k = 0; k < 3; k++) {
             const double bk = custom ? dv.b[3 * i + k] : dv.Epair[3 * i + k] + dv.Erec[3 * i + k] + cs * dv.perm[3 * i + k];
             dv.b[3 * i + k] = bk;
             v[0] += fabs(al * bk);
-            double x0;
-            const size_t g = (size_t) 3 * gi + k;
-            switch (guess) {
-            case 0: x0 = al * bk; break;
-            case 1: x0 = 0.0; break;
-            case 2: x0 = dv.hist[h0 * hs + g]; break;
-            case 3: x0 = 3 * dv.hist[h0 * hs + g] - 3 * dv.hist[h1 * hs + g] + dv.hist[h2 * hs + g]; break;
-            default:
-                x0 = 4 * dv.hist[h0 * hs + g] - 6 * dv.hist[h1 * hs + g] + 4 * dv.hist[h2 * hs + g] - dv.hist[h3 * hs + g];
-            }
+            const double x0 = guess == 0 ? al * bk : historyGuess(dv, guess, (size_t) 3 * gi + k, hs);
             dv.x[3 * i + k] = (guess >= 2 && !(al > 0)) ? 0.0 : x0;
         }
     }
