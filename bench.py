@@ -250,16 +250,19 @@ def md_positions(S, phase, count):
     return [S.pos + 0.01 * np.sin(2 * np.pi * st / 100 + phase) for st in range(count)]
 
 
-def md_leg(pkg, S, make, lanes, dev, steps=30):
+def md_leg(pkg, S, make, lanes, dev, steps=60):
     """MD-like use: positions move smoothly every step (amplitude 0.01 nm, period 100 steps, random phases,
     as the reference harness's moving timing, core/cuda/tests/test_cuda.cpp:351-372), new step every call,
     mu4 predictor, the Verlet list kept with the default 0.15 nm skin (as the reference engine's); host call with
-    host positions and forces.  Both precisions."""
+    host positions and forces.  Both precisions; mixed again with the predicted steps' first passes apart
+    (PGM_B200_DUAL=0) for the dual first pass's gain."""
     import torch
     rng = np.random.default_rng(7)
     phase = rng.uniform(0, 2 * np.pi, S.pos.shape)
     out = {}
-    for name, prec in (("mixed", pkg.MIXED), ("fp64", pkg.FP64)):
+    for name, prec in (("mixed", pkg.MIXED), ("fp64", pkg.FP64), ("mixed_separate_first_passes", pkg.MIXED)):
+        if name == "mixed_separate_first_passes":
+            os.environ["PGM_B200_DUAL"] = "0"
         eng = pkg.Engine(pkg.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=S.order, tol=TOL, max_iter=200,
                                       peek=0.65, predictor=2, ke=pkg.systems.KE_DEFAULT, precision=prec,
                                       device=dev.index or 0))
@@ -278,9 +281,12 @@ def md_leg(pkg, S, make, lanes, dev, steps=30):
         out[name] = {"evals_per_s": 1.0 / dt, "mean_cg_iterations": float(np.mean(its)),
                      "list_builds": eng.list_builds()}
         eng.close()
+        os.environ.pop("PGM_B200_DUAL", None)
     out["mixed_over_fp64"] = out["mixed"]["evals_per_s"] / out["fp64"]["evals_per_s"]
+    out["dual_first_pass_gain"] = out["mixed"]["evals_per_s"] / out["mixed_separate_first_passes"]["evals_per_s"]
     out["note"] = ("host call with host positions and forces (positions generated before the timed loop); "
-                   "predictor mu4; Verlet list, skin 0.15 nm")
+                   "predictor mu4; Verlet list, skin 0.15 nm; predicted steps take the dual first pass "
+                   "(mixed_separate_first_passes: the same with the two passes apart)")
     return out
 
 
@@ -445,7 +451,8 @@ def reference_gpu_leg(pkg, S, steps, warmup):
         out["step"] = {"evals_per_s": steps / (ms / 1e3), "ms_per_eval": ms / steps,
                        "cg_iterations": int(np.median(its)), "list_builds": eng.list_builds(), "steps": steps}
         E, F = eng.compute(S.pos, S.box)
-        E0, F0, kind = _oracle_reference(pkg, S, 1e-10)
+        ref = _oracle_reference(pkg, S, 1e-10)
+        E0, F0, kind = ref["energy"], ref["forces"], ref["kind"]
         out["accuracy"] = {"oracle": kind, "force_rel_rms": float(np.linalg.norm(F - F0) / np.linalg.norm(F0)),
                            "energy_rel": float(abs(E - E0) / abs(E0))}
         eng.close()

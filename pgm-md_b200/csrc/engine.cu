@@ -1669,8 +1669,8 @@ struct Engine::Impl {
                 return;
             }
             if (dualFirstPass()) {
-                // x0 first; (q, perm) into the grid and dS, x0 into the second grid and dS2; the two transforms
-                // on the main stream while the records finish on the side stream; one pair sweep for both fields
+                // x0 first; (q, perm) into the grid and dS, x0 into the second grid and dS2; one pair sweep for
+                // both direct fields
                 Dev d2 = d;   // the second source set: its grid, its float copy, its reciprocal field
                 d2.grid = dGrid2.p;
                 d2.dS = dDS2.p;
@@ -1680,12 +1680,18 @@ struct Engine::Impl {
                 CU(cudaMemsetAsync(d2.grid, 0, gridTotal * realSize(), sm));
                 launchSpread<R>(sm, d, 0, d.perm);
                 launchSpread<R>(sm, d2, 1, d.x);
+                // the pair sweep on the side stream after its records and the spreads' float copies, beside the
+                // transforms and gathers here (the transforms in sequence: one spectrum buffer, one set of the
+                // grid kernel's barrier words)
+                CU(cudaEventRecord(evFork, sm));
+                CU(cudaStreamWaitEvent(sd, evFork, 0));
+                pairField<R, true, true>(sd, d, 0);
+                CU(cudaEventRecord(evJoin, sd));
                 transformPair<R>(sm, d, false);
-                transformPair<R>(sm, d2, false);
-                CU(cudaStreamWaitEvent(sm, evJoin, 0));
-                pairField<R, true, true>(sm, d, 0);
                 launchGather<R, false>(sm, d, 0);
+                transformPair<R>(sm, d2, false);
                 launchGather<R, false>(sm, d2, 0);
+                CU(cudaStreamWaitEvent(sm, evJoin, 0));
                 k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
                 Dev d3 = d;   // T x0: the second set's pair and reciprocal fields
                 d3.Epair = dEpair2.as<double>();
