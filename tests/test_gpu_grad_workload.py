@@ -43,6 +43,10 @@ def check(got, fd, what, lim=1e-5, elem=(1e-5, 1e-3)):
 # the largest element error of the 64-water batch moves between 3e-5 and 5e-5 from run to run with the float
 # atomics' order; the FP64 path holds every element to 1e-5.)
 FM_ELEM = {PKG.FP64: (1e-5, 1e-3), PKG.MIXED: (1e-4, 1e-2)}
+# and the kind's norm: FP64 1e-5; mixed 2e-5, because a kind with one type (the water's bond dipole) is a single
+# element, measured on a B200 between 0.6e-5 and 1.2e-5 from run to run (the same amplification of the mixed
+# forces' error through w)
+FM_NORM = {PKG.FP64: 1e-5, PKG.MIXED: 2e-5}
 
 
 def engine(S, precision, tol=1e-8):
@@ -100,7 +104,7 @@ def test_water64_batch_force_matching_gradients(water64, precision):
             else:
                 part, ty = g[name][off:off + S.n], S.types
             fd = d[f"b{k}_dL_{name}"]
-            check(per_type(part, ty, len(fd)), fd, (int(k), name), elem=FM_ELEM[precision])
+            check(per_type(part, ty, len(fd)), fd, (int(k), name), lim=FM_NORM[precision], elem=FM_ELEM[precision])
         off += S.n
         coff += len(S.cov_atom)
 
@@ -136,4 +140,5 @@ def test_dimethylphenol8550_force_matching_gradients(dmp, precision):
     assert abs(L - float(d["loss"])) <= (1e-6 if precision == PKG.FP64 else 1e-5) * float(d["loss"])
     for name in NAMES:
         ty = S.cov_types if name == "cov_strength" else S.types
-        check(per_type(g[name], ty, len(d["dL_" + name])), d["dL_" + name], name, elem=FM_ELEM[precision])
+        check(per_type(g[name], ty, len(d["dL_" + name])), d["dL_" + name], name, lim=FM_NORM[precision],
+              elem=FM_ELEM[precision])
