@@ -112,6 +112,7 @@ struct Dev {
     // dipoles
     void* dS;                 // slot-order R4 (dipole xyz, charge w) for the pair passes
     void* dS2;                // the second source set of a dual pair pass (the predicted guess's dipoles)
+    long long* gridFix;       // mixed precision: the spread's 64-bit fixed-point grid (null: float atomics on grid)
     double* perm;             // 3n
     double* mu;               // 3n
     double* dtot;             // 3n

@@ -206,7 +206,7 @@ struct Engine::Impl {
     // device
     Buf dSys, dAtomSys, dQ, dR, dAlpha, dPosIn, dWrap, dCellOf, dCellRank, dBase, dFr, dCellCount, dCellStart,
         dSlotAtom, dSlotTmp, dPosS, dOrigS, dWrapS, dSpl, dBaseS, dRadS, dList, dListCount, dPairA, dPairB, dPairC, dFlags, dDS, dPerm, dMu, dDtot, dB, dX, dRv, dZ, dP, dAp,
-        dDS2, dEpair2, dErec2, dGrid2,
+        dDS2, dEpair2, dErec2, dGrid2, dGridFix, dGridFix2,
         dScal, dPartial, dGPartial, dHrec, dFm, dPmeRec, dPmeBins, dSrcW, dGPart, dPcgPartial, dBinCount, dActive, dActSys, dSysCounter, dEpair, dErec, dFpair, dSpair, dFrec, dEtot, dFin, dPot, dForces, dResults,
         dConvPartial, dConvOff, dGrid, dSpec, dInfl, dTwiddle, dModuli, dCovAtom, dCovPartner, dCovStrength, dCovByAtomOff,
         dCovByAtom, dCovByPartnerOff, dCovByPartner, dChunkSys, dChunkBegin, dChunkEnd, dHist, dGlobal, dCtl,
@@ -285,7 +285,7 @@ struct Engine::Impl {
         plans64.clear();
         Buf* all[] = {&dSys, &dAtomSys, &dQ, &dR, &dAlpha, &dPosIn, &dWrap, &dCellOf, &dCellRank, &dBase, &dFr,
                       &dCellCount, &dCellStart, &dSlotAtom, &dSlotTmp, &dPosS, &dOrigS, &dWrapS, &dSpl, &dBaseS, &dRadS, &dList, &dListCount, &dPairA, &dPairB, &dPairC, &dFlags, &dDS,
-                      &dDS2, &dEpair2, &dErec2, &dGrid2,
+                      &dDS2, &dEpair2, &dErec2, &dGrid2, &dGridFix, &dGridFix2,
                       &dPerm, &dMu, &dDtot, &dB, &dX, &dRv, &dZ, &dP, &dAp, &dScal, &dPartial, &dGPartial, &dHrec, &dFm, &dPmeRec, &dPmeBins, &dSrcW, &dGPart,
                       &dPcgPartial, &dBinCount, &dActive, &dActSys, &dSysCounter, &dEpair,
                       &dErec, &dFpair, &dSpair, &dFrec, &dEtot, &dFin, &dPot, &dForces, &dResults, &dConvPartial,
@@ -776,6 +776,12 @@ struct Engine::Impl {
         upload(dConvOff, convOff, st);
         dGrid.ensure(gridTotal * R);
         dGrid2.ensure(gridTotal * R);
+        if (mixed()) {   // (the fixed-point spread grids start cleared; each conversion clears them again)
+            dGridFix.ensure(gridTotal * 8);
+            dGridFix2.ensure(gridTotal * 8);
+            CU(cudaMemset(dGridFix.p, 0, gridTotal * 8));
+            CU(cudaMemset(dGridFix2.p, 0, gridTotal * 8));
+        }
         dSpec.ensure(specTotal * 2 * R);
         dInfl.ensure(specTotal * R);
         if (refining()) {
@@ -954,7 +960,10 @@ struct Engine::Impl {
         d.order = s.order;
         d.totalCells = totalCells;
         d.gridTotal = gridTotal;
-        d.gridWords = gridTotal * (long long) (realSize() / 4);
+        // (with the fixed-point spread the conversion rewrites the float grid and clears the fixed-point one: the
+        // CG update clears nothing)
+        d.gridFix = spreadFix() ? dGridFix.as<long long>() : nullptr;
+        d.gridWords = spreadFix() ? 0 : gridTotal * (long long) (realSize() / 4);
         d.ctl = dCtl.as<Ctl>();
         d.ke = s.ke;
         d.tol = s.tol;
@@ -1080,10 +1089,13 @@ struct Engine::Impl {
     }
 
     // ------------------------------------------------------------------------------------------ launches
-    template <typename R> void fftChain(cudaStream_t sm, const Dev& d, bool energy, bool gate) {
+    // fix: the spread before went to the fixed-point grid (converted first)
+    template <typename R> void fftChain(cudaStream_t sm, const Dev& d, bool energy, bool gate, bool fix = false) {
         typedef typename CplxT<R>::T C;
         constexpr bool dbl = std::is_same<R, double>::value;
         const bool shadow = dbl && mixed();   // the FP64 refinement's transforms of a mixed engine
+        if (fix && !dbl)
+            gridFromFix(sm, d);
         for (size_t k = 0; k < groups.size(); k++) {
             auto& g = groups[k];
             const cufftHandle plan = shadow ? plans64[k].first : g.r2c;
@@ -1229,6 +1241,20 @@ struct Engine::Impl {
     }
 
     bool planesMode() const { return planesOk && pmeWant == 1; }
+    // The mixed spread into the 64-bit fixed-point grid (the warp-per-atom kernels; PGM_B200_FLOAT_GRID=1 keeps
+    // float atomics on the float grid, for comparison).
+    bool fixMode() const {
+        const char* e = std::getenv("PGM_B200_FLOAT_GRID");
+        return mixed() && !(e && e[0] == '1');
+    }
+    // whether the field passes' spread (launchSpread) writes the fixed-point grid: the warp-per-atom kernel only
+    bool spreadFix() const { return fixMode() && !planesMode() && !linesMode() && !tilesMode(); }
+    void gridFromFix(cudaStream_t sm, const Dev& d) {
+        const int blocks = (int) std::min<long long>((gridTotal + 255) / 256, 4 * 148);
+        k_grid_from_fix<<<blocks, 256, 0, sm>>>(d);
+        CU(cudaGetLastError());
+    }
+
     // the float4 line spread and gather: mixed precision, orders 4, 5, 6 and 8, any number of systems
     bool linesMode() const {
         return pmeWant == 2 && mixed() && (s.order == 4 || s.order == 5 || s.order == 6 || s.order == 8);
@@ -1414,12 +1440,17 @@ struct Engine::Impl {
         }
     }
 
-    template <typename R> void transformPair(cudaStream_t sm, const Dev& d, bool gate) {
+    // fix: the spread before went to the fixed-point grid (the grid kernel converts on its load, the others after a
+    // conversion kernel)
+    template <typename R> void transformPair(cudaStream_t sm, const Dev& d, bool gate, bool fix = false) {
         constexpr bool dbl = std::is_same<R, double>::value;
+        fix = fix && !dbl && d.gridFix;
         if (dbl == mixed() || tfMode == TF_CUFFT) {   // (the FP64 shadow of a mixed engine: cuFFT)
-            fftChain<R>(sm, d, false, gate);
+            fftChain<R>(sm, d, false, gate, fix);
             return;
         }
+        if (fix && tfMode != TF_GRID && tfMode != TF_PCG)
+            gridFromFix(sm, d);
         if (tfMode == TF_SPLIT) {
             splitChain<R>(sm, d, gate);
             return;
@@ -1435,7 +1466,7 @@ struct Engine::Impl {
             cfg.stream = sm;
             cfg.attrs = at;
             cfg.numAttrs = 1;
-            CU(cudaLaunchKernelEx(&cfg, fftgKernel<R>(fftgKc), d, gate ? 1 : 0));
+            CU(cudaLaunchKernelEx(&cfg, fftgKernel<R>(fftgKc), d, (gate ? 1 : 0) | (fix ? 2 : 0)));
             return;
         }
         cudaLaunchConfig_t cfg = {};
@@ -1550,7 +1581,7 @@ struct Engine::Impl {
         launchSpread<R>(sm, d, spreadMode, vec);
         CU(cudaEventRecord(evFork, sm));
         CU(cudaStreamWaitEvent(sd, evFork, 0));
-        transformPair<R>(sd, d, gate);
+        transformPair<R>(sd, d, gate, spreadFix());
         pairField<R, WITHQ>(sm, d, gate ? 1 : 0);
         CU(cudaEventRecord(evJoin, sd));
         CU(cudaStreamWaitEvent(sm, evJoin, 0));
@@ -1671,8 +1702,9 @@ struct Engine::Impl {
             if (dualFirstPass()) {
                 // x0 first; (q, perm) into the grid and dS, x0 into the second grid and dS2; one pair sweep for
                 // both direct fields
-                Dev d2 = d;   // the second source set: its grid, its float copy, its reciprocal field
+                Dev d2 = d;   // the second source set: its grids, its float copy, its reciprocal field
                 d2.grid = dGrid2.p;
+                d2.gridFix = d.gridFix ? dGridFix2.as<long long>() : nullptr;
                 d2.dS = dDS2.p;
                 d2.Erec = dErec2.as<double>();
                 k_cg_guess<<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
@@ -1687,9 +1719,9 @@ struct Engine::Impl {
                 CU(cudaStreamWaitEvent(sd, evFork, 0));
                 pairField<R, true, true>(sd, d, 0);
                 CU(cudaEventRecord(evJoin, sd));
-                transformPair<R>(sm, d, false);
+                transformPair<R>(sm, d, false, spreadFix());
                 launchGather<R, false>(sm, d, 0);
-                transformPair<R>(sm, d2, false);
+                transformPair<R>(sm, d2, false, spreadFix());
                 launchGather<R, false>(sm, d2, 0);
                 CU(cudaStreamWaitEvent(sm, evJoin, 0));
                 k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
@@ -1703,7 +1735,7 @@ struct Engine::Impl {
             }
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
             launchSpread<R>(sm, d, 0, d.perm);
-            transformPair<R>(sm, d, false);
+            transformPair<R>(sm, d, false, spreadFix());
             CU(cudaStreamWaitEvent(sm, evJoin, 0));
             pairField<R, true>(sm, d, 0);
             launchGather<R, false>(sm, d, 0);
@@ -1744,7 +1776,7 @@ struct Engine::Impl {
         launchSpread<R>(sm, d, 0, d.dtot);
         CU(cudaEventRecord(evFork, sm));
         CU(cudaStreamWaitEvent(sd, evFork, 0));
-        fftChain<R>(sd, d, true, false);
+        fftChain<R>(sd, d, true, false, spreadFix());
         {
             const long long threads = (long long) n * pairGS;
             const int blocks = (int) ((threads + 255) / 256);
@@ -2971,6 +3003,8 @@ void Engine::kernelTimes(int reps, double* ms, void* flush, size_t flushBytes) {
         run(float());
     else
         run(double());
+    if (d.gridFix)   // (the timed spreads added to the fixed-point grid with no conversion after them)
+        CU(cudaMemsetAsync(d.gridFix, 0, I.gridTotal * 8, I.st));
     CU(cudaGetLastError());
     cudaEventDestroy(a);
     cudaEventDestroy(b);

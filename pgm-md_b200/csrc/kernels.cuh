@@ -8,6 +8,7 @@
 #include "common.cuh"
 
 #include <cooperative_groups.h>
+#include <type_traits>
 
 namespace pgmb200 {
 
@@ -15,6 +16,26 @@ __device__ __forceinline__ int wrapIndex(int g, int K) {
     g += (g < 0) ? K : 0;
     g -= (g >= K) ? K : 0;
     return g;
+}
+
+// The mixed spread's 64-bit fixed point: contributions rounded to multiples of 2^-32 and added as integers, so
+// the grid's sums do not depend on the order of the atomics (the evaluation repeats bit for bit); the grid is
+// converted to float once before the transforms.
+constexpr float GRID_FIX_SCALE = 4294967296.0f;   // 2^32
+__device__ __forceinline__ void gridFixAdd(long long* g, float v) {
+    atomicAdd((unsigned long long*) g, (unsigned long long) __float2ll_rn(v * GRID_FIX_SCALE));
+}
+__device__ __forceinline__ float gridFixTake(long long* g) {   // the value, and the word cleared for the next spread
+    const long long v = *g;
+    *g = 0;
+    return (float) ((double) v * (1.0 / 4294967296.0));
+}
+
+// The fixed-point grid to the float grid (every point), clearing the fixed-point grid.
+__global__ void k_grid_from_fix(Dev dv) {
+    const size_t n = (size_t) dv.gridTotal, stride = (size_t) gridDim.x * blockDim.x;
+    for (size_t k = (size_t) blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
+        ((float*) dv.grid)[k] = gridFixTake(dv.gridFix + k);
 }
 
 // Block-wide compaction of the systems still iterating (scal[DONE] == 0) into actSys / actOff / actCount, in
@@ -881,6 +902,7 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
     const R e2 = (R) (S.K[2] * (d0 * S.recip[2] + d1 * S.recip[5] + d2 * S.recip[8]));
     const R qr = (R) qv;
     R* grid = (R*) dv.grid + S.gridOff;
+    long long* gfix = std::is_same<R, float>::value && dv.gridFix ? dv.gridFix + S.gridOff : nullptr;
     const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
     if (P > 0) {
         // lane -> (j2, j3), loop over j1: consecutive lanes hit consecutive grid points of one row, and
@@ -900,10 +922,18 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
             const R c23 = t2 * t3;
             const R a = qr * c23 + e1 * u2 * t3 + e2 * t2 * u3;
             const R b = e0 * c23;
-            R* col = grid + (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2);
+            const size_t col = (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2);
+            if (gfix) {
 #pragma unroll
-            for (int j1 = 0; j1 < PP; j1++)
-                atomicAdd(col + (size_t) wrapIndex(b0 - j1, K0) * plane, a * sth[wib][0][j1] + b * sdth[wib][0][j1]);
+                for (int j1 = 0; j1 < PP; j1++)
+                    gridFixAdd(gfix + col + (size_t) wrapIndex(b0 - j1, K0) * plane,
+                               (float) (a * sth[wib][0][j1] + b * sdth[wib][0][j1]));
+            } else {
+#pragma unroll
+                for (int j1 = 0; j1 < PP; j1++)
+                    atomicAdd(grid + col + (size_t) wrapIndex(b0 - j1, K0) * plane,
+                              a * sth[wib][0][j1] + b * sdth[wib][0][j1]);
+            }
         }
 #pragma unroll
         for (int lr = 0; lr < LROUNDS; lr++) {
@@ -915,8 +945,12 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
                 const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
                 const R c23 = t2 * t3;
                 const R w = (qr * c23 + e1 * u2 * t3 + e2 * t2 * u3) * sth[wib][0][j1] + e0 * c23 * sdth[wib][0][j1];
-                atomicAdd(grid + (size_t) wrapIndex(b0 - j1, K0) * plane + (size_t) wrapIndex(b1 - j2, K1) * K2 +
-                              wrapIndex(b2 - j3, K2), w);
+                const size_t at = (size_t) wrapIndex(b0 - j1, K0) * plane + (size_t) wrapIndex(b1 - j2, K1) * K2 +
+                                  wrapIndex(b2 - j3, K2);
+                if (gfix)
+                    gridFixAdd(gfix + at, (float) w);
+                else
+                    atomicAdd(grid + at, w);
             }
         }
     } else {
@@ -928,7 +962,11 @@ __global__ void __launch_bounds__(256) k_spread(Dev dv, int mode, double* vec) {
             const R t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
             const R w = t3 * (t2 * (qr * t1 + e0 * u1) + e1 * t1 * u2) + e2 * t1 * t2 * u3;
             const int g1 = wrapIndex(b0 - j1, K0), g2 = wrapIndex(b1 - j2, K1), g3 = wrapIndex(b2 - j3, K2);
-            atomicAdd(&grid[((size_t) g1 * K1 + g2) * K2 + g3], w);
+            const size_t at = ((size_t) g1 * K1 + g2) * K2 + g3;
+            if (gfix)
+                gridFixAdd(gfix + at, (float) w);
+            else
+                atomicAdd(&grid[at], w);
         }
     }
 }
@@ -1457,8 +1495,10 @@ template <typename R, int KC>
 __global__ void __launch_bounds__(FftgThreads<R>::n) k_fft_grid(Dev dv, int gateDone) {
     typedef typename CplxT<R>::T C;
     const int s = blockIdx.y;
-    if (gateDone && dv.scal[s * NSCAL + SC_DONE] != 0.0)
+    if ((gateDone & 1) && dv.scal[s * NSCAL + SC_DONE] != 0.0)
         return;   // every block of the system
+    // gateDone & 2: the spread went to the fixed-point grid; its plane is converted (and cleared) on the load
+    long long* const fx = (gateDone & 2) ? dv.gridFix : nullptr;
     const SysDev& S = dv.sys[s];
     const int K0 = KC > 0 ? KC : S.K[0], K1 = KC > 0 ? KC : S.K[1], K2 = KC > 0 ? KC : S.K[2];
     const int K2h = K2 / 2 + 1, P = (K1 + 1) / 2, ly = K1 + 1, lx = K0 + 1;
@@ -1489,11 +1529,17 @@ __global__ void __launch_bounds__(FftgThreads<R>::n) k_fft_grid(Dev dv, int gate
     C* const plane = spec + (size_t) x * nline;
     unsigned* const bar = dv.fftgBar + 2 * s;
     // 1. plane x: rows 2p, 2p + 1 as one complex row [pair][z]; z; separation into y-lines [kz][y]; y
+    long long* const fxx = fx ? fx + S.gridOff + (size_t) x * K1 * K2 : nullptr;
     for (int e = tid; e < P * K2; e += nT) {
         const int pr = qd(e, K2, iK2), z = e - pr * K2;
         C v;
-        v.x = gx[2 * pr * K2 + z];
-        v.y = (2 * pr + 1 < K1) ? gx[(2 * pr + 1) * K2 + z] : (R) 0;
+        if (fxx) {
+            v.x = (R) gridFixTake(fxx + 2 * pr * K2 + z);
+            v.y = (2 * pr + 1 < K1) ? (R) gridFixTake(fxx + (2 * pr + 1) * K2 + z) : (R) 0;
+        } else {
+            v.x = gx[2 * pr * K2 + z];
+            v.y = (2 * pr + 1 < K1) ? gx[(2 * pr + 1) * K2 + z] : (R) 0;
+        }
         b0[e] = v;
     }
     __syncthreads();

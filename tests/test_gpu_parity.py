@@ -203,6 +203,29 @@ def test_repeatable_bits():
     assert np.array_equal(a.forces, b.forces) or rel_rms(a.forces, b.forces) < 1e-14
 
 
+@pytest.mark.parametrize("mode", [0, 3])
+def test_mixed_repeatable_bits(mode):
+    """Mixed precision repeats bit for bit: the spread adds 64-bit fixed-point contributions (integer sums do not
+    depend on the atomics' order) and every other sum has a fixed order.  The real 8550-atom liquid, cuFFT
+    (transforms 0, a conversion kernel before the transforms) and the grid kernel (3, the conversion on its load),
+    three evaluations each, and a new engine on the same input."""
+    S, _ = load_dmp_real()
+    runs = []
+    for _ in range(2):
+        eng = make_engine(S, PKG.MIXED, tol=1e-5, peek=0.65)
+        eng.set_transforms(mode)
+        assert eng.transforms() == mode
+        for _ in range(3):
+            r = eng.compute(S.pos, S.box)
+            runs.append((r.energy, r.forces.copy(), eng.induced_dipoles().copy(), r.iterations))
+        eng.close()
+    e0, f0, mu0, it0 = runs[0]
+    for e, f, mu, it in runs[1:]:
+        assert e == e0 and it == it0
+        assert np.array_equal(f, f0)
+        assert np.array_equal(mu, mu0)
+
+
 def test_errors_are_status_codes():
     S = PKG.systems.tiny_triclinic(nmol=4, seed=1)
     eng = make_engine(S, PKG.FP64)
