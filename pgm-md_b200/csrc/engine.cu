@@ -1600,12 +1600,18 @@ struct Engine::Impl {
 
     // The Verlet list's build: cells, slots, the list at cutoff + skin (positions already in posIn).
     void enqueueBuild(cudaStream_t sm, const Dev& d) {
+        enqueueCells(sm, d);
+        listKernel(sm, d);
+        CU(cudaGetLastError());
+    }
+
+    // The first half of a build: wraps, cells and the slot order with its slot-order copies.
+    void enqueueCells(cudaStream_t sm, const Dev& d) {
         const int tb = (n + 255) / 256;
         k_prep<<<tb, 256, 0, sm>>>(d, nullptr, 2);
         k_cell_scan<<<1, 1024, 0, sm>>>(d);
         k_cell_scatter<<<tb, 256, 0, sm>>>(d);
         k_cell_sort<<<(totalCells + 7) / 8, 256, 0, sm>>>(d);
-        listKernel(sm, d);
         CU(cudaGetLastError());
     }
 
@@ -1619,18 +1625,22 @@ struct Engine::Impl {
 
     // The pair-list step of an evaluation: positions in (PME base and fraction), the stale test, the build when
     // stale (a conditional node of the graph, its body captured after the main capture; without graphs a host
-    // decision), the slot-order positions with the build's wraps.
-    void enqueueListStep(cudaStream_t sm, const Dev& d) {
+    // decision), the slot-order positions with the build's wraps.  Without a skin the list's rows are left to the
+    // caller (listKernel after this step, on a stream of its choice: nothing before it reads the list; the
+    // refreshed slot copies equal the cell sort's bit for bit), and the call returns true.
+    bool enqueueListStep(cudaStream_t sm, const Dev& d) {
         const int tb = (n + 255) / 256;
         k_prep<<<tb, 256, 0, sm>>>(d, dPosIn.as<double>(), 1);
-        if (!verletList()) {   // no skin: a build at every evaluation, without the stale test or a conditional node
+        const bool rowsLeft = !verletList();
+        if (rowsLeft) {   // no skin: a build at every evaluation, without the stale test or a conditional node
             CU(cudaMemsetAsync(d.cellCount, 0, (size_t) totalCells * sizeof(int), sm));
-            enqueueBuild(sm, d);
+            enqueueCells(sm, d);
         } else {
             enqueueStaleBuild(sm, d);
         }
         k_refresh_positions<<<tb, 256, 0, sm>>>(d);
         CU(cudaGetLastError());
+        return rowsLeft;
     }
 
     // Ends the work captured so far on st with a conditional node (IF or WHILE on `cond`): the node follows
@@ -1675,12 +1685,14 @@ struct Engine::Impl {
     template <typename R> void enqueuePre(cudaStream_t sm, cudaStream_t sd, const Dev& d) {
         const int tb = (n + 255) / 256;
         CU(cudaMemsetAsync(d.flags, 0, flagBytes(), sm));
-        enqueueListStep(sm, d);
+        const bool rowsLeft = enqueueListStep(sm, d);
         if (s.polarizable) {
-            // the pairs within the cutoff and their G1, G2 (side stream) beside the permanent field's PME half
-            // (main stream)
+            // the list's rows when built here, the pairs within the cutoff and their G1, G2 (side stream) beside
+            // the permanent field's PME half (main stream)
             CU(cudaEventRecord(evFork, sm));
             CU(cudaStreamWaitEvent(sd, evFork, 0));
+            if (rowsLeft)
+                listKernel(sd, d);
             pairRecords<R>(sd, d);
             CU(cudaEventRecord(evJoin, sd));
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
@@ -1736,9 +1748,9 @@ struct Engine::Impl {
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
             launchSpread<R>(sm, d, 0, d.perm);
             transformPair<R>(sm, d, false, spreadFix());
+            launchGather<R, false>(sm, d, 0);   // (the reciprocal half needs no pair list)
             CU(cudaStreamWaitEvent(sm, evJoin, 0));
             pairField<R, true>(sm, d, 0);
-            launchGather<R, false>(sm, d, 0);
             k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
             CU(cudaGetLastError());
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
@@ -1748,6 +1760,8 @@ struct Engine::Impl {
             // the loop's first spread needs a clear grid (each iteration clears it for the next one)
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
         } else {
+            if (rowsLeft)
+                listKernel(sm, d);
             pairRecords<R>(sm, d);
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
             if (std::is_same<R, float>::value && planesMode())
