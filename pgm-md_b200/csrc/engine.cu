@@ -249,6 +249,20 @@ struct Engine::Impl {
     int graphCells = -1;               // cell count the graph was captured with
     int graphTiles[2] = {-1, -1};      // tile groups and capacity the graph was captured with
     bool graphDual = false;            // the graph's first pass is the dual one (a predicted guess)
+    // CG iterations captured ahead of the while node (one system): the fewest iterations of the last 4
+    // evaluations, so that an evaluation like those runs its loop without the while node's per-iteration cost
+    // and the node only takes what is left (an evaluation that converges earlier gates the rest off).  The graph
+    // is captured again after 3 evaluations when fewer iterations would do, or at least two more; one more only
+    // after 16 (so that counts that alternate do not recapture every few evaluations).
+    int graphUnroll = 0;               // iterations unrolled in the captured graph
+    int unrollWant = 0;                // what the next capture unrolls
+    int recentIt[4] = {0};             // iteration counts of the last evaluations (ring)
+    int recentCount = 0, evalsSinceCapture = 0;
+    bool unrollStale() const {
+        if (nsys != 1 || evalsSinceCapture < 3 || unrollWant == graphUnroll)
+            return false;
+        return unrollWant < graphUnroll || unrollWant >= graphUnroll + 2 || evalsSinceCapture >= 16;
+    }
     bool capturing = false;
 
     // last evaluation
@@ -1829,10 +1843,14 @@ struct Engine::Impl {
         cudaGraph_t body = nullptr;
         capturing = true;
         listBody = nullptr;
+        const int unroll = (loopNode && nsys == 1) ? unrollWant : 0;
         try {
             enqueuePre<R>(st, side, d);
-            if (loopNode)   // the CG loop
+            if (loopNode) {   // the CG loop: unrolled iterations (gated by the system's convergence), then the node
+                for (int u = 0; u < unroll; u++)
+                    enqueueIteration<R>(st, side, d);
                 body = appendConditional(st, handle, cudaGraphCondTypeWhile);
+            }
             else if (s.polarizable)
                 launchPersistent(st, d);
             enqueuePost<R>(st, side, d);
@@ -1874,6 +1892,8 @@ struct Engine::Impl {
         CU(cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority));
         graphCells = totalCells;
         graphDual = dualFirstPass();
+        graphUnroll = unroll;
+        evalsSinceCapture = 0;
         {
             int G, cap, groups;
             tileGeometry(G, cap, groups);
@@ -2014,7 +2034,7 @@ struct Engine::Impl {
         int tG, tCap, tGroups;
         tileGeometry(tG, tCap, tGroups);
         if ((grew || totalCells != graphCells || tGroups != graphTiles[0] || tCap != graphTiles[1] ||
-             dualFirstPass() != graphDual) && exec) {
+             dualFirstPass() != graphDual || unrollStale()) && exec) {
             cudaGraphExecDestroy(exec);
             exec = nullptr;
         }
@@ -2096,6 +2116,16 @@ struct Engine::Impl {
         }
         lastResults.assign(hResults, hResults + nsys * NRES);
         haveResult = true;
+        if (nsys == 1 && s.polarizable) {   // the unroll of the next capture
+            recentIt[recentCount++ % 4] = (int) hResults[14];
+            evalsSinceCapture++;
+            static const char* env = std::getenv("PGM_B200_UNROLL");   // (a cap; 0 keeps the plain while node)
+            const int cap = env ? std::atoi(env) : 16;
+            int m = recentIt[0];
+            for (int k = 1; k < std::min(recentCount, 4); k++)
+                m = std::min(m, recentIt[k]);
+            unrollWant = std::max(0, std::min(m, cap));
+        }
         if (pendingSlot >= 0) {
             histHead = pendingSlot;
             histCount = std::min(histCount + 1, 4);
