@@ -258,8 +258,9 @@ struct Engine::Impl {
     int unrollWant = 0;                // what the next capture unrolls
     int recentIt[4] = {0};             // iteration counts of the last evaluations (ring)
     int recentCount = 0, evalsSinceCapture = 0;
+    bool graphLoop = false;            // the captured graph holds the CG loop's while node
     bool unrollStale() const {
-        if (nsys != 1 || evalsSinceCapture < 3 || unrollWant == graphUnroll)
+        if (!graphLoop || nsys != 1 || evalsSinceCapture < 3 || unrollWant == graphUnroll)
             return false;
         return unrollWant < graphUnroll || unrollWant >= graphUnroll + 2 || evalsSinceCapture >= 16;
     }
@@ -1206,7 +1207,7 @@ struct Engine::Impl {
         CU(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, devId));
         CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, devId));
         const int* K = sysK[0].data();
-        pcgSmem = (3 * (size_t) FFT_MAXK + 2 * (size_t) fftgBuf) * 8 + (size_t) K[1] * K[2] * 8;
+        pcgSmem = (3 * (size_t) FFT_MAXK + 2 * (size_t) fftgBuf) * 8;
         if (!coop || pcgSmem > (size_t) optin || K[0] + PCG_MIN_PAIR_BLOCKS > sms)
             return;
         PcgKernel kfn = persistentKernel(pairGS);
@@ -1399,7 +1400,9 @@ struct Engine::Impl {
         cfg.stream = sm;
         cfg.attrs = at;
         cfg.numAttrs = 1;
-        CU(cudaLaunchKernelEx(&cfg, kfn, d, planeNyc, vec));
+        Dev dp = d;   // (its spread always goes to the fixed-point grid)
+        dp.gridFix = dGridFix.as<long long>();
+        CU(cudaLaunchKernelEx(&cfg, kfn, dp, planeNyc, vec));
     }
 
     bool persistentMode() const { return tfMode == TF_PCG; }
@@ -1710,7 +1713,7 @@ struct Engine::Impl {
             pairRecords<R>(sd, d);
             CU(cudaEventRecord(evJoin, sd));
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
-            if (std::is_same<R, float>::value && (planesMode() || persistentMode()))
+            if (std::is_same<R, float>::value && planesMode())
                 enqueuePlaneBins(sm, d);
             k_perm<<<tb, 256, 0, sm>>>(d);
             k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
@@ -1893,6 +1896,7 @@ struct Engine::Impl {
         graphCells = totalCells;
         graphDual = dualFirstPass();
         graphUnroll = unroll;
+        graphLoop = loopNode;
         evalsSinceCapture = 0;
         {
             int G, cap, groups;

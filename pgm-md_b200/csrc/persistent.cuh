@@ -4,22 +4,24 @@
 // Every CG iteration of core/pgm_core.cpp:351-385 (A v = v/alpha - T v; T v = pair + reciprocal + self field)
 // runs inside the kernel, with grid barriers between its phases instead of kernel boundaries and graph nodes:
 //
-//   S  (every block, a chunk of slots)  p = z + beta p; the pair pass's float copy of p and the PME weights
-//      (q, e_a = K_a p . recip[:, a]) of each slot;                                               grid barrier
-//   F  blocks 0 .. K0-1 own the x-planes of the PME grid: the plane is spread in shared memory from the atoms
-//      whose stencil reaches it (64-bit fixed-point shared atomics, so the sums do not depend on their order),
-//      transformed along z and y, the x-lines exchanged through L2 (two barriers of the plane blocks), the
-//      influence product, transformed back, and the potential gathered at the same atoms: each atom's field
-//      sums of this plane go to a slot of their own (one of p per atom), summed later in a fixed order.
+//   S  (every block, a warp per slot of its chunk)  p = z + beta p; the pair pass's float copy of p; the PME
+//      weights (q, e_a = K_a p . recip[:, a]) and the spread of the atom into the 64-bit fixed-point grid
+//      (global atomics, the same points and arithmetic as k_spread; integer sums do not depend on their order,
+//      so the solve repeats bit for bit);                                                         grid barrier
+//   F  blocks 0 .. K0-1 own the x-planes of the PME grid: the plane is read from the fixed-point grid (and
+//      cleared for the next spread), transformed along z and y, the x-lines exchanged through L2 (two barriers
+//      of the plane blocks), the influence product, transformed back and stored to the potential grid.
 //      Blocks K0 .. end run the direct-space field pass of the iteration's direction over the pair records.
 //                                                                                                  grid barrier
-//   A  (every block) A p rows, the block's share of p . A p;                                        grid barrier
+//   G  (every block, a warp per slot of its chunk) E_rec at the atom from the potential grid, the atom's row of
+//      A p and the block's share of p . A p;                                                        grid barrier
 //   U  (every block) alph from the shares (fixed order), x, r, z of its slots, shares of z'.(r' - r), r'.z',
 //      max |z'|;                                                                                    grid barrier
 //   C  (every block, identically) beta, rz, err, the iteration count and the convergence test.
 //
-// Every reduction sums in a fixed order, so the solve repeats bit for bit.  Barrier waits are bounded (about
-// a second); a block that gives up sets flags[11] and returns, and the host reports the evaluation as failed.
+// Every reduction sums in a fixed order.  Data other blocks wrote in this launch is read past L1 (__ldcg).
+// Barrier waits are bounded (about a second); a block that gives up sets flags[11] and returns, and the host
+// reports the evaluation as failed.
 #pragma once
 
 #include "kernels.cuh"
@@ -29,8 +31,6 @@ namespace pgmb200 {
 constexpr int PCG_THREADS = 512;
 constexpr int PCG_MIN_PAIR_BLOCKS = 16;      // blocks left for the pair pass beside the plane blocks
 constexpr int PCG_BLOCKS_PER_SM = 1;         // resident blocks per SM (two, at 64 registers, measured slower)
-constexpr float PCG_FIX = 4294967296.0f;     // 2^32: the fixed-point scale of the shared-memory spread
-constexpr float PCG_UNFIX = 2.3283064365386963e-10f;   // 2^-32
 
 // The spline record of one atom of the plane bins (order P): its slot, b1, b2 and b0 mod K0, and theta and
 // dtheta of the three dimensions, c[dim 2P + kind P + j].
@@ -63,6 +63,153 @@ struct PlaneAtoms {
         return start[j1] + t - cum[j1];
     }
 };
+
+// The spread of slot s (its atom's weights w = (q, e0, e1, e2)) into the 64-bit fixed-point grid by the calling
+// warp: the evaluation's spline coefficients staged in the warp's shared rows, lane -> stencil column (j2, j3),
+// loop over j1, the leftover columns' points over the lanes: the points and the per-point arithmetic of k_spread,
+// so both add the same integers.
+template <int P>
+__device__ __forceinline__ void pcgSpreadSlot(const Dev& dv, const SysDev& S, long long* gfix, int s, float4 w,
+                                             float (*sth)[3][P], float (*sdth)[3][P], int wib, int lane) {
+    const int i = dv.slotAtom[s];
+    const float* sp = (const float*) dv.spl + (size_t) s * 9 * MAXP;
+    for (int k = lane; k < 6 * P; k += 32) {
+        const int kind = k / (3 * P), dim = (k / P) % 3, j = k % P;
+        const float v = sp[(kind * 3 + dim) * MAXP + j];
+        if (kind == 0)
+            sth[wib][dim][j] = v;
+        else
+            sdth[wib][dim][j] = v;
+    }
+    const int bl = lane < 3 ? dv.pmeBase[3 * i + lane] : 0;
+    const int b0 = __shfl_sync(0xffffffffu, bl, 0), b1 = __shfl_sync(0xffffffffu, bl, 1),
+              b2 = __shfl_sync(0xffffffffu, bl, 2);
+    __syncwarp();
+    const float qr = w.x, e0 = w.y, e1 = w.z, e2 = w.w;
+    const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
+    const size_t plane = (size_t) K1 * K2;
+    constexpr int NPAIR = P * P, FULL = NPAIR / 32, LEFT = NPAIR % 32, LROUNDS = (LEFT * P + 31) / 32;
+    constexpr int LEFTD = LEFT > 0 ? LEFT : 1;
+#pragma unroll
+    for (int rd = 0; rd < FULL; rd++) {
+        const int pr = lane + 32 * rd;
+        const int j2 = pr / P, j3 = pr % P;
+        const float t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
+        const float t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+        const float c23 = t2 * t3;
+        const float a = qr * c23 + e1 * u2 * t3 + e2 * t2 * u3;
+        const float b = e0 * c23;
+        const size_t col = (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2);
+#pragma unroll
+        for (int j1 = 0; j1 < P; j1++)
+            gridFixAdd(gfix + col + (size_t) wrapIndex(b0 - j1, K0) * plane,
+                       (float) (a * sth[wib][0][j1] + b * sdth[wib][0][j1]));
+    }
+#pragma unroll
+    for (int lr = 0; lr < LROUNDS; lr++) {
+        const int k = lane + 32 * lr;
+        if (k < LEFT * P) {
+            const int pr = 32 * FULL + k % LEFTD, j1 = k / LEFTD;
+            const int j2 = pr / P, j3 = pr % P;
+            const float t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
+            const float t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+            const float c23 = t2 * t3;
+            const float v = (qr * c23 + e1 * u2 * t3 + e2 * t2 * u3) * sth[wib][0][j1] + e0 * c23 * sdth[wib][0][j1];
+            gridFixAdd(gfix + (size_t) wrapIndex(b0 - j1, K0) * plane + (size_t) wrapIndex(b1 - j2, K1) * K2 +
+                           wrapIndex(b2 - j3, K2),
+                       (float) v);
+        }
+    }
+    __syncwarp();   // (the next slot of this warp overwrites the shared rows)
+}
+
+// E_rec at the atom of slot s from the potential grid gpot (written by other blocks in this launch: read past
+// L1) by the calling warp: f_a = sum (d theta_a) theta theta phi over the stencil (lane -> column (j2, j3), loop
+// over j1, the leftover columns' points over the lanes), E_rec = -sum_a K_a recip[:, a] f_a
+// (core/pgm_core.cpp:241-264), the lanes' sums in double.
+// CGA (the CG iterations): instead of E_rec, the row of A p = p / alpha - (E_pair + E_rec + cs p)
+// (core/pgm_core.cpp:363) at the atom, and the returned share p_k (A p)_k of lanes k < 3 (0 elsewhere).
+template <int P, bool CGA>
+__device__ __forceinline__ double pcgGatherSlot(const Dev& dv, const SysDev& S, const float* gpot, int s,
+                                               float (*sth)[3][P], float (*sdth)[3][P], int wib, int lane,
+                                               double cs) {
+    const int i = dv.slotAtom[s];
+    const float* sp = (const float*) dv.spl + (size_t) s * 9 * MAXP;
+    for (int k = lane; k < 6 * P; k += 32) {
+        const int kind = k / (3 * P), dim = (k / P) % 3, j = k % P;
+        const float v = sp[(kind * 3 + dim) * MAXP + j];
+        if (kind == 0)
+            sth[wib][dim][j] = v;
+        else
+            sdth[wib][dim][j] = v;
+    }
+    const int bl = lane < 3 ? dv.pmeBase[3 * i + lane] : 0;
+    const int b0 = __shfl_sync(0xffffffffu, bl, 0), b1 = __shfl_sync(0xffffffffu, bl, 1),
+              b2 = __shfl_sync(0xffffffffu, bl, 2);
+    __syncwarp();
+    const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
+    const size_t plane = (size_t) K1 * K2;
+    constexpr int NPAIR = P * P, FULL = NPAIR / 32, LEFT = NPAIR % 32, LROUNDS = (LEFT * P + 31) / 32;
+    constexpr int LEFTD = LEFT > 0 ? LEFT : 1;
+    float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+#pragma unroll
+    for (int rd = 0; rd < FULL; rd++) {
+        const int pr = lane + 32 * rd;
+        const int j2 = pr / P, j3 = pr % P;
+        const float* col = gpot + (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2);
+        float St = 0.f, Su = 0.f;
+#pragma unroll
+        for (int j1 = 0; j1 < P; j1++) {
+            const float ph = __ldcg(col + (size_t) wrapIndex(b0 - j1, K0) * plane);
+            St += sth[wib][0][j1] * ph;
+            Su += sdth[wib][0][j1] * ph;
+        }
+        const float t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
+        const float t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+        f0 += Su * t2 * t3;
+        f1 += St * u2 * t3;
+        f2 += St * t2 * u3;
+    }
+#pragma unroll
+    for (int lr = 0; lr < LROUNDS; lr++) {
+        const int k = lane + 32 * lr;
+        if (k < LEFT * P) {
+            const int pr = 32 * FULL + k % LEFTD, j1 = k / LEFTD;
+            const int j2 = pr / P, j3 = pr % P;
+            const float ph = __ldcg(gpot + (size_t) wrapIndex(b0 - j1, K0) * plane +
+                                    (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2));
+            const float t1 = sth[wib][0][j1], u1 = sdth[wib][0][j1];
+            const float t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
+            const float t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+            f0 += u1 * t2 * t3 * ph;
+            f1 += t1 * u2 * t3 * ph;
+            f2 += t1 * t2 * u3 * ph;
+        }
+    }
+    double F[3] = {(double) f0, (double) f1, (double) f2};
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            F[k] += __shfl_xor_sync(0xffffffffu, F[k], o);
+    double share = 0.0;
+    if (lane < 3) {
+        const int k = lane;
+        const double E = -(S.K[0] * S.recip[3 * k] * F[0] + S.K[1] * S.recip[3 * k + 1] * F[1] +
+                           S.K[2] * S.recip[3 * k + 2] * F[2]);
+        if (CGA) {
+            const double al = dv.alpha[i], pk = dv.p[3 * i + k];
+            const double Tp = __ldcg(dv.Epair + 3 * i + k) + E + cs * pk;
+            const double apk = (al > 0) ? pk / al - Tp : 0.0;
+            dv.Ap[3 * i + k] = apk;
+            share = pk * apk;
+        } else {
+            dv.Erec[3 * i + k] = E;
+        }
+    }
+    __syncwarp();
+    return share;
+}
 
 // Direct-space field of the direction p (mixed pair records) at slots g0, g0 + gstride, ...: GS lanes per slot,
 // E_i = sum_j -p_j G1 + (p_j . x) x G2 (core/pgm_core.cpp:274-284), products in float, sums across lanes in
@@ -159,9 +306,7 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
     C* W2 = W1 + FFT_MAXK;
     C* const b0 = W2 + FFT_MAXK;
     C* const b1 = b0 + dv.fftgBuf;
-    unsigned long long* const plane = (unsigned long long*) (b1 + dv.fftgBuf);
     const C* tw = (const C*) dv.twiddle;
-    PlaneAtoms<P> pa;
     if (planeBlock) {
         for (int m = tid; m < K0; m += nT)
             W0[m] = tw[S.twOff[0] + m];
@@ -169,79 +314,63 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
             W1[m] = tw[S.twOff[1] + m];
         for (int m = tid; m < K2; m += nT)
             W2[m] = tw[S.twOff[2] + m];
-        pa.init(dv.pmeBinStart, x, K0, nyc);
     }
     C* const spec = (C*) dv.spec + S.specOff;
     C* const myPlane = spec + (size_t) x * nline;
-    const PmeRec<P>* rec = (const PmeRec<P>*) dv.pmeRec;
-    float4* const srcW = dv.srcW;
-    float4* const gpart = dv.gpart;
     double* const part = dv.pcgPartial;
+    // the warp-per-slot phases (spread, gather): the warps' shared spline rows, the fixed-point charge grid and
+    // the float potential grid
+    __shared__ float psth[PCG_THREADS / 32][3][P], psdth[PCG_THREADS / 32][3][P];
+    const int wib = tid >> 5, wl = tid & 31, nwarps = nT >> 5;
+    long long* const gfix = dv.gridFix + S.gridOff;
+    float* const gpot = (float*) dv.grid + S.gridOff;
+    (void) nyc;
     const double cs = 4.0 * S.beta * S.beta * S.beta / (3.0 * SQRT_PI);
     // the block's chunk of slots for the per-atom phases
     const int per = (n + nb - 1) / nb, s0 = x * per, s1 = min(n, s0 + per);
     double rz = sc[SC_RZ], beta = sc[SC_BETA], it = sc[SC_IT];
     const double norm = sc[SC_NORM];
     for (;;) {
-        // ---- S: direction p = z + beta p (or the pass's sources); float copy for the pair pass; PME weights
-        for (int s = s0 + tid; s < s1; s += nT) {
+        // ---- S: a warp per slot: direction p = z + beta p (or the pass's sources), the float copy for the pair
+        // pass, the PME weights (q, e_a = K_a p . recip[:, a]) and the spread
+        for (int s = s0 + wib; s < s1; s += nwarps) {
             const int i = dv.slotAtom[s];
-            double d[3];
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
+            double dl = 0.0;
+            if (wl < 3) {
                 if (PASS == 0) {
-                    d[k] = dv.z[3 * i + k] + beta * dv.p[3 * i + k];
-                    dv.p[3 * i + k] = d[k];
+                    dl = dv.z[3 * i + wl] + beta * dv.p[3 * i + wl];
+                    dv.p[3 * i + wl] = dl;
                 } else {
-                    d[k] = vec[3 * i + k];
+                    dl = vec[3 * i + wl];
                 }
             }
+            const double d0 = __shfl_sync(0xffffffffu, dl, 0), d1 = __shfl_sync(0xffffffffu, dl, 1),
+                         d2 = __shfl_sync(0xffffffffu, dl, 2);
             const float qf = PASS == 2 ? (float) dv.q[i] : 0.f;
-            ((float4*) dv.dS)[s] = make_float4((float) d[0], (float) d[1], (float) d[2], qf);
-            srcW[s] = make_float4(qf, (float) (S.K[0] * (d[0] * S.recip[0] + d[1] * S.recip[3] + d[2] * S.recip[6])),
-                                  (float) (S.K[1] * (d[0] * S.recip[1] + d[1] * S.recip[4] + d[2] * S.recip[7])),
-                                  (float) (S.K[2] * (d[0] * S.recip[2] + d[1] * S.recip[5] + d[2] * S.recip[8])));
+            if (wl == 0)
+                ((float4*) dv.dS)[s] = make_float4((float) d0, (float) d1, (float) d2, qf);
+            const float4 w = make_float4(qf, (float) (S.K[0] * (d0 * S.recip[0] + d1 * S.recip[3] + d2 * S.recip[6])),
+                                         (float) (S.K[1] * (d0 * S.recip[1] + d1 * S.recip[4] + d2 * S.recip[7])),
+                                         (float) (S.K[2] * (d0 * S.recip[2] + d1 * S.recip[5] + d2 * S.recip[8])));
+            pcgSpreadSlot<P>(dv, S, gfix, s, w, psth, psdth, wib, wl);
         }
         if (!fftgBarrier(gbar, (unsigned) nb, dv.flags))
             return;
         // ---- F: the plane blocks' reciprocal part, the other blocks' direct part
         if (planeBlock) {
-            for (int e = tid; e < K1 * K2; e += nT)
-                plane[e] = 0ull;
-            __syncthreads();
-            for (int t = tid; t < pa.total(); t += nT) {
-                int j1;
-                const PmeRec<P>& r = rec[pa.locate(t, j1)];
-                const int4 id = r.idx;
-                const float4 w = __ldcg(srcW + id.x);
-                float c[4 * P];   // (in registers before the atomics, which would otherwise force reloads)
-#pragma unroll
-                for (int k = 0; k < 4 * P; k++)
-                    c[k] = r.c[2 * P + k];
-                const float t1 = r.c[j1], u1 = r.c[P + j1];
-                const float qe = w.x * t1 + w.y * u1, e1t = w.z * t1, e2t = w.w * t1;
-                int col[P];
-#pragma unroll
-                for (int j3 = 0; j3 < P; j3++)
-                    col[j3] = wrapIndex(id.z - j3, K2);
-#pragma unroll
-                for (int j2 = 0; j2 < P; j2++) {
-                    const float A2 = c[j2] * qe + e1t * c[P + j2], B2 = e2t * c[j2];
-                    unsigned long long* row = plane + wrapIndex(id.y - j2, K1) * K2;
-#pragma unroll
-                    for (int j3 = 0; j3 < P; j3++) {
-                        const float v = A2 * c[2 * P + j3] + B2 * c[3 * P + j3];
-                        atomicAdd(row + col[j3], (unsigned long long) __float2ll_rn(v * PCG_FIX));
-                    }
-                }
-            }
-            __syncthreads();
-            // plane x: rows 2p, 2p + 1 as one complex row [pair][z]; z; separation into y-lines [kz][y]; y
+            // plane x from the fixed-point grid (cleared for the next spread): rows 2p, 2p + 1 as one complex row
+            // [pair][z]; z; separation into y-lines [kz][y]; y
+            long long* const fxx = gfix + (size_t) x * K1 * K2;
+            auto take = [](long long* g) {
+                const long long v = __ldcg(g);
+                __stcg(g, 0ll);
+                return (float) ((double) v * (1.0 / 4294967296.0));
+            };
             for (int e = tid; e < NP * K2; e += nT) {
                 const int pr = qd(e, K2, iK2), z = e - pr * K2;
                 C v;
-                v.x = __ll2float_rn((long long) plane[2 * pr * K2 + z]) * PCG_UNFIX;
-                v.y = (2 * pr + 1 < K1) ? __ll2float_rn((long long) plane[(2 * pr + 1) * K2 + z]) * PCG_UNFIX : 0.f;
+                v.x = take(fxx + 2 * pr * K2 + z);
+                v.y = (2 * pr + 1 < K1) ? take(fxx + (2 * pr + 1) * K2 + z) : 0.f;
                 b0[e] = v;
             }
             __syncthreads();
@@ -330,35 +459,12 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
             }
             __syncthreads();
             const C* Zt = fftLinesK<float, 1, KC>(O2, Gy, NP, K2, K2, W2);
-            // gather at the same atoms: this plane's part of f_a = sum (d theta_a) theta theta phi
-            const float* phi = (const float*) Zt;   // row y at [(y / 2) K2 + z] component y & 1
-            for (int t = tid; t < pa.total(); t += nT) {
-                int j1;
-                const PmeRec<P>& r = rec[pa.locate(t, j1)];
-                const int4 id = r.idx;
-                int col[P];
-#pragma unroll
-                for (int j3 = 0; j3 < P; j3++)
-                    col[j3] = wrapIndex(id.z - j3, K2);
-                float A = 0.f, B = 0.f, Cc = 0.f;
-#pragma unroll
-                for (int j2 = 0; j2 < P; j2++) {
-                    const int yy = wrapIndex(id.y - j2, K1);
-                    const float* row = phi + 2 * ((yy >> 1) * K2) + (yy & 1);
-                    float st = 0.f, su = 0.f;
-#pragma unroll
-                    for (int j3 = 0; j3 < P; j3++) {
-                        const float ph = row[2 * col[j3]];
-                        st += r.c[4 * P + j3] * ph;
-                        su += r.c[5 * P + j3] * ph;
-                    }
-                    const float t2 = r.c[2 * P + j2], u2 = r.c[3 * P + j2];
-                    A += t2 * st;
-                    B += u2 * st;
-                    Cc += t2 * su;
-                }
-                const float t1 = r.c[j1], u1 = r.c[P + j1];
-                gpart[(size_t) j1 * n + id.x] = make_float4(u1 * A, t1 * B, t1 * Cc, 0.f);
+            float* const gx = gpot + (size_t) x * K1 * K2;   // plane x of the potential
+            for (int e = tid; e < NP * K2; e += nT) {
+                const int pr = qd(e, K2, iK2), z = e - pr * K2;
+                gx[2 * pr * K2 + z] = Zt[e].x;
+                if (2 * pr + 1 < K1)
+                    gx[(2 * pr + 1) * K2 + z] = Zt[e].y;
             }
         } else {
             const int groups = nT / GS;
@@ -366,49 +472,16 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
         }
         if (!fftgBarrier(gbar, (unsigned) nb, dv.flags))
             return;
-        if (PASS != 0) {   // one field pass: E_rec per atom from the plane shares, then done
-            for (int s = s0 + tid; s < s1; s += nT) {
-                const int i = dv.slotAtom[s];
-                double f[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-                for (int j1 = 0; j1 < P; j1++) {
-                    const float4 g = __ldcg(gpart + (size_t) j1 * n + s);
-                    f[0] += g.x;
-                    f[1] += g.y;
-                    f[2] += g.z;
-                }
-#pragma unroll
-                for (int k = 0; k < 3; k++)
-                    dv.Erec[3 * i + k] = -(S.K[0] * S.recip[3 * k] * f[0] + S.K[1] * S.recip[3 * k + 1] * f[1] +
-                                           S.K[2] * S.recip[3 * k + 2] * f[2]);
-            }
+        // ---- G: E_rec at the chunk's atoms (a field pass), or the rows of A p and the block's share of p . A p
+        if (PASS != 0) {   // one field pass: E_pair and E_rec written
+            for (int s = s0 + wib; s < s1; s += nwarps)
+                pcgGatherSlot<P, false>(dv, S, gpot, s, psth, psdth, wib, wl, cs);
             return;
         }
-        // ---- A: rows of A p, the block's share of p . A p
         {
             double v[1] = {0.0};
-            for (int s = s0 + tid; s < s1; s += nT) {
-                const int i = dv.slotAtom[s];
-                double f[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-                for (int j1 = 0; j1 < P; j1++) {
-                    const float4 g = __ldcg(gpart + (size_t) j1 * n + s);
-                    f[0] += g.x;
-                    f[1] += g.y;
-                    f[2] += g.z;
-                }
-                const double al = dv.alpha[i];
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    const double Erec = -(S.K[0] * S.recip[3 * k] * f[0] + S.K[1] * S.recip[3 * k + 1] * f[1] +
-                                          S.K[2] * S.recip[3 * k + 2] * f[2]);
-                    const double pk = dv.p[3 * i + k];
-                    const double Tp = __ldcg(dv.Epair + 3 * i + k) + Erec + cs * pk;
-                    const double apk = (al > 0) ? pk / al - Tp : 0.0;
-                    dv.Ap[3 * i + k] = apk;
-                    v[0] += pk * apk;
-                }
-            }
+            for (int s = s0 + wib; s < s1; s += nwarps)
+                v[0] += pcgGatherSlot<P, true>(dv, S, gpot, s, psth, psdth, wib, wl, cs);
             blockReduce<1>(v, 0u);
             if (tid == 0)
                 part[(size_t) x * 4] = v[0];

@@ -404,12 +404,14 @@ class Engine:
     def transforms(self):
         return int(self._L.pgm_engine_transforms(self._h))
 
-    def autotune(self, pos, box, reps=20, candidates=(4, 8, 16, 32)):
-        """Picks the lanes per atom of the pair passes and the kind of field-pass transforms by timing whole
-        evaluations of this system (batched engines: pass the batch's positions and boxes): every pair of
-        (lanes, transforms) the grids allow, each the median of ``reps`` new-step evaluations on the device
-        (inputs resident, no host copies).  Keeps the fastest; every candidate's time is in
-        ``self.autotune_report`` [ms].  Returns the lanes."""
+    def autotune(self, pos, box, reps=20, candidates=(4, 8, 16, 32), reproducible=True):
+        """Picks the lanes per atom of the pair passes, the kind of field-pass transforms and the PME kernels by
+        timing whole evaluations of this system (batched engines: pass the batch's positions and boxes): every
+        (lanes, transforms, PME kernels) the grids allow, each the median of ``reps`` new-step evaluations on the
+        device (inputs resident, no host copies).  Every candidate's time is in ``self.autotune_report`` [ms].
+        Keeps the fastest of those whose results repeat bit for bit (reproducible=True: in mixed precision the
+        warp-per-atom spread into the 64-bit fixed-point grid, PME kernels 0; the others add float atomics), or
+        of all (reproducible=False).  Returns the lanes."""
         batched = getattr(self, "nsys", 1) > 1
         if batched:
             self.compute_batch(pos, box)
@@ -428,7 +430,8 @@ class Engine:
                     self.set_pair_lanes(lanes)
                     self.time_evaluations(2)   # (captures the graph of this choice)
                     report[(lanes, mode, pme)] = self.time_evaluations(reps)
-        lanes, mode, pme = min(report, key=report.get)
+        pool = {k: v for k, v in report.items() if k[2] == 0} if reproducible else report
+        lanes, mode, pme = min(pool or report, key=(pool or report).get)
         self.set_pair_lanes(lanes)
         self.set_transforms(mode)
         self.set_pme_kernels(pme)

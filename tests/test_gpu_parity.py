@@ -203,12 +203,13 @@ def test_repeatable_bits():
     assert np.array_equal(a.forces, b.forces) or rel_rms(a.forces, b.forces) < 1e-14
 
 
-@pytest.mark.parametrize("mode", [0, 3])
+@pytest.mark.parametrize("mode", [0, 3, 4])
 def test_mixed_repeatable_bits(mode):
     """Mixed precision repeats bit for bit: the spread adds 64-bit fixed-point contributions (integer sums do not
     depend on the atomics' order) and every other sum has a fixed order.  The real 8550-atom liquid, cuFFT
-    (transforms 0, a conversion kernel before the transforms) and the grid kernel (3, the conversion on its load),
-    three evaluations each, and a new engine on the same input."""
+    (transforms 0, a conversion kernel before the transforms), the grid kernel (3, the conversion on its load) and
+    the persistent CG kernel (4, its own spread and gather phases), three evaluations each, and a new engine on
+    the same input."""
     S, _ = load_dmp_real()
     runs = []
     for _ in range(2):
