@@ -188,6 +188,7 @@ struct Engine::Impl {
     bool clusterOk = false;    // the systems' grids and the GPU allow the cluster kernel
     bool splitOk = false;      // the systems' x extents allow the x-line kernel
     bool gridOk = false;       // the systems' grids and the GPU allow the grid-transform kernel
+    bool gridEnergyOk = false; // ... and its variant with the reciprocal energy for the final pass
     bool pcgOk = false;        // the persistent CG kernel applies (mixed, one system, grid kernel, order 6)
     bool planesOk = false;     // the plane-owner spread and gather apply (mixed, one system, order 6)
     int pmeWant = 0;           // the caller's choice of spread / gather kernels: 0 a warp per atom, 1 plane tiles,
@@ -1165,8 +1166,17 @@ struct Engine::Impl {
         return clusters > 0;
     }
 
-    // The grid-transform kernel: compiled for one cubic grid size (32, 40, 48, 64), or for any grid.
-    template <typename R> static void (*fftgKernel(int kc))(Dev, int) {
+    // The grid-transform kernel: compiled for one cubic grid size (32, 40, 48, 64), or for any grid; energy: the
+    // final pass's variant that also sums the reciprocal energy and strain.
+    template <typename R> static void (*fftgKernel(int kc, bool energy = false))(Dev, int) {
+        if (energy)
+            switch (kc) {
+            case 32: return k_fft_grid<R, 32, true>;
+            case 40: return k_fft_grid<R, 40, true>;
+            case 48: return k_fft_grid<R, 48, true>;
+            case 64: return k_fft_grid<R, 64, true>;
+            default: return k_fft_grid<R, 0, true>;
+            }
         switch (kc) {
         case 32: return k_fft_grid<R, 32>;
         case 40: return k_fft_grid<R, 40>;
@@ -1190,6 +1200,13 @@ struct Engine::Impl {
         int perSm = 0;
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fftgKernel<R>(fftgKc), FftgThreads<R>::n,
                                                          fftgSmem));
+        // the final pass's variant: every block resident too, and a conv partial of its own for each x-plane
+        CU(cudaFuncSetAttribute((const void*) fftgKernel<R>(fftgKc, true),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fftgSmem));
+        int perSmE = 0;
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmE, fftgKernel<R>(fftgKc, true), FftgThreads<R>::n,
+                                                         fftgSmem));
+        gridEnergyOk = (long long) perSmE * sms >= (long long) maxK0 * nsys && maxK0 <= convBlocks;
         return (long long) perSm * sms >= (long long) maxK0 * nsys;
     }
 
@@ -1457,6 +1474,22 @@ struct Engine::Impl {
         }
     }
 
+    // The grid-transform kernel (cooperative: the blocks of a system meet at two barriers); energy: the final
+    // pass's variant.
+    template <typename R> void launchGrid(cudaStream_t sm, const Dev& d, int flags, bool energy) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.gridDim = dim3(maxK0, nsys);
+        cfg.blockDim = dim3(FftgThreads<R>::n);
+        cfg.dynamicSmemBytes = fftgSmem;
+        cfg.stream = sm;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        CU(cudaLaunchKernelEx(&cfg, fftgKernel<R>(fftgKc, energy), d, flags));
+    }
+
     // fix: the spread before went to the fixed-point grid (the grid kernel converts on its load, the others after a
     // conversion kernel)
     template <typename R> void transformPair(cudaStream_t sm, const Dev& d, bool gate, bool fix = false) {
@@ -1473,17 +1506,7 @@ struct Engine::Impl {
             return;
         }
         if (tfMode == TF_GRID || tfMode == TF_PCG) {   // cooperative: the blocks of a system meet at two barriers
-            cudaLaunchConfig_t cfg = {};
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributeCooperative;
-            at[0].val.cooperative = 1;
-            cfg.gridDim = dim3(maxK0, nsys);
-            cfg.blockDim = dim3(FftgThreads<R>::n);
-            cfg.dynamicSmemBytes = fftgSmem;
-            cfg.stream = sm;
-            cfg.attrs = at;
-            cfg.numAttrs = 1;
-            CU(cudaLaunchKernelEx(&cfg, fftgKernel<R>(fftgKc), d, (gate ? 1 : 0) | (fix ? 2 : 0)));
+            launchGrid<R>(sm, d, (gate ? 1 : 0) | (fix ? 2 : 0), false);
             return;
         }
         cudaLaunchConfig_t cfg = {};
@@ -1807,7 +1830,12 @@ struct Engine::Impl {
         launchSpread<R>(sm, d, 0, d.dtot);
         CU(cudaEventRecord(evFork, sm));
         CU(cudaStreamWaitEvent(sd, evFork, 0));
-        fftChain<R>(sd, d, true, false, spreadFix());
+        // the final pass's transforms with the reciprocal energy: the grid kernel's energy variant where the field
+        // passes run the grid kernel, else cuFFT and the product kernel
+        if ((tfMode == TF_GRID || tfMode == TF_PCG) && gridEnergyOk && std::is_same<R, float>::value == mixed())
+            launchGrid<R>(sd, d, (spreadFix() && std::is_same<R, float>::value && d.gridFix) ? 2 : 0, true);
+        else
+            fftChain<R>(sd, d, true, false, spreadFix());
         {
             const long long threads = (long long) n * pairGS;
             const int blocks = (int) ((threads + 255) / 256);

@@ -1491,7 +1491,10 @@ __device__ __forceinline__ bool fftgBarrier(unsigned* bar, unsigned nb, int* fla
 __global__ void k_barrier_probe(unsigned* bar, int* flags) { fftgBarrier(bar, gridDim.x + 1, flags); }
 
 // KC > 0: every grid of the launch is KC^3 (compile-time passes and index maps); 0: any grid.
-template <typename R, int KC>
+// ENERGY (the final pass): also the reciprocal energy (1/2) sum w G |F|^2 and its strain derivative, as k_conv
+// sums them, from the x-lines' spectrum before the product; block x writes conv partial x of its system and clears
+// partials x + K0, x + 2 K0, ... up to the system's convBlocks (the host requires K0 <= convBlocks).
+template <typename R, int KC, bool ENERGY = false>
 __global__ void __launch_bounds__(FftgThreads<R>::n) k_fft_grid(Dev dv, int gateDone) {
     typedef typename CplxT<R>::T C;
     const int s = blockIdx.y;
@@ -1576,14 +1579,47 @@ __global__ void __launch_bounds__(FftgThreads<R>::n) k_fft_grid(Dev dv, int gate
     __syncthreads();
     C* Fx = fftLinesK<R, -1, KC>(b0, b1, nl, K0, lx, W0);
     const R* infl = (const R*) dv.infl + S.specOff;
+    double acc[ENERGY ? NCONV : 1];
+#pragma unroll
+    for (int k = 0; k < (ENERGY ? NCONV : 1); k++)
+        acc[k] = 0.0;
+    const double fac = PI_D * PI_D / (S.beta * S.beta);
     for (int e = tid; e < lpb * K0; e += nT) {
         const int xx = qd(e, lpb, iLpb), li = e - xx * lpb;
         if (li < nl) {
             const R gk = infl[(size_t) xx * nline + l0 + li];
             C& v = Fx[li * lx + xx];
+            if (ENERGY && (xx != 0 || l0 + li != 0)) {   // (the k = 0 term is left out, as k_conv does)
+                const int l = l0 + li, m3 = l % K2h, m2 = l / K2h, m1 = xx;
+                const double w = (m3 == 0 || ((K2 & 1) == 0 && m3 == K2 / 2)) ? 1.0 : 2.0;
+                const double nrm = (double) v.x * v.x + (double) v.y * v.y;
+                const double en = 0.5 * w * (double) gk * nrm;
+                acc[0] += en;
+                const double mm1 = (m1 <= K0 / 2) ? m1 : m1 - K0, mm2 = (m2 <= K1 / 2) ? m2 : m2 - K1, mm3 = m3;
+                double ms[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+                    ms[k] = mm1 * S.recip[3 * k] + mm2 * S.recip[3 * k + 1] + mm3 * S.recip[3 * k + 2];
+                const double m2s = ms[0] * ms[0] + ms[1] * ms[1] + ms[2] * ms[2];
+                const double c2 = 2.0 * (fac + 1.0 / m2s);
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int b = 0; b < 3; b++)
+                        acc[ENERGY ? 1 + 3 * a + b : 0] += en * ((a == b ? -1.0 : 0.0) + c2 * ms[a] * ms[b]);
+            }
             v.x *= gk;
             v.y *= gk;
         }
+    }
+    if (ENERGY) {
+        blockReduce<NCONV>(acc, 0u);
+        if (tid == 0)
+            for (int k = 0; k < NCONV; k++)
+                dv.convPartial[(size_t) (dv.convPartialOff[s] + x) * NCONV + k] = acc[k];
+        if (tid < NCONV * 16)
+            for (int b = x + K0 * (1 + tid / NCONV); b < S.convBlocks; b += 16 * K0)
+                dv.convPartial[(size_t) (dv.convPartialOff[s] + b) * NCONV + tid % NCONV] = 0.0;
     }
     __syncthreads();
     const C* Gx = fftLinesK<R, 1, KC>(Fx, Fx == b0 ? b1 : b0, nl, K0, lx, W0);
