@@ -147,7 +147,7 @@ struct Engine::Impl {
     Settings s;
     cudaStream_t st = nullptr, side = nullptr;
     cudaStream_t callerStream = nullptr;
-    cudaEvent_t evFork = nullptr, evJoin = nullptr, evCaller = nullptr, evDone = nullptr;
+    cudaEvent_t evFork = nullptr, evJoin = nullptr, evCaller = nullptr, evDone = nullptr, evPerm = nullptr;
     int devId = 0;
 
     // systems and atoms (host)
@@ -333,8 +333,9 @@ struct Engine::Impl {
         if (evJoin) cudaEventDestroy(evJoin);
         if (evCaller) cudaEventDestroy(evCaller);
         if (evDone) cudaEventDestroy(evDone);
+        if (evPerm) cudaEventDestroy(evPerm);
         st = side = nullptr;
-        evFork = evJoin = evCaller = evDone = nullptr;
+        evFork = evJoin = evCaller = evDone = evPerm = nullptr;
     }
 
     bool mixed() const { return s.precision != 0; }
@@ -357,6 +358,7 @@ struct Engine::Impl {
         CU(cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming));
         CU(cudaEventCreateWithFlags(&evCaller, cudaEventDisableTiming));
         CU(cudaEventCreateWithFlags(&evDone, cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&evPerm, cudaEventDisableTiming));
         CU(cudaMallocHost((void**) &hFlags, 16 * sizeof(int)));
         CU(cudaMallocHost((void**) &hCtl, sizeof(Ctl)));
         useGraph = envInt("PGM_B200_NO_GRAPH", 0) == 0;
@@ -1728,13 +1730,18 @@ struct Engine::Impl {
         const bool rowsLeft = enqueueListStep(sm, d);
         if (s.polarizable) {
             // the list's rows when built here, the pairs within the cutoff and their G1, G2 (side stream) beside
-            // the permanent field's PME half (main stream)
+            // the permanent field's PME half (main stream).  Without a skin, on the plain first pass, the record
+            // kernel also forms the permanent field's direct part (after the permanent spread wrote the sources),
+            // in place of a pair pass of its own.
+            const bool fuseField = rowsLeft && !persistentMode() && !dualFirstPass();
             CU(cudaEventRecord(evFork, sm));
             CU(cudaStreamWaitEvent(sd, evFork, 0));
             if (rowsLeft)
                 listKernel(sd, d);
-            pairRecords<R>(sd, d);
-            CU(cudaEventRecord(evJoin, sd));
+            if (!fuseField) {
+                pairRecords<R>(sd, d);
+                CU(cudaEventRecord(evJoin, sd));
+            }
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
             if (std::is_same<R, float>::value && planesMode())
                 enqueuePlaneBins(sm, d);
@@ -1787,10 +1794,18 @@ struct Engine::Impl {
             }
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
             launchSpread<R>(sm, d, 0, d.perm);
+            if (fuseField) {   // the records with the permanent field's direct part, once the sources are written
+                CU(cudaEventRecord(evPerm, sm));
+                CU(cudaStreamWaitEvent(sd, evPerm, 0));
+                k_pair_kernels<R, true><<<(n + 7) / 8, 256, 0, sd>>>(d);
+                CU(cudaGetLastError());
+                CU(cudaEventRecord(evJoin, sd));
+            }
             transformPair<R>(sm, d, false, spreadFix());
             launchGather<R, false>(sm, d, 0);   // (the reciprocal half needs no pair list)
             CU(cudaStreamWaitEvent(sm, evJoin, 0));
-            pairField<R, true>(sm, d, 0);
+            if (!fuseField)
+                pairField<R, true>(sm, d, 0);
             k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
             CU(cudaGetLastError());
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));

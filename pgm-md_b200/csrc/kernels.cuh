@@ -568,7 +568,10 @@ template <> struct PairRec<float> { static constexpr bool storeX = true; };
 // The pair records of every listed pair (the list of the evaluation) in precision R with G0..G3 by
 // core/pgm_math.h:77-93 via pairKernels, from the current slot-order positions (also after new positions on a
 // kept list), one warp per slot, the pairs of its row over the lanes.
-template <typename R>
+// FIELD: also the direct-space field of the charges and dipoles dS (the permanent field pass, core/pgm_core.cpp:
+// 274-284: E_i = sum_j (q_j G1 + (d_j . x) G2) x - d_j G1) from the same G1, G2 and x, written to Epair, as
+// k_pair_field<R, true> would (per-lane sums in R, across the lanes in double).
+template <typename R, bool FIELD = false>
 __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
     typedef typename V2T<R>::T R2;
     typedef typename V4T<R>::T R4;
@@ -585,6 +588,8 @@ __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
     R2* crow = dv.pairC ? (R2*) dv.pairC + (size_t) slot * dv.cap : nullptr;
     const int cnt = dv.listCount[slot];
     const R beta = (R) S.beta;
+    R f0 = 0, f1 = 0, f2 = 0;   // (FIELD) the lane's field sums
+    const R4* dS = (const R4*) dv.dS;
     for (int t = lane; t < cnt; t += 32) {
         const uint32_t e = row[t];
         const int js = entrySlot(e);
@@ -598,6 +603,13 @@ __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
         const R a = R(1) / fsqrt(R(2) * (Rr * Rr + Rj * Rj));
         R G[4];
         pairKernels<R, 4>(a, beta, r, G);
+        if (FIELD) {
+            const R4 dj = dS[js];
+            const R c = (dj.x * xr0 + dj.y * xr1 + dj.z * xr2) * G[2] + dj.w * G[1];
+            f0 += c * xr0 - dj.x * G[1];
+            f1 += c * xr1 - dj.y * G[1];
+            f2 += c * xr2 - dj.z * G[1];
+        }
         R2 vb;
         if constexpr (STORE_X) {
             R4 va;
@@ -618,6 +630,21 @@ __global__ void __launch_bounds__(256) k_pair_kernels(Dev dv) {
             vc.x = G[0];
             vc.y = G[3];
             crow[t] = vc;
+        }
+    }
+    if (FIELD) {
+        double E0 = f0, E1 = f1, E2 = f2;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            E0 += __shfl_xor_sync(0xffffffffu, E0, o);
+            E1 += __shfl_xor_sync(0xffffffffu, E1, o);
+            E2 += __shfl_xor_sync(0xffffffffu, E2, o);
+        }
+        if (lane == 0) {
+            const int i = dv.slotAtom[slot];
+            dv.Epair[3 * i] = E0;
+            dv.Epair[3 * i + 1] = E1;
+            dv.Epair[3 * i + 2] = E2;
         }
     }
 }

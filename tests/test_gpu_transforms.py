@@ -42,6 +42,8 @@ def test_transforms_single_system(precision, mode, name):
     lim_e, lim_f = (1e-12, 1e-12) if precision == 0 else (1e-6, 1e-5)
     assert abs(a.energy - b.energy) <= lim_e * abs(a.energy)
     assert rel_rms(b.forces, a.forces) <= lim_f
+    # the strain derivative too (the grid kernel's final pass sums the k-space strain itself)
+    assert np.abs(b.strain - a.strain).max() <= lim_f * np.abs(a.strain).max()
     assert a.iterations == b.iterations or precision == 1
 
 
@@ -62,6 +64,7 @@ def test_grid_transforms_compiled_sizes(precision, K):
     lim_e, lim_f = (1e-12, 1e-12) if precision == 0 else (1e-6, 1e-5)
     assert abs(a.energy - b.energy) <= lim_e * abs(a.energy)
     assert rel_rms(b.forces, a.forces) <= lim_f
+    assert np.abs(b.strain - a.strain).max() <= lim_f * np.abs(a.strain).max()
 
 
 @pytest.mark.parametrize("mode", [1, 2, 3])
@@ -86,6 +89,9 @@ def test_transforms_batch(precision, mode):
     lim = 1e-12 if precision == 0 else 1e-6
     assert np.all(np.abs(a["energies"] - b["energies"]) <= lim * np.abs(a["energies"]))
     assert rel_rms(b["forces"], a["forces"]) <= (1e-12 if precision == 0 else 1e-5)
+    sa, sb = np.asarray(a["strain"]).reshape(len(systems), -1), np.asarray(b["strain"]).reshape(len(systems), -1)
+    scale = np.abs(sa).max(axis=1, keepdims=True)
+    assert np.all(np.abs(sb - sa) <= (1e-12 if precision == 0 else 1e-5) * scale)
 
 
 def test_transforms_need_small_235_grids():
