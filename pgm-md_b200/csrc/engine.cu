@@ -1219,8 +1219,8 @@ struct Engine::Impl {
     // (one per SM), and its shared memory.
     void preparePersistent() {
         pcgOk = false;
-        if (!mixed() || nsys != 1 || !gridOk || !planesOk || s.order != 6 || !s.polarizable)
-            return;   // (it takes the plane-owner kernels' bins)
+        if (!mixed() || nsys != 1 || !gridOk || s.order != 6 || !s.polarizable)
+            return;
         int sms = 0, coop = 0, optin = 0;
         CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, devId));
         CU(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, devId));
@@ -1237,10 +1237,6 @@ struct Engine::Impl {
             return;
         pcgBlocks = sms * std::min(perSm, PCG_BLOCKS_PER_SM);   // (the plane blocks, 0 .. K0-1, one per SM)
         pcgOk = true;
-        dPmeRec.ensure((size_t) n * sizeof(PmeRec<6>));
-        dPmeBins.ensure((FFT_MAXK + 1) * sizeof(int));
-        dSrcW.ensure((size_t) n * sizeof(float4));
-        dGPart.ensure((size_t) 6 * n * sizeof(float4));
         dPcgPartial.ensure((size_t) 2 * pcgBlocks * 4 * 8);
     }
 

@@ -32,36 +32,11 @@ constexpr int PCG_THREADS = 512;
 constexpr int PCG_MIN_PAIR_BLOCKS = 16;      // blocks left for the pair pass beside the plane blocks
 constexpr int PCG_BLOCKS_PER_SM = 1;         // resident blocks per SM (two, at 64 registers, measured slower)
 
-// The spline record of one atom of the plane bins (order P): its slot, b1, b2 and b0 mod K0, and theta and
+// The spline record of one atom of the plane-owner kernels' bins (order P): its slot, b1, b2 and b0 mod K0, and theta and
 // dtheta of the three dimensions, c[dim 2P + kind P + j].
 template <int P> struct PmeRec {
     int4 idx;
     float c[6 * P];
-};
-
-// The atoms that reach plane x: those of b0 = (x + j1) mod K0 for j1 < P, bins b0 nyc .. b0 nyc + nyc - 1 (the
-// plane-owner kernels' bins by x-plane and row chunk, contiguous per x-plane; nyc = 1: bins by x-plane only);
-// t-th of them -> (j1, record index).
-template <int P>
-struct PlaneAtoms {
-    int start[P], cum[P + 1];
-    __device__ __forceinline__ void init(const int* binStart, int x, int K0, int nyc) {
-        cum[0] = 0;
-#pragma unroll
-        for (int j = 0; j < P; j++) {
-            const int b = wrapIndex(x + j, K0) * nyc;
-            start[j] = binStart[b];
-            cum[j + 1] = cum[j] + binStart[b + nyc] - binStart[b];
-        }
-    }
-    __device__ __forceinline__ int total() const { return cum[P]; }
-    __device__ __forceinline__ int locate(int t, int& j1) const {
-        j1 = 0;
-#pragma unroll
-        for (int j = 1; j < P; j++)
-            j1 += (t >= cum[j]) ? 1 : 0;
-        return start[j1] + t - cum[j1];
-    }
 };
 
 // The spread of slot s (its atom's weights w = (q, e0, e1, e2)) into the 64-bit fixed-point grid by the calling
