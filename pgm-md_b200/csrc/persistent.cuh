@@ -4,7 +4,7 @@
 // Every CG iteration of core/pgm_core.cpp:351-385 (A v = v/alpha - T v; T v = pair + reciprocal + self field)
 // runs inside the kernel, with grid barriers between its phases instead of kernel boundaries and graph nodes:
 //
-//   S  (every block, a warp per slot of its chunk)  p = z + beta p; the pair pass's float copy of p; the PME
+//   S  (every block, a half-warp per slot of its chunk)  p = z + beta p; the pair pass's float copy of p; the PME
 //      weights (q, e_a = K_a p . recip[:, a]) and the spread of the atom into the 64-bit fixed-point grid
 //      (global atomics, the same points and arithmetic as k_spread; integer sums do not depend on their order,
 //      so the solve repeats bit for bit);                                                         grid barrier
@@ -13,7 +13,7 @@
 //      of the plane blocks), the influence product, transformed back and stored to the potential grid.
 //      Blocks K0 .. end run the direct-space field pass of the iteration's direction over the pair records.
 //                                                                                                  grid barrier
-//   G  (every block, a warp per slot of its chunk) E_rec at the atom from the potential grid, the atom's row of
+//   G  (every block, a half-warp per slot of its chunk) E_rec at the atom from the potential grid, the atom's row of
 //      A p and the block's share of p . A p;                                                        grid barrier
 //   U  (every block) alph from the shares (fixed order), x, r, z of its slots, shares of z'.(r' - r), r'.z',
 //      max |z'|;                                                                                    grid barrier
@@ -32,45 +32,41 @@ constexpr int PCG_THREADS = 512;
 constexpr int PCG_MIN_PAIR_BLOCKS = 16;      // blocks left for the pair pass beside the plane blocks
 constexpr int PCG_BLOCKS_PER_SM = 1;         // resident blocks per SM (two, at 64 registers, measured slower)
 
-// The spline record of one atom of the plane-owner kernels' bins (order P): its slot, b1, b2 and b0 mod K0, and theta and
-// dtheta of the three dimensions, c[dim 2P + kind P + j].
+// The spline record of one atom of the plane-owner kernels' bins (order P): its slot, b1, b2 and b0 mod K0, and
+// theta and dtheta of the three dimensions, c[dim 2P + kind P + j].
 template <int P> struct PmeRec {
     int4 idx;
     float c[6 * P];
 };
 
-// The spread of slot s (its atom's weights w = (q, e0, e1, e2)) into the 64-bit fixed-point grid by the calling
-// warp: the evaluation's spline coefficients staged in the warp's shared rows, lane -> stencil column (j2, j3),
-// loop over j1, the leftover columns' points over the lanes: the points and the per-point arithmetic of k_spread,
-// so both add the same integers.
+// The spread of slot s (its atom's weights w = (q, e0, e1, e2)) into the 64-bit fixed-point grid by a half-warp
+// (16 lanes hl, mask `mask`, shared rows `row` for the evaluation's spline coefficients): a stencil column
+// (j2, j3) per lane and round, a loop over j1; the two halves of a warp keep two atoms' loads and atomics in
+// flight.  The points and per-point arithmetic of k_spread, so both add the same integers.
 template <int P>
-__device__ __forceinline__ void pcgSpreadSlot(const Dev& dv, const SysDev& S, long long* gfix, int s, float4 w,
-                                             float (*sth)[3][P], float (*sdth)[3][P], int wib, int lane) {
+__device__ __forceinline__ void pcgSpreadHalf(const Dev& dv, const SysDev& S, long long* gfix, int s, float4 w,
+                                             float (*sth)[3][P], float (*sdth)[3][P], int row, int hl,
+                                             unsigned mask) {
     const int i = dv.slotAtom[s];
     const float* sp = (const float*) dv.spl + (size_t) s * 9 * MAXP;
-    for (int k = lane; k < 6 * P; k += 32) {
+    for (int k = hl; k < 6 * P; k += 16) {
         const int kind = k / (3 * P), dim = (k / P) % 3, j = k % P;
         const float v = sp[(kind * 3 + dim) * MAXP + j];
         if (kind == 0)
-            sth[wib][dim][j] = v;
+            sth[row][dim][j] = v;
         else
-            sdth[wib][dim][j] = v;
+            sdth[row][dim][j] = v;
     }
-    const int bl = lane < 3 ? dv.pmeBase[3 * i + lane] : 0;
-    const int b0 = __shfl_sync(0xffffffffu, bl, 0), b1 = __shfl_sync(0xffffffffu, bl, 1),
-              b2 = __shfl_sync(0xffffffffu, bl, 2);
-    __syncwarp();
+    const int bl = hl < 3 ? dv.pmeBase[3 * i + hl] : 0;
+    const int b0 = __shfl_sync(mask, bl, 0, 16), b1 = __shfl_sync(mask, bl, 1, 16), b2 = __shfl_sync(mask, bl, 2, 16);
+    __syncwarp(mask);
     const float qr = w.x, e0 = w.y, e1 = w.z, e2 = w.w;
     const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
     const size_t plane = (size_t) K1 * K2;
-    constexpr int NPAIR = P * P, FULL = NPAIR / 32, LEFT = NPAIR % 32, LROUNDS = (LEFT * P + 31) / 32;
-    constexpr int LEFTD = LEFT > 0 ? LEFT : 1;
-#pragma unroll
-    for (int rd = 0; rd < FULL; rd++) {
-        const int pr = lane + 32 * rd;
-        const int j2 = pr / P, j3 = pr % P;
-        const float t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
-        const float t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+    for (int c = hl; c < P * P; c += 16) {
+        const int j2 = c / P, j3 = c % P;
+        const float t2 = sth[row][1][j2], u2 = sdth[row][1][j2];
+        const float t3 = sth[row][2][j3], u3 = sdth[row][2][j3];
         const float c23 = t2 * t3;
         const float a = qr * c23 + e1 * u2 * t3 + e2 * t2 * u3;
         const float b = e0 * c23;
@@ -78,98 +74,61 @@ __device__ __forceinline__ void pcgSpreadSlot(const Dev& dv, const SysDev& S, lo
 #pragma unroll
         for (int j1 = 0; j1 < P; j1++)
             gridFixAdd(gfix + col + (size_t) wrapIndex(b0 - j1, K0) * plane,
-                       (float) (a * sth[wib][0][j1] + b * sdth[wib][0][j1]));
+                       (float) (a * sth[row][0][j1] + b * sdth[row][0][j1]));
     }
-#pragma unroll
-    for (int lr = 0; lr < LROUNDS; lr++) {
-        const int k = lane + 32 * lr;
-        if (k < LEFT * P) {
-            const int pr = 32 * FULL + k % LEFTD, j1 = k / LEFTD;
-            const int j2 = pr / P, j3 = pr % P;
-            const float t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
-            const float t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
-            const float c23 = t2 * t3;
-            const float v = (qr * c23 + e1 * u2 * t3 + e2 * t2 * u3) * sth[wib][0][j1] + e0 * c23 * sdth[wib][0][j1];
-            gridFixAdd(gfix + (size_t) wrapIndex(b0 - j1, K0) * plane + (size_t) wrapIndex(b1 - j2, K1) * K2 +
-                           wrapIndex(b2 - j3, K2),
-                       (float) v);
-        }
-    }
-    __syncwarp();   // (the next slot of this warp overwrites the shared rows)
+    __syncwarp(mask);   // (the next slot of this half-warp overwrites the shared rows)
 }
 
 // E_rec at the atom of slot s from the potential grid gpot (written by other blocks in this launch: read past
-// L1) by the calling warp: f_a = sum (d theta_a) theta theta phi over the stencil (lane -> column (j2, j3), loop
-// over j1, the leftover columns' points over the lanes), E_rec = -sum_a K_a recip[:, a] f_a
-// (core/pgm_core.cpp:241-264), the lanes' sums in double.
-// CGA (the CG iterations): instead of E_rec, the row of A p = p / alpha - (E_pair + E_rec + cs p)
-// (core/pgm_core.cpp:363) at the atom, and the returned share p_k (A p)_k of lanes k < 3 (0 elsewhere).
+// L1) by a half-warp (as pcgSpreadHalf): f_a = sum (d theta_a) theta theta phi over the stencil, E_rec =
+// -sum_a K_a recip[:, a] f_a (core/pgm_core.cpp:241-264), the lanes' sums in double; or (CGA, the CG iterations)
+// instead the atom's row of A p = p / alpha - (E_pair + E_rec + cs p) (core/pgm_core.cpp:363) and the returned
+// share p_k (A p)_k of lanes hl = k < 3 (0 elsewhere).
 template <int P, bool CGA>
-__device__ __forceinline__ double pcgGatherSlot(const Dev& dv, const SysDev& S, const float* gpot, int s,
-                                               float (*sth)[3][P], float (*sdth)[3][P], int wib, int lane,
-                                               double cs) {
+__device__ __forceinline__ double pcgGatherHalf(const Dev& dv, const SysDev& S, const float* gpot, int s,
+                                               float (*sth)[3][P], float (*sdth)[3][P], int row, int hl,
+                                               unsigned mask, double cs) {
     const int i = dv.slotAtom[s];
     const float* sp = (const float*) dv.spl + (size_t) s * 9 * MAXP;
-    for (int k = lane; k < 6 * P; k += 32) {
+    for (int k = hl; k < 6 * P; k += 16) {
         const int kind = k / (3 * P), dim = (k / P) % 3, j = k % P;
         const float v = sp[(kind * 3 + dim) * MAXP + j];
         if (kind == 0)
-            sth[wib][dim][j] = v;
+            sth[row][dim][j] = v;
         else
-            sdth[wib][dim][j] = v;
+            sdth[row][dim][j] = v;
     }
-    const int bl = lane < 3 ? dv.pmeBase[3 * i + lane] : 0;
-    const int b0 = __shfl_sync(0xffffffffu, bl, 0), b1 = __shfl_sync(0xffffffffu, bl, 1),
-              b2 = __shfl_sync(0xffffffffu, bl, 2);
-    __syncwarp();
+    const int bl = hl < 3 ? dv.pmeBase[3 * i + hl] : 0;
+    const int b0 = __shfl_sync(mask, bl, 0, 16), b1 = __shfl_sync(mask, bl, 1, 16), b2 = __shfl_sync(mask, bl, 2, 16);
+    __syncwarp(mask);
     const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
     const size_t plane = (size_t) K1 * K2;
-    constexpr int NPAIR = P * P, FULL = NPAIR / 32, LEFT = NPAIR % 32, LROUNDS = (LEFT * P + 31) / 32;
-    constexpr int LEFTD = LEFT > 0 ? LEFT : 1;
     float f0 = 0.f, f1 = 0.f, f2 = 0.f;
-#pragma unroll
-    for (int rd = 0; rd < FULL; rd++) {
-        const int pr = lane + 32 * rd;
-        const int j2 = pr / P, j3 = pr % P;
+    for (int c = hl; c < P * P; c += 16) {
+        const int j2 = c / P, j3 = c % P;
         const float* col = gpot + (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2);
         float St = 0.f, Su = 0.f;
 #pragma unroll
         for (int j1 = 0; j1 < P; j1++) {
             const float ph = __ldcg(col + (size_t) wrapIndex(b0 - j1, K0) * plane);
-            St += sth[wib][0][j1] * ph;
-            Su += sdth[wib][0][j1] * ph;
+            St += sth[row][0][j1] * ph;
+            Su += sdth[row][0][j1] * ph;
         }
-        const float t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
-        const float t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
+        const float t2 = sth[row][1][j2], u2 = sdth[row][1][j2];
+        const float t3 = sth[row][2][j3], u3 = sdth[row][2][j3];
         f0 += Su * t2 * t3;
         f1 += St * u2 * t3;
         f2 += St * t2 * u3;
     }
-#pragma unroll
-    for (int lr = 0; lr < LROUNDS; lr++) {
-        const int k = lane + 32 * lr;
-        if (k < LEFT * P) {
-            const int pr = 32 * FULL + k % LEFTD, j1 = k / LEFTD;
-            const int j2 = pr / P, j3 = pr % P;
-            const float ph = __ldcg(gpot + (size_t) wrapIndex(b0 - j1, K0) * plane +
-                                    (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2));
-            const float t1 = sth[wib][0][j1], u1 = sdth[wib][0][j1];
-            const float t2 = sth[wib][1][j2], u2 = sdth[wib][1][j2];
-            const float t3 = sth[wib][2][j3], u3 = sdth[wib][2][j3];
-            f0 += u1 * t2 * t3 * ph;
-            f1 += t1 * u2 * t3 * ph;
-            f2 += t1 * t2 * u3 * ph;
-        }
-    }
     double F[3] = {(double) f0, (double) f1, (double) f2};
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
+    for (int o = 8; o > 0; o >>= 1)
 #pragma unroll
         for (int k = 0; k < 3; k++)
-            F[k] += __shfl_xor_sync(0xffffffffu, F[k], o);
+            F[k] += __shfl_xor_sync(mask, F[k], o, 16);
     double share = 0.0;
-    if (lane < 3) {
-        const int k = lane;
+    if (hl < 3) {
+        const int k = hl;
         const double E = -(S.K[0] * S.recip[3 * k] * F[0] + S.K[1] * S.recip[3 * k + 1] * F[1] +
                            S.K[2] * S.recip[3 * k + 2] * F[2]);
         if (CGA) {
@@ -182,7 +141,7 @@ __device__ __forceinline__ double pcgGatherSlot(const Dev& dv, const SysDev& S, 
             dv.Erec[3 * i + k] = E;
         }
     }
-    __syncwarp();
+    __syncwarp(mask);
     return share;
 }
 
@@ -293,10 +252,11 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
     C* const spec = (C*) dv.spec + S.specOff;
     C* const myPlane = spec + (size_t) x * nline;
     double* const part = dv.pcgPartial;
-    // the warp-per-slot phases (spread, gather): the warps' shared spline rows, the fixed-point charge grid and
-    // the float potential grid
-    __shared__ float psth[PCG_THREADS / 32][3][P], psdth[PCG_THREADS / 32][3][P];
-    const int wib = tid >> 5, wl = tid & 31, nwarps = nT >> 5;
+    // the half-warp-per-slot phases (spread, gather): the half-warps' shared spline rows, the fixed-point charge
+    // grid and the float potential grid
+    __shared__ float psth[PCG_THREADS / 16][3][P], psdth[PCG_THREADS / 16][3][P];
+    const int hrow = tid >> 4, hl = tid & 15, nhalves = nT >> 4;   // the half-warp phases
+    const unsigned hmask = 0xffffu << (tid & 16);
     long long* const gfix = dv.gridFix + S.gridOff;
     float* const gpot = (float*) dv.grid + S.gridOff;
     (void) nyc;
@@ -306,28 +266,28 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
     double rz = sc[SC_RZ], beta = sc[SC_BETA], it = sc[SC_IT];
     const double norm = sc[SC_NORM];
     for (;;) {
-        // ---- S: a warp per slot: direction p = z + beta p (or the pass's sources), the float copy for the pair
-        // pass, the PME weights (q, e_a = K_a p . recip[:, a]) and the spread
-        for (int s = s0 + wib; s < s1; s += nwarps) {
+        // ---- S: a half-warp per slot: direction p = z + beta p (or the pass's sources), the float copy for the
+        // pair pass, the PME weights (q, e_a = K_a p . recip[:, a]) and the spread
+        for (int s = s0 + hrow; s < s1; s += nhalves) {
             const int i = dv.slotAtom[s];
             double dl = 0.0;
-            if (wl < 3) {
+            if (hl < 3) {
                 if (PASS == 0) {
-                    dl = dv.z[3 * i + wl] + beta * dv.p[3 * i + wl];
-                    dv.p[3 * i + wl] = dl;
+                    dl = dv.z[3 * i + hl] + beta * dv.p[3 * i + hl];
+                    dv.p[3 * i + hl] = dl;
                 } else {
-                    dl = vec[3 * i + wl];
+                    dl = vec[3 * i + hl];
                 }
             }
-            const double d0 = __shfl_sync(0xffffffffu, dl, 0), d1 = __shfl_sync(0xffffffffu, dl, 1),
-                         d2 = __shfl_sync(0xffffffffu, dl, 2);
+            const double d0 = __shfl_sync(hmask, dl, 0, 16), d1 = __shfl_sync(hmask, dl, 1, 16),
+                         d2 = __shfl_sync(hmask, dl, 2, 16);
             const float qf = PASS == 2 ? (float) dv.q[i] : 0.f;
-            if (wl == 0)
+            if (hl == 0)
                 ((float4*) dv.dS)[s] = make_float4((float) d0, (float) d1, (float) d2, qf);
             const float4 w = make_float4(qf, (float) (S.K[0] * (d0 * S.recip[0] + d1 * S.recip[3] + d2 * S.recip[6])),
                                          (float) (S.K[1] * (d0 * S.recip[1] + d1 * S.recip[4] + d2 * S.recip[7])),
                                          (float) (S.K[2] * (d0 * S.recip[2] + d1 * S.recip[5] + d2 * S.recip[8])));
-            pcgSpreadSlot<P>(dv, S, gfix, s, w, psth, psdth, wib, wl);
+            pcgSpreadHalf<P>(dv, S, gfix, s, w, psth, psdth, hrow, hl, hmask);
         }
         if (!fftgBarrier(gbar, (unsigned) nb, dv.flags))
             return;
@@ -449,14 +409,14 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
             return;
         // ---- G: E_rec at the chunk's atoms (a field pass), or the rows of A p and the block's share of p . A p
         if (PASS != 0) {   // one field pass: E_pair and E_rec written
-            for (int s = s0 + wib; s < s1; s += nwarps)
-                pcgGatherSlot<P, false>(dv, S, gpot, s, psth, psdth, wib, wl, cs);
+            for (int s = s0 + hrow; s < s1; s += nhalves)
+                pcgGatherHalf<P, false>(dv, S, gpot, s, psth, psdth, hrow, hl, hmask, cs);
             return;
         }
         {
             double v[1] = {0.0};
-            for (int s = s0 + wib; s < s1; s += nwarps)
-                v[0] += pcgGatherSlot<P, true>(dv, S, gpot, s, psth, psdth, wib, wl, cs);
+            for (int s = s0 + hrow; s < s1; s += nhalves)
+                v[0] += pcgGatherHalf<P, true>(dv, S, gpot, s, psth, psdth, hrow, hl, hmask, cs);
             blockReduce<1>(v, 0u);
             if (tid == 0)
                 part[(size_t) x * 4] = v[0];
