@@ -4,7 +4,7 @@
 // Every CG iteration of core/pgm_core.cpp:351-385 (A v = v/alpha - T v; T v = pair + reciprocal + self field)
 // runs inside the kernel, with grid barriers between its phases instead of kernel boundaries and graph nodes:
 //
-//   S  (every block, a half-warp per slot of its chunk)  p = z + beta p; the pair pass's float copy of p; the PME
+//   S  (every block, 8 lanes per slot of its chunk)  p = z + beta p; the pair pass's float copy of p; the PME
 //      weights (q, e_a = K_a p . recip[:, a]) and the spread of the atom into the 64-bit fixed-point grid
 //      (global atomics, the same points and arithmetic as k_spread; integer sums do not depend on their order,
 //      so the solve repeats bit for bit);                                                         grid barrier
@@ -13,7 +13,7 @@
 //      of the plane blocks), the influence product, transformed back and stored to the potential grid.
 //      Blocks K0 .. end run the direct-space field pass of the iteration's direction over the pair records.
 //                                                                                                  grid barrier
-//   G  (every block, a half-warp per slot of its chunk) E_rec at the atom from the potential grid, the atom's row of
+//   G  (every block, 8 lanes per slot of its chunk) E_rec at the atom from the potential grid, the atom's row of
 //      A p and the block's share of p . A p;                                                        grid barrier
 //   U  (every block) alph from the shares (fixed order), x, r, z of its slots, shares of z'.(r' - r), r'.z',
 //      max |z'|;                                                                                    grid barrier
@@ -30,6 +30,7 @@ namespace pgmb200 {
 
 constexpr int PCG_THREADS = 512;
 constexpr int PCG_MIN_PAIR_BLOCKS = 16;      // blocks left for the pair pass beside the plane blocks
+constexpr int PCG_SLOT_LANES = 8;            // lanes per slot in the spread and gather phases
 constexpr int PCG_BLOCKS_PER_SM = 1;         // resident blocks per SM (two, at 64 registers, measured slower)
 
 // The spline record of one atom of the plane-owner kernels' bins (order P): its slot, b1, b2 and b0 mod K0, and
@@ -39,17 +40,17 @@ template <int P> struct PmeRec {
     float c[6 * P];
 };
 
-// The spread of slot s (its atom's weights w = (q, e0, e1, e2)) into the 64-bit fixed-point grid by a half-warp
-// (16 lanes hl, mask `mask`, shared rows `row` for the evaluation's spline coefficients): a stencil column
-// (j2, j3) per lane and round, a loop over j1; the two halves of a warp keep two atoms' loads and atomics in
+// The spread of slot s (its atom's weights w = (q, e0, e1, e2)) into the 64-bit fixed-point grid by a group of L
+// lanes (lane hl, mask `mask`, shared rows `row` for the evaluation's spline coefficients): a stencil column
+// (j2, j3) per lane and round, a loop over j1; the groups of a warp keep several atoms' loads and atomics in
 // flight.  The points and per-point arithmetic of k_spread, so both add the same integers.
-template <int P>
+template <int P, int L>
 __device__ __forceinline__ void pcgSpreadHalf(const Dev& dv, const SysDev& S, long long* gfix, int s, float4 w,
                                              float (*sth)[3][P], float (*sdth)[3][P], int row, int hl,
                                              unsigned mask) {
     const int i = dv.slotAtom[s];
     const float* sp = (const float*) dv.spl + (size_t) s * 9 * MAXP;
-    for (int k = hl; k < 6 * P; k += 16) {
+    for (int k = hl; k < 6 * P; k += L) {
         const int kind = k / (3 * P), dim = (k / P) % 3, j = k % P;
         const float v = sp[(kind * 3 + dim) * MAXP + j];
         if (kind == 0)
@@ -58,12 +59,12 @@ __device__ __forceinline__ void pcgSpreadHalf(const Dev& dv, const SysDev& S, lo
             sdth[row][dim][j] = v;
     }
     const int bl = hl < 3 ? dv.pmeBase[3 * i + hl] : 0;
-    const int b0 = __shfl_sync(mask, bl, 0, 16), b1 = __shfl_sync(mask, bl, 1, 16), b2 = __shfl_sync(mask, bl, 2, 16);
+    const int b0 = __shfl_sync(mask, bl, 0, L), b1 = __shfl_sync(mask, bl, 1, L), b2 = __shfl_sync(mask, bl, 2, L);
     __syncwarp(mask);
     const float qr = w.x, e0 = w.y, e1 = w.z, e2 = w.w;
     const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
     const size_t plane = (size_t) K1 * K2;
-    for (int c = hl; c < P * P; c += 16) {
+    for (int c = hl; c < P * P; c += L) {
         const int j2 = c / P, j3 = c % P;
         const float t2 = sth[row][1][j2], u2 = sdth[row][1][j2];
         const float t3 = sth[row][2][j3], u3 = sdth[row][2][j3];
@@ -80,17 +81,17 @@ __device__ __forceinline__ void pcgSpreadHalf(const Dev& dv, const SysDev& S, lo
 }
 
 // E_rec at the atom of slot s from the potential grid gpot (written by other blocks in this launch: read past
-// L1) by a half-warp (as pcgSpreadHalf): f_a = sum (d theta_a) theta theta phi over the stencil, E_rec =
+// L1) by a group of L lanes (as pcgSpreadHalf): f_a = sum (d theta_a) theta theta phi over the stencil, E_rec =
 // -sum_a K_a recip[:, a] f_a (core/pgm_core.cpp:241-264), the lanes' sums in double; or (CGA, the CG iterations)
 // instead the atom's row of A p = p / alpha - (E_pair + E_rec + cs p) (core/pgm_core.cpp:363) and the returned
 // share p_k (A p)_k of lanes hl = k < 3 (0 elsewhere).
-template <int P, bool CGA>
+template <int P, bool CGA, int L>
 __device__ __forceinline__ double pcgGatherHalf(const Dev& dv, const SysDev& S, const float* gpot, int s,
                                                float (*sth)[3][P], float (*sdth)[3][P], int row, int hl,
                                                unsigned mask, double cs) {
     const int i = dv.slotAtom[s];
     const float* sp = (const float*) dv.spl + (size_t) s * 9 * MAXP;
-    for (int k = hl; k < 6 * P; k += 16) {
+    for (int k = hl; k < 6 * P; k += L) {
         const int kind = k / (3 * P), dim = (k / P) % 3, j = k % P;
         const float v = sp[(kind * 3 + dim) * MAXP + j];
         if (kind == 0)
@@ -99,12 +100,12 @@ __device__ __forceinline__ double pcgGatherHalf(const Dev& dv, const SysDev& S, 
             sdth[row][dim][j] = v;
     }
     const int bl = hl < 3 ? dv.pmeBase[3 * i + hl] : 0;
-    const int b0 = __shfl_sync(mask, bl, 0, 16), b1 = __shfl_sync(mask, bl, 1, 16), b2 = __shfl_sync(mask, bl, 2, 16);
+    const int b0 = __shfl_sync(mask, bl, 0, L), b1 = __shfl_sync(mask, bl, 1, L), b2 = __shfl_sync(mask, bl, 2, L);
     __syncwarp(mask);
     const int K0 = S.K[0], K1 = S.K[1], K2 = S.K[2];
     const size_t plane = (size_t) K1 * K2;
     float f0 = 0.f, f1 = 0.f, f2 = 0.f;
-    for (int c = hl; c < P * P; c += 16) {
+    for (int c = hl; c < P * P; c += L) {
         const int j2 = c / P, j3 = c % P;
         const float* col = gpot + (size_t) wrapIndex(b1 - j2, K1) * K2 + wrapIndex(b2 - j3, K2);
         float St = 0.f, Su = 0.f;
@@ -122,10 +123,10 @@ __device__ __forceinline__ double pcgGatherHalf(const Dev& dv, const SysDev& S, 
     }
     double F[3] = {(double) f0, (double) f1, (double) f2};
 #pragma unroll
-    for (int o = 8; o > 0; o >>= 1)
+    for (int o = L / 2; o > 0; o >>= 1)
 #pragma unroll
         for (int k = 0; k < 3; k++)
-            F[k] += __shfl_xor_sync(mask, F[k], o, 16);
+            F[k] += __shfl_xor_sync(mask, F[k], o, L);
     double share = 0.0;
     if (hl < 3) {
         const int k = hl;
@@ -254,9 +255,11 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
     double* const part = dv.pcgPartial;
     // the half-warp-per-slot phases (spread, gather): the half-warps' shared spline rows, the fixed-point charge
     // grid and the float potential grid
-    __shared__ float psth[PCG_THREADS / 16][3][P], psdth[PCG_THREADS / 16][3][P];
-    const int hrow = tid >> 4, hl = tid & 15, nhalves = nT >> 4;   // the half-warp phases
-    const unsigned hmask = 0xffffu << (tid & 16);
+    constexpr int SL = PCG_SLOT_LANES;
+    __shared__ float psth[PCG_THREADS / SL][3][P], psdth[PCG_THREADS / SL][3][P];
+    // the slot-group phases: SL lanes per slot
+    const int hrow = tid / SL, hl = tid % SL, nhalves = nT / SL;
+    const unsigned hmask = ((1u << SL) - 1u) << (tid & 31 & ~(SL - 1));
     long long* const gfix = dv.gridFix + S.gridOff;
     float* const gpot = (float*) dv.grid + S.gridOff;
     (void) nyc;
@@ -266,7 +269,7 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
     double rz = sc[SC_RZ], beta = sc[SC_BETA], it = sc[SC_IT];
     const double norm = sc[SC_NORM];
     for (;;) {
-        // ---- S: a half-warp per slot: direction p = z + beta p (or the pass's sources), the float copy for the
+        // ---- S: SL lanes per slot: direction p = z + beta p (or the pass's sources), the float copy for the
         // pair pass, the PME weights (q, e_a = K_a p . recip[:, a]) and the spread
         for (int s = s0 + hrow; s < s1; s += nhalves) {
             const int i = dv.slotAtom[s];
@@ -279,15 +282,15 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
                     dl = vec[3 * i + hl];
                 }
             }
-            const double d0 = __shfl_sync(hmask, dl, 0, 16), d1 = __shfl_sync(hmask, dl, 1, 16),
-                         d2 = __shfl_sync(hmask, dl, 2, 16);
+            const double d0 = __shfl_sync(hmask, dl, 0, SL), d1 = __shfl_sync(hmask, dl, 1, SL),
+                         d2 = __shfl_sync(hmask, dl, 2, SL);
             const float qf = PASS == 2 ? (float) dv.q[i] : 0.f;
             if (hl == 0)
                 ((float4*) dv.dS)[s] = make_float4((float) d0, (float) d1, (float) d2, qf);
             const float4 w = make_float4(qf, (float) (S.K[0] * (d0 * S.recip[0] + d1 * S.recip[3] + d2 * S.recip[6])),
                                          (float) (S.K[1] * (d0 * S.recip[1] + d1 * S.recip[4] + d2 * S.recip[7])),
                                          (float) (S.K[2] * (d0 * S.recip[2] + d1 * S.recip[5] + d2 * S.recip[8])));
-            pcgSpreadHalf<P>(dv, S, gfix, s, w, psth, psdth, hrow, hl, hmask);
+            pcgSpreadHalf<P, SL>(dv, S, gfix, s, w, psth, psdth, hrow, hl, hmask);
         }
         if (!fftgBarrier(gbar, (unsigned) nb, dv.flags))
             return;
@@ -410,13 +413,13 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
         // ---- G: E_rec at the chunk's atoms (a field pass), or the rows of A p and the block's share of p . A p
         if (PASS != 0) {   // one field pass: E_pair and E_rec written
             for (int s = s0 + hrow; s < s1; s += nhalves)
-                pcgGatherHalf<P, false>(dv, S, gpot, s, psth, psdth, hrow, hl, hmask, cs);
+                pcgGatherHalf<P, false, SL>(dv, S, gpot, s, psth, psdth, hrow, hl, hmask, cs);
             return;
         }
         {
             double v[1] = {0.0};
             for (int s = s0 + hrow; s < s1; s += nhalves)
-                v[0] += pcgGatherHalf<P, true>(dv, S, gpot, s, psth, psdth, hrow, hl, hmask, cs);
+                v[0] += pcgGatherHalf<P, true, SL>(dv, S, gpot, s, psth, psdth, hrow, hl, hmask, cs);
             blockReduce<1>(v, 0u);
             if (tid == 0)
                 part[(size_t) x * 4] = v[0];
