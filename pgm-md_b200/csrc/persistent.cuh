@@ -77,7 +77,7 @@ __device__ __forceinline__ void pcgSpreadHalf(const Dev& dv, const SysDev& S, lo
             gridFixAdd(gfix + col + (size_t) wrapIndex(b0 - j1, K0) * plane,
                        (float) (a * sth[row][0][j1] + b * sdth[row][0][j1]));
     }
-    __syncwarp(mask);   // (the next slot of this half-warp overwrites the shared rows)
+    __syncwarp(mask);   // (the next slot of this group overwrites the shared rows)
 }
 
 // E_rec at the atom of slot s from the potential grid gpot (written by other blocks in this launch: read past
@@ -253,8 +253,8 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
     C* const spec = (C*) dv.spec + S.specOff;
     C* const myPlane = spec + (size_t) x * nline;
     double* const part = dv.pcgPartial;
-    // the half-warp-per-slot phases (spread, gather): the half-warps' shared spline rows, the fixed-point charge
-    // grid and the float potential grid
+    // the slot-group phases (spread, gather): the groups' shared spline rows, the fixed-point charge grid and the
+    // float potential grid
     constexpr int SL = PCG_SLOT_LANES;
     __shared__ float psth[PCG_THREADS / SL][3][P], psdth[PCG_THREADS / SL][3][P];
     // the slot-group phases: SL lanes per slot
