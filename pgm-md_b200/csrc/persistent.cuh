@@ -428,19 +428,31 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
             return;
         // ---- U: alph, x, r, z; shares of z'.(r' - r), r'.z', max|z'|
         {
+            // the first slot's p, x, r, A p and alpha are loaded before the total of p . A p is formed
+            const int sF = s0 + tid;
+            const bool hasF = sF < s1;
+            const int iF = hasF ? dv.slotAtom[sF] : 0;
+            double pF[3] = {0, 0, 0}, xF[3] = {0, 0, 0}, rF[3] = {0, 0, 0}, aF[3] = {0, 0, 0}, alF = 0.0;
+            if (hasF) {
+                alF = dv.alpha[iF];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    pF[k] = dv.p[3 * iF + k];
+                    xF[k] = dv.x[3 * iF + k];
+                    rF[k] = dv.r[3 * iF + k];
+                    aF[k] = dv.Ap[3 * iF + k];
+                }
+            }
             double pap[1];
             pcgTotals<1>(part, nb, 0u, pap);
             const double alph = rz / fmax(pap[0], 1e-300);
             double v[3] = {0.0, 0.0, 0.0};
-            for (int s = s0 + tid; s < s1; s += nT) {
-                const int i = dv.slotAtom[s];
-                const double al = dv.alpha[i];
+            auto update = [&](int i, double al, const double* pk, const double* xk, const double* rk, const double* ak) {
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    const double pk = dv.p[3 * i + k];
-                    dv.x[3 * i + k] += alph * pk;
-                    const double rold = dv.r[3 * i + k];
-                    const double rn = rold - alph * dv.Ap[3 * i + k];
+                    dv.x[3 * i + k] = xk[k] + alph * pk[k];
+                    const double rold = rk[k];
+                    const double rn = rold - alph * ak[k];
                     const double zn = al * rn;
                     dv.r[3 * i + k] = rn;
                     dv.z[3 * i + k] = zn;
@@ -448,6 +460,20 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
                     v[1] += rn * zn;
                     v[2] = fmax(v[2], fabs(zn));
                 }
+            };
+            if (hasF)
+                update(iF, alF, pF, xF, rF, aF);
+            for (int s = sF + nT; s < s1; s += nT) {
+                const int i = dv.slotAtom[s];
+                double pk[3], xk[3], rk[3], ak[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    pk[k] = dv.p[3 * i + k];
+                    xk[k] = dv.x[3 * i + k];
+                    rk[k] = dv.r[3 * i + k];
+                    ak[k] = dv.Ap[3 * i + k];
+                }
+                update(i, dv.alpha[i], pk, xk, rk, ak);
             }
             blockReduce<3>(v, 4u);
             if (tid == 0) {
