@@ -44,21 +44,41 @@ template <int P> struct PmeRec {
 // lanes (lane hl, mask `mask`, shared rows `row` for the evaluation's spline coefficients): a stencil column
 // (j2, j3) per lane and round, a loop over j1; the groups of a warp keep several atoms' loads and atomics in
 // flight.  The points and per-point arithmetic of k_spread, so both add the same integers.
-template <int P, int L>
-__device__ __forceinline__ void pcgSpreadHalf(const Dev& dv, const SysDev& S, long long* gfix, int s, float4 w,
-                                             float (*sth)[3][P], float (*sdth)[3][P], int row, int hl,
-                                             unsigned mask) {
-    const int i = dv.slotAtom[s];
-    const float* sp = (const float*) dv.spl + (size_t) s * 9 * MAXP;
-    for (int k = hl; k < 6 * P; k += L) {
-        const int kind = k / (3 * P), dim = (k / P) % 3, j = k % P;
-        const float v = sp[(kind * 3 + dim) * MAXP + j];
-        if (kind == 0)
-            sth[row][dim][j] = v;
-        else
-            sdth[row][dim][j] = v;
+// The group's share of slot s's spline coefficients (k = hl, hl + L, ...) and base index (lanes hl < 3), loaded
+// ahead of the direction update that the spread waits for.
+template <int P, int L> struct SpreadPre {
+    float c[(6 * P + L - 1) / L];
+    int bl;
+    __device__ __forceinline__ void load(const Dev& dv, int s, int i, int hl) {
+        const float* sp = (const float*) dv.spl + (size_t) s * 9 * MAXP;
+#pragma unroll
+        for (int m = 0; m < (6 * P + L - 1) / L; m++) {
+            const int k = hl + m * L;
+            if (k < 6 * P) {
+                const int kind = k / (3 * P), dim = (k / P) % 3, j = k % P;
+                c[m] = sp[(kind * 3 + dim) * MAXP + j];
+            }
+        }
+        bl = hl < 3 ? dv.pmeBase[3 * i + hl] : 0;
     }
-    const int bl = hl < 3 ? dv.pmeBase[3 * i + hl] : 0;
+};
+
+template <int P, int L>
+__device__ __forceinline__ void pcgSpreadHalf(const Dev& dv, const SysDev& S, long long* gfix, float4 w,
+                                             const SpreadPre<P, L>& pre, float (*sth)[3][P], float (*sdth)[3][P],
+                                             int row, int hl, unsigned mask) {
+#pragma unroll
+    for (int m = 0; m < (6 * P + L - 1) / L; m++) {
+        const int k = hl + m * L;
+        if (k < 6 * P) {
+            const int kind = k / (3 * P), dim = (k / P) % 3, j = k % P;
+            if (kind == 0)
+                sth[row][dim][j] = pre.c[m];
+            else
+                sdth[row][dim][j] = pre.c[m];
+        }
+    }
+    const int bl = pre.bl;
     const int b0 = __shfl_sync(mask, bl, 0, L), b1 = __shfl_sync(mask, bl, 1, L), b2 = __shfl_sync(mask, bl, 2, L);
     __syncwarp(mask);
     const float qr = w.x, e0 = w.y, e1 = w.z, e2 = w.w;
@@ -90,6 +110,12 @@ __device__ __forceinline__ double pcgGatherHalf(const Dev& dv, const SysDev& S, 
                                                float (*sth)[3][P], float (*sdth)[3][P], int row, int hl,
                                                unsigned mask, double cs) {
     const int i = dv.slotAtom[s];
+    double alI = 0.0, pI = 0.0, eI = 0.0;   // (CGA) the inputs of the atom's A p row, loaded first
+    if (CGA && hl < 3) {
+        alI = dv.alpha[i];
+        pI = dv.p[3 * i + hl];
+        eI = __ldcg(dv.Epair + 3 * i + hl);
+    }
     const float* sp = (const float*) dv.spl + (size_t) s * 9 * MAXP;
     for (int k = hl; k < 6 * P; k += L) {
         const int kind = k / (3 * P), dim = (k / P) % 3, j = k % P;
@@ -133,11 +159,10 @@ __device__ __forceinline__ double pcgGatherHalf(const Dev& dv, const SysDev& S, 
         const double E = -(S.K[0] * S.recip[3 * k] * F[0] + S.K[1] * S.recip[3 * k + 1] * F[1] +
                            S.K[2] * S.recip[3 * k + 2] * F[2]);
         if (CGA) {
-            const double al = dv.alpha[i], pk = dv.p[3 * i + k];
-            const double Tp = __ldcg(dv.Epair + 3 * i + k) + E + cs * pk;
-            const double apk = (al > 0) ? pk / al - Tp : 0.0;
+            const double Tp = eI + E + cs * pI;
+            const double apk = (alI > 0) ? pI / alI - Tp : 0.0;
             dv.Ap[3 * i + k] = apk;
-            share = pk * apk;
+            share = pI * apk;
         } else {
             dv.Erec[3 * i + k] = E;
         }
@@ -273,6 +298,8 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
         // pair pass, the PME weights (q, e_a = K_a p . recip[:, a]) and the spread
         for (int s = s0 + hrow; s < s1; s += nhalves) {
             const int i = dv.slotAtom[s];
+            SpreadPre<P, SL> pre;
+            pre.load(dv, s, i, hl);
             double dl = 0.0;
             if (hl < 3) {
                 if (PASS == 0) {
@@ -290,7 +317,7 @@ __global__ void __launch_bounds__(PCG_THREADS, PCG_BLOCKS_PER_SM) k_cg_persisten
             const float4 w = make_float4(qf, (float) (S.K[0] * (d0 * S.recip[0] + d1 * S.recip[3] + d2 * S.recip[6])),
                                          (float) (S.K[1] * (d0 * S.recip[1] + d1 * S.recip[4] + d2 * S.recip[7])),
                                          (float) (S.K[2] * (d0 * S.recip[2] + d1 * S.recip[5] + d2 * S.recip[8])));
-            pcgSpreadHalf<P, SL>(dv, S, gfix, s, w, psth, psdth, hrow, hl, hmask);
+            pcgSpreadHalf<P, SL>(dv, S, gfix, w, pre, psth, psdth, hrow, hl, hmask);
         }
         if (!fftgBarrier(gbar, (unsigned) nb, dv.flags))
             return;
