@@ -1492,13 +1492,20 @@ __device__ __forceinline__ unsigned ldAcquireGpu(const unsigned* p) {
 // Barrier of nb blocks over an arrival counter that only grows between resets (the flags and barrier words are
 // cleared at the start of every call): the blocks of barrier k arrive as numbers k nb .. k nb + nb - 1 and leave
 // once the counter has reached (k + 1) nb.  The wait is bounded: false, with flags[11] set, when it gave up.
+__device__ __forceinline__ unsigned atomAddReleaseGpu(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// The arrival is a release (it orders the block's writes before it, made the thread's own by the block barrier
+// ahead of it) and the wait an acquire load, so no separate fences are needed.
 __device__ __forceinline__ bool fftgBarrier(unsigned* bar, unsigned nb, int* flags) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
-        __threadfence();
-        const unsigned old = atomicAdd(bar, 1u);
+        const unsigned old = atomAddReleaseGpu(bar, 1u);
         const unsigned target = (old / nb + 1) * nb;
         if (old + 1 != target)
             for (unsigned it = 0; (int) (ldAcquireGpu(bar) - target) < 0; it++)
@@ -1507,7 +1514,6 @@ __device__ __forceinline__ bool fftgBarrier(unsigned* bar, unsigned nb, int* fla
                     atomicExch(flags + 11, 1);
                     break;
                 }
-        __threadfence();
     }
     __syncthreads();
     return ok != 0;
