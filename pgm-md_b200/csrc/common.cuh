@@ -413,14 +413,15 @@ __device__ __forceinline__ bool chunkFinish(const Dev& dv, int chunk, int s, dou
 #pragma unroll
         for (int k = 0; k < NV; k++)
             dv.partial[(size_t) chunk * 16 + k] = v[k];
-        __threadfence();
-        const int t = atomicAdd(&dv.sysCounter[s], 1);
+        // the arrival releases this thread's partials and, for the last chunk, acquires the others' (the block
+        // barrier below passes them on to the block's threads)
+        int t;
+        asm volatile("atom.add.acq_rel.gpu.global.s32 %0, [%1], 1;" : "=r"(t) : "l"(&dv.sysCounter[s]) : "memory");
         isLast = (t == dv.sys[s].chunkCount - 1);
     }
     __syncthreads();
     if (!isLast)
         return false;
-    __threadfence();
     const SysDev& S = dv.sys[s];
     // the system's chunk partials in a fixed order: value k = tid mod 16, chunk group tid / 16 takes chunks
     // group, group + 16, ...; the groups' sums then in group order (deterministic)
