@@ -1729,23 +1729,59 @@ struct Engine::Impl {
             // the permanent field's PME half (main stream).  Without a skin, on the plain first pass, the record
             // kernel also forms the permanent field's direct part (after the permanent spread wrote the sources),
             // in place of a pair pass of its own.
-            const bool fuseField = rowsLeft && !persistentMode() && !dualFirstPass();
+            const bool fuseField = rowsLeft && !dualFirstPass();
+            const bool pcg = std::is_same<R, float>::value && persistentMode();
+            if (fuseField) {
+                // the permanent field's PME half on the side stream, whose higher priority lets the cooperative grid
+                // kernel's blocks in ahead of the list build's; the list's rows and then the records with the
+                // permanent field's direct part (once the spread wrote the sources) on the main stream
+                CU(cudaEventRecord(evFork, sm));
+                CU(cudaStreamWaitEvent(sd, evFork, 0));
+                k_splines<R><<<(3 * n + 255) / 256, 256, 0, sd>>>(d);
+                if (std::is_same<R, float>::value && planesMode())
+                    enqueuePlaneBins(sd, d);
+                k_perm<<<tb, 256, 0, sd>>>(d);
+                k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sd>>>(d);
+                CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sd));
+                launchSpread<R>(sd, d, 0, d.perm);
+                CU(cudaEventRecord(evPerm, sd));
+                transformPair<R>(sd, d, false, spreadFix());
+                launchGather<R, false>(sd, d, 0);
+                CU(cudaEventRecord(evJoin, sd));
+                listKernel(sm, d);
+                CU(cudaStreamWaitEvent(sm, evPerm, 0));
+                k_pair_kernels<R, true><<<(n + 7) / 8, 256, 0, sm>>>(d);
+                CU(cudaStreamWaitEvent(sm, evJoin, 0));
+                k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+                CU(cudaGetLastError());
+                if (pcg) {   // A x0 as one pass of the persistent kernel, then the loop's set-up
+                    launchPersistent(sm, d, 1, d.x);
+                    k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+                    CU(cudaGetLastError());
+                    return;
+                }
+                CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
+                fieldPass<R, false>(sm, sd, d, 1, d.x, false);
+                k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+                CU(cudaGetLastError());
+                // the loop's first spread needs a clear grid (each iteration clears it for the next one)
+                CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
+                return;
+            }
             CU(cudaEventRecord(evFork, sm));
             CU(cudaStreamWaitEvent(sd, evFork, 0));
             if (rowsLeft)
                 listKernel(sd, d);
-            if (!fuseField) {
-                pairRecords<R>(sd, d);
-                CU(cudaEventRecord(evJoin, sd));
-            }
+            pairRecords<R>(sd, d);
+            CU(cudaEventRecord(evJoin, sd));
             k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
             if (std::is_same<R, float>::value && planesMode())
                 enqueuePlaneBins(sm, d);
             k_perm<<<tb, 256, 0, sm>>>(d);
             k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
-            if (std::is_same<R, float>::value && persistentMode()) {
+            if (pcg) {
                 // the two passes before the loop as one cooperative launch each (the persistent kernel's
-                // machinery: PME planes in shared memory beside the direct-space pass)
+                // machinery: the PME planes transformed beside the direct-space pass)
                 CU(cudaStreamWaitEvent(sm, evJoin, 0));
                 launchPersistent(sm, d, 2, d.perm);
                 k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
@@ -1790,18 +1826,10 @@ struct Engine::Impl {
             }
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
             launchSpread<R>(sm, d, 0, d.perm);
-            if (fuseField) {   // the records with the permanent field's direct part, once the sources are written
-                CU(cudaEventRecord(evPerm, sm));
-                CU(cudaStreamWaitEvent(sd, evPerm, 0));
-                k_pair_kernels<R, true><<<(n + 7) / 8, 256, 0, sd>>>(d);
-                CU(cudaGetLastError());
-                CU(cudaEventRecord(evJoin, sd));
-            }
             transformPair<R>(sm, d, false, spreadFix());
             launchGather<R, false>(sm, d, 0);   // (the reciprocal half needs no pair list)
             CU(cudaStreamWaitEvent(sm, evJoin, 0));
-            if (!fuseField)
-                pairField<R, true>(sm, d, 0);
+            pairField<R, true>(sm, d, 0);
             k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
             CU(cudaGetLastError());
             CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
