@@ -668,7 +668,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
             "config": config(S, {"parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                                  "pair_lanes": lanes, "transforms": TRANSFORMS[mixed.transforms()],
-                                 "pme_kernels": mixed.pme_kernels(), "bitwise_reproducible": True,
+                                 "pme_kernels": mixed.pme_kernels(),
+                                 "bitwise_reproducible": mixed.pme_kernels() == 0,
                                  "cg_iterations": int(np.median(its_mixed)),
                                  "fp64_evals_per_s": fp64_value, "mixed_over_fp64": value / fp64_value}),
             "fp64": {"value": fp64_value, "unit": "evals/s", "steps": fsteps, "pair_lanes": lanes64,
