@@ -1729,12 +1729,12 @@ struct Engine::Impl {
             // the permanent field's PME half (main stream).  Without a skin, on the plain first pass, the record
             // kernel also forms the permanent field's direct part (after the permanent spread wrote the sources),
             // in place of a pair pass of its own.
-            const bool fuseField = rowsLeft && !dualFirstPass();
             const bool pcg = std::is_same<R, float>::value && persistentMode();
-            if (fuseField) {
+            if (!dualFirstPass()) {
                 // the permanent field's PME half on the side stream, whose higher priority lets the cooperative grid
-                // kernel's blocks in ahead of the list build's; the list's rows and then the records with the
-                // permanent field's direct part (once the spread wrote the sources) on the main stream
+                // kernel's blocks in ahead of the list build's; on the main stream the list's rows and then the
+                // records with the permanent field's direct part (once the spread wrote the sources), or, with a
+                // kept list, its compaction and records and then the permanent field's pair pass
                 CU(cudaEventRecord(evFork, sm));
                 CU(cudaStreamWaitEvent(sd, evFork, 0));
                 k_splines<R><<<(3 * n + 255) / 256, 256, 0, sd>>>(d);
@@ -1748,9 +1748,15 @@ struct Engine::Impl {
                 transformPair<R>(sd, d, false, spreadFix());
                 launchGather<R, false>(sd, d, 0);
                 CU(cudaEventRecord(evJoin, sd));
-                listKernel(sm, d);
-                CU(cudaStreamWaitEvent(sm, evPerm, 0));
-                k_pair_kernels<R, true><<<(n + 7) / 8, 256, 0, sm>>>(d);
+                if (rowsLeft) {
+                    listKernel(sm, d);
+                    CU(cudaStreamWaitEvent(sm, evPerm, 0));
+                    k_pair_kernels<R, true><<<(n + 7) / 8, 256, 0, sm>>>(d);
+                } else {
+                    pairRecords<R>(sm, d);
+                    CU(cudaStreamWaitEvent(sm, evPerm, 0));
+                    pairField<R, true>(sm, d, 0);
+                }
                 CU(cudaStreamWaitEvent(sm, evJoin, 0));
                 k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
                 CU(cudaGetLastError());
@@ -1779,17 +1785,6 @@ struct Engine::Impl {
                 enqueuePlaneBins(sm, d);
             k_perm<<<tb, 256, 0, sm>>>(d);
             k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
-            if (pcg) {
-                // the two passes before the loop as one cooperative launch each (the persistent kernel's
-                // machinery: the PME planes transformed beside the direct-space pass)
-                CU(cudaStreamWaitEvent(sm, evJoin, 0));
-                launchPersistent(sm, d, 2, d.perm);
-                k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
-                launchPersistent(sm, d, 1, d.x);
-                k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
-                CU(cudaGetLastError());
-                return;
-            }
             if (dualFirstPass()) {
                 // x0 first; (q, perm) into the grid and dS, x0 into the second grid and dS2; one pair sweep for
                 // both direct fields
@@ -1824,20 +1819,6 @@ struct Engine::Impl {
                 CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
                 return;
             }
-            CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
-            launchSpread<R>(sm, d, 0, d.perm);
-            transformPair<R>(sm, d, false, spreadFix());
-            launchGather<R, false>(sm, d, 0);   // (the reciprocal half needs no pair list)
-            CU(cudaStreamWaitEvent(sm, evJoin, 0));
-            pairField<R, true>(sm, d, 0);
-            k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
-            CU(cudaGetLastError());
-            CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
-            fieldPass<R, false>(sm, sd, d, 1, d.x, false);
-            k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
-            CU(cudaGetLastError());
-            // the loop's first spread needs a clear grid (each iteration clears it for the next one)
-            CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
         } else {
             if (rowsLeft)
                 listKernel(sm, d);

@@ -117,3 +117,26 @@ def test_persistent_kernel_with_plane_owner_passes(name):
     assert abs(r.energy - e_ref) <= 1e-6 * abs(e_ref)
     assert np.linalg.norm(r.forces - F) <= 1e-5 * np.linalg.norm(F)
     eng.close()
+
+
+@pytest.mark.parametrize("mode", [3, 4])
+def test_kept_list_first_pass(mode):
+    """With a kept Verlet list (skin 0.15 nm) the first pass compacts the list and forms the permanent field's pair
+    part on the main stream beside its PME half on the side stream; the graph loop (3) and the persistent kernel
+    (4), two calls at the same positions (the list built once), against the reference outputs on the real
+    8550-atom liquid at tol 1e-10."""
+    S, d = golden("dmp8550_real")
+    e = PKG.Engine(PKG.Settings(cutoff=S.cutoff, beta=S.beta, grid=S.grid, order=6, tol=1e-10, max_iter=500,
+                                peek=0.0, predictor=0, ke=PKG.systems.KE_DEFAULT, precision=PKG.MIXED, skin=0.15))
+    e.set_system(S)
+    e.set_pair_lanes(16)
+    e.set_transforms(mode)
+    assert e.transforms() == mode
+    e_ref = float(d["energy"])
+    F = np.asarray(d["forces"], np.float64)
+    for _ in range(2):
+        r = e.compute(S.pos, S.box)
+        assert abs(r.energy - e_ref) <= 1e-6 * abs(e_ref), (r.energy, e_ref)
+        assert np.linalg.norm(r.forces - F) <= 1e-5 * np.linalg.norm(F)
+    assert e.list_builds() == 1
+    e.close()
