@@ -1600,13 +1600,14 @@ struct Engine::Impl {
         CU(cudaGetLastError());
     }
 
-    // A predicted step (guess from history, not from E_perm): the permanent field and T x0 from one pair sweep
-    // over the records and two PME passes, the second on its own grid (the transforms in sequence: they share
-    // the spectrum buffer and the grid kernel's barrier words).  The engine's own passes otherwise.
-    // (PGM_B200_DUAL=0 keeps the two passes apart, for comparison)
+    // A predicted step (guess from history, not from E_perm) with PGM_B200_DUAL=1: the permanent field and T x0
+    // from one pair sweep over the records and two PME passes, the second on its own grid (the transforms in
+    // sequence: they share the spectrum buffer and the grid kernel's barrier words).  By default the two passes
+    // stay apart: since the first pass runs its PME half beside the list work on the high-priority stream, apart
+    // is the faster of the two.
     bool dualFirstPass() const {
         const char* e = std::getenv("PGM_B200_DUAL");
-        if (e && e[0] == '0')
+        if (!(e && e[0] == '1'))
             return false;
         return s.polarizable && hCtl && hCtl->guess >= 1 && !hCtl->customRhs && !persistentMode() && !refining() &&
                !planesMode() && !tilesMode();
@@ -1774,51 +1775,46 @@ struct Engine::Impl {
                 CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
                 return;
             }
+            // a predicted step (dualFirstPass): x0 from the history first; (q, perm) into the grid and dS, x0 into
+            // the second grid and dS2, both PME halves on the high-priority side stream (the transforms in sequence:
+            // one spectrum buffer, one set of the grid kernel's barrier words); on the main stream the list's rows
+            // and records, then one pair sweep for both direct fields once the spreads wrote their sources
+            Dev d2 = d;   // the second source set: its grids, its float copy, its reciprocal field
+            d2.grid = dGrid2.p;
+            d2.gridFix = d.gridFix ? dGridFix2.as<long long>() : nullptr;
+            d2.dS = dDS2.p;
+            d2.Erec = dErec2.as<double>();
             CU(cudaEventRecord(evFork, sm));
             CU(cudaStreamWaitEvent(sd, evFork, 0));
-            if (rowsLeft)
-                listKernel(sd, d);
-            pairRecords<R>(sd, d);
-            CU(cudaEventRecord(evJoin, sd));
-            k_splines<R><<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
+            k_splines<R><<<(3 * n + 255) / 256, 256, 0, sd>>>(d);
             if (std::is_same<R, float>::value && planesMode())
-                enqueuePlaneBins(sm, d);
-            k_perm<<<tb, 256, 0, sm>>>(d);
-            k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sm>>>(d);
-            if (dualFirstPass()) {
-                // x0 first; (q, perm) into the grid and dS, x0 into the second grid and dS2; one pair sweep for
-                // both direct fields
-                Dev d2 = d;   // the second source set: its grids, its float copy, its reciprocal field
-                d2.grid = dGrid2.p;
-                d2.gridFix = d.gridFix ? dGridFix2.as<long long>() : nullptr;
-                d2.dS = dDS2.p;
-                d2.Erec = dErec2.as<double>();
-                k_cg_guess<<<(3 * n + 255) / 256, 256, 0, sm>>>(d);
-                CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
-                CU(cudaMemsetAsync(d2.grid, 0, gridTotal * realSize(), sm));
-                launchSpread<R>(sm, d, 0, d.perm);
-                launchSpread<R>(sm, d2, 1, d.x);
-                // the pair sweep on the side stream after its records and the spreads' float copies, beside the
-                // transforms and gathers here (the transforms in sequence: one spectrum buffer, one set of the
-                // grid kernel's barrier words)
-                CU(cudaEventRecord(evFork, sm));
-                CU(cudaStreamWaitEvent(sd, evFork, 0));
-                pairField<R, true, true>(sd, d, 0);
-                CU(cudaEventRecord(evJoin, sd));
-                transformPair<R>(sm, d, false, spreadFix());
-                launchGather<R, false>(sm, d, 0);
-                transformPair<R>(sm, d2, false, spreadFix());
-                launchGather<R, false>(sm, d2, 0);
-                CU(cudaStreamWaitEvent(sm, evJoin, 0));
-                k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
-                Dev d3 = d;   // T x0: the second set's pair and reciprocal fields
-                d3.Epair = dEpair2.as<double>();
-                d3.Erec = dErec2.as<double>();
-                k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d3);
-                CU(cudaGetLastError());
-                CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
-                return;
-            }
+                enqueuePlaneBins(sd, d);
+            k_perm<<<tb, 256, 0, sd>>>(d);
+            k_influence<R><<<dim3(convBlocks, nsys), 256, 0, sd>>>(d);
+            k_cg_guess<<<(3 * n + 255) / 256, 256, 0, sd>>>(d);
+            CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sd));
+            CU(cudaMemsetAsync(d2.grid, 0, gridTotal * realSize(), sd));
+            launchSpread<R>(sd, d, 0, d.perm);
+            launchSpread<R>(sd, d2, 1, d.x);
+            CU(cudaEventRecord(evPerm, sd));
+            transformPair<R>(sd, d, false, spreadFix());
+            launchGather<R, false>(sd, d, 0);
+            transformPair<R>(sd, d2, false, spreadFix());
+            launchGather<R, false>(sd, d2, 0);
+            CU(cudaEventRecord(evJoin, sd));
+            if (rowsLeft)
+                listKernel(sm, d);
+            pairRecords<R>(sm, d);
+            CU(cudaStreamWaitEvent(sm, evPerm, 0));
+            pairField<R, true, true>(sm, d, 0);
+            CU(cudaStreamWaitEvent(sm, evJoin, 0));
+            k_cg_b<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d);
+            Dev d3 = d;   // T x0: the second set's pair and reciprocal fields
+            d3.Epair = dEpair2.as<double>();
+            d3.Erec = dErec2.as<double>();
+            k_cg_init<<<(int) chunkSys.size(), CHUNK, 0, sm>>>(d3);
+            CU(cudaGetLastError());
+            CU(cudaMemsetAsync(d.grid, 0, gridTotal * realSize(), sm));
         } else {
             if (rowsLeft)
                 listKernel(sm, d);

@@ -1,8 +1,9 @@
 """The dual first pass of a predicted step: with a guess from the history (mu3 / mu4 / the last solution), x0
 does not depend on the permanent field, so the engine forms x0 first and takes E_perm and T x0 from one sweep
 over the pair records and two PME passes (two grids), where an unpredicted step needs the permanent field before
-x0 = alpha E_perm.  Checked over MD-like steps of the real 8550-atom liquid (mu4, Verlet list kept) against the
-same engine with the two passes apart (PGM_B200_DUAL=0) and against a fresh unpredicted evaluation at tol 1e-10.
+x0 = alpha E_perm.  It runs with PGM_B200_DUAL=1 (the two passes apart are the default, and the faster).  Checked
+over MD-like steps of the real 8550-atom liquid (mu4, Verlet list kept) against the same engine with the two
+passes apart (PGM_B200_DUAL=0) and against a fresh unpredicted evaluation at tol 1e-10.
 
 Bars: FP64 energies within 1e-10 relative and the same CG iterations as the separate passes (the same sums, in
 another order only where atomics add), forces within 1e-9 relative RMS; mixed energies within 1e-6, forces 1e-5,
@@ -72,7 +73,10 @@ def test_dual_first_pass_predicted_steps_save_iterations():
     """mu4 over the trajectory: later steps take fewer CG iterations than the first (unpredicted) one."""
     S, _ = load_dmp_real()
     e = engine(S, PKG.MIXED, tol=1e-5)
-    its = [e.compute(pos, S.box).iterations for pos in trajectory(S, 6)]
+    os.environ["PGM_B200_DUAL"] = "1"
+    try:
+        its = [e.compute(pos, S.box).iterations for pos in trajectory(S, 6)]
+    finally:
+        os.environ.pop("PGM_B200_DUAL", None)
     e.close()
     assert its[-1] < its[0], its
-    assert os.environ.get("PGM_B200_DUAL", "1") != "0"
